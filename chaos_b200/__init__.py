@@ -1,0 +1,23 @@
+"""chaos_b200: the B200 (sm_100a) engine for Chaoslab's ensemble hot path.
+
+`propagate(sys, x0, N; k, tau, seed, reducers)` of the Julia package Chaoslab (src/Tangent/propagate.jl:279-290),
+running in the fused orbit kernels of libchaoslab_b200 (chaos_b200/csrc) behind the C ABI of
+include/chaoslab_b200.h. This Python package is the host side of that boundary: the reference's systems and
+reducers as parameter records, the argument checks, chunking, error and summary records.
+"""
+from .foundation import FALLBACK_REASONS, DeviceError, NumericalHealthError
+from .propagate import FrameSpec, PropagationResult, build_run, bytes_per_orbit, chunk_size, probe, propagate, propagate_frames
+from .reducers import (CGS, FLI, GALI, MEGNO, MGS, RGS, SALI, AugmentedQR, Benettin, GivensQR, HouseholderQR,
+                       QRSpectrum)
+from .systems import (FroeschleMap, Gauss, HenonHeilesFlow, IntegratorMap, LinearSymplecticMap, StandardMap,
+                      StandardMapChain, WrappedStandardMap, energy_start, lift, random_energy_starts, section_interval,
+                      torus_state)
+
+__all__ = [
+    "propagate", "propagate_frames", "FrameSpec", "PropagationResult", "build_run", "bytes_per_orbit", "chunk_size",
+    "probe", "NumericalHealthError", "DeviceError", "FALLBACK_REASONS",
+    "QRSpectrum", "CGS", "MGS", "RGS", "HouseholderQR", "AugmentedQR", "GivensQR", "Benettin", "SALI", "GALI",
+    "MEGNO", "FLI",
+    "StandardMap", "WrappedStandardMap", "FroeschleMap", "StandardMapChain", "LinearSymplecticMap", "IntegratorMap",
+    "Gauss", "HenonHeilesFlow", "torus_state", "lift", "energy_start", "random_energy_starts", "section_interval",
+]

@@ -1,0 +1,160 @@
+"""ctypes mirror of include/chaoslab_b200.h (the C ABI of libchaoslab_b200).
+
+The structs here are byte-for-byte the ones in the header; `tests/test_abi.py` checks their sizes and offsets
+against the compiled library.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+ABI_VERSION = 1
+MAX_FRAMES = 3
+MAX_REDUCERS = 4
+MAX_DIM = 16
+MAX_K = 8
+
+# enum cl_system_kind
+SYS_STANDARD, SYS_WRAPPED_STANDARD, SYS_FROESCHLE, SYS_CHAIN, SYS_LINEAR, SYS_HH_GAUSS = 1, 2, 3, 4, 5, 6
+# enum cl_reducer_kind
+RED_QR, RED_BENETTIN, RED_SALI, RED_GALI, RED_MEGNO, RED_FLI = 1, 2, 3, 4, 5, 6
+# enum cl_qr_alg
+QR_CGS, QR_MGS, QR_RGS, QR_HOUSEHOLDER, QR_AUGMENTED, QR_GIVENS = 1, 2, 3, 4, 5, 6
+# enum cl_precision
+PREC_FP64, PREC_MIXED = 0, 1
+# enum cl_status
+OK, EINVAL, ENODEVICE, EUNSUPPORTED, ENOMEM, EDEVICE_LOST = 0, -1, -2, -3, -4, -9
+
+
+class cl_system(C.Structure):
+    _fields_ = [
+        ("kind", C.c_int32),
+        ("n_sites", C.c_int32),
+        ("ring", C.c_int32),
+        ("gauss_maxiter", C.c_int32),
+        ("K", C.c_double),
+        ("eps", C.c_double),
+        ("nu", C.c_double),
+        ("kappa", C.c_double),
+        ("mu", C.c_double),
+        ("gauss_tol", C.c_double),
+        ("dt", C.c_double),
+        ("A", C.c_double * (MAX_DIM * MAX_DIM)),
+    ]
+
+
+class cl_reducer(C.Structure):
+    _fields_ = [
+        ("kind", C.c_int32),
+        ("alg", C.c_int32),
+        ("replace", C.c_int32),
+        ("pad", C.c_int32),
+        ("orthogonality_tol", C.c_double),
+    ]
+
+
+class cl_frame(C.Structure):
+    _fields_ = [
+        ("k", C.c_int32),
+        ("n_reducers", C.c_int32),
+        ("reducers", cl_reducer * MAX_REDUCERS),
+    ]
+
+
+class cl_run(C.Structure):
+    _fields_ = [
+        ("abi_version", C.c_int32),
+        ("d", C.c_int32),
+        ("s", C.c_int32),
+        ("tau", C.c_int32),
+        ("N", C.c_int64),
+        ("n0", C.c_int64),
+        ("steps", C.c_int64),
+        ("n_frames", C.c_int32),
+        ("precision", C.c_int32),
+        ("seed", C.c_uint64),
+        ("orbit_base", C.c_int64),
+        ("sys", cl_system),
+        ("frames", cl_frame * MAX_FRAMES),
+    ]
+
+
+class cl_buffers(C.Structure):
+    _fields_ = [
+        ("x0", C.c_void_p),
+        ("x", C.c_void_p),
+        ("W0", C.c_void_p * MAX_FRAMES),
+        ("W", C.c_void_p * MAX_FRAMES),
+        ("states", C.c_void_p * MAX_FRAMES),
+        ("code", C.c_void_p * MAX_FRAMES),
+        ("hstep", C.c_void_p * MAX_FRAMES),
+    ]
+
+
+class cl_prov(C.Structure):
+    _fields_ = [
+        ("device", C.c_char * 96),
+        ("variant", C.c_char * 160),
+        ("launch_steps", C.c_int64),
+        ("launches", C.c_int64),
+        ("gpu_ms", C.c_double),
+        ("block", C.c_int32),
+        ("grid", C.c_int32),
+        ("regs", C.c_int32),
+        ("orbits_per_block", C.c_int32),
+    ]
+
+
+class cl_probe(C.Structure):
+    _fields_ = [
+        ("loadable", C.c_int32),
+        ("functional", C.c_int32),
+        ("compiles", C.c_int32),
+        ("sm", C.c_int32),
+        ("free_bytes", C.c_int64),
+        ("total_bytes", C.c_int64),
+        ("sm_count", C.c_int32),
+        ("pad", C.c_int32),
+        ("device", C.c_char * 96),
+    ]
+
+
+def state_bytes(kind: int, k: int) -> int:
+    """Bytes of one reducer state in the Julia isbits layout (T = Float64)."""
+    return {RED_QR: 16 * k + 72, RED_BENETTIN: 48, RED_SALI: 72, RED_GALI: 24 * k + 32,
+            RED_MEGNO: 200, RED_FLI: 96}[kind]
+
+
+def frame_state_bytes(frame: cl_frame) -> int:
+    return sum(state_bytes(frame.reducers[r].kind, frame.k) for r in range(frame.n_reducers))
+
+
+def declare(lib: C.CDLL) -> C.CDLL:
+    """Set the argument and result types of every entry point of libchaoslab_b200."""
+    P = C.POINTER
+    lib.cl_b200_propagate.argtypes = [P(cl_run), C.c_int64, P(cl_buffers), P(cl_prov)]
+    lib.cl_b200_propagate.restype = C.c_int
+    lib.cl_b200_propagate_device.argtypes = [P(cl_run), C.c_int64, P(cl_buffers), C.c_int32, C.c_void_p]
+    lib.cl_b200_propagate_device.restype = C.c_int
+    lib.cl_b200_check.argtypes = [P(cl_run)]
+    lib.cl_b200_check.restype = C.c_int
+    lib.cl_b200_state_bytes.argtypes = [P(cl_run), C.c_int32]
+    lib.cl_b200_state_bytes.restype = C.c_int64
+    lib.cl_b200_probe.argtypes = [P(cl_probe)]
+    lib.cl_b200_probe.restype = C.c_int
+    lib.cl_b200_last_error.argtypes = [C.c_char_p, C.c_size_t]
+    lib.cl_b200_last_error.restype = C.c_int
+    lib.cl_b200_version.argtypes = []
+    lib.cl_b200_version.restype = C.c_char_p
+    lib.cl_b200_launch_count.argtypes = []
+    lib.cl_b200_launch_count.restype = C.c_int64
+    lib.cl_b200_menu_size.argtypes = []
+    lib.cl_b200_menu_size.restype = C.c_int32
+    lib.cl_b200_menu_key.argtypes = [C.c_int32]
+    lib.cl_b200_menu_key.restype = C.c_char_p
+    return lib
+
+
+# Every symbol include/chaoslab_b200.h declares (checked by the CPU tests against the built library).
+EXPORTS = ("cl_b200_propagate", "cl_b200_propagate_device", "cl_b200_check", "cl_b200_state_bytes",
+           "cl_b200_probe", "cl_b200_last_error", "cl_b200_version", "cl_b200_launch_count",
+           "cl_b200_menu_size", "cl_b200_menu_key")

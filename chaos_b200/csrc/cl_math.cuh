@@ -1,0 +1,147 @@
+// cl_math.cuh -- scalar arithmetic of the orbit kernels with Julia's Float64 semantics.
+//
+// Every kernel translation unit is compiled with -fmad=false: nothing is fused unless written as fma(), exactly as
+// Julia contracts nothing (src/Foundation/product.jl:9-20 makes the frame product's fusion explicit). The Float32
+// tangent path of the mixed kernels writes its fusions as __fmaf_rn() where it wants them.
+//
+// Transcendentals (Julia's Base libm has no device counterpart):
+//   cl_sincos: Cody-Waite reduction by pi/2 with a three-part constant (Cody and Waite 1980): k = rint(x 2/pi),
+//              r = ((x - k P1) - k P2) - k P3 each step one fma (the first is exact), then the Taylor polynomials of
+//              sin (to x^17) and cos (to x^16) on [-pi/4, pi/4] in Horner form, and the quadrant of k. About 1 ulp
+//              for |x| < 2^30; non-finite input gives NaN like `_sin` / `_cos` (src/Systems/standard_map.jl:13-14).
+//   cl_log:    x = m 2^e with m in [sqrt(1/2), sqrt(2)], f = m - 1, s = f / (2 + f), and the identity
+//              log(1 + f) = f - f^2/2 + s (f^2/2 + R(s^2)), R the atanh series 2z/3 + 2z^2/5 + ... to z^9, plus e ln 2
+//              with ln 2 split so that e LN2_HI is exact.
+// The constants come from chaos_b200/csrc/derive_constants.py (mathematical definitions, rounded once).
+#pragma once
+
+#include <cstdint>
+
+#include "cl_constants.h"
+
+namespace cl {
+
+__device__ __forceinline__ bool isfin(double x) { return isfinite(x); }
+__device__ __forceinline__ bool isfin(float x) { return isfinite(x); }
+
+// Julia max / min for IEEE floats: NaN if either is NaN; max prefers +0, min prefers -0.
+template <typename T>
+__device__ __forceinline__ T jl_max(T x, T y) {
+    if (isnan(x) || isnan(y)) return x - y;
+    if (x == y) return signbit(x) ? y : x;
+    return x > y ? x : y;
+}
+template <typename T>
+__device__ __forceinline__ T jl_min(T x, T y) {
+    if (isnan(x) || isnan(y)) return x - y;
+    if (x == y) return signbit(x) ? x : y;
+    return x < y ? x : y;
+}
+
+__device__ __forceinline__ void cl_sincos(double x, double* sn, double* cs) {
+    if (!isfin(x)) { *sn = x - x; *cs = x - x; return; }
+    if (x == 0.0) { *sn = x; *cs = 1.0; return; }
+    const double k = rint(x * CL_TWO_OVER_PI);
+    double r = fma(-k, CL_PIO2_1, x);
+    r = fma(-k, CL_PIO2_2, r);
+    r = fma(-k, CL_PIO2_3, r);
+    const double z = r * r;
+    double ps = CL_SIN_T17;
+    ps = fma(ps, z, CL_SIN_T15);
+    ps = fma(ps, z, CL_SIN_T13);
+    ps = fma(ps, z, CL_SIN_T11);
+    ps = fma(ps, z, CL_SIN_T9);
+    ps = fma(ps, z, CL_SIN_T7);
+    ps = fma(ps, z, CL_SIN_T5);
+    ps = fma(ps, z, CL_SIN_T3);
+    const double s = fma(r * z, ps, r);
+    double pc = CL_COS_T16;
+    pc = fma(pc, z, CL_COS_T14);
+    pc = fma(pc, z, CL_COS_T12);
+    pc = fma(pc, z, CL_COS_T10);
+    pc = fma(pc, z, CL_COS_T8);
+    pc = fma(pc, z, CL_COS_T6);
+    pc = fma(pc, z, CL_COS_T4);
+    pc = fma(pc, z, CL_COS_T2);
+    const double c = fma(z, pc, 1.0);
+    const double q = k - 4.0 * floor(k * 0.25);
+    if (q == 0.0) { *sn = s; *cs = c; }
+    else if (q == 1.0) { *sn = c; *cs = -s; }
+    else if (q == 2.0) { *sn = -s; *cs = -c; }
+    else { *sn = -c; *cs = s; }
+}
+__device__ __forceinline__ double cl_sin(double x) { double s, c; cl_sincos(x, &s, &c); return s; }
+__device__ __forceinline__ double cl_cos(double x) { double s, c; cl_sincos(x, &s, &c); return c; }
+
+__device__ __forceinline__ double cl_log(double x) {
+    if (isnan(x)) return x;
+    if (x < 0.0) return __longlong_as_double(0x7ff8000000000000LL);
+    if (x == 0.0) return -__longlong_as_double(0x7ff0000000000000LL);
+    if (isinf(x)) return x;
+    double e = 0.0;
+    unsigned long long b = static_cast<unsigned long long>(__double_as_longlong(x));
+    if (x < 2.2250738585072014e-308) { b = static_cast<unsigned long long>(__double_as_longlong(x * 0x1p54)); e = -54.0; }
+    e += static_cast<double>(static_cast<long long>((b >> 52) & 0x7ffULL) - 1023);
+    double m = __longlong_as_double(static_cast<long long>((b & 0x000fffffffffffffULL) | 0x3ff0000000000000ULL));
+    if (m > CL_SQRT2) { m = m * 0.5; e = e + 1.0; }
+    const double f = m - 1.0;
+    const double s = f / (2.0 + f);
+    const double z = s * s;
+    double R = CL_LOG_T9;
+    R = fma(R, z, CL_LOG_T8);
+    R = fma(R, z, CL_LOG_T7);
+    R = fma(R, z, CL_LOG_T6);
+    R = fma(R, z, CL_LOG_T5);
+    R = fma(R, z, CL_LOG_T4);
+    R = fma(R, z, CL_LOG_T3);
+    R = fma(R, z, CL_LOG_T2);
+    R = fma(R, z, CL_LOG_T1);
+    R = R * z;
+    const double hfsq = 0.5 * f * f;
+    return e * CL_LN2_HI - ((hfsq - (s * (hfsq + R) + e * CL_LN2_LO)) - f);
+}
+
+// Neumaier compensated sum (src/Foundation/Foundation.jl:48-68); always Float64.
+struct CS { double s, c; };
+__device__ __forceinline__ void cs_add(CS& a, double y) {
+    const double t = a.s + y;
+    const double c = fabs(a.s) >= fabs(y) ? (a.s - t) + y : (y - t) + a.s;
+    a.s = t;
+    a.c = a.c + c;
+}
+__device__ __forceinline__ double cs_total(const CS& a) { return a.s + a.c; }
+
+// safe_norm (src/Foundation/norm.jl:8-12) of a contiguous vector of N entries with stride 1, left folds.
+template <int N, typename T>
+__device__ __forceinline__ T safe_norm(const T* v) {
+    T m = fabs(v[0]);
+#pragma unroll
+    for (int i = 1; i < N; ++i) m = jl_max(m, static_cast<T>(fabs(v[i])));
+    if (!(isfin(m) && m > T(0))) return m;
+    T q = v[0] / m;
+    T s = q * q;
+#pragma unroll
+    for (int i = 1; i < N; ++i) { q = v[i] / m; s = s + q * q; }
+    return m * sqrt(s);
+}
+
+// The element-type constants of the tolerances.
+template <typename T> struct Eps;
+template <> struct Eps<double> {
+    static __device__ __forceinline__ double eps() { return 0x1p-52; }
+    static __device__ __forceinline__ double floatmin() { return 2.2250738585072014e-308; }
+};
+template <> struct Eps<float> {
+    static __device__ __forceinline__ float eps() { return 0x1p-23f; }
+    static __device__ __forceinline__ float floatmin() { return 1.17549435e-38f; }
+};
+
+// splitmix64 finalizer `_mix` (src/Tangent/initial.jl:2-7), bitwise.
+__device__ __forceinline__ uint64_t mix64(uint64_t z) {
+    z += 0x9e3779b97f4a7c15ULL;
+    z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ULL;
+    z = (z ^ (z >> 27)) * 0x94d049bb133111ebULL;
+    return z ^ (z >> 31);
+}
+
+}  // namespace cl

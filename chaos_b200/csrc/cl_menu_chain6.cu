@@ -1,0 +1,73 @@
+// Generated by chaos_b200/csrc/gen_menu.py (do not edit): compiled orbit-kernel instances, group "chain6".
+#include "cl_registry.cuh"
+
+namespace cl {
+namespace {
+
+cudaError_t L0(const cl_run& r, const KArgs& a, const double* A, cudaStream_t s, LaunchInfo* i) {
+    return launch_instance<SysChain<6>, double, Frame<8, RQR<2>>, NoFrame, NoFrame, 1>(r, a, A, s, i);
+}
+const Registrar R0("s4d12p0|k8:QR2|", L0);
+
+cudaError_t L1(const cl_run& r, const KArgs& a, const double* A, cudaStream_t s, LaunchInfo* i) {
+    return launch_instance<SysChain<6>, double, Frame<8, RQR<4>>, NoFrame, NoFrame, 1>(r, a, A, s, i);
+}
+const Registrar R1("s4d12p0|k8:QR4|", L1);
+
+cudaError_t L2(const cl_run& r, const KArgs& a, const double* A, cudaStream_t s, LaunchInfo* i) {
+    return launch_instance<SysChain<6>, double, Frame<8, RGALI<false>>, NoFrame, NoFrame, 1>(r, a, A, s, i);
+}
+const Registrar R2("s4d12p0|k8:GALI|", L2);
+
+cudaError_t L3(const cl_run& r, const KArgs& a, const double* A, cudaStream_t s, LaunchInfo* i) {
+    return launch_instance<SysChain<6>, double, Frame<2, RQR<2>>, NoFrame, NoFrame, 1>(r, a, A, s, i);
+}
+const Registrar R3("s4d12p0|k2:QR2|", L3);
+
+cudaError_t L4(const cl_run& r, const KArgs& a, const double* A, cudaStream_t s, LaunchInfo* i) {
+    return launch_instance<SysChain<6>, double, Frame<2, RSALI>, NoFrame, NoFrame, 1>(r, a, A, s, i);
+}
+const Registrar R4("s4d12p0|k2:SALI|", L4);
+
+cudaError_t L5(const cl_run& r, const KArgs& a, const double* A, cudaStream_t s, LaunchInfo* i) {
+    return launch_instance<SysChain<6>, double, Frame<2, RMEGNO<true>>, NoFrame, NoFrame, 1>(r, a, A, s, i);
+}
+const Registrar R5("s4d12p0|k2:MEGNO1|", L5);
+
+cudaError_t L6(const cl_run& r, const KArgs& a, const double* A, cudaStream_t s, LaunchInfo* i) {
+    return launch_instance<SysChain<6>, float, Frame<8, RQR<2>>, NoFrame, NoFrame, 1>(r, a, A, s, i);
+}
+const Registrar R6("s4d12p1|k8:QR2|", L6);
+
+cudaError_t L7(const cl_run& r, const KArgs& a, const double* A, cudaStream_t s, LaunchInfo* i) {
+    return launch_instance<SysChain<6>, float, Frame<8, RQR<4>>, NoFrame, NoFrame, 1>(r, a, A, s, i);
+}
+const Registrar R7("s4d12p1|k8:QR4|", L7);
+
+cudaError_t L8(const cl_run& r, const KArgs& a, const double* A, cudaStream_t s, LaunchInfo* i) {
+    return launch_instance<SysChain<6>, float, Frame<8, RGALI<false>>, NoFrame, NoFrame, 1>(r, a, A, s, i);
+}
+const Registrar R8("s4d12p1|k8:GALI|", L8);
+
+cudaError_t L9(const cl_run& r, const KArgs& a, const double* A, cudaStream_t s, LaunchInfo* i) {
+    return launch_instance<SysChain<6>, float, Frame<2, RQR<2>>, NoFrame, NoFrame, 1>(r, a, A, s, i);
+}
+const Registrar R9("s4d12p1|k2:QR2|", L9);
+
+cudaError_t L10(const cl_run& r, const KArgs& a, const double* A, cudaStream_t s, LaunchInfo* i) {
+    return launch_instance<SysChain<6>, float, Frame<2, RSALI>, NoFrame, NoFrame, 1>(r, a, A, s, i);
+}
+const Registrar R10("s4d12p1|k2:SALI|", L10);
+
+cudaError_t L11(const cl_run& r, const KArgs& a, const double* A, cudaStream_t s, LaunchInfo* i) {
+    return launch_instance<SysChain<6>, float, Frame<2, RMEGNO<true>>, NoFrame, NoFrame, 1>(r, a, A, s, i);
+}
+const Registrar R11("s4d12p1|k2:MEGNO1|", L11);
+
+cudaError_t L12(const cl_run& r, const KArgs& a, const double* A, cudaStream_t s, LaunchInfo* i) {
+    return launch_instance<SysChain<6>, double, Frame<1, RBenettin>, NoFrame, NoFrame, 1>(r, a, A, s, i);
+}
+const Registrar R12("s4d12p0|k1:BEN|", L12);
+
+}  // namespace
+}  // namespace cl

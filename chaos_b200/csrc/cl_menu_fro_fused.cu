@@ -1,0 +1,13 @@
+// Generated by chaos_b200/csrc/gen_menu.py (do not edit): compiled orbit-kernel instances, group "fro_fused".
+#include "cl_registry.cuh"
+
+namespace cl {
+namespace {
+
+cudaError_t L0(const cl_run& r, const KArgs& a, const double* A, cudaStream_t s, LaunchInfo* i) {
+    return launch_instance<SysFroeschle, double, Frame<4, RQR<4>>, Frame<4, RGALI<true>>, NoFrame, 2>(r, a, A, s, i);
+}
+const Registrar R0("s3d4p0|k4:QR4|k4:GALI,SALI|", L0);
+
+}  // namespace
+}  // namespace cl

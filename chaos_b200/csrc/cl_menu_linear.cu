@@ -1,0 +1,118 @@
+// Generated by chaos_b200/csrc/gen_menu.py (do not edit): compiled orbit-kernel instances, group "linear".
+#include "cl_registry.cuh"
+
+namespace cl {
+namespace {
+
+cudaError_t L0(const cl_run& r, const KArgs& a, const double* A, cudaStream_t s, LaunchInfo* i) {
+    return launch_instance<SysLinear<2>, double, Frame<1, RBenettin>, NoFrame, NoFrame, 1>(r, a, A, s, i);
+}
+const Registrar R0("s5d2p0|k1:BEN|", L0);
+
+cudaError_t L1(const cl_run& r, const KArgs& a, const double* A, cudaStream_t s, LaunchInfo* i) {
+    return launch_instance<SysLinear<2>, double, Frame<1, RQR<1>>, NoFrame, NoFrame, 1>(r, a, A, s, i);
+}
+const Registrar R1("s5d2p0|k1:QR1|", L1);
+
+cudaError_t L2(const cl_run& r, const KArgs& a, const double* A, cudaStream_t s, LaunchInfo* i) {
+    return launch_instance<SysLinear<2>, double, Frame<1, RQR<2>>, NoFrame, NoFrame, 1>(r, a, A, s, i);
+}
+const Registrar R2("s5d2p0|k1:QR2|", L2);
+
+cudaError_t L3(const cl_run& r, const KArgs& a, const double* A, cudaStream_t s, LaunchInfo* i) {
+    return launch_instance<SysLinear<2>, double, Frame<1, RQR<3>>, NoFrame, NoFrame, 1>(r, a, A, s, i);
+}
+const Registrar R3("s5d2p0|k1:QR3|", L3);
+
+cudaError_t L4(const cl_run& r, const KArgs& a, const double* A, cudaStream_t s, LaunchInfo* i) {
+    return launch_instance<SysLinear<2>, double, Frame<1, RQR<4>>, NoFrame, NoFrame, 1>(r, a, A, s, i);
+}
+const Registrar R4("s5d2p0|k1:QR4|", L4);
+
+cudaError_t L5(const cl_run& r, const KArgs& a, const double* A, cudaStream_t s, LaunchInfo* i) {
+    return launch_instance<SysLinear<2>, double, Frame<1, RQR<5>>, NoFrame, NoFrame, 1>(r, a, A, s, i);
+}
+const Registrar R5("s5d2p0|k1:QR5|", L5);
+
+cudaError_t L6(const cl_run& r, const KArgs& a, const double* A, cudaStream_t s, LaunchInfo* i) {
+    return launch_instance<SysLinear<2>, double, Frame<1, RQR<6>>, NoFrame, NoFrame, 1>(r, a, A, s, i);
+}
+const Registrar R6("s5d2p0|k1:QR6|", L6);
+
+cudaError_t L7(const cl_run& r, const KArgs& a, const double* A, cudaStream_t s, LaunchInfo* i) {
+    return launch_instance<SysLinear<2>, double, Frame<2, RQR<1>>, NoFrame, NoFrame, 1>(r, a, A, s, i);
+}
+const Registrar R7("s5d2p0|k2:QR1|", L7);
+
+cudaError_t L8(const cl_run& r, const KArgs& a, const double* A, cudaStream_t s, LaunchInfo* i) {
+    return launch_instance<SysLinear<2>, double, Frame<2, RQR<2>>, NoFrame, NoFrame, 1>(r, a, A, s, i);
+}
+const Registrar R8("s5d2p0|k2:QR2|", L8);
+
+cudaError_t L9(const cl_run& r, const KArgs& a, const double* A, cudaStream_t s, LaunchInfo* i) {
+    return launch_instance<SysLinear<2>, double, Frame<2, RQR<3>>, NoFrame, NoFrame, 1>(r, a, A, s, i);
+}
+const Registrar R9("s5d2p0|k2:QR3|", L9);
+
+cudaError_t L10(const cl_run& r, const KArgs& a, const double* A, cudaStream_t s, LaunchInfo* i) {
+    return launch_instance<SysLinear<2>, double, Frame<2, RQR<4>>, NoFrame, NoFrame, 1>(r, a, A, s, i);
+}
+const Registrar R10("s5d2p0|k2:QR4|", L10);
+
+cudaError_t L11(const cl_run& r, const KArgs& a, const double* A, cudaStream_t s, LaunchInfo* i) {
+    return launch_instance<SysLinear<2>, double, Frame<2, RQR<5>>, NoFrame, NoFrame, 1>(r, a, A, s, i);
+}
+const Registrar R11("s5d2p0|k2:QR5|", L11);
+
+cudaError_t L12(const cl_run& r, const KArgs& a, const double* A, cudaStream_t s, LaunchInfo* i) {
+    return launch_instance<SysLinear<2>, double, Frame<2, RQR<6>>, NoFrame, NoFrame, 1>(r, a, A, s, i);
+}
+const Registrar R12("s5d2p0|k2:QR6|", L12);
+
+cudaError_t L13(const cl_run& r, const KArgs& a, const double* A, cudaStream_t s, LaunchInfo* i) {
+    return launch_instance<SysLinear<2>, double, Frame<2, RSALI>, NoFrame, NoFrame, 1>(r, a, A, s, i);
+}
+const Registrar R13("s5d2p0|k2:SALI|", L13);
+
+cudaError_t L14(const cl_run& r, const KArgs& a, const double* A, cudaStream_t s, LaunchInfo* i) {
+    return launch_instance<SysLinear<2>, double, Frame<2, RGALI<false>>, NoFrame, NoFrame, 1>(r, a, A, s, i);
+}
+const Registrar R14("s5d2p0|k2:GALI|", L14);
+
+cudaError_t L15(const cl_run& r, const KArgs& a, const double* A, cudaStream_t s, LaunchInfo* i) {
+    return launch_instance<SysLinear<2>, double, Frame<2, RMEGNO<true>>, NoFrame, NoFrame, 1>(r, a, A, s, i);
+}
+const Registrar R15("s5d2p0|k2:MEGNO1|", L15);
+
+cudaError_t L16(const cl_run& r, const KArgs& a, const double* A, cudaStream_t s, LaunchInfo* i) {
+    return launch_instance<SysLinear<2>, double, Frame<2, RFLI<true>>, NoFrame, NoFrame, 1>(r, a, A, s, i);
+}
+const Registrar R16("s5d2p0|k2:FLI1|", L16);
+
+cudaError_t L17(const cl_run& r, const KArgs& a, const double* A, cudaStream_t s, LaunchInfo* i) {
+    return launch_instance<SysLinear<2>, double, Frame<2, RMEGNO<false>, RFLI<false>, RQR<6>>, NoFrame, NoFrame, 1>(r, a, A, s, i);
+}
+const Registrar R17("s5d2p0|k2:MEGNO0,FLI0,QR6|", L17);
+
+cudaError_t L18(const cl_run& r, const KArgs& a, const double* A, cudaStream_t s, LaunchInfo* i) {
+    return launch_instance<SysLinear<2>, double, Frame<2, RMEGNO<false>, RSALI>, NoFrame, NoFrame, 1>(r, a, A, s, i);
+}
+const Registrar R18("s5d2p0|k2:MEGNO0,SALI|", L18);
+
+cudaError_t L19(const cl_run& r, const KArgs& a, const double* A, cudaStream_t s, LaunchInfo* i) {
+    return launch_instance<SysLinear<2>, double, Frame<2, RFLI<false>, RSALI>, NoFrame, NoFrame, 1>(r, a, A, s, i);
+}
+const Registrar R19("s5d2p0|k2:FLI0,SALI|", L19);
+
+cudaError_t L20(const cl_run& r, const KArgs& a, const double* A, cudaStream_t s, LaunchInfo* i) {
+    return launch_instance<SysLinear<2>, double, Frame<2, RMEGNO<false>, RFLI<false>, RSALI>, NoFrame, NoFrame, 1>(r, a, A, s, i);
+}
+const Registrar R20("s5d2p0|k2:MEGNO0,FLI0,SALI|", L20);
+
+cudaError_t L21(const cl_run& r, const KArgs& a, const double* A, cudaStream_t s, LaunchInfo* i) {
+    return launch_instance<SysLinear<2>, double, Frame<2>, NoFrame, NoFrame, 1>(r, a, A, s, i);
+}
+const Registrar R21("s5d2p0|k2:|", L21);
+
+}  // namespace
+}  // namespace cl

@@ -1,0 +1,83 @@
+// Generated by chaos_b200/csrc/gen_menu.py (do not edit): compiled orbit-kernel instances, group "linear4".
+#include "cl_registry.cuh"
+
+namespace cl {
+namespace {
+
+cudaError_t L0(const cl_run& r, const KArgs& a, const double* A, cudaStream_t s, LaunchInfo* i) {
+    return launch_instance<SysLinear<4>, double, Frame<2, RQR<1>>, NoFrame, NoFrame, 1>(r, a, A, s, i);
+}
+const Registrar R0("s5d4p0|k2:QR1|", L0);
+
+cudaError_t L1(const cl_run& r, const KArgs& a, const double* A, cudaStream_t s, LaunchInfo* i) {
+    return launch_instance<SysLinear<4>, double, Frame<2, RQR<2>>, NoFrame, NoFrame, 1>(r, a, A, s, i);
+}
+const Registrar R1("s5d4p0|k2:QR2|", L1);
+
+cudaError_t L2(const cl_run& r, const KArgs& a, const double* A, cudaStream_t s, LaunchInfo* i) {
+    return launch_instance<SysLinear<4>, double, Frame<2, RQR<3>>, NoFrame, NoFrame, 1>(r, a, A, s, i);
+}
+const Registrar R2("s5d4p0|k2:QR3|", L2);
+
+cudaError_t L3(const cl_run& r, const KArgs& a, const double* A, cudaStream_t s, LaunchInfo* i) {
+    return launch_instance<SysLinear<4>, double, Frame<2, RQR<4>>, NoFrame, NoFrame, 1>(r, a, A, s, i);
+}
+const Registrar R3("s5d4p0|k2:QR4|", L3);
+
+cudaError_t L4(const cl_run& r, const KArgs& a, const double* A, cudaStream_t s, LaunchInfo* i) {
+    return launch_instance<SysLinear<4>, double, Frame<2, RQR<5>>, NoFrame, NoFrame, 1>(r, a, A, s, i);
+}
+const Registrar R4("s5d4p0|k2:QR5|", L4);
+
+cudaError_t L5(const cl_run& r, const KArgs& a, const double* A, cudaStream_t s, LaunchInfo* i) {
+    return launch_instance<SysLinear<4>, double, Frame<2, RQR<6>>, NoFrame, NoFrame, 1>(r, a, A, s, i);
+}
+const Registrar R5("s5d4p0|k2:QR6|", L5);
+
+cudaError_t L6(const cl_run& r, const KArgs& a, const double* A, cudaStream_t s, LaunchInfo* i) {
+    return launch_instance<SysLinear<4>, double, Frame<2, RGALI<false>>, NoFrame, NoFrame, 1>(r, a, A, s, i);
+}
+const Registrar R6("s5d4p0|k2:GALI|", L6);
+
+cudaError_t L7(const cl_run& r, const KArgs& a, const double* A, cudaStream_t s, LaunchInfo* i) {
+    return launch_instance<SysLinear<4>, double, Frame<4, RQR<1>>, NoFrame, NoFrame, 1>(r, a, A, s, i);
+}
+const Registrar R7("s5d4p0|k4:QR1|", L7);
+
+cudaError_t L8(const cl_run& r, const KArgs& a, const double* A, cudaStream_t s, LaunchInfo* i) {
+    return launch_instance<SysLinear<4>, double, Frame<4, RQR<2>>, NoFrame, NoFrame, 1>(r, a, A, s, i);
+}
+const Registrar R8("s5d4p0|k4:QR2|", L8);
+
+cudaError_t L9(const cl_run& r, const KArgs& a, const double* A, cudaStream_t s, LaunchInfo* i) {
+    return launch_instance<SysLinear<4>, double, Frame<4, RQR<3>>, NoFrame, NoFrame, 1>(r, a, A, s, i);
+}
+const Registrar R9("s5d4p0|k4:QR3|", L9);
+
+cudaError_t L10(const cl_run& r, const KArgs& a, const double* A, cudaStream_t s, LaunchInfo* i) {
+    return launch_instance<SysLinear<4>, double, Frame<4, RQR<4>>, NoFrame, NoFrame, 1>(r, a, A, s, i);
+}
+const Registrar R10("s5d4p0|k4:QR4|", L10);
+
+cudaError_t L11(const cl_run& r, const KArgs& a, const double* A, cudaStream_t s, LaunchInfo* i) {
+    return launch_instance<SysLinear<4>, double, Frame<4, RQR<5>>, NoFrame, NoFrame, 1>(r, a, A, s, i);
+}
+const Registrar R11("s5d4p0|k4:QR5|", L11);
+
+cudaError_t L12(const cl_run& r, const KArgs& a, const double* A, cudaStream_t s, LaunchInfo* i) {
+    return launch_instance<SysLinear<4>, double, Frame<4, RQR<6>>, NoFrame, NoFrame, 1>(r, a, A, s, i);
+}
+const Registrar R12("s5d4p0|k4:QR6|", L12);
+
+cudaError_t L13(const cl_run& r, const KArgs& a, const double* A, cudaStream_t s, LaunchInfo* i) {
+    return launch_instance<SysLinear<4>, double, Frame<4, RGALI<false>>, NoFrame, NoFrame, 1>(r, a, A, s, i);
+}
+const Registrar R13("s5d4p0|k4:GALI|", L13);
+
+cudaError_t L14(const cl_run& r, const KArgs& a, const double* A, cudaStream_t s, LaunchInfo* i) {
+    return launch_instance<SysLinear<4>, double, Frame<1, RBenettin>, NoFrame, NoFrame, 1>(r, a, A, s, i);
+}
+const Registrar R14("s5d4p0|k1:BEN|", L14);
+
+}  // namespace
+}  // namespace cl

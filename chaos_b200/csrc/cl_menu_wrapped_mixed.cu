@@ -1,0 +1,28 @@
+// Generated by chaos_b200/csrc/gen_menu.py (do not edit): compiled orbit-kernel instances, group "wrapped_mixed".
+#include "cl_registry.cuh"
+
+namespace cl {
+namespace {
+
+cudaError_t L0(const cl_run& r, const KArgs& a, const double* A, cudaStream_t s, LaunchInfo* i) {
+    return launch_instance<SysWrapped, float, Frame<2, RQR<2>>, NoFrame, NoFrame, 1>(r, a, A, s, i);
+}
+const Registrar R0("s2d2p1|k2:QR2|", L0);
+
+cudaError_t L1(const cl_run& r, const KArgs& a, const double* A, cudaStream_t s, LaunchInfo* i) {
+    return launch_instance<SysWrapped, float, Frame<2, RQR<4>>, NoFrame, NoFrame, 1>(r, a, A, s, i);
+}
+const Registrar R1("s2d2p1|k2:QR4|", L1);
+
+cudaError_t L2(const cl_run& r, const KArgs& a, const double* A, cudaStream_t s, LaunchInfo* i) {
+    return launch_instance<SysWrapped, float, Frame<2, RQR<6>>, NoFrame, NoFrame, 1>(r, a, A, s, i);
+}
+const Registrar R2("s2d2p1|k2:QR6|", L2);
+
+cudaError_t L3(const cl_run& r, const KArgs& a, const double* A, cudaStream_t s, LaunchInfo* i) {
+    return launch_instance<SysWrapped, float, Frame<1, RBenettin>, NoFrame, NoFrame, 1>(r, a, A, s, i);
+}
+const Registrar R3("s2d2p1|k1:BEN|", L3);
+
+}  // namespace
+}  // namespace cl

@@ -1,0 +1,251 @@
+// cl_systems.cuh -- the maps of the fixed menu as device functors (src/Systems, src/Integrators).
+//
+// The orbit body evaluates the tangent at the OLD point and then advances the point (src/Tangent/orbit.jl:49-52).
+// Each system splits that step in three so one point can drive several tangent frames:
+//   jac(x, J)        everything the step needs at the old point (one sincos per distinct argument: `forward`
+//                    and `tangent` of the reference evaluate the same arguments, so sharing them changes no bit)
+//   apply<K>(J, W)   W <- tangent * W: for Real = double `fused_product` (src/Foundation/product.jl:9-20) on the
+//                    reference's dense tangent matrix, including its 0 and 1 entries, or the band product of
+//                    `ChainTangent` (chain_tangent.jl:62-78); for Real = float the same product exploiting the
+//                    matrix structure
+//   forward(x, J)    the new point, Float64 in every kernel, operation for operation the reference's `forward`.
+#pragma once
+
+#include "cl_math.cuh"
+#include "cl_reducers.cuh"
+
+namespace cl {
+
+// pi in Float64 as `_pi` builds it (src/Systems/standard_map.jl:46): 3.141592653589793 + 1.2246467991473532e-16.
+__device__ __forceinline__ double jl_pi() {
+    const double hi = 3.141592653589793, lo = 1.2246467991473532e-16;
+    return hi + lo;
+}
+
+// fused_product of a dense D x D tangent M (column-major) with the D x K frame W, in place.
+template <int D, int K>
+__device__ __forceinline__ void fused_dense(const double* M, double* W) {
+    double Wn[D * K];
+#pragma unroll
+    for (int j = 0; j < K; ++j)
+#pragma unroll
+        for (int i = 0; i < D; ++i) {
+            double acc = M[i] * W[j * D];
+#pragma unroll
+            for (int q = 1; q < D; ++q) acc = fma(M[i + q * D], W[q + j * D], acc);
+            Wn[i + j * D] = acc;
+        }
+#pragma unroll
+    for (int l = 0; l < D * K; ++l) W[l] = Wn[l];
+}
+template <int D, int K>
+__device__ __forceinline__ void fused_dense(const double* M, float* W) {   // mixed kernels: Float32 dense product
+    float Wn[D * K];
+#pragma unroll
+    for (int j = 0; j < K; ++j)
+#pragma unroll
+        for (int i = 0; i < D; ++i) {
+            float acc = static_cast<float>(M[i]) * W[j * D];
+#pragma unroll
+            for (int q = 1; q < D; ++q) acc = __fmaf_rn(static_cast<float>(M[i + q * D]), W[q + j * D], acc);
+            Wn[i + j * D] = acc;
+        }
+#pragma unroll
+    for (int l = 0; l < D * K; ++l) W[l] = Wn[l];
+}
+
+// ---- StandardMap (standard_map.jl:8-44) and WrappedStandardMap (wrapped_standard_map.jl:12-57) -----------------
+struct StdJac { double s, c; };   // sin x, K cos x at the old x
+
+struct SysStandard {
+    static constexpr int D = 2, S = 2;
+    using Jac = StdJac;
+    double K;
+    __device__ __forceinline__ void jac(const double* x, StdJac& J) const {
+        double sn, cs; cl_sincos(x[0], &sn, &cs);
+        J.s = sn; J.c = K * cs;
+    }
+    // _dt: [[1 + c, 1], [c, 1]]
+    template <int KK>
+    __device__ __forceinline__ void apply(const StdJac& J, double* W) const {
+        const double o = 1.0;
+        const double M[4] = {o + J.c, J.c, o, o};
+        fused_dense<2, KK>(M, W);
+    }
+    template <int KK>
+    __device__ __forceinline__ void apply(const StdJac& J, float* W) const {
+        const float c = static_cast<float>(J.c), opc = static_cast<float>(1.0 + J.c);
+#pragma unroll
+        for (int j = 0; j < KK; ++j) {
+            const float w0 = W[2 * j], w1 = W[2 * j + 1];
+            W[2 * j] = __fmaf_rn(opc, w0, w1);
+            W[2 * j + 1] = __fmaf_rn(c, w0, w1);
+        }
+    }
+    __device__ __forceinline__ void forward(double* x, const StdJac& J) const {
+        const double p = x[1] + K * J.s;
+        x[0] = x[0] + p;
+        x[1] = p;
+    }
+};
+
+// _reduce (wrapped_standard_map.jl:15-28)
+__device__ __forceinline__ void wrap_reduce(double u, double tp, double& r, double& a) {
+    a = floor(u / tp);
+    r = u - tp * a;
+    if (r < 0) { r += tp; a -= 1; }
+    if (r >= tp) { r -= tp; a += 1; }
+}
+
+struct SysWrapped : SysStandard {
+    static constexpr int S = 4;
+    // forward (wrapped_standard_map.jl:30-37) with _checked (:23-28)
+    __device__ __forceinline__ void forward(double* z, const StdJac& J) const {
+        const double tp = 2 * jl_pi();
+        double p, a, x, b;
+        wrap_reduce(z[1] + K * J.s, tp, p, a);
+        const double n = z[3] + a;
+        wrap_reduce(z[0] + p, tp, x, b);
+        const double m = z[2] + n + b;
+        const double lim = 0x1p53;
+        if (fabs(m) < lim && fabs(n) < lim) { z[0] = x; z[1] = p; z[2] = m; z[3] = n; }
+        else { const double nan = __longlong_as_double(0x7ff8000000000000LL); z[0] = z[1] = z[2] = z[3] = nan; }
+    }
+};
+
+// ---- FroeschleMap (froeschle_map.jl:9-58) ---------------------------------------------------------------------
+struct FroJac { double x1, x2, s1, s2, c12, a, b, c; };
+
+struct SysFroeschle {
+    static constexpr int D = 4, S = 4;
+    using Jac = FroJac;
+    double nu, kappa, mu;
+    __device__ __forceinline__ void jac(const double* z, FroJac& J) const {
+        J.x1 = z[0] + z[2];
+        J.x2 = z[1] + z[3];
+        double c1, c2, s12;
+        cl_sincos(J.x1, &J.s1, &c1);
+        cl_sincos(J.x2, &J.s2, &c2);
+        cl_sincos(J.x1 + J.x2, &s12, &J.c12);
+        const double t = mu * s12;               // _abc (:35-39)
+        J.a = -nu * c1 - t;
+        J.b = -t;
+        J.c = -kappa * c2 - t;
+    }
+    // M = [[I, I], [A, I + A]] (_f3_tangent :42-47), the dense fused product with every 0 and 1 entry
+    template <int KK>
+    __device__ __forceinline__ void apply(const FroJac& J, double* W) const {
+        const double o = 1.0, Z = 0.0;
+        const double M[16] = {o, Z, J.a, J.b, Z, o, J.b, J.c, o, Z, o + J.a, J.b, Z, o, J.b, o + J.c};
+        fused_dense<4, KK>(M, W);
+    }
+    // Float32: top = W_q + W_p, bottom = A (W_q + W_p) + W_p
+    template <int KK>
+    __device__ __forceinline__ void apply(const FroJac& J, float* W) const {
+        const float a = static_cast<float>(J.a), b = static_cast<float>(J.b), c = static_cast<float>(J.c);
+#pragma unroll
+        for (int j = 0; j < KK; ++j) {
+            float* w = W + 4 * j;
+            const float t1 = w[0] + w[2], t2 = w[1] + w[3];
+            const float b1 = __fmaf_rn(a, t1, __fmaf_rn(b, t2, w[2]));
+            const float b2 = __fmaf_rn(b, t1, __fmaf_rn(c, t2, w[3]));
+            w[0] = t1; w[1] = t2; w[2] = b1; w[3] = b2;
+        }
+    }
+    __device__ __forceinline__ void forward(double* z, const FroJac& J) const {   // :20-25
+        const double f = mu * (1.0 - J.c12);
+        const double p1 = z[2] - nu * J.s1 - f;
+        const double p2 = z[3] - kappa * J.s2 - f;
+        z[0] = J.x1; z[1] = J.x2; z[2] = p1; z[3] = p2;
+    }
+};
+
+// ---- LinearSymplecticMap (linear_symplectic.jl): z' = A z (fused StaticArrays product), tangent A ----------------
+template <int DD>
+struct SysLinear {
+    static constexpr int D = DD, S = DD;
+    double A[D * D];   // the d x d matrix (column-major), passed by value: kernel-parameter (constant bank) loads
+    struct Jac {};
+    __device__ __forceinline__ void jac(const double*, Jac&) const {}
+    template <int KK, typename T>
+    __device__ __forceinline__ void apply(const Jac&, T* W) const { fused_dense<D, KK>(A, W); }
+    __device__ __forceinline__ void forward(double* z, const Jac&) const {
+        double zn[D];
+#pragma unroll
+        for (int i = 0; i < D; ++i) {
+            double acc = A[i] * z[0];
+#pragma unroll
+            for (int q = 1; q < D; ++q) acc = fma(A[i + q * D], z[q], acc);
+            zn[i] = acc;
+        }
+#pragma unroll
+        for (int i = 0; i < D; ++i) z[i] = zn[i];
+    }
+};
+
+// ---- StandardMapChain with the banded ChainTangent (standard_map_chain.jl, chain_tangent.jl) -------------------
+template <int NS>
+struct ChainJac { double g[NS], gl[NS], gr[NS], sq[NS], sl[NS], sr[NS]; };
+
+template <int NS>
+struct SysChain {
+    static constexpr int D = 2 * NS, S = 2 * NS;
+    using Jac = ChainJac<NS>;
+    double K, eps;
+    int ring;
+    __device__ __forceinline__ int left(int j) const { return j > 0 ? j - 1 : (ring ? NS - 1 : -1); }
+    __device__ __forceinline__ int right(int j) const { return j < NS - 1 ? j + 1 : (ring ? 0 : -1); }
+    // _chain_tangent (chain_tangent.jl:84-91) at the old positions, and the sines `_force` needs (:164-170)
+    __device__ __forceinline__ void jac(const double* z, ChainJac<NS>& J) const {
+#pragma unroll
+        for (int j = 0; j < NS; ++j) {
+            const int kl = left(j), kr = right(j);
+            double sq, cq; cl_sincos(z[j], &sq, &cq);
+            double sl = 0.0, cl_ = 0.0, sr = 0.0, cr = 0.0;
+            if (kl >= 0) { double s_, c_; cl_sincos(z[j] - z[kl], &s_, &c_); sl = s_; cl_ = eps * c_; }
+            if (kr >= 0) { double s_, c_; cl_sincos(z[j] - z[kr], &s_, &c_); sr = s_; cr = eps * c_; }
+            J.g[j] = (K * cq + cl_) + cr;
+            J.gl[j] = -cl_;
+            J.gr[j] = -cr;
+            J.sq[j] = sq; J.sl[j] = sl; J.sr[j] = sr;
+        }
+    }
+    // `ChainTangent * W`: GW = _band(W_q); top = (W_q + GW) + W_p, bottom = GW + W_p (chain_tangent.jl:62-78)
+    template <int KK, typename T>
+    __device__ __forceinline__ void apply(const ChainJac<NS>& J, T* W) const {
+#pragma unroll
+        for (int col = 0; col < KK; ++col) {
+            T* Wq = W + col * D;
+            T v[NS];
+#pragma unroll
+            for (int j = 0; j < NS; ++j) {
+                const int kl = left(j), kr = right(j);
+                T t = static_cast<T>(J.g[j]) * Wq[j];
+                if (kl >= 0) t = t + static_cast<T>(J.gl[j]) * Wq[kl];
+                if (kr >= 0) t = t + static_cast<T>(J.gr[j]) * Wq[kr];
+                v[j] = t;
+            }
+#pragma unroll
+            for (int j = 0; j < NS; ++j) {
+                const T wq = Wq[j], wp = Wq[NS + j];
+                Wq[j] = (wq + v[j]) + wp;
+                Wq[NS + j] = v[j] + wp;
+            }
+        }
+    }
+    // forward: p_j' = p_j + (K sin q_j + eps s_j), s_j = 0 + sin(q_j - q_left) + sin(q_j - q_right); q_j' = q_j + p_j'
+    __device__ __forceinline__ void forward(double* z, const ChainJac<NS>& J) const {
+        double p[NS];
+#pragma unroll
+        for (int j = 0; j < NS; ++j) {
+            double s = 0.0;
+            if (left(j) >= 0) s = s + J.sl[j];
+            if (right(j) >= 0) s = s + J.sr[j];
+            p[j] = z[NS + j] + (K * J.sq[j] + eps * s);
+        }
+#pragma unroll
+        for (int j = 0; j < NS; ++j) { z[j] = z[j] + p[j]; z[NS + j] = p[j]; }
+    }
+};
+
+}  // namespace cl

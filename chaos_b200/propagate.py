@@ -1,0 +1,266 @@
+"""`propagate` on the B200: the host side of the drop-in boundary.
+
+Mirrors `propagate(sys, x0, N; k, tau, seed, reducers, backend, chunk, W0)` of src/Tangent/propagate.jl:267-290
+and its record `PropagationResult` (:20-26): the same argument checks and ArgumentErrors (ValueError here), the
+same chunking rule (`chunk_size`, :10-18), the same per-orbit failure handling (the lowest failing orbit id throws
+its `NumericalHealthError`, :111-113) and the same host-side `reducer_final` summaries (:116-118), with the device
+chunk running in libchaoslab_b200 through its C ABI. There is no CPU path in this package: the reference keeps its
+own CPU backend; a device failure is raised as `DeviceError` with the reference's fallback reason index.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+import os
+import platform
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _abi
+from ._lib import last_error, lib
+from .foundation import DeviceError, NumericalHealthError
+from .reducers import GALI, SALI, Reducer, chain_dtype
+from .systems import System
+
+STATUS_OK, STATUS_STATE, STATUS_W, STATUS_REDUCER = 0, 1, 2, 3
+CHUNK_HEADROOM = 0.5
+PRECISIONS = {"fp64": _abi.PREC_FP64, "mixed": _abi.PREC_MIXED}
+
+
+@dataclass
+class FrameSpec:
+    """One tangent frame of a run: k deviation vectors, its reducer chain, optional initial frames (n, d, k)."""
+    k: int
+    reducers: tuple = ()
+    W0: np.ndarray | None = None
+
+
+@dataclass
+class PropagationResult:
+    """`PropagationResult(x, W, finals, provenance)` (propagate.jl:20-26) plus the raw device records."""
+    x: np.ndarray                # (n, s)
+    W: np.ndarray                # (n, d, k)
+    finals: list | None          # per orbit, a tuple of reducer_final dicts (None when not requested)
+    provenance: dict
+    states: np.ndarray | None = None   # structured array in the Julia isbits layout
+    code: np.ndarray | None = None
+    hstep: np.ndarray | None = None
+    reducers: tuple = field(default=())
+
+
+def bytes_per_orbit(d: int, k: int, s: int | None = None) -> int:
+    """sizeof(T)(s + d k + 2k) + 16 (propagate.jl:1-6)."""
+    s = d if s is None else s
+    return 8 * (s + d * k + 2 * k) + 16
+
+
+def chunk_size(free_bytes: int, d: int, k: int, f: float = CHUNK_HEADROOM, reducer_bytes: int = 0,
+               s: int | None = None) -> int:
+    """floor(f free / (bytes_per_orbit + reducer_bytes)), at least 1 (propagate.jl:10-18)."""
+    return max(1, math.floor(f * free_bytes / (bytes_per_orbit(d, k, s) + reducer_bytes)))
+
+
+def _check_steps(N: int, tau: int) -> None:
+    if not (tau >= 1 and N >= 1 and N % tau == 0):
+        raise ValueError(f"N must be a positive multiple of tau, got N = {N}, tau = {tau}")
+
+
+def _check_frame(sys: System, fr: FrameSpec) -> None:
+    d = sys.d
+    if not 1 <= fr.k <= d:
+        raise ValueError(f"k must be in 1:{d}, got {fr.k}")
+    rs = tuple(fr.reducers)
+    for i, r in enumerate(rs):
+        if not isinstance(r, Reducer):
+            raise TypeError(f"{r!r} is not a reducer of the compiled menu")
+        if isinstance(r, SALI) and i > 0 and isinstance(rs[i - 1], GALI):
+            continue   # SALI of the GALI frame's columns 1-2
+        r.check(d, fr.k)
+
+
+def build_run(sys: System, N: int, tau: int, frames: list[FrameSpec], precision: str = "fp64", seed: int = 0,
+              n0: int = 0, steps: int = 0, orbit_base: int = 0) -> _abi.cl_run:
+    run = _abi.cl_run()
+    run.abi_version = _abi.ABI_VERSION
+    run.d, run.s, run.tau = sys.d, sys.s, int(tau)
+    run.N, run.n0, run.steps = int(N), int(n0), int(steps)
+    run.n_frames = len(frames)
+    run.precision = PRECISIONS[precision]
+    run.seed = int(seed) % (1 << 64)
+    run.orbit_base = int(orbit_base)
+    run.sys = sys.to_cl()
+    for f, fr in enumerate(frames):
+        run.frames[f].k = fr.k
+        run.frames[f].n_reducers = len(fr.reducers)
+        for i, r in enumerate(fr.reducers):
+            run.frames[f].reducers[i] = r.to_cl()
+    return run
+
+
+def _first_bad(v: np.ndarray) -> float:
+    flat = np.asarray(v, dtype=np.float64).ravel(order="F")
+    bad = np.flatnonzero(~np.isfinite(flat))
+    return float(flat[bad[0]])
+
+
+def _health_error(code, x, W, step, orbit, backend):   # orbit.jl:63-68
+    if code == STATUS_STATE:
+        return NumericalHealthError("state", _first_bad(x), math.inf, step, orbit, backend)
+    return NumericalHealthError("deviation matrix", _first_bad(W), math.inf, step, orbit, backend)
+
+
+def _reducer_error(reducers, st, orbit, backend):   # orbit.jl:34-37: the first failed reducer of the chain
+    for i, r in enumerate(reducers):
+        sub = st[f"r{i}"]
+        if isinstance(r, GALI) and i + 1 < len(reducers) and isinstance(reducers[i + 1], SALI):
+            pass
+        if r.failed(sub):
+            return r.error(sub, orbit, backend)
+    raise AssertionError("STATUS_REDUCER without a failed reducer")
+
+
+def _finals(reducers, st_row, d):
+    out = []
+    for i, r in enumerate(reducers):
+        sub = st_row[f"r{i}"]
+        out.append(r.final(sub, d) if isinstance(r, GALI) else r.final(sub))
+    return tuple(out)
+
+
+def probe() -> dict:
+    """`Foundation.probe` record of the device (loadable, functional, device, compiles) plus memory."""
+    p = _abi.cl_probe()
+    rc = lib().cl_b200_probe(C.byref(p))
+    return dict(loadable=bool(p.loadable), functional=bool(p.functional), compiles=bool(p.compiles) and rc == 0,
+                device=p.device.decode(), sm=p.sm, sm_count=p.sm_count, free_bytes=p.free_bytes,
+                total_bytes=p.total_bytes)
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data
+
+
+def propagate_frames(sys: System, x0, N: int, frames: list[FrameSpec], *, tau: int = 1, seed: int = 0,
+                     precision: str = "fp64", chunk: int | None = None, launch_steps: int | None = None,
+                     finals: bool = True, throw: bool = True) -> list[PropagationResult]:
+    """Integrate every orbit of x0 once and carry each frame of `frames` along it; frame f's result is the
+    reference's `propagate(sys, x0, N; k = frames[f].k, tau, seed, reducers = frames[f].reducers,
+    W0 = frames[f].W0)`."""
+    x0 = np.ascontiguousarray(np.asarray(x0, dtype=np.float64))
+    if x0.ndim != 2:
+        raise ValueError("x0 must be an (n, s) array")
+    n, s = x0.shape
+    N, tau = int(N), int(tau)
+    _check_steps(N, tau)
+    d = sys.d
+    if s < d:
+        raise ValueError(f"state length {s} is below the system dimension {d}")
+    if s != sys.s:
+        raise ValueError(f"state length {s} does not match {sys.name} (s = {sys.s})")
+    if chunk is not None and chunk < 1:
+        raise ValueError(f"chunk must be positive, got {chunk}")
+    if not 1 <= len(frames) <= _abi.MAX_FRAMES:
+        raise ValueError("one to three frames")
+    if launch_steps is not None and (launch_steps < 1 or launch_steps % tau):
+        raise ValueError(f"forced steps per launch must be a positive multiple of tau, got L = {launch_steps}, tau = {tau}")
+    W0s = []
+    for fr in frames:
+        _check_frame(sys, fr)
+        if fr.W0 is not None:
+            W0 = np.asarray(fr.W0, dtype=np.float64)
+            if W0.shape[0] != n:
+                raise ValueError("W0 needs one matrix per orbit")
+            if W0.shape[1:] != (d, fr.k):
+                raise ValueError(f"W0 matrices must be {d} x {fr.k}")
+            W0s.append(np.ascontiguousarray(W0.transpose(0, 2, 1)))   # column-major per orbit
+        else:
+            W0s.append(None)
+    run = build_run(sys, N, tau, frames, precision, seed, steps=launch_steps or 0)
+    L = lib()
+    rc = L.cl_b200_check(C.byref(run))
+    if rc != 0:
+        msg = last_error()
+        if rc == _abi.EINVAL:
+            raise ValueError(msg)
+        raise DeviceError(rc, msg)
+    dtypes = [chain_dtype(fr.reducers, d, fr.k) for fr in frames]
+    rbytes = sum(dt.itemsize for dt in dtypes)
+    if chunk is None:
+        pr = probe()
+        kk = max(fr.k for fr in frames)
+        csize = chunk_size(pr["free_bytes"], d, kk, reducer_bytes=rbytes, s=s) if pr["free_bytes"] else n
+    else:
+        csize = chunk
+    csize = min(csize, n) if n else 1
+    x = np.empty((n, s))
+    Wout = [np.empty((n, fr.k, d)) for fr in frames]
+    states = [np.zeros(n, dtype=dt) if dt.itemsize else None for dt in dtypes]
+    codes = [np.zeros(n, dtype=np.int8) for _ in frames]
+    hsteps = [np.zeros(n, dtype=np.int64) for _ in frames]
+    prov_dev = _abi.cl_prov()
+    gpu_ms, chunks = 0.0, 0
+    errors: list = [None] * len(frames)
+    for lo in range(0, n, csize):
+        hi = min(lo + csize, n)
+        run.orbit_base = lo
+        bufs = _abi.cl_buffers()
+        bufs.x0 = x0[lo:hi].ctypes.data
+        bufs.x = x[lo:hi].ctypes.data
+        for f in range(len(frames)):
+            bufs.W0[f] = None if W0s[f] is None else W0s[f][lo:hi].ctypes.data
+            bufs.W[f] = Wout[f][lo:hi].ctypes.data
+            bufs.states[f] = None if states[f] is None else states[f][lo:hi].ctypes.data
+            bufs.code[f] = codes[f][lo:hi].ctypes.data
+            bufs.hstep[f] = hsteps[f][lo:hi].ctypes.data
+        rc = L.cl_b200_propagate(C.byref(run), hi - lo, C.byref(bufs), C.byref(prov_dev))
+        if rc != 0:
+            raise DeviceError(rc, last_error())
+        gpu_ms += prov_dev.gpu_ms
+        chunks += 1
+        for f, fr in enumerate(frames):   # lowest failing orbit id first (propagate.jl:111-113)
+            if errors[f] is not None:
+                continue
+            bad = np.flatnonzero(codes[f][lo:hi] != STATUS_OK)
+            if bad.size:
+                i = lo + int(bad[0])
+                c = int(codes[f][i])
+                if c == STATUS_REDUCER:
+                    errors[f] = _reducer_error(tuple(fr.reducers), states[f][i], i + 1, "gpu")
+                else:
+                    errors[f] = _health_error(c, x[i], Wout[f][i].T, int(hsteps[f][i]), i + 1, "gpu")
+    if throw:
+        for e in errors:
+            if e is not None:
+                raise e
+    results = []
+    for f, fr in enumerate(frames):
+        prov = dict(backend="gpu", device=prov_dev.device.decode(), backend_fallback_reason="",
+                    precision="Float64" if precision == "fp64" else "Float64 orbit / Float32 tangent",
+                    threads=os.cpu_count(), cpu=platform.processor() or platform.machine(), seed=seed, tau=tau,
+                    k=fr.k, chunk_size=csize, headroom=CHUNK_HEADROOM, gpu_chunks=chunks, gpu_chunk_size=csize,
+                    launch_steps=int(prov_dev.launch_steps), launches_per_chunk=int(prov_dev.launches),
+                    kernel=prov_dev.variant.decode(), gpu_ms=gpu_ms, registers=int(prov_dev.regs))
+        for r in fr.reducers:
+            prov.update(r.provenance())
+        W = Wout[f].transpose(0, 2, 1)
+        fin = None
+        if finals and states[f] is not None:
+            fin = [_finals(tuple(fr.reducers), states[f][i], d) for i in range(n)]
+        elif finals:
+            fin = [() for _ in range(n)]
+        results.append(PropagationResult(x=x, W=W, finals=fin, provenance=prov, states=states[f], code=codes[f],
+                                         hstep=hsteps[f], reducers=tuple(fr.reducers)))
+    return results
+
+
+def propagate(sys: System, x0, N: int, *, k: int, tau: int = 1, seed: int = 0, reducers=(), backend: str = "gpu",
+              chunk: int | None = None, W0=None, precision: str = "fp64", launch_steps: int | None = None,
+              finals: bool = True) -> PropagationResult:
+    """propagate(sys, x0, N; k, tau=1, seed, reducers=(), backend=:gpu, chunk=nothing, W0=nothing) on the B200
+    (src/Tangent/propagate.jl:267-290). `x0` is (n, s); `W0` (n, d, k) or None for the seeded frames;
+    `precision` is "fp64" (the reference's arithmetic) or "mixed" (Float32 tangent frames)."""
+    if backend not in ("gpu", "auto"):
+        raise ValueError("backend must be :gpu or :auto here; the CPU path is the reference's own")
+    return propagate_frames(sys, x0, N, [FrameSpec(int(k), tuple(reducers), W0)], tau=tau, seed=seed,
+                            precision=precision, chunk=chunk, launch_steps=launch_steps, finals=finals)[0]

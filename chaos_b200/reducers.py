@@ -1,0 +1,327 @@
+"""Reducers of the fixed menu (src/Lyapunov, src/Indicators) with their host-side protocol.
+
+The device runs `reducer_step` for every handoff (fused into the orbit kernel) and hands back each state in the
+isbits layout of the Julia struct (T = Float64). Here each reducer knows that layout as a numpy structured dtype
+and runs the host half of the reducer protocol (src/Tangent/Tangent.jl:21-111) on it: `final` (`reducer_final`),
+`failed` (`reducer_failed`), `error` (`reducer_error`) and `provenance` (`reducer_provenance`), with the same
+arithmetic as the reference.
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+from . import _abi
+from .foundation import EPS, NumericalHealthError
+
+
+def _cs(name):
+    return [(name + "_s", "<f8"), (name + "_c", "<f8")]
+
+
+def _tot(s, c):
+    return float(np.float64(s) + np.float64(c))
+
+
+class Orthonormalizer:
+    code: int
+    name: str
+    gs_family = False
+
+    def __repr__(self):
+        return type(self).__name__ + "()"
+
+    def __eq__(self, other):
+        return type(self) is type(other)
+
+    def __hash__(self):
+        return hash(type(self).__name__)
+
+
+class CGS(Orthonormalizer):
+    code, name, gs_family = _abi.QR_CGS, "CGS", True
+
+
+class MGS(Orthonormalizer):
+    code, name, gs_family = _abi.QR_MGS, "MGS", True
+
+
+class RGS(Orthonormalizer):
+    code, name, gs_family = _abi.QR_RGS, "RGS", True
+
+
+class HouseholderQR(Orthonormalizer):
+    code, name = _abi.QR_HOUSEHOLDER, "V-H"
+
+
+class AugmentedQR(Orthonormalizer):
+    code, name = _abi.QR_AUGMENTED, "V-A"
+
+
+class GivensQR(Orthonormalizer):
+    code, name = _abi.QR_GIVENS, "V-G"
+
+
+class Reducer:
+    kind: int
+    replaces = True
+
+    def to_cl(self) -> _abi.cl_reducer:
+        return _abi.cl_reducer(kind=self.kind)
+
+    def dtype(self, d: int, k: int) -> np.dtype:
+        raise NotImplementedError
+
+    def check(self, d: int, k: int) -> None:
+        """`reducer_init` argument checks (ArgumentError in the reference)."""
+
+    def failed(self, st) -> bool:
+        return int(st["code"]) != 0
+
+    def provenance(self) -> dict:
+        return {}
+
+    def __repr__(self):
+        return type(self).__name__ + "()"
+
+
+class QRSpectrum(Reducer):
+    """QRSpectrum(alg; orthogonality_tol=8.0), src/Lyapunov/qr_spectrum.jl:14-96."""
+    kind = _abi.RED_QR
+
+    def __init__(self, alg: Orthonormalizer, orthogonality_tol: float = 8.0):
+        self.alg, self.orthogonality_tol = alg, float(orthogonality_tol)
+
+    def __repr__(self):
+        return f"QRSpectrum({self.alg!r})"
+
+    def to_cl(self):
+        return _abi.cl_reducer(kind=self.kind, alg=self.alg.code, orthogonality_tol=self.orthogonality_tol)
+
+    def dtype(self, d, k):   # QRState{Float64,K}, qr_spectrum.jl:22-33
+        return np.dtype([("sums", "<f8", (k, 2)), ("n", "<i8"), ("G_max", "<f8"), ("orth_max", "<f8"),
+                         ("count_max", "<i8"), ("code", "i1"), ("_p0", "V7"), ("column", "<i8"),
+                         ("value", "<f8"), ("threshold", "<f8"), ("step", "<i8")])
+
+    def final(self, st):   # qr_spectrum.jl:85-91
+        k = st["sums"].shape[0]
+        n = int(st["n"])
+        s = st["sums"][:, 0].astype(np.float64)
+        c = st["sums"][:, 1].astype(np.float64)
+        lam = np.array([0.0 if n == 0 else _tot(s[i], c[i]) / n for i in range(k)])
+        return dict(n=n, sum=s.copy(), comp=c.copy(), **{"lambda": lam}, G_max=float(st["G_max"]),
+                    orth_max=float(st["orth_max"]), count_max=int(st["count_max"]))
+
+    def error(self, st, orbit, backend):   # qr_spectrum.jl:80-83
+        kind = "orthogonality" if int(st["code"]) == 4 else "orthonormalisation breakdown"
+        return NumericalHealthError(kind, float(st["value"]), float(st["threshold"]), int(st["step"]), orbit,
+                                    backend, int(st["column"]))
+
+    def provenance(self):
+        return dict(estimator="qr", orthonormalizer=self.alg.name, orthogonality_tol=self.orthogonality_tol)
+
+
+class Benettin(Reducer):
+    """Benettin(), src/Lyapunov/benettin.jl:11-53 (k = 1)."""
+    kind = _abi.RED_BENETTIN
+
+    def check(self, d, k):
+        if k != 1:
+            raise ValueError(f"Benettin needs k = 1, got k = {k}")
+
+    def dtype(self, d, k):
+        return np.dtype(_cs("sum") + [("n", "<i8"), ("code", "i1"), ("_p0", "V7"), ("value", "<f8"),
+                                      ("step", "<i8")])
+
+    def final(self, st):
+        n = int(st["n"])
+        lam = 0.0 if n == 0 else _tot(st["sum_s"], st["sum_c"]) / n
+        return dict(n=n, sum=np.array([st["sum_s"]]), comp=np.array([st["sum_c"]]), **{"lambda": np.array([lam])})
+
+    def error(self, st, orbit, backend):
+        v = float(st["value"])
+        return NumericalHealthError("deviation matrix", v, 0.0 if math.isfinite(v) else math.inf, int(st["step"]),
+                                    orbit, backend, 1)
+
+    def provenance(self):
+        return dict(estimator="benettin")
+
+
+class SALI(Reducer):
+    """SALI(), src/Indicators/sali.jl:14-68 (k = 2)."""
+    kind = _abi.RED_SALI
+
+    def check(self, d, k):
+        if k != 2:
+            raise ValueError(f"SALI needs k = 2, got k = {k}")
+
+    def dtype(self, d, k):
+        return np.dtype(_cs("s1") + _cs("s2") + [("sali", "<f8"), ("value", "<f8"), ("n", "<i8"), ("step", "<i8"),
+                                                 ("code", "i1"), ("column", "i1"), ("_p0", "V6")])
+
+    def final(self, st):   # sali.jl:55-59
+        s = np.array([st["s1_s"], st["s2_s"]], dtype=np.float64)
+        c = np.array([st["s1_c"], st["s2_c"]], dtype=np.float64)
+        n = int(st["n"])
+        L = 0.0 if n == 0 else -((s[0] + s[1]) + (c[0] + c[1]))
+        return dict(n=n, sali=float(st["sali"]), L=float(L), sum=s, comp=c, floor=4 * EPS)
+
+    def error(self, st, orbit, backend):
+        v = float(st["value"])
+        return NumericalHealthError("deviation matrix", v, 0.0 if math.isfinite(v) else math.inf, int(st["step"]),
+                                    orbit, backend, int(st["column"]))
+
+    def provenance(self):
+        return dict(indicator="sali")
+
+
+class GALI(Reducer):
+    """GALI(), src/Indicators/gali.jl:17-201 (2 <= k <= d)."""
+    kind = _abi.RED_GALI
+
+    def check(self, d, k):
+        if not 2 <= k <= d:
+            raise ValueError("GALI needs 2 <= k <= d")
+
+    def dtype(self, d, k):   # GALIState{Float64, D, K, K-1}
+        return np.dtype([("s", "<f8", (k,)), ("c", "<f8", (k,)), ("gali", "<f8", (k - 1,)), ("value", "<f8"),
+                         ("n", "<i8"), ("step", "<i8"), ("code", "i1"), ("_p0", "V7"), ("column", "<i8")])
+
+    def final(self, st, d=None):   # gali.jl:319-332
+        k = st["s"].shape[0]
+        n = int(st["n"])
+        L = None
+        if d is not None and k == d:
+            if n == 0:
+                L = 0.0
+            else:
+                s, c = np.float64(st["s"][0]), np.float64(st["c"][0])
+                for i in range(1, k):
+                    s = s + np.float64(st["s"][i])
+                    c = c + np.float64(st["c"][i])
+                L = float(-(s + c))
+        floors = np.array([2 * (i + 1) * EPS for i in range(1, k)])
+        return dict(n=n, gali=st["gali"].astype(np.float64).copy(), L=L, sum=st["s"].astype(np.float64).copy(),
+                    comp=st["c"].astype(np.float64).copy(), floor=floors)
+
+    def error(self, st, orbit, backend):
+        v = float(st["value"])
+        thr = math.inf if not math.isfinite(v) else (0.0 if v == 0 else float(np.finfo(np.float64).tiny))
+        return NumericalHealthError("deviation matrix", v, thr, int(st["step"]), orbit, backend, int(st["column"]))
+
+    def provenance(self):
+        return dict(indicator="gali")
+
+
+_MEGNO_SUMS = ["s", "R1", "R2", "Q", "Q2"]
+
+
+class MEGNO(Reducer):
+    """MEGNO(; replace=True), src/Indicators/megno.jl:29-113 (k = 2)."""
+    kind = _abi.RED_MEGNO
+
+    def __init__(self, replace: bool = True):
+        self.replace = bool(replace)
+        self.replaces = self.replace
+
+    def __repr__(self):
+        return f"MEGNO(replace={self.replace})"
+
+    def to_cl(self):
+        return _abi.cl_reducer(kind=self.kind, replace=int(self.replace))
+
+    def check(self, d, k):
+        if k != 2:
+            raise ValueError(f"MEGNO needs k = 2, got k = {k}")
+
+    def dtype(self, d, k):
+        f = []
+        for col in ("c1", "c2"):
+            for nm in _MEGNO_SUMS:
+                f += _cs(f"{col}_{nm}")
+        return np.dtype(f + [("value", "<f8"), ("n", "<i8"), ("K", "<i8"), ("step", "<i8"), ("code", "i1"),
+                             ("column", "i1"), ("_p0", "V6")])
+
+    @staticmethod
+    def series(st, col, n, K):   # megno.jl:97-102
+        if K == 0:
+            return 0.0, 0.0, 0.0
+        f = np.float64
+        tn = f(n)
+        R1 = f(st[f"{col}_R1_s"]) + f(st[f"{col}_R1_c"])
+        Q = f(st[f"{col}_Q_s"]) + f(st[f"{col}_Q_c"])
+        Q2 = f(st[f"{col}_Q2_s"]) + f(st[f"{col}_Q2_c"])
+        return float(2 * R1 / tn), float(Q / f(K)), float(f(n // K) * Q2 / (tn * tn * tn))
+
+    def final(self, st):   # megno.jl:104-111
+        n, K = int(st["n"]), int(st["K"])
+        y1, b1, e1 = self.series(st, "c1", n, K)
+        y2, b2, e2 = self.series(st, "c2", n, K)
+        pair = lambda nm, comp: np.array([st[f"c1_{nm}_{comp}"], st[f"c2_{nm}_{comp}"]], dtype=np.float64)  # noqa
+        tot = lambda nm: np.array([_tot(st[f"c1_{nm}_s"], st[f"c1_{nm}_c"]), _tot(st[f"c2_{nm}_s"], st[f"c2_{nm}_c"])])  # noqa
+        return dict(n=n, handoffs=K, Y=np.array([y1, y2]), Ybar=np.array([b1, b2]), Ybar20=np.array([e1, e2]),
+                    sum=pair("s", "s"), comp=pair("s", "c"), R1=tot("R1"), R2=tot("R2"), Q=tot("Q"), Q2=tot("Q2"))
+
+    def error(self, st, orbit, backend):
+        v = float(st["value"])
+        return NumericalHealthError("deviation matrix", v, 0.0 if math.isfinite(v) else math.inf, int(st["step"]),
+                                    orbit, backend, int(st["column"]))
+
+    def provenance(self):
+        return dict(indicator="megno", convention="weights at the end of the window, mean over the handoffs 1..K")
+
+
+class FLI(Reducer):
+    """FLI(; replace=True), src/Indicators/fli.jl:26-96 (k = 2)."""
+    kind = _abi.RED_FLI
+
+    def __init__(self, replace: bool = True):
+        self.replace = bool(replace)
+        self.replaces = self.replace
+
+    def __repr__(self):
+        return f"FLI(replace={self.replace})"
+
+    def to_cl(self):
+        return _abi.cl_reducer(kind=self.kind, replace=int(self.replace))
+
+    def check(self, d, k):
+        if k != 2:
+            raise ValueError(f"FLI needs k = 2, got k = {k}")
+
+    def dtype(self, d, k):
+        return np.dtype(_cs("s1") + _cs("s2") + [("f1", "<f8"), ("fB", "<f8"), ("value", "<f8"), ("n", "<i8"),
+                                                 ("step", "<i8"), ("step1", "<i8"), ("stepB", "<i8"), ("code", "i1"),
+                                                 ("column", "i1"), ("colB", "i1"), ("_p0", "V5")])
+
+    def final(self, st):   # fli.jl:224-227
+        return dict(n=int(st["n"]), fli=float(st["fB"]), fli1=float(st["f1"]),
+                    sum=np.array([st["s1_s"], st["s2_s"]], dtype=np.float64),
+                    comp=np.array([st["s1_c"], st["s2_c"]], dtype=np.float64),
+                    stepB=int(st["stepB"]), colB=int(st["colB"]), step1=int(st["step1"]))
+
+    def error(self, st, orbit, backend):
+        v = float(st["value"])
+        return NumericalHealthError("deviation matrix", v, 0.0 if math.isfinite(v) else math.inf, int(st["step"]),
+                                    orbit, backend, int(st["column"]))
+
+    def provenance(self):
+        return dict(indicator="fli")
+
+
+def chain_dtype(reducers, d: int, k: int) -> np.dtype:
+    """The isbits layout of the Julia tuple of the chain's states (each field 8-byte aligned, sizes multiples of 8)."""
+    fields, off = [], 0
+    names, formats, offsets = [], [], []
+    for i, r in enumerate(reducers):
+        dt = r.dtype(d, k)
+        assert dt.itemsize == _abi.state_bytes(r.kind, k), (r, dt.itemsize)
+        names.append(f"r{i}")
+        formats.append(dt)
+        offsets.append(off)
+        off += dt.itemsize
+    del fields
+    if not reducers:
+        return np.dtype([])
+    return np.dtype({"names": names, "formats": formats, "offsets": offsets, "itemsize": off})

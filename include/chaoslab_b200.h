@@ -1,0 +1,222 @@
+/*
+ * chaoslab_b200.h -- C ABI of libchaoslab_b200, the B200 (sm_100a) engine for Chaoslab's ensemble hot path
+ * `propagate(sys, x0s, N; k, tau, seed, reducers)`.
+ *
+ * The reference reaches its device through Julia hooks, not a C ABI: `Tangent._run_chunk!` launches the
+ * KernelAbstractions kernel `_orbit_kernel!` (src/Tangent/propagate.jl:32-50, launch at :105, synchronize :106),
+ * and ext/ChaoslabCUDAExt.jl:16-93 fills the device hooks of src/Foundation/Foundation.jl:84-104. A Julia
+ * package extension binds the entry points below with `ccall` in place of that launch (the binding is shown in
+ * INTEGRATION.md). The ABI carries only plain pointers, sizes and POD structs.
+ *
+ * Layouts (all host buffers are owned by the caller; no pointer is kept after a call returns):
+ *  - x0, x   : n_orbits x s doubles, orbit-major (Julia `Vector{SVector{s,Float64}}`).
+ *  - W0, W   : n_orbits x (d*k) doubles per frame, each matrix column-major (Julia `Vector{SMatrix{d,k,Float64}}`).
+ *  - states  : n_orbits x cl_b200_state_bytes(run, f) bytes per frame, the isbits layout of the Julia tuple of
+ *              reducer states (QRState, BenettinState, SALIState, GALIState, MEGNOState, FLIState with T = Float64),
+ *              so `reducer_final` / `reducer_error` run unchanged on the host.
+ *  - code    : n_orbits int8 per frame (STATUS_OK 0, STATE 1, W 2, REDUCER 3; src/Tangent/orbit.jl:1).
+ *  - hstep   : n_orbits int64 per frame, the global step of the failing handoff, else the last step reached.
+ *
+ * Frames: one call integrates each orbit once and carries up to CL_MAX_FRAMES tangent frames along it, each with
+ * its own k and reducer chain. A frame behaves as a separate reference `propagate` run on the same orbit and W0
+ * (its own status, failing step, W and states); the orbit stops only when every frame has stopped. One frame is
+ * exactly the reference call.
+ *
+ * Return codes: 0 success; negative values map one to one onto the reference's FALLBACK_REASONS indices
+ * (src/Foundation/Foundation.jl:71-75): -2 no functional device (reason 2), -3 kernel not built for this system /
+ * chain / precision (reason 3), -4 device out of memory (reason 4), -9 device lost or a bounded device wait
+ * timed out (reason 9); -1 is an invalid argument (the reference throws ArgumentError before any work).
+ * Per-orbit numerical failures are not call errors: they come back in code / hstep / states.
+ */
+#ifndef CHAOSLAB_B200_H
+#define CHAOSLAB_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#define CL_API __attribute__((visibility("default")))
+#else
+#define CL_API
+#endif
+
+#define CL_B200_ABI_VERSION 1
+#define CL_MAX_FRAMES 3
+#define CL_MAX_REDUCERS 4
+#define CL_MAX_DIM 16
+#define CL_MAX_K 8
+
+/* Systems (src/Systems): the fixed menu the compiled kernels cover. */
+enum cl_system_kind {
+    CL_SYS_STANDARD = 1,         /* StandardMap(K), d = s = 2                       standard_map.jl:8-44        */
+    CL_SYS_WRAPPED_STANDARD = 2, /* WrappedStandardMap(K), d = 2, s = 4              wrapped_standard_map.jl:12-57 */
+    CL_SYS_FROESCHLE = 3,        /* FroeschleMap(nu, kappa, mu), d = s = 4           froeschle_map.jl:9-58       */
+    CL_SYS_CHAIN = 4,            /* StandardMapChain(N, K, eps), d = s = 2N          standard_map_chain.jl:11-31 */
+    CL_SYS_LINEAR = 5,           /* LinearSymplecticMap(A), d = s                    linear_symplectic.jl:1-40   */
+    CL_SYS_HH_GAUSS = 6          /* IntegratorMap(Gauss(Float64, 3; tol), HenonHeilesFlow(), dt), d = s = 4
+                                    integrator_map.jl:12-23, gauss.jl:49-192, flow_models.jl:101-103        */
+};
+
+/* Reducers (src/Lyapunov, src/Indicators). */
+enum cl_reducer_kind {
+    CL_RED_QR = 1,       /* QRSpectrum(alg; orthogonality_tol)   qr_spectrum.jl:14-96 */
+    CL_RED_BENETTIN = 2, /* Benettin()                          benettin.jl:11-53    */
+    CL_RED_SALI = 3,     /* SALI()                              sali.jl:14-68        */
+    CL_RED_GALI = 4,     /* GALI()                              gali.jl:17-201       */
+    CL_RED_MEGNO = 5,    /* MEGNO(; replace)                    megno.jl:29-113      */
+    CL_RED_FLI = 6       /* FLI(; replace)                      fli.jl:26-96         */
+};
+
+/* Orthonormalizers of QRSpectrum (orthonormalize.jl:5-12, householder.jl:5-10). */
+enum cl_qr_alg {
+    CL_QR_CGS = 1,
+    CL_QR_MGS = 2,
+    CL_QR_RGS = 3,
+    CL_QR_HOUSEHOLDER = 4,
+    CL_QR_AUGMENTED = 5,
+    CL_QR_GIVENS = 6
+};
+
+/* Arithmetic of the tangent frames. The orbit, the Gauss-Legendre solve and the log sums are Float64 in both. */
+enum cl_precision {
+    CL_PREC_FP64 = 0, /* plain kernel: the reference's Float64 algorithm, operation for operation           */
+    CL_PREC_MIXED = 1 /* tangent frames and their QR / norms in Float32, log sums Float64 (Neumaier)         */
+};
+
+enum cl_status {
+    CL_OK = 0,
+    CL_EINVAL = -1,
+    CL_ENODEVICE = -2,
+    CL_EUNSUPPORTED = -3,
+    CL_ENOMEM = -4,
+    CL_EDEVICE_LOST = -9
+};
+
+typedef struct cl_system {
+    int32_t kind;          /* enum cl_system_kind                                                       */
+    int32_t n_sites;       /* CL_SYS_CHAIN: N in 2..8                                                   */
+    int32_t ring;          /* CL_SYS_CHAIN: 1 for boundary = :ring (N >= 3), 0 for :open                */
+    int32_t gauss_maxiter; /* CL_SYS_HH_GAUSS: fixed-point iteration cap (reference default 50)         */
+    double K;              /* standard maps and chain                                                   */
+    double eps;            /* chain coupling                                                            */
+    double nu, kappa, mu;  /* Froeschle parameters                                                      */
+    double gauss_tol;      /* absolute stage tolerance; NaN = the reference's 8 eps max(1, |Y|) bound   */
+    double dt;             /* IntegratorMap step tau of the flow                                        */
+    double A[CL_MAX_DIM * CL_MAX_DIM]; /* CL_SYS_LINEAR: d x d matrix, column-major                     */
+} cl_system;
+
+typedef struct cl_reducer {
+    int32_t kind;             /* enum cl_reducer_kind                                   */
+    int32_t alg;              /* CL_RED_QR: enum cl_qr_alg                              */
+    int32_t replace;          /* CL_RED_MEGNO / CL_RED_FLI: the `replace` keyword (0/1) */
+    int32_t pad;
+    double orthogonality_tol; /* CL_RED_QR: reference default 8.0                       */
+} cl_reducer;
+
+typedef struct cl_frame {
+    int32_t k;          /* deviation vectors, 1 <= k <= d */
+    int32_t n_reducers; /* 0..CL_MAX_REDUCERS             */
+    cl_reducer reducers[CL_MAX_REDUCERS];
+} cl_frame;
+
+typedef struct cl_run {
+    int32_t abi_version; /* CL_B200_ABI_VERSION                                                          */
+    int32_t d;           /* dimension(sys)                                                               */
+    int32_t s;           /* state length (>= d; 4 for the wrapped standard map's winding counts)         */
+    int32_t tau;         /* handoff interval                                                             */
+    int64_t N;           /* steps of the whole run, a positive multiple of tau                           */
+    int64_t n0;          /* first global step of this launch: 0 starts fresh, > 0 continues carried state */
+    int64_t steps;       /* steps in this launch (a multiple of tau); 0 means N - n0                     */
+    int32_t n_frames;    /* 1..CL_MAX_FRAMES                                                             */
+    int32_t precision;   /* enum cl_precision                                                            */
+    uint64_t seed;       /* seed of the Haar frames drawn when a frame's W0 is NULL                      */
+    int64_t orbit_base;  /* id of orbit 0 of this call minus one (orbit ids are 1-based, as in Julia)    */
+    cl_system sys;
+    cl_frame frames[CL_MAX_FRAMES];
+} cl_run;
+
+/* Buffers of one call. For n0 == 0, x0 / W0 are read and x / W / states / code / hstep written; W0[f] may be
+ * NULL (seeded Haar frame). For n0 > 0, x / W / states / code are read as the carried state (x0, W0 unused), an
+ * orbit whose code is not 0 is not advanced, and everything is written back in place. */
+typedef struct cl_buffers {
+    const double* x0;
+    double* x;
+    const double* W0[CL_MAX_FRAMES];
+    double* W[CL_MAX_FRAMES];
+    void* states[CL_MAX_FRAMES];
+    int8_t* code[CL_MAX_FRAMES];
+    int64_t* hstep[CL_MAX_FRAMES];
+} cl_buffers;
+
+/* What a call ran, for the run's provenance (propagate.jl:260-264 records backend, device, launch_steps,
+ * launches_per_chunk; these are the device-side counterparts). */
+typedef struct cl_prov {
+    char device[96];      /* device name                                    */
+    char variant[160];    /* compiled kernel instance that ran              */
+    int64_t launch_steps; /* steps per launch                               */
+    int64_t launches;     /* kernel launches of the orbit kernel            */
+    double gpu_ms;        /* device time of the orbit kernel launches       */
+    int32_t block;        /* threads per block                              */
+    int32_t grid;         /* blocks per launch                              */
+    int32_t regs;         /* registers per thread of the instance           */
+    int32_t orbits_per_block;
+} cl_prov;
+
+/* Backend probe: the (loadable, functional, device, compiles, gpu_faster) record of Foundation.probe
+ * (src/Foundation/Foundation.jl:92-93, ext/ChaoslabCUDAExt.jl:87-91). */
+typedef struct cl_probe {
+    int32_t loadable;
+    int32_t functional;
+    int32_t compiles;
+    int32_t sm;          /* compute capability x 10, e.g. 100 */
+    int64_t free_bytes;  /* Foundation.free_memory             */
+    int64_t total_bytes;
+    int32_t sm_count;
+    int32_t pad;
+    char device[96];
+} cl_probe;
+
+/* propagate one chunk, host buffers: copies in, runs the orbit kernel in launches of at most run->steps steps,
+ * copies out. Replaces `_run_chunk!` (src/Tangent/propagate.jl:92-119) for a device chunk. */
+CL_API int cl_b200_propagate(const cl_run* run, int64_t n_orbits, const cl_buffers* host, cl_prov* prov);
+
+/* The same on device buffers already resident in GPU memory, enqueued on `stream` (a cudaStream_t; NULL is the
+ * legacy default stream). `soa` = 1 takes x / W as structure-of-arrays (component-major: element c of orbit i at
+ * c * n_orbits + i) for coalesced loads; 0 takes the orbit-major host layout. States and code / hstep are always
+ * orbit-major. Returns after the launch is enqueued. */
+CL_API int cl_b200_propagate_device(const cl_run* run, int64_t n_orbits, const cl_buffers* dev, int32_t soa, void* stream);
+
+/* 0 when a compiled kernel instance covers `run`, else CL_EINVAL (ill-formed run, message in cl_b200_last_error)
+ * or CL_EUNSUPPORTED (well-formed, but not in the compiled menu: the caller falls back with reason 3). */
+CL_API int cl_b200_check(const cl_run* run);
+
+/* Bytes per orbit of frame f's reducer-state tuple in the Julia isbits layout (0 for an empty chain). */
+CL_API int64_t cl_b200_state_bytes(const cl_run* run, int32_t frame);
+
+/* Fill `out`; returns 0 when a B200-class device is functional. */
+CL_API int cl_b200_probe(cl_probe* out);
+
+/* Copy the message of the last failed call on this thread; returns its length. */
+CL_API int cl_b200_last_error(char* buf, size_t len);
+
+/* Library version string. */
+CL_API const char* cl_b200_version(void);
+
+/* Number of orbit-kernel launches since the library was loaded (a device-launch counter for audits). */
+CL_API int64_t cl_b200_launch_count(void);
+
+/* The compiled menu: number of kernel instances, and the key of instance i (NULL outside 0..size-1). A key reads
+ * "s<system kind>d<d>p<precision>|k<k>:<reducer>,...|..." with reducers QR<alg>, BEN, SALI, GALI, MEGNO<replace>,
+ * FLI<replace>, one "|"-terminated group per frame. No reference counterpart (Julia compiles on demand). */
+CL_API int32_t cl_b200_menu_size(void);
+CL_API const char* cl_b200_menu_key(int32_t i);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CHAOSLAB_B200_H */

@@ -1,0 +1,149 @@
+"""TEST INFRASTRUCTURE: Python binding of the CPU oracle (liboracle.so). Only tests/, __graft_entry__.smoke() and
+the cpu_baseline / reference legs of bench.py import this module; the product never does.
+
+`oracle_frames` runs the serial restatement of the reference's per-orbit body on the same cl_run the B200 library
+takes and returns the same records (x, W, states, code, hstep per frame).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+from chaos_b200 import _abi
+from chaos_b200.propagate import FrameSpec, build_run
+from chaos_b200.reducers import chain_dtype
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "liboracle.so")
+MATH = {"portable": 0, "libm": 1}
+_lib = None
+
+
+def build() -> str:
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+    return LIB_PATH
+
+
+def lib() -> C.CDLL:
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            build()
+        L = C.CDLL(LIB_PATH)
+        P = C.POINTER
+        dp = P(C.c_double)
+        L.oracle_propagate.argtypes = [P(_abi.cl_run), C.c_int64, P(_abi.cl_buffers), C.c_int32, C.c_int32]
+        L.oracle_propagate.restype = C.c_int
+        L.oracle_sincos.argtypes = [C.c_int32, dp, dp, dp, C.c_int64]
+        L.oracle_log.argtypes = [C.c_int32, dp, dp, C.c_int64]
+        L.oracle_fused_product.argtypes = [dp, dp, dp, C.c_int32, C.c_int32, C.c_int32]
+        L.oracle_safe_norm.argtypes = [dp, C.c_int32]
+        L.oracle_safe_norm.restype = C.c_double
+        ip = P(C.c_int32)
+        L.oracle_orthonormalize.argtypes = [C.c_int32, dp, C.c_int32, C.c_int32, dp, dp, ip, ip, ip]
+        L.oracle_window_Gw.argtypes = [dp, C.c_int32]
+        L.oracle_window_Gw.restype = C.c_double
+        L.oracle_orth_loss.argtypes = [dp, C.c_int32, C.c_int32]
+        L.oracle_orth_loss.restype = C.c_double
+        L.oracle_seeded_frame.argtypes = [C.c_uint64, C.c_int64, C.c_int32, C.c_int32, dp]
+        L.oracle_gauss3_step.argtypes = [dp, C.c_double, C.c_int32, C.c_double, dp]
+        L.oracle_max_threads.restype = C.c_int32
+        _lib = L
+    return _lib
+
+
+def _dp(a):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def sincos(x, math="portable"):
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    s, c = np.empty_like(x), np.empty_like(x)
+    lib().oracle_sincos(MATH[math], _dp(x), _dp(s), _dp(c), x.size)
+    return s, c
+
+
+def log(x, math="portable"):
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    y = np.empty_like(x)
+    lib().oracle_log(MATH[math], _dp(x), _dp(y), x.size)
+    return y
+
+
+def fused_product(A, B):
+    A = np.asfortranarray(A, dtype=np.float64)
+    B = np.asfortranarray(B, dtype=np.float64)
+    m, p = A.shape
+    n = B.shape[1]
+    Cm = np.zeros((m, n), order="F")
+    lib().oracle_fused_product(_dp(A), _dp(B), _dp(Cm), m, p, n)
+    return Cm
+
+
+def orthonormalize(alg: int, W):
+    W = np.asfortranarray(W, dtype=np.float64)
+    d, k = W.shape
+    Q, R = np.zeros((d, k), order="F"), np.zeros((k, k), order="F")
+    cnt, st, col = C.c_int32(), C.c_int32(), C.c_int32()
+    lib().oracle_orthonormalize(alg, _dp(W), d, k, _dp(Q), _dp(R), C.byref(cnt), C.byref(st), C.byref(col))
+    return Q, R, cnt.value, st.value, col.value
+
+
+def window_Gw(R):
+    R = np.asfortranarray(R, dtype=np.float64)
+    return lib().oracle_window_Gw(_dp(R), R.shape[0])
+
+
+def seeded_frame(seed, orbit, d, k):
+    W = np.zeros((d, k), order="F")
+    lib().oracle_seeded_frame(seed % (1 << 64), orbit, d, k, _dp(W))
+    return W
+
+
+def gauss3_step(z, h, maxiter=50, tol=float("nan")):
+    z = np.ascontiguousarray(z, dtype=np.float64).copy()
+    T = np.zeros((4, 4), order="F")
+    lib().oracle_gauss3_step(_dp(z), h, maxiter, tol, _dp(T))
+    return z, T
+
+
+def oracle_frames(sys, x0, N, frames: list[FrameSpec], *, tau=1, seed=0, math="portable", threads=0,
+                  launch_steps=None, orbit_base=0):
+    """Run the oracle; returns a list (per frame) of dicts x (n, s), W (n, d, k), states, code, hstep."""
+    x0 = np.ascontiguousarray(np.asarray(x0, dtype=np.float64))
+    n, s = x0.shape
+    d = sys.d
+    run = build_run(sys, N, tau, frames, "fp64", seed, orbit_base=orbit_base)
+    x = np.empty((n, s))
+    W0s, Ws, sts, codes, hs = [], [], [], [], []
+    for fr in frames:
+        W0s.append(None if fr.W0 is None else np.ascontiguousarray(np.asarray(fr.W0, dtype=np.float64).transpose(0, 2, 1)))
+        Ws.append(np.empty((n, fr.k, d)))
+        dt = chain_dtype(tuple(fr.reducers), d, fr.k)
+        sts.append(np.zeros(n, dtype=dt) if dt.itemsize else None)
+        codes.append(np.zeros(n, dtype=np.int8))
+        hs.append(np.zeros(n, dtype=np.int64))
+    total = int(N)
+    L = int(launch_steps) if launch_steps else total
+    done = 0
+    while done < total:
+        run.n0 = done
+        run.steps = min(L, total - done)
+        b = _abi.cl_buffers()
+        b.x0 = x0.ctypes.data
+        b.x = x.ctypes.data
+        for f in range(len(frames)):
+            b.W0[f] = None if W0s[f] is None else W0s[f].ctypes.data
+            b.W[f] = Ws[f].ctypes.data
+            b.states[f] = None if sts[f] is None else sts[f].ctypes.data
+            b.code[f] = codes[f].ctypes.data
+            b.hstep[f] = hs[f].ctypes.data
+        rc = lib().oracle_propagate(C.byref(run), n, C.byref(b), MATH[math], threads)
+        if rc != 0:
+            raise ValueError(f"oracle_propagate returned {rc}")
+        done += run.steps
+    return [dict(x=x, W=Ws[f].transpose(0, 2, 1), states=sts[f], code=codes[f], hstep=hs[f])
+            for f in range(len(frames))]

@@ -1,0 +1,218 @@
+// oracle/oracle_capi.cpp -- TEST INFRASTRUCTURE (the CPU oracle). Only tests/, __graft_entry__.smoke() and the
+// cpu_baseline / reference legs of bench.py load liboracle.so; the product never does.
+//
+// C entry points of the oracle. `oracle_propagate` is the serial per-orbit body of the reference
+// (`_orbit_body`, src/Tangent/orbit.jl:44-60, driven as `_orbit_kernel!` drives it, src/Tangent/propagate.jl:32-50,
+// including the carried-state relaunch n0 > 0), run over orbits on a pool of std::threads that take chunks of orbits from an atomic counter; orbits are independent, so the result
+// does not depend on the thread count (propagate.jl:272-273). It takes the same cl_run / cl_buffers as
+// libchaoslab_b200 (orbit-major host layout only).
+#include <algorithm>
+#include <atomic>
+#include <thread>
+#include <cstdio>
+#include <cstring>
+#include <vector>
+
+#include "oracle.hpp"
+
+using namespace orc;
+
+namespace {
+
+constexpr int8_t STATUS_OK = 0, STATUS_STATE = 1, STATUS_W = 2, STATUS_REDUCER = 3;   // orbit.jl:1
+
+int64_t frame_state_bytes(const cl_frame& f) {
+    int64_t b = 0;
+    for (int r = 0; r < f.n_reducers; ++r) b += state_bytes_of(f.reducers[r], f.k);
+    return b;
+}
+
+// _status, orbit.jl:3: all(isfinite, x) ? (all(isfinite, W) ? OK : W) : STATE
+int8_t status_of(const double* x, int s, const double* W, int dk) {
+    for (int i = 0; i < s; ++i) if (!isfin(x[i])) return STATUS_STATE;
+    for (int i = 0; i < dk; ++i) if (!isfin(W[i])) return STATUS_W;
+    return STATUS_OK;
+}
+
+template <int MM>
+void run_orbit(const cl_run& run, int64_t i, const cl_buffers& b) {
+    const int d = run.d, s = run.s, nf = run.n_frames;
+    const int64_t n0 = run.n0;
+    const int64_t steps = run.steps > 0 ? run.steps : run.N - n0;
+    double x[CL_MAX_DIM];
+    double W[CL_MAX_FRAMES][CL_MAX_DIM * CL_MAX_K];
+    std::vector<uint8_t> st[CL_MAX_FRAMES];
+    bool alive[CL_MAX_FRAMES];
+    int8_t code[CL_MAX_FRAMES];
+    int64_t hstep[CL_MAX_FRAMES];
+    const double* xin = (n0 == 0 && b.x0) ? b.x0 : b.x;
+    std::memcpy(x, xin + i * s, sizeof(double) * s);
+    bool any = false;
+    for (int f = 0; f < nf; ++f) {
+        const int k = run.frames[f].k;
+        const int64_t sb = frame_state_bytes(run.frames[f]);
+        st[f].assign(static_cast<size_t>(sb), 0);
+        if (n0 == 0) {
+            if (b.W0[f]) std::memcpy(W[f], b.W0[f] + i * d * k, sizeof(double) * d * k);
+            else seeded_frame<MM>(run.seed, run.orbit_base + i + 1, d, k, W[f]);
+            code[f] = STATUS_OK;
+            alive[f] = true;
+        } else {
+            std::memcpy(W[f], b.W[f] + i * d * k, sizeof(double) * d * k);
+            if (sb) std::memcpy(st[f].data(), static_cast<const uint8_t*>(b.states[f]) + i * sb, sb);
+            code[f] = b.code[f][i];
+            hstep[f] = b.hstep[f] ? b.hstep[f][i] : 0;
+            alive[f] = code[f] == STATUS_OK;   // a failed orbit keeps its status and step (propagate.jl:34)
+        }
+        any = any || alive[f];
+    }
+    if (!any) return;   // frozen: nothing is written
+
+    Systems<MM> sysf;
+    (void)sysf;
+    Chain<MM> chain{run.sys.n_sites, run.sys.K, run.sys.eps, run.sys.ring != 0};
+    Gauss3 gauss(run.sys.gauss_maxiter, run.sys.gauss_tol);
+    int64_t n = n0;
+    const int tau = run.tau;
+    const int64_t handoffs = steps / tau;
+    for (int64_t h = 0; h < handoffs; ++h) {
+        for (int t = 0; t < tau; ++t) {
+            if (run.sys.kind == CL_SYS_CHAIN) {
+                double g[CL_MAX_DIM / 2], gl[CL_MAX_DIM / 2], gr[CL_MAX_DIM / 2];
+                chain.band(x, g, gl, gr);
+                for (int f = 0; f < nf; ++f) if (alive[f]) chain.apply(g, gl, gr, W[f], run.frames[f].k);
+                chain.forward(x);
+            } else {
+                double M[CL_MAX_DIM * CL_MAX_DIM];
+                switch (run.sys.kind) {
+                    case CL_SYS_STANDARD: Systems<MM>::standard(run.sys.K, x, M); break;
+                    case CL_SYS_WRAPPED_STANDARD: Systems<MM>::wrapped(run.sys.K, x, M); break;
+                    case CL_SYS_FROESCHLE: Systems<MM>::froeschle(run.sys.nu, run.sys.kappa, run.sys.mu, x, M); break;
+                    case CL_SYS_LINEAR: Systems<MM>::linear(run.sys.A, d, x, M); break;
+                    case CL_SYS_HH_GAUSS: gauss.step(x, run.sys.dt, M); break;
+                }
+                for (int f = 0; f < nf; ++f) {
+                    if (!alive[f]) continue;
+                    double Wn[CL_MAX_DIM * CL_MAX_K];
+                    fused_product(M, W[f], Wn, d, d, run.frames[f].k);
+                    std::memcpy(W[f], Wn, sizeof(double) * d * run.frames[f].k);
+                }
+            }
+        }
+        n += tau;
+        bool still = false;
+        for (int f = 0; f < nf; ++f) {
+            if (!alive[f]) continue;
+            const cl_frame& fr = run.frames[f];
+            const int8_t c = status_of(x, s, W[f], d * fr.k);
+            if (c != STATUS_OK) { code[f] = c; hstep[f] = n; alive[f] = false; continue; }
+            // _apply (orbit.jl:23-28): every reducer runs, each on the W the one before returned
+            uint8_t* p = st[f].data();
+            for (int r = 0; r < fr.n_reducers; ++r) {
+                Reducers<MM>::step(fr.reducers[r], p, n, W[f], d, fr.k);
+                p += state_bytes_of(fr.reducers[r], fr.k);
+            }
+            p = st[f].data();
+            bool failed = false;
+            for (int r = 0; r < fr.n_reducers; ++r) {
+                failed = failed || Reducers<MM>::failed(fr.reducers[r], p, fr.k);
+                p += state_bytes_of(fr.reducers[r], fr.k);
+            }
+            if (failed) { code[f] = STATUS_REDUCER; hstep[f] = n; alive[f] = false; continue; }
+            still = true;
+        }
+        if (!still) break;
+    }
+    for (int f = 0; f < nf; ++f) {
+        if (alive[f]) {   // orbit.jl:58: the final status check runs only at step N
+            code[f] = n == run.N ? status_of(x, s, W[f], d * run.frames[f].k) : STATUS_OK;
+            hstep[f] = n;
+        }
+    }
+    std::memcpy(b.x + i * s, x, sizeof(double) * s);
+    for (int f = 0; f < nf; ++f) {
+        const int k = run.frames[f].k;
+        const int64_t sb = frame_state_bytes(run.frames[f]);
+        const bool frozen_before = n0 > 0 && b.code[f][i] != STATUS_OK;
+        if (frozen_before) continue;
+        std::memcpy(b.W[f] + i * d * k, W[f], sizeof(double) * d * k);
+        if (sb) std::memcpy(static_cast<uint8_t*>(b.states[f]) + i * sb, st[f].data(), sb);
+        b.code[f][i] = code[f];
+        if (b.hstep[f]) b.hstep[f][i] = hstep[f];
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+int64_t oracle_state_bytes(const cl_run* run, int32_t f) { return frame_state_bytes(run->frames[f]); }
+
+// Propagate n orbits on the CPU; math_mode 0 = portable functions, 1 = glibc; threads <= 0 = all.
+int oracle_propagate(const cl_run* run, int64_t n, const cl_buffers* b, int32_t math_mode, int32_t threads) {
+    if (run->N <= 0 || run->tau <= 0 || run->N % run->tau != 0) return CL_EINVAL;
+    const int64_t steps = run->steps > 0 ? run->steps : run->N - run->n0;
+    if (steps % run->tau != 0 || run->n0 + steps > run->N) return CL_EINVAL;
+    if (run->n_frames < 1 || run->n_frames > CL_MAX_FRAMES) return CL_EINVAL;
+    const int hw = static_cast<int>(std::max(1u, std::thread::hardware_concurrency()));
+    const int nt = static_cast<int>(std::min<int64_t>(threads > 0 ? threads : hw, std::max<int64_t>(n, 1)));
+    std::atomic<int64_t> next{0};
+    auto worker = [&]() {
+        for (;;) {
+            const int64_t lo = next.fetch_add(16);
+            if (lo >= n) return;
+            const int64_t hi = std::min<int64_t>(lo + 16, n);
+            for (int64_t i = lo; i < hi; ++i) {
+                if (math_mode == MATH_LIBM) run_orbit<MATH_LIBM>(*run, i, *b);
+                else run_orbit<MATH_PORTABLE>(*run, i, *b);
+            }
+        }
+    };
+    std::vector<std::thread> pool;
+    for (int t = 1; t < nt; ++t) pool.emplace_back(worker);
+    worker();
+    for (auto& th : pool) th.join();
+    return 0;
+}
+
+void oracle_sincos(int32_t mode, const double* x, double* s, double* c, int64_t n) {
+    for (int64_t i = 0; i < n; ++i) {
+        if (mode == MATH_LIBM) Math<MATH_LIBM>::sincos(x[i], s + i, c + i);
+        else p_sincos(x[i], s + i, c + i);
+    }
+}
+
+void oracle_log(int32_t mode, const double* x, double* y, int64_t n) {
+    for (int64_t i = 0; i < n; ++i) y[i] = mode == MATH_LIBM ? std::log(x[i]) : p_log(x[i]);
+}
+
+void oracle_fused_product(const double* A, const double* B, double* C, int32_t m, int32_t p, int32_t nn) {
+    fused_product(A, B, C, m, p, nn);
+}
+
+double oracle_safe_norm(const double* v, int32_t n) { return safe_norm(v, n); }
+
+int32_t oracle_orthonormalize(int32_t alg, const double* W, int32_t d, int32_t k, double* Q, double* R,
+                              int32_t* count, int32_t* status, int32_t* column) {
+    const QRResult r = orthonormalize(alg, W, d, k, Q, R);
+    *count = r.count; *status = r.status; *column = r.column;
+    return 0;
+}
+
+double oracle_window_Gw(const double* R, int32_t k) { return window_Gw(R, k); }
+double oracle_orth_loss(const double* Q, int32_t d, int32_t k) { return orth_loss(Q, d, k); }
+
+void oracle_seeded_frame(uint64_t seed, int64_t orbit, int32_t d, int32_t k, double* W) {
+    seeded_frame<MATH_PORTABLE>(seed, orbit, d, k, W);
+}
+
+// One Gauss-3 step of the Henon-Heiles flow: advances z (4) and writes the 4 x 4 tangent T.
+int32_t oracle_gauss3_step(double* z, double h, int32_t maxiter, double tol, double* T) {
+    Gauss3 g(maxiter, tol);
+    g.step(z, h, T);
+    return 0;
+}
+
+int32_t oracle_max_threads(void) { return static_cast<int32_t>(std::max(1u, std::thread::hardware_concurrency())); }
+
+}  // extern "C"

@@ -1,0 +1,147 @@
+"""Parity of the B200 FP64 kernels with the CPU oracle, bit for bit.
+
+The plain (FP64) kernels evaluate the reference's arithmetic operation for operation with the same portable
+sin / cos / log as the oracle's MATH_PORTABLE mode, so every record -- final point, frames, the reducer states in
+the Julia layout, status codes and failing steps -- must agree bitwise on the same inputs, chaotic orbits
+included. Each case runs the same seeded inputs through `chaos_b200.propagate_frames` (the C ABI on the GPU) and
+`oracle.oracle_frames` (serial C++ on the CPU).
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from chaos_b200 import (CGS, FLI, GALI, MEGNO, MGS, RGS, SALI, AugmentedQR, Benettin, FroeschleMap, GivensQR,
+                        HouseholderQR, LinearSymplecticMap, QRSpectrum, StandardMap, StandardMapChain,
+                        WrappedStandardMap, propagate_frames, torus_state)
+from chaos_b200.propagate import FrameSpec
+from helpers import haar_frames, identity_frames, same_bits, states_equal, uniform_starts
+
+pytestmark = pytest.mark.gpu
+
+QRS = [CGS(), MGS(), RGS(), HouseholderQR(), AugmentedQR(), GivensQR()]
+
+
+def _compare(sys, x0, N, frames, tau, oracle, launch_steps=None, seed=7):
+    dev = propagate_frames(sys, x0, N, frames, tau=tau, seed=seed, finals=False, throw=False,
+                           launch_steps=launch_steps)
+    ref = oracle.oracle_frames(sys, x0, N, frames, tau=tau, seed=seed, math="portable")
+    for f in range(len(frames)):
+        assert same_bits(dev[f].x, ref[f]["x"]), f"x differs (frame {f})"
+        assert np.array_equal(dev[f].code, ref[f]["code"]), f"code differs (frame {f})"
+        assert np.array_equal(dev[f].hstep, ref[f]["hstep"]), f"hstep differs (frame {f})"
+        assert same_bits(dev[f].W, ref[f]["W"]), f"W differs (frame {f})"
+        assert states_equal(dev[f].states, ref[f]["states"]), f"states differ (frame {f})"
+    return dev, ref
+
+
+def _chains_k2():
+    return [(QRSpectrum(a),) for a in QRS] + [(SALI(),), (GALI(),), (MEGNO(),), (FLI(),),
+                                              (MEGNO(replace=False), FLI(replace=False), QRSpectrum(GivensQR())),
+                                              (MEGNO(replace=False), SALI()), (FLI(replace=False), SALI()),
+                                              (MEGNO(replace=False), FLI(replace=False), SALI()), ()]
+
+
+@pytest.mark.parametrize("chain", [(Benettin(),)] + [(QRSpectrum(a),) for a in QRS], ids=repr)
+@pytest.mark.parametrize("wrapped", [False, True])
+def test_standard_k1(oracle, chain, wrapped):
+    n = 257
+    z = uniform_starts(n, 2, 11)
+    sys = WrappedStandardMap(6.0) if wrapped else StandardMap(6.0)
+    x0 = np.array([torus_state(v) for v in z]) if wrapped else z
+    W0 = haar_frames(n, 2, 1, 12)
+    _compare(sys, x0, 3000, [FrameSpec(1, chain, W0)], 1, oracle)
+
+
+@pytest.mark.parametrize("chain", _chains_k2(), ids=repr)
+@pytest.mark.parametrize("wrapped", [False, True])
+def test_standard_k2(oracle, chain, wrapped):
+    n = 300
+    z = uniform_starts(n, 2, 21)
+    sys = WrappedStandardMap(6.0) if wrapped else StandardMap(6.0)
+    x0 = np.array([torus_state(v) for v in z]) if wrapped else z
+    W0 = identity_frames(n, 2, 2)
+    _compare(sys, x0, 4000, [FrameSpec(2, chain, W0)], 1, oracle)
+
+
+@pytest.mark.parametrize("tau", [1, 5, 10])
+def test_standard_tau_and_relaunch(oracle, tau):
+    n = 200
+    x0 = uniform_starts(n, 2, 31)
+    fr = [FrameSpec(2, (QRSpectrum(MGS()),), haar_frames(n, 2, 2, 32))]
+    one, _ = _compare(StandardMap(1.5), x0, 2000, fr, tau, oracle)
+    # step-chunked relaunch carrying the state (propagate.jl:101-109) gives the same bits
+    many, _ = _compare(StandardMap(1.5), x0, 2000, fr, tau, oracle, launch_steps=10 * tau)
+    assert same_bits(one[0].W, many[0].W) and states_equal(one[0].states, many[0].states)
+
+
+@pytest.mark.parametrize("k,chain", [(1, (Benettin(),)), (1, (QRSpectrum(MGS()),))]
+                         + [(2, c) for c in _chains_k2()]
+                         + [(k, (QRSpectrum(a),)) for k in (3, 4) for a in QRS]
+                         + [(k, (GALI(),)) for k in (3, 4)] + [(4, (GALI(), SALI()))], ids=repr)
+def test_froeschle(oracle, k, chain):
+    n = 256
+    x0 = uniform_starts(n, 4, 41)
+    W0 = haar_frames(n, 4, k, 42)
+    _compare(FroeschleMap(1.5, 1.5, 0.05), x0, 2000, [FrameSpec(k, chain, W0)], 10, oracle)
+
+
+def test_froeschle_fused_frames(oracle):
+    """QRSpectrum(Householder) and GALI_4 + SALI carried along one orbit (the coupled-maps ensemble)."""
+    n = 512
+    x0 = uniform_starts(n, 4, 51)
+    W0 = identity_frames(n, 4, 4)
+    frames = [FrameSpec(4, (QRSpectrum(HouseholderQR()),), W0), FrameSpec(4, (GALI(), SALI()), W0)]
+    dev, _ = _compare(FroeschleMap(1.5, 1.5, 0.05), x0, 5000, frames, 10, oracle)
+    # each frame equals its own single-frame run (a separate reference call on the same orbit and W0)
+    for f in range(2):
+        single = propagate_frames(FroeschleMap(1.5, 1.5, 0.05), x0, 5000, [frames[f]], tau=10, finals=False,
+                                  throw=False)[0]
+        assert same_bits(single.W, dev[f].W) and states_equal(single.states, dev[f].states)
+
+
+@pytest.mark.parametrize("N_sites", range(2, 9))
+@pytest.mark.parametrize("ring", [False, True])
+def test_chain(oracle, N_sites, ring):
+    if ring and N_sites < 3:
+        pytest.skip("a ring needs N >= 3")
+    d = 2 * N_sites
+    n = 128
+    sys = StandardMapChain(N_sites, 1.2, 0.05, boundary="ring" if ring else "open")
+    x0 = uniform_starts(n, d, 60 + N_sites)
+    k = min(d, 8)
+    for chain in ((QRSpectrum(MGS()),), (QRSpectrum(HouseholderQR()),), (GALI(),)):
+        _compare(sys, x0, 500, [FrameSpec(k, chain, haar_frames(n, d, k, 70))], 5, oracle)
+    for chain in ((QRSpectrum(MGS()),), (SALI(),), (MEGNO(),)):
+        _compare(sys, x0, 500, [FrameSpec(2, chain, haar_frames(n, d, 2, 71))], 5, oracle)
+
+
+@pytest.mark.parametrize("k,chain", [(1, (Benettin(),)), (2, (QRSpectrum(MGS()),)), (2, (MEGNO(),)), (2, (SALI(),))],
+                         ids=repr)
+def test_linear(oracle, k, chain):
+    A = np.array([[2.0, 1.0], [1.0, 1.0]])
+    n = 64
+    x0 = uniform_starts(n, 2, 80, -1, 1)
+    _compare(LinearSymplecticMap(A), x0, 300, [FrameSpec(k, chain, haar_frames(n, 2, k, 81))], 1, oracle)
+
+
+def test_seeded_frames(oracle):
+    """W0 = nothing: the seeded Haar frames are drawn on the device, bit-identical to the oracle's stream."""
+    n = 300
+    x0 = uniform_starts(n, 4, 90)
+    _compare(FroeschleMap(1.5, 1.5, 0.05), x0, 200, [FrameSpec(4, (QRSpectrum(MGS()),), None)], 10, oracle,
+             seed=123)
+
+
+def test_failures_match(oracle):
+    """Orbits that fail -- non-finite start (STATUS_STATE), overflowing frame (STATUS_W), a zero column
+    (QR pivot breakdown) -- report the same code, step and reducer record."""
+    n = 64
+    x0 = uniform_starts(n, 2, 100)
+    x0[3, 0] = np.nan
+    W0 = haar_frames(n, 2, 2, 101)
+    W0[5, :, 1] = 0.0                       # zero second column: MGS pivot failure at the first handoff
+    W0[7] *= 1e300                          # overflows within a few steps of K = 6
+    for chain in ((QRSpectrum(MGS()),), (QRSpectrum(HouseholderQR()),), (SALI(),), (MEGNO(),), (FLI(),), (GALI(),)):
+        dev, ref = _compare(StandardMap(6.0), x0, 50, [FrameSpec(2, chain, W0)], 5, oracle)
+        assert dev[0].code[3] == 1 and dev[0].code[7] in (2, 3)
