@@ -45,6 +45,10 @@ void run_orbit(const cl_run& run, int64_t i, const cl_buffers& b) {
     bool alive[CL_MAX_FRAMES];
     int8_t code[CL_MAX_FRAMES];
     int64_t hstep[CL_MAX_FRAMES];
+    // A chain (GALI, SALI) with k > 2 holds the SALI record of a separate k = 2 run on the same orbit and the first
+    // two columns of W0: that run's own frame is carried here and evolved by the same tangent products.
+    double Ws[CL_MAX_FRAMES][CL_MAX_DIM * 2];
+    int sali_slot[CL_MAX_FRAMES];
     const double* xin = (n0 == 0 && b.x0) ? b.x0 : b.x;
     std::memcpy(x, xin + i * s, sizeof(double) * s);
     bool any = false;
@@ -65,6 +69,13 @@ void run_orbit(const cl_run& run, int64_t i, const cl_buffers& b) {
             alive[f] = code[f] == STATUS_OK;   // a failed orbit keeps its status and step (propagate.jl:34)
         }
         any = any || alive[f];
+        sali_slot[f] = -1;
+        const cl_frame& fr = run.frames[f];
+        for (int r = 1; r < fr.n_reducers; ++r)
+            if (fr.reducers[r].kind == CL_RED_SALI && fr.reducers[r - 1].kind == CL_RED_GALI && fr.k > 2) sali_slot[f] = r;
+        // the separate run's frame: W0's first two columns (carried launches restore them from the GALI frame's
+        // unit columns, which equal the SALI run's frame at every handoff)
+        if (sali_slot[f] >= 0) std::memcpy(Ws[f], W[f], sizeof(double) * d * 2);
     }
     if (!any) return;   // frozen: nothing is written
 
@@ -80,7 +91,11 @@ void run_orbit(const cl_run& run, int64_t i, const cl_buffers& b) {
             if (run.sys.kind == CL_SYS_CHAIN) {
                 double g[CL_MAX_DIM / 2], gl[CL_MAX_DIM / 2], gr[CL_MAX_DIM / 2];
                 chain.band(x, g, gl, gr);
-                for (int f = 0; f < nf; ++f) if (alive[f]) chain.apply(g, gl, gr, W[f], run.frames[f].k);
+                for (int f = 0; f < nf; ++f) {
+                    if (!alive[f]) continue;
+                    chain.apply(g, gl, gr, W[f], run.frames[f].k);
+                    if (sali_slot[f] >= 0) chain.apply(g, gl, gr, Ws[f], 2);
+                }
                 chain.forward(x);
             } else {
                 double M[CL_MAX_DIM * CL_MAX_DIM];
@@ -96,6 +111,10 @@ void run_orbit(const cl_run& run, int64_t i, const cl_buffers& b) {
                     double Wn[CL_MAX_DIM * CL_MAX_K];
                     fused_product(M, W[f], Wn, d, d, run.frames[f].k);
                     std::memcpy(W[f], Wn, sizeof(double) * d * run.frames[f].k);
+                    if (sali_slot[f] >= 0) {
+                        fused_product(M, Ws[f], Wn, d, d, 2);
+                        std::memcpy(Ws[f], Wn, sizeof(double) * d * 2);
+                    }
                 }
             }
         }
@@ -109,7 +128,8 @@ void run_orbit(const cl_run& run, int64_t i, const cl_buffers& b) {
             // _apply (orbit.jl:23-28): every reducer runs, each on the W the one before returned
             uint8_t* p = st[f].data();
             for (int r = 0; r < fr.n_reducers; ++r) {
-                Reducers<MM>::step(fr.reducers[r], p, n, W[f], d, fr.k);
+                if (r == sali_slot[f]) Reducers<MM>::step(fr.reducers[r], p, n, Ws[f], d, 2);
+                else Reducers<MM>::step(fr.reducers[r], p, n, W[f], d, fr.k);
                 p += state_bytes_of(fr.reducers[r], fr.k);
             }
             p = st[f].data();
