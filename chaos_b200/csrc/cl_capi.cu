@@ -105,6 +105,10 @@ int validate(const cl_run& r) {
         return fail(CL_EINVAL, msg);
     }
     if (r.s != sys_state_len(r.sys, d)) return fail(CL_EINVAL, "state length does not match the system");
+    if (r.sys.kind == CL_SYS_HH_GAUSS) {
+        if (r.sys.gauss_maxiter < 2) return fail(CL_EINVAL, "maxiter must be at least 2");
+        if (!(std::isfinite(r.sys.dt) && r.sys.dt != 0.0)) return fail(CL_EINVAL, "the step dt must be finite and nonzero");
+    }
     if (r.n_frames < 1 || r.n_frames > CL_MAX_FRAMES) return fail(CL_EINVAL, "n_frames must be in 1..3");
     if (r.precision != CL_PREC_FP64 && r.precision != CL_PREC_MIXED) return fail(CL_EINVAL, "unknown precision");
     for (int f = 0; f < r.n_frames; ++f) {

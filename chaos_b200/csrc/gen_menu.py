@@ -106,6 +106,14 @@ def menu():
             for ch in (["QR2"], ["SALI"], ["MEGNO1"]):
                 add(g, SYS_CHAIN, d, prec, [(2, ch)])
         add(g, SYS_CHAIN, d, 0, [(1, ["BEN"])])
+    # IntegratorMap(Gauss(Float64, 3), HenonHeilesFlow(), dt)
+    for ch in (["MEGNO0", "FLI0", "QR6"], ["QR2"], ["QR6"], ["MEGNO1"], ["FLI1"], ["SALI"], ["GALI"]):
+        add("hh", SYS_HH, 4, 0, [(2, ch)])
+    for ch in (["QR2"], ["QR4"], ["GALI"]):
+        add("hh", SYS_HH, 4, 0, [(4, ch)])
+    add("hh", SYS_HH, 4, 0, [(1, ["BEN"])])
+    add("hh_mixed", SYS_HH, 4, 1, [(2, ["MEGNO0", "FLI0", "QR6"])])
+    add("hh_mixed", SYS_HH, 4, 1, [(2, ["QR2"])])
     return groups
 
 

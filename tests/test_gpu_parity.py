@@ -141,7 +141,21 @@ def test_failures_match(oracle):
     x0[3, 0] = np.nan
     W0 = haar_frames(n, 2, 2, 101)
     W0[5, :, 1] = 0.0                       # zero second column: MGS pivot failure at the first handoff
-    W0[7] *= 1e300                          # overflows within a few steps of K = 6
+    W0[7] *= 1e307                          # overflows within the first handoff interval (K = 6)
     for chain in ((QRSpectrum(MGS()),), (QRSpectrum(HouseholderQR()),), (SALI(),), (MEGNO(),), (FLI(),), (GALI(),)):
         dev, ref = _compare(StandardMap(6.0), x0, 50, [FrameSpec(2, chain, W0)], 5, oracle)
         assert dev[0].code[3] == 1 and dev[0].code[7] in (2, 3)
+
+
+@pytest.mark.parametrize("k,chain", [(2, (MEGNO(replace=False), FLI(replace=False), QRSpectrum(GivensQR()))),
+                                     (2, (QRSpectrum(MGS()),)), (2, (SALI(),)), (4, (QRSpectrum(HouseholderQR()),)),
+                                     (4, (GALI(),)), (1, (Benettin(),))], ids=repr)
+@pytest.mark.parametrize("tol", [1e-14, None])
+def test_henon_heiles_gauss3(oracle, k, chain, tol):
+    """IntegratorMap(Gauss(Float64, 3; tol), HenonHeilesFlow(), 0.01): the fixed-point solve, the 12 x 12 tangent
+    solve and the reducers, bit for bit against the oracle, on E = 1/8 energy-shell starts."""
+    from chaos_b200 import Gauss, HenonHeilesFlow, IntegratorMap, random_energy_starts
+    n = 96
+    x0 = random_energy_starts(1 / 8, n, seed=5)
+    sysm = IntegratorMap(Gauss(3, tol=tol), HenonHeilesFlow(), 0.01)
+    _compare(sysm, x0, 600, [FrameSpec(k, chain, haar_frames(n, 4, k, 6))], 10, oracle)
