@@ -43,31 +43,31 @@ METRIC = "orbit-steps/s (4D coupled standard maps, QRSpectrum(Householder) + GAL
 
 # ---- algorithmic operation counts ---------------------------------------------------------------------------------
 # Counting convention: add, sub, mul = 1, fma = 2, div and sqrt = 1, compare/select = 0. The transcendentals are this
-# library's own FP64 polynomials, so they are counted by the arithmetic they execute: one sincos = 3 fma (reduction)
-# + 1 mul + 2 x 8 fma + 1 mul/fma (poly assembly) + 2 mul/sub (quadrant) = 44 flops; one log = 1 div + 2 add + 9 fma
-# + ~10 add/mul = 31 flops. Per orbit-step of the workload above:
+# library's own polynomials, counted by the arithmetic they execute: one FP64 sincos = 3 fma (reduction) + 1 mul
+# + 2 x 8 fma + 1 mul/fma (assembly) + 2 mul/sub (quadrant) = 44 flops; one FP64 log = 1 div + 2 add + 9 fma +
+# ~10 add/mul = 31 flops. Per orbit-step of the workload above:
 def flops_per_orbit_step(tau: int = TAU, mixed: bool = False) -> dict:
-    sincos, log = 44, 31
     d, k = 4, 4
-    map_ = 3 * sincos + 16                        # x' (2), x1'+x2' (1), _abc (5), forward (8)
+    log64, sincos64 = 31, 44
     if mixed:
-        tangent32 = 2 * k * (2 + 2 * 4)           # per frame: 2 adds + 2 x (2 fma) per column, structured
-        tangent64 = 0
+        # the orbit's three values by the split evaluation (reduction 10 + one polynomial 18 = 28 FP64 flops each);
+        # the tangent's three complementary values in Float32 (two degree-5 polynomials, 24 flops each)
+        map64 = 3 * 28 + 16
+        map32 = 3 * 24 + 8
+        tangent32 = 2 * k * (2 + 2 * 4)          # per frame: 2 adds + 2 x (2 fma) per column, structured
     else:
-        tangent64 = 2 * d * k * (1 + 2 * (d - 1))  # per frame fused_product: 1 mul + (d-1) fma per entry, 2 frames
-        tangent32 = 0
+        map64 = 3 * sincos64 + 16                # x' (2), x1'+x2' (1), _abc (5), forward (8)
+        tangent64 = 2 * d * k * (1 + 2 * (d - 1))  # per frame fused_product: 1 mul + (d-1) fma per entry
     # per handoff: Householder QR d = k = 4 (3 reflectors + Q formation + sign fix), window_Gw, orth_loss
     hh = 3 * (2 * d + 3 + 2 * d + 2 + d + 4 * (2 * d + d)) + 3 * 4 * (2 * d + 2 * d) + 2 * d * k
     gw = 60 + 2 * k * k * 2
     orth = k * k * (2 * d)
-    qr = hh + gw + orth + k * (log + 4)
-    # GALI_4: norms (3d + 1 each), logs, unit columns, nested MGS twice, SALI (2 norms)
-    gali = k * (3 * d + 2) + k * (log + 4) + d * k + 2 * sum(j * 4 * d for j in range(k)) + k * (3 * d + 2) + 2 * (3 * d + 2)
-    handoff = qr + gali
-    if mixed:   # norms, QR and GALI in Float32; the logs and Neumaier sums Float64
-        logs64 = 2 * k * (log + 4)
-        return dict(fp64=map_ + logs64 / tau, fp32=tangent32 + (handoff - logs64) / tau)
-    return dict(fp64=map_ + tangent64 + handoff / tau, fp32=0.0)
+    gali = k * (3 * d + 2) + d * k + 2 * sum(j * 4 * d for j in range(k)) + k * (3 * d + 2) + 2 * (3 * d + 2)
+    handoff = hh + gw + orth + gali
+    nlogs = 2 * k
+    if mixed:   # frames, norms, QR and GALI in Float32; logs as hardware log2 times ln 2, sums Float64
+        return dict(fp64=map64 + nlogs * (1 + 4) / tau, fp32=map32 + tangent32 + handoff / tau)
+    return dict(fp64=map64 + tangent64 + (handoff + nlogs * (log64 + 4)) / tau, fp32=0.0)
 
 
 class ClockSampler:

@@ -118,6 +118,20 @@ class cl_probe(C.Structure):
     ]
 
 
+class cl_ensemble_class(C.Structure):
+    _fields_ = [
+        ("run", cl_run),
+        ("n_orbits", C.c_int64),
+        ("order", C.c_void_p),
+        ("K", C.c_void_p),
+        ("N", C.c_void_p),
+        ("escape", C.c_double),
+        ("minb", C.c_int32),
+        ("unroll", C.c_int32),
+        ("buf", cl_buffers),
+    ]
+
+
 def state_bytes(kind: int, k: int) -> int:
     """Bytes of one reducer state in the Julia isbits layout (T = Float64)."""
     return {RED_QR: 16 * k + 72, RED_BENETTIN: 48, RED_SALI: 72, RED_GALI: 24 * k + 32,
@@ -147,6 +161,18 @@ def declare(lib: C.CDLL) -> C.CDLL:
     lib.cl_b200_version.restype = C.c_char_p
     lib.cl_b200_launch_count.argtypes = []
     lib.cl_b200_launch_count.restype = C.c_int64
+    lib.cl_b200_ensemble_device.argtypes = [P(cl_ensemble_class), C.c_int32, C.c_void_p]
+    lib.cl_b200_ensemble_device.restype = C.c_int
+    lib.cl_b200_ensemble.argtypes = [P(cl_ensemble_class), C.c_int32, P(cl_prov)]
+    lib.cl_b200_ensemble.restype = C.c_int
+    lib.cl_b200_ensemble_tune.argtypes = [P(cl_ensemble_class), C.c_int64, C.c_int64, C.c_void_p]
+    lib.cl_b200_ensemble_tune.restype = C.c_int
+    lib.cl_b200_ensemble_graph_create.argtypes = [P(cl_ensemble_class), C.c_int32, P(C.c_void_p)]
+    lib.cl_b200_ensemble_graph_create.restype = C.c_int
+    lib.cl_b200_ensemble_graph_launch.argtypes = [C.c_void_p, C.c_void_p]
+    lib.cl_b200_ensemble_graph_launch.restype = C.c_int
+    lib.cl_b200_ensemble_graph_destroy.argtypes = [C.c_void_p]
+    lib.cl_b200_ensemble_graph_destroy.restype = C.c_int
     lib.cl_b200_menu_size.argtypes = []
     lib.cl_b200_menu_size.restype = C.c_int32
     lib.cl_b200_menu_key.argtypes = [C.c_int32]
@@ -157,4 +183,6 @@ def declare(lib: C.CDLL) -> C.CDLL:
 # Every symbol include/chaoslab_b200.h declares (checked by the CPU tests against the built library).
 EXPORTS = ("cl_b200_propagate", "cl_b200_propagate_device", "cl_b200_check", "cl_b200_state_bytes",
            "cl_b200_probe", "cl_b200_last_error", "cl_b200_version", "cl_b200_launch_count",
-           "cl_b200_menu_size", "cl_b200_menu_key")
+           "cl_b200_menu_size", "cl_b200_menu_key", "cl_b200_ensemble_device", "cl_b200_ensemble",
+           "cl_b200_ensemble_tune", "cl_b200_ensemble_graph_create", "cl_b200_ensemble_graph_launch",
+           "cl_b200_ensemble_graph_destroy")

@@ -175,6 +175,13 @@ struct DevBufs {
 }  // namespace
 
 void register_instance(const char* key, LaunchFn fn) { registry_list().push_back(Instance{key, fn}); }
+
+// Shared with the ensemble entry points (cl_ensemble_capi.cu).
+int capi_fail(int code, const std::string& msg) { return fail(code, msg); }
+int capi_map_cuda(cudaError_t e, const char* where) { return map_cuda(e, where); }
+int capi_validate(const cl_run& r) { return validate(r); }
+int64_t capi_frame_bytes(const cl_frame& f) { return frame_bytes(f); }
+void capi_count_launch() { g_launches.fetch_add(1); }
 const Instance* find_instance(const std::string& key) {
     for (const Instance& in : registry_list())
         if (key == in.key) return &in;

@@ -1,0 +1,347 @@
+// cl_ensemble_capi.cu -- the ensemble entry points of include/chaoslab_b200.h: class checks, the per-class
+// persistent launches on concurrent streams, the autotuner and the CUDA-graph capture.
+#include <cuda_runtime.h>
+
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/chaoslab_b200.h"
+#include "cl_ensemble.cuh"
+
+namespace cl {
+
+int capi_fail(int code, const std::string& msg);      // cl_capi.cu
+int capi_map_cuda(cudaError_t e, const char* where);  // cl_capi.cu
+int capi_validate(const cl_run& r);                   // cl_capi.cu
+int64_t capi_frame_bytes(const cl_frame& f);          // cl_capi.cu
+void capi_count_launch();                             // cl_capi.cu
+
+namespace {
+std::vector<std::pair<std::string, ELaunchFn>>& ereg() {
+    static std::vector<std::pair<std::string, ELaunchFn>> v;
+    return v;
+}
+ELaunchFn find_ensemble(const std::string& key) {
+    for (auto& p : ereg()) if (p.first == key) return p.second;
+    return nullptr;
+}
+std::mutex g_tune_mu;
+std::map<std::string, ETune> g_tuned;   // tuned variant per (instance key, tau)
+
+int sm_count() {
+    int dev = 0, n = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+    return n > 0 ? n : 1;
+}
+
+std::string tune_key(const cl_run& r) { return run_key(r) + "t" + std::to_string(r.tau); }
+
+ETune variant_of(const cl_ensemble_class& c) {
+    ETune t{128, 2, 1};
+    {
+        std::lock_guard<std::mutex> g(g_tune_mu);
+        auto it = g_tuned.find(tune_key(c.run));
+        if (it != g_tuned.end()) t = it->second;
+    }
+    if (c.minb > 0) t.minb = c.minb;
+    if (c.unroll > 0) t.unroll = c.unroll;
+    if (t.unroll != 1 && t.unroll != c.run.tau) t.unroll = 1;
+    return t;
+}
+
+int check_class(const cl_ensemble_class& c, ELaunchFn* fn) {
+    int v = capi_validate(c.run);
+    if (v) return v;
+    if (c.run.n_frames != 1) return capi_fail(CL_EINVAL, "an ensemble class carries one frame");
+    if (c.run.n0 != 0 || (c.run.steps != 0 && c.run.steps != c.run.N)) return capi_fail(CL_EINVAL, "ensembles start fresh and run whole");
+    if (c.minb != 0 && c.minb != 1 && c.minb != 2 && c.minb != 4) return capi_fail(CL_EINVAL, "minb must be 0, 1, 2 or 4");
+    if (c.unroll < 0) return capi_fail(CL_EINVAL, "unroll must be >= 0");
+    *fn = find_ensemble(run_key(c.run));
+    if (!*fn) return capi_fail(CL_EUNSUPPORTED, "no compiled ensemble kernel for " + run_key(c.run));
+    return 0;
+}
+
+EArgs eargs(const cl_ensemble_class& c, unsigned long long* counter, int64_t n_limit = -1, int64_t N_cap = -1) {
+    EArgs a;
+    std::memset(&a, 0, sizeof a);
+    a.n = n_limit >= 0 && n_limit < c.n_orbits ? n_limit : c.n_orbits;
+    a.counter = counter;
+    a.order = reinterpret_cast<const i64*>(c.order);
+    a.x_in = c.buf.x0;
+    a.x_out = c.buf.x;
+    a.W_in = c.buf.W0[0];
+    a.W_out = c.buf.W[0];
+    a.states = static_cast<uint64_t*>(c.buf.states[0]);
+    a.code = c.buf.code[0];
+    a.hstep = reinterpret_cast<i64*>(c.buf.hstep[0]);
+    a.Kp = c.K;
+    a.Np = N_cap >= 0 ? nullptr : reinterpret_cast<const i64*>(c.N);
+    a.N = N_cap >= 0 ? N_cap : c.run.N;
+    a.tau = c.run.tau;
+    a.escape = c.escape;
+    a.seed = c.run.seed;
+    a.orbit_base = c.run.orbit_base;
+    for (int r = 0; r < c.run.frames[0].n_reducers; ++r) a.prm[r].orthogonality_tol = c.run.frames[0].reducers[r].orthogonality_tol;
+    return a;
+}
+
+struct Forks {   // side streams and events of one enqueue; released after the work (or the capture) ends
+    std::vector<cudaStream_t> streams;
+    std::vector<cudaEvent_t> events;
+    ~Forks() {
+        for (cudaEvent_t e : events) cudaEventDestroy(e);
+        for (cudaStream_t s : streams) cudaStreamDestroy(s);
+    }
+};
+
+int enqueue_classes(const cl_ensemble_class* cs, int nc, unsigned long long* counters, cudaStream_t st,
+                    LaunchInfo* info, Forks& fk) {
+    std::vector<ELaunchFn> fns(nc);
+    for (int c = 0; c < nc; ++c) {
+        int v = check_class(cs[c], &fns[c]);
+        if (v) return v;
+    }
+    cudaError_t e = cudaMemsetAsync(counters, 0, sizeof(unsigned long long) * nc, st);
+    if (e != cudaSuccess) return capi_map_cuda(e, "queue reset");
+    // fork: every class on its own stream, joined back into `st`
+    cudaEvent_t fork;
+    if ((e = cudaEventCreateWithFlags(&fork, cudaEventDisableTiming)) != cudaSuccess) return capi_map_cuda(e, "event");
+    fk.events.push_back(fork);
+    cudaEventRecord(fork, st);
+    std::vector<cudaStream_t> ss(nc, nullptr);
+    std::vector<cudaEvent_t> done(nc, nullptr);
+    int rc = 0;
+    const int sms = sm_count();
+    for (int c = 0; c < nc && rc == 0; ++c) {
+        cudaStreamCreateWithFlags(&ss[c], cudaStreamNonBlocking);
+        cudaEventCreateWithFlags(&done[c], cudaEventDisableTiming);
+        fk.streams.push_back(ss[c]);
+        fk.events.push_back(done[c]);
+        cudaStreamWaitEvent(ss[c], fork, 0);
+        const ETune t = variant_of(cs[c]);
+        const int grid = sms * t.minb;
+        e = fns[c](cs[c].run, eargs(cs[c], counters + c), grid, t, ss[c], info);
+        capi_count_launch();
+        if (e != cudaSuccess) rc = capi_map_cuda(e, "ensemble kernel launch");
+        cudaEventRecord(done[c], ss[c]);
+        cudaStreamWaitEvent(st, done[c], 0);
+    }
+    return rc;
+}
+
+struct Graph {
+    cudaGraphExec_t exec = nullptr;
+    cudaGraph_t graph = nullptr;
+    unsigned long long* counters = nullptr;
+};
+
+}  // namespace
+
+void register_ensemble(const char* key, ELaunchFn fn) { ereg().emplace_back(key, fn); }
+
+}  // namespace cl
+
+using namespace cl;
+
+extern "C" {
+
+int cl_b200_ensemble_device(const cl_ensemble_class* classes, int32_t n_classes, void* stream) {
+    if (!classes || n_classes < 1) return capi_fail(CL_EINVAL, "no classes");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    unsigned long long* counters = nullptr;
+    cudaError_t e = cudaMallocAsync(reinterpret_cast<void**>(&counters), sizeof(unsigned long long) * n_classes, st);
+    if (e != cudaSuccess) return capi_map_cuda(e, "queue heads");
+    int rc;
+    {
+        Forks fk;
+        rc = enqueue_classes(classes, n_classes, counters, st, nullptr, fk);
+    }
+    cudaFreeAsync(counters, st);
+    return rc;
+}
+
+int cl_b200_ensemble(const cl_ensemble_class* classes, int32_t n_classes, cl_prov* prov) {
+    if (!classes || n_classes < 1) return capi_fail(CL_EINVAL, "no classes");
+    std::vector<cl_ensemble_class> dc(classes, classes + n_classes);
+    std::vector<void*> allocs;
+    auto alloc = [&](void** p, size_t b) -> cudaError_t {
+        if (!b) { *p = nullptr; return cudaSuccess; }
+        cudaError_t e = cudaMalloc(p, b);
+        if (e == cudaSuccess) allocs.push_back(*p);
+        return e;
+    };
+    auto cleanup = [&]() { for (void* p : allocs) cudaFree(p); };
+    cudaStream_t st;
+    cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+    int rc = 0;
+    for (int c = 0; c < n_classes && rc == 0; ++c) {
+        ELaunchFn fn;
+        if ((rc = check_class(classes[c], &fn))) break;
+        const cl_ensemble_class& h = classes[c];
+        cl_ensemble_class& d = dc[c];
+        const int64_t n = h.n_orbits, s = h.run.s, dk = int64_t(h.run.d) * h.run.frames[0].k;
+        const int64_t sb = capi_frame_bytes(h.run.frames[0]);
+        void *x0, *x, *W0 = nullptr, *W, *stt, *code, *hs, *ord = nullptr, *K = nullptr, *N = nullptr;
+        cudaError_t e = cudaSuccess;
+        if ((e = alloc(&x0, 8 * n * s)) || (e = alloc(&x, 8 * n * s)) || (e = alloc(&W, 8 * n * dk)) ||
+            (e = alloc(&stt, sb * n)) || (e = alloc(&code, n)) || (e = alloc(&hs, 8 * n)) ||
+            (h.buf.W0[0] && (e = alloc(&W0, 8 * n * dk))) || (h.order && (e = alloc(&ord, 8 * n))) ||
+            (h.K && (e = alloc(&K, 8 * n))) || (h.N && (e = alloc(&N, 8 * n)))) {
+            rc = capi_map_cuda(e, "alloc");
+            break;
+        }
+        cudaMemcpyAsync(x0, h.buf.x0, 8 * n * s, cudaMemcpyHostToDevice, st);
+        if (W0) cudaMemcpyAsync(W0, h.buf.W0[0], 8 * n * dk, cudaMemcpyHostToDevice, st);
+        if (ord) cudaMemcpyAsync(ord, h.order, 8 * n, cudaMemcpyHostToDevice, st);
+        if (K) cudaMemcpyAsync(K, h.K, 8 * n, cudaMemcpyHostToDevice, st);
+        if (N) cudaMemcpyAsync(N, h.N, 8 * n, cudaMemcpyHostToDevice, st);
+        d.buf.x0 = static_cast<double*>(x0); d.buf.x = static_cast<double*>(x);
+        d.buf.W0[0] = static_cast<double*>(W0); d.buf.W[0] = static_cast<double*>(W);
+        d.buf.states[0] = stt; d.buf.code[0] = static_cast<int8_t*>(code); d.buf.hstep[0] = static_cast<int64_t*>(hs);
+        d.order = static_cast<int64_t*>(ord); d.K = static_cast<double*>(K); d.N = static_cast<int64_t*>(N);
+    }
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    if (rc == 0) {
+        cudaEventRecord(e0, st);
+        rc = cl_b200_ensemble_device(dc.data(), n_classes, st);
+        cudaEventRecord(e1, st);
+    }
+    for (int c = 0; c < n_classes && rc == 0; ++c) {
+        const cl_ensemble_class& h = classes[c];
+        const cl_ensemble_class& d = dc[c];
+        const int64_t n = h.n_orbits, s = h.run.s, dk = int64_t(h.run.d) * h.run.frames[0].k;
+        const int64_t sb = capi_frame_bytes(h.run.frames[0]);
+        cudaMemcpyAsync(h.buf.x, d.buf.x, 8 * n * s, cudaMemcpyDeviceToHost, st);
+        cudaMemcpyAsync(h.buf.W[0], d.buf.W[0], 8 * n * dk, cudaMemcpyDeviceToHost, st);
+        if (sb) cudaMemcpyAsync(h.buf.states[0], d.buf.states[0], sb * n, cudaMemcpyDeviceToHost, st);
+        cudaMemcpyAsync(h.buf.code[0], d.buf.code[0], n, cudaMemcpyDeviceToHost, st);
+        if (h.buf.hstep[0]) cudaMemcpyAsync(h.buf.hstep[0], d.buf.hstep[0], 8 * n, cudaMemcpyDeviceToHost, st);
+    }
+    cudaError_t e = cudaStreamSynchronize(st);
+    if (rc == 0 && e != cudaSuccess) rc = capi_map_cuda(e, "synchronize");
+    if (rc == 0 && prov) {
+        std::memset(prov, 0, sizeof *prov);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        prov->gpu_ms = ms;
+        prov->launches = n_classes;
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceProp p;
+        if (cudaGetDeviceProperties(&p, dev) == cudaSuccess) std::snprintf(prov->device, sizeof prov->device, "%s", p.name);
+        std::snprintf(prov->variant, sizeof prov->variant, "ensemble x%d", n_classes);
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaStreamDestroy(st);
+    cleanup();
+    return rc;
+}
+
+int cl_b200_ensemble_tune(cl_ensemble_class* cls, int64_t sample_orbits, int64_t sample_steps, void* stream) {
+    if (!cls) return capi_fail(CL_EINVAL, "NULL class");
+    ELaunchFn fn;
+    int rc = check_class(*cls, &fn);
+    if (rc) return rc;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const int tau = cls->run.tau;
+    int64_t steps = sample_steps > 0 ? sample_steps : 20 * tau;
+    steps = (steps + tau - 1) / tau * tau;
+    unsigned long long* counter = nullptr;
+    cudaError_t e = cudaMalloc(reinterpret_cast<void**>(&counter), sizeof(unsigned long long));
+    if (e != cudaSuccess) return capi_map_cuda(e, "queue head");
+    const int sms = sm_count();
+    ETune best{128, 2, 1};
+    float best_ms = 1e30f;
+    const int unrolls[2] = {1, (tau == 5 || tau == 10 || tau == 20) ? tau : 1};
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    for (int minb : {1, 2, 4})
+        for (int u = 0; u < 2; ++u) {
+            if (u == 1 && unrolls[1] == 1) continue;
+            ETune t{128, minb, unrolls[u]};
+            EArgs a = eargs(*cls, counter, sample_orbits, steps);
+            a.escape = 0.0;
+            float ms = 0.f;
+            for (int rep = 0; rep < 2; ++rep) {   // the first run warms up
+                cudaMemsetAsync(counter, 0, sizeof(unsigned long long), st);
+                cudaEventRecord(e0, st);
+                e = fn(cls->run, a, sms * minb, t, st, nullptr);
+                cudaEventRecord(e1, st);
+                if (e != cudaSuccess) break;
+                cudaEventSynchronize(e1);
+                cudaEventElapsedTime(&ms, e0, e1);
+            }
+            if (e != cudaSuccess) { rc = capi_map_cuda(e, "tune launch"); break; }
+            if (ms < best_ms) { best_ms = ms; best = t; }
+        }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaFree(counter);
+    if (rc) return rc;
+    {
+        std::lock_guard<std::mutex> g(g_tune_mu);
+        g_tuned[tune_key(cls->run)] = best;
+    }
+    cls->minb = best.minb;
+    cls->unroll = best.unroll;
+    return 0;
+}
+
+int cl_b200_ensemble_graph_create(const cl_ensemble_class* classes, int32_t n_classes, void** graph) {
+    if (!classes || n_classes < 1 || !graph) return capi_fail(CL_EINVAL, "bad arguments");
+    Graph* g = new Graph();
+    cudaError_t e = cudaMalloc(reinterpret_cast<void**>(&g->counters), sizeof(unsigned long long) * n_classes);
+    if (e != cudaSuccess) { delete g; return capi_map_cuda(e, "queue heads"); }
+    cudaStream_t st;
+    cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+    int rc = 0;
+    if ((e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal)) != cudaSuccess) rc = capi_map_cuda(e, "capture");
+    Forks fk;
+    if (rc == 0) {
+        rc = enqueue_classes(classes, n_classes, g->counters, st, nullptr, fk);
+        cudaGraph_t gr = nullptr;
+        e = cudaStreamEndCapture(st, &gr);
+        if (rc == 0 && e != cudaSuccess) rc = capi_map_cuda(e, "end capture");
+        g->graph = gr;
+        if (rc == 0 && (e = cudaGraphInstantiate(&g->exec, gr, 0)) != cudaSuccess) rc = capi_map_cuda(e, "instantiate");
+    }
+    cudaStreamDestroy(st);
+    if (rc) {
+        if (g->exec) cudaGraphExecDestroy(g->exec);
+        if (g->graph) cudaGraphDestroy(g->graph);
+        cudaFree(g->counters);
+        delete g;
+        return rc;
+    }
+    *graph = g;
+    return 0;
+}
+
+int cl_b200_ensemble_graph_launch(void* graph, void* stream) {
+    Graph* g = static_cast<Graph*>(graph);
+    if (!g || !g->exec) return capi_fail(CL_EINVAL, "no graph");
+    cudaError_t e = cudaGraphLaunch(g->exec, static_cast<cudaStream_t>(stream));
+    capi_count_launch();
+    return e == cudaSuccess ? 0 : capi_map_cuda(e, "graph launch");
+}
+
+int cl_b200_ensemble_graph_destroy(void* graph) {
+    Graph* g = static_cast<Graph*>(graph);
+    if (!g) return 0;
+    if (g->exec) cudaGraphExecDestroy(g->exec);
+    if (g->graph) cudaGraphDestroy(g->graph);
+    if (g->counters) cudaFree(g->counters);
+    delete g;
+    return 0;
+}
+
+}  // extern "C"

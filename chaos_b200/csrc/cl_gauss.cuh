@@ -35,6 +35,7 @@ struct GaussJac { double T[16]; double xn[4]; };
 struct SysGauss3HH {
     static constexpr int D = 4, S = 4;
     using Jac = GaussJac;
+    template <typename R> using JacR = GaussJac;
     double h, tol;
     int maxiter;
 
@@ -144,24 +145,20 @@ struct SysGauss3HH {
         return ok;
     }
 
+    // vector_field_jacobian (flow_core.jl:79-83) at a stage: [[0, I], [-Hs, 0]] with the Henon-Heiles Hessian
+    // Hs = [[1 + 2 q2, 2 q1], [2 q1, 1 - 2 q2]] (flow_models.jl:103); column-major 4 x 4.
+    static __device__ __forceinline__ void hh_jac(const double* y, double* Jm) {
+        const double h11 = 1 + 2 * y[1], h21 = 2 * y[0], h12 = 2 * y[0], h22 = 1 - 2 * y[1];
+        Jm[0] = 0; Jm[1] = 0; Jm[2] = -h11; Jm[3] = -h21;
+        Jm[4] = 0; Jm[5] = 0; Jm[6] = -h12; Jm[7] = -h22;
+        Jm[8] = 1; Jm[9] = 0; Jm[10] = 0; Jm[11] = 0;
+        Jm[12] = 0; Jm[13] = 1; Jm[14] = 0; Jm[15] = 0;
+    }
+
     // The 12 x 12 solve of tangent_advance and the assembly of T (Float64, reference order).
-    __device__ __noinline__ static void tangent64(const double Y[3][4], double hstep, double* T) {
-        double J[3][4];   // per stage the Hessian entries h11, h21 (= h12), h22 of the force
-#pragma unroll
-        for (int i = 0; i < 3; ++i) {
-            J[i][0] = 1 + 2 * Y[i][1];
-            J[i][1] = 2 * Y[i][0];
-            J[i][2] = 2 * Y[i][0];
-            J[i][3] = 1 - 2 * Y[i][1];
-        }
-        // vector_field_jacobian entry (r, c) of stage j: [[0, I], [-Hs, 0]]
-        auto jac = [&](int j, int r, int c) -> double {
-            if (r < 2) return (c == r + 2) ? 1.0 : 0.0;
-            if (c >= 2) return 0.0;
-            const int rr = r - 2;
-            const double hs = (rr == 0) ? (c == 0 ? J[j][0] : J[j][2]) : (c == 0 ? J[j][1] : J[j][3]);
-            return -hs;
-        };
+    static __device__ __noinline__ void tangent64(const double* Yflat, double hstep, double* T) {
+        double Jm[3][16];
+        for (int i = 0; i < 3; ++i) hh_jac(Yflat + 4 * i, Jm[i]);
         double M[144], B[48];
         for (int c = 0; c < 12; ++c)
             for (int r = 0; r < 12; ++r) M[r + 12 * c] = r == c ? 1.0 : 0.0;
@@ -170,8 +167,8 @@ struct SysGauss3HH {
                 const double f = hstep * (Ahi(i, j) + Alo(i, j));
                 for (int c = 0; c < 4; ++c)
                     for (int r = 0; r < 4; ++r) {
-                        double& e = M[(i * 4 + r) + 12 * (j * 4 + c)];
-                        e = e - f * jac(j, r, c);
+                        const int at = (i * 4 + r) + 12 * (j * 4 + c);
+                        M[at] = M[at] - f * Jm[j][r + 4 * c];
                     }
             }
         for (int c = 0; c < 4; ++c)
@@ -180,11 +177,18 @@ struct SysGauss3HH {
         for (int j = 0; j < 12; ++j) {
             int p = j;
             double pm = fabs(M[j + 12 * j]);
-            for (int i = j + 1; i < 12; ++i) { const double a = fabs(M[i + 12 * j]); if (a > pm) { pm = a; p = i; } }
+            for (int i = j + 1; i < 12; ++i) {
+                const double av = fabs(M[i + 12 * j]);
+                if (av > pm) { pm = av; p = i; }
+            }
             ipiv[j] = p;
             if (M[p + 12 * j] != 0.0) {
                 if (p != j)
-                    for (int c = 0; c < 12; ++c) { const double t = M[j + 12 * c]; M[j + 12 * c] = M[p + 12 * c]; M[p + 12 * c] = t; }
+                    for (int c = 0; c < 12; ++c) {
+                        const double t = M[j + 12 * c];
+                        M[j + 12 * c] = M[p + 12 * c];
+                        M[p + 12 * c] = t;
+                    }
                 const double rp = 1.0 / M[j + 12 * j];
                 for (int i = j + 1; i < 12; ++i) M[i + 12 * j] = M[i + 12 * j] * rp;
             }
@@ -196,20 +200,23 @@ struct SysGauss3HH {
         }
         for (int j = 0; j < 12; ++j)
             if (ipiv[j] != j)
-                for (int c = 0; c < 4; ++c) { const double t = B[j + 12 * c]; B[j + 12 * c] = B[ipiv[j] + 12 * c]; B[ipiv[j] + 12 * c] = t; }
+                for (int c = 0; c < 4; ++c) {
+                    const double t = B[j + 12 * c];
+                    B[j + 12 * c] = B[ipiv[j] + 12 * c];
+                    B[ipiv[j] + 12 * c] = t;
+                }
         for (int c = 0; c < 4; ++c) {
-            double* b = B + 12 * c;
+            double* bc = B + 12 * c;
             for (int k = 0; k < 12; ++k)
-                if (b[k] != 0.0)
-                    for (int i = k + 1; i < 12; ++i) b[i] = b[i] - b[k] * M[i + 12 * k];
+                if (bc[k] != 0.0)
+                    for (int i = k + 1; i < 12; ++i) bc[i] = bc[i] - bc[k] * M[i + 12 * k];
             for (int k = 11; k >= 0; --k)
-                if (b[k] != 0.0) {
-                    b[k] = b[k] / M[k + 12 * k];
-                    for (int i = 0; i < k; ++i) b[i] = b[i] - b[k] * M[i + 12 * k];
+                if (bc[k] != 0.0) {
+                    bc[k] = bc[k] / M[k + 12 * k];
+                    for (int i = 0; i < k; ++i) bc[i] = bc[i] - bc[k] * M[i + 12 * k];
                 }
         }
         double Wn[16];
-#pragma unroll
         for (int l = 0; l < 16; ++l) Wn[l] = (l % 4) == (l / 4) ? 1.0 : 0.0;
         for (int i = 0; i < 3; ++i) {
             double P[16];
@@ -217,14 +224,12 @@ struct SysGauss3HH {
                 for (int ii = 0; ii < 4; ++ii) P[ii + 4 * jj] = 0.0;
                 for (int l = 0; l < 4; ++l) {
                     const double temp = B[(i * 4 + l) + 12 * jj];
-                    for (int ii = 0; ii < 4; ++ii) P[ii + 4 * jj] = P[ii + 4 * jj] + temp * jac(i, ii, l);
+                    for (int ii = 0; ii < 4; ++ii) P[ii + 4 * jj] = P[ii + 4 * jj] + temp * Jm[i][ii + 4 * l];
                 }
             }
             const double f = hstep * (bhi(i) + blo(i));
-#pragma unroll
             for (int l = 0; l < 16; ++l) Wn[l] = Wn[l] + f * P[l];
         }
-#pragma unroll
         for (int l = 0; l < 16; ++l) T[l] = Wn[l];
     }
 
@@ -239,7 +244,7 @@ struct SysGauss3HH {
             for (int l = 0; l < 4; ++l) Jc.xn[l] = nan;
             return;
         }
-        tangent64(Y, h, Jc.T);
+        tangent64(&Y[0][0], h, Jc.T);
 #pragma unroll
         for (int l = 0; l < 4; ++l) Jc.xn[l] = x[l] + inc[l];
     }

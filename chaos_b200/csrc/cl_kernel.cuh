@@ -229,7 +229,7 @@ __global__ void __launch_bounds__(128) orbit_kernel(const KArgs a, const Sys sys
     const i64 handoffs = a.steps / a.tau;
     for (i64 h = 0; h < handoffs; ++h) {
         for (int t = 0; t < a.tau; ++t) {
-            typename Sys::Jac J;
+            typename Sys::template JacR<Real> J;
             sys.jac(x, J);
             if (fr0.alive) sys.template apply<F0::K>(J, fr0.W);
             if (NF > 1 && fr1.alive) sys.template apply<F1::K>(J, fr1.W);

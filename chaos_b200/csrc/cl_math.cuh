@@ -70,10 +70,81 @@ __device__ __forceinline__ void cl_sincos(double x, double* sn, double* cs) {
     else if (q == 2.0) { *sn = -s; *cs = -c; }
     else { *sn = -c; *cs = s; }
 }
+// ---- split evaluation for the mixed kernels ------------------------------------------------------------------------
+// The same reduction as cl_sincos, then only the polynomial one Float64 value needs (the quadrant picks sin- or
+// cos-form coefficients), so sin(x) or cos(x) comes out bit-identical to cl_sincos at about half the FP64 work;
+// the complementary function comes in Float32 from the same reduced argument (Taylor to x^11 / x^10, ~1 ulp of
+// float), for the Float32 tangent entries.
+struct Reduced { double r, z, x; int q; };
+__device__ __forceinline__ Reduced cl_reduce(double x) {
+    Reduced w;
+    w.x = x;
+    const double k = rint(x * CL_TWO_OVER_PI);
+    double r = fma(-k, CL_PIO2_1, x);
+    r = fma(-k, CL_PIO2_2, r);
+    r = fma(-k, CL_PIO2_3, r);
+    w.r = r;
+    w.z = r * r;
+    w.q = static_cast<int>(k - 4.0 * floor(k * 0.25));
+    return w;
+}
+// cos-form (cosf = true) or sin-form polynomial of the reduced argument, exactly as cl_sincos evaluates it.
+__device__ __forceinline__ double cl_poly(const Reduced& w, bool cosf) {
+    const double z = w.z;
+    double p = cosf ? CL_COS_T16 : CL_SIN_T17;
+    p = fma(p, z, cosf ? CL_COS_T14 : CL_SIN_T15);
+    p = fma(p, z, cosf ? CL_COS_T12 : CL_SIN_T13);
+    p = fma(p, z, cosf ? CL_COS_T10 : CL_SIN_T11);
+    p = fma(p, z, cosf ? CL_COS_T8 : CL_SIN_T9);
+    p = fma(p, z, cosf ? CL_COS_T6 : CL_SIN_T7);
+    p = fma(p, z, cosf ? CL_COS_T4 : CL_SIN_T5);
+    p = fma(p, z, cosf ? CL_COS_T2 : CL_SIN_T3);
+    return cosf ? fma(z, p, 1.0) : fma(w.r * z, p, w.r);
+}
+// sin(x) bit-identical to cl_sincos's: quadrant 0 s, 1 c, 2 -s, 3 -c
+__device__ __forceinline__ double cl_sin_split(const Reduced& w) {
+    if (!isfin(w.x)) return w.x - w.x;
+    if (w.x == 0.0) return w.x;
+    const double v = cl_poly(w, (w.q & 1) != 0);
+    return w.q >= 2 ? -v : v;
+}
+// cos(x) bit-identical to cl_sincos's: quadrant 0 c, 1 -s, 2 -c, 3 s
+__device__ __forceinline__ double cl_cos_split(const Reduced& w) {
+    if (!isfin(w.x)) return w.x - w.x;
+    if (w.x == 0.0) return 1.0;
+    const double v = cl_poly(w, (w.q & 1) != 0 ? false : true);
+    return (w.q == 1 || w.q == 2) ? -v : v;
+}
+// Float32 sin / cos from the same reduction.
+__device__ __forceinline__ void cl_sincos32(const Reduced& w, float* sn, float* cs) {
+    if (!isfin(w.x)) { const float nan = __int_as_float(0x7fc00000); *sn = nan; *cs = nan; return; }
+    const float r = static_cast<float>(w.r), z = r * r;
+    float ps = static_cast<float>(CL_SIN_T11);
+    ps = __fmaf_rn(ps, z, static_cast<float>(CL_SIN_T9));
+    ps = __fmaf_rn(ps, z, static_cast<float>(CL_SIN_T7));
+    ps = __fmaf_rn(ps, z, static_cast<float>(CL_SIN_T5));
+    ps = __fmaf_rn(ps, z, static_cast<float>(CL_SIN_T3));
+    const float s = __fmaf_rn(r * z, ps, r);
+    float pc = static_cast<float>(CL_COS_T10);
+    pc = __fmaf_rn(pc, z, static_cast<float>(CL_COS_T8));
+    pc = __fmaf_rn(pc, z, static_cast<float>(CL_COS_T6));
+    pc = __fmaf_rn(pc, z, static_cast<float>(CL_COS_T4));
+    pc = __fmaf_rn(pc, z, static_cast<float>(CL_COS_T2));
+    const float c = __fmaf_rn(z, pc, 1.0f);
+    switch (w.q) {
+        case 0: *sn = s; *cs = c; break;
+        case 1: *sn = c; *cs = -s; break;
+        case 2: *sn = -s; *cs = -c; break;
+        default: *sn = -c; *cs = s; break;
+    }
+}
+
 __device__ __forceinline__ double cl_sin(double x) { double s, c; cl_sincos(x, &s, &c); return s; }
 __device__ __forceinline__ double cl_cos(double x) { double s, c; cl_sincos(x, &s, &c); return c; }
 
-__device__ __forceinline__ double cl_log(double x) {
+__device__ __forceinline__ double cl_log(double x);
+
+__device__ __forceinline__ double cl_log_impl(double x) {
     if (isnan(x)) return x;
     if (x < 0.0) return __longlong_as_double(0x7ff8000000000000LL);
     if (x == 0.0) return -__longlong_as_double(0x7ff0000000000000LL);
@@ -100,6 +171,7 @@ __device__ __forceinline__ double cl_log(double x) {
     const double hfsq = 0.5 * f * f;
     return e * CL_LN2_HI - ((hfsq - (s * (hfsq + R) + e * CL_LN2_LO)) - f);
 }
+__device__ __forceinline__ double cl_log(double x) { return cl_log_impl(x); }
 
 // Neumaier compensated sum (src/Foundation/Foundation.jl:48-68); always Float64.
 struct CS { double s, c; };
@@ -123,6 +195,42 @@ __device__ __forceinline__ T safe_norm(const T* v) {
 #pragma unroll
     for (int i = 1; i < N; ++i) { q = v[i] / m; s = s + q * q; }
     return m * sqrt(s);
+}
+
+// Norm, division and maximum of the reducers and the QR family. Float64: the reference's safe_norm, IEEE division
+// and Julia's NaN-propagating max, so the plain kernels stay operation-for-operation. Float32 (mixed kernels): the
+// unscaled norm sqrt(sum v^2) when the sum is a normal float (the scaled safe_norm otherwise), the fast reciprocal
+// division (2 ulp) and fmaxf; the frames are renormalised every handoff, so their entries stay far inside the
+// float range, and non-finite values are caught by the status check before any reducer runs.
+template <int N, typename T>
+__device__ __forceinline__ T nrm(const T* v) {
+    if constexpr (sizeof(T) == 8) {
+        return safe_norm<N>(v);
+    } else {
+        float s = v[0] * v[0];
+#pragma unroll
+        for (int i = 1; i < N; ++i) s = __fmaf_rn(v[i], v[i], s);
+        if (s >= 1e-30f && s <= 1e30f) return __fsqrt_rn(s);
+        return safe_norm<N>(v);
+    }
+}
+template <typename T>
+__device__ __forceinline__ T dv(T a, T b) {
+    if constexpr (sizeof(T) == 8) return a / b;
+    else return __fdividef(a, b);
+}
+template <typename T>
+__device__ __forceinline__ T mx(T a, T b) {
+    if constexpr (sizeof(T) == 8) return jl_max(a, b);
+    else return fmaxf(a, b);
+}
+
+// The logarithm of a norm or pivot, summed in Float64 either way: cl_log for the plain kernels; for the mixed
+// kernels the hardware log2 of the Float32 value (relative error ~2^-22) times ln 2 in Float64.
+template <typename T>
+__device__ __forceinline__ double lnr(T a) {
+    if constexpr (sizeof(T) == 8) return cl_log(a);
+    else return static_cast<double>(__log2f(a)) * 0.6931471805599453;
 }
 
 // The element-type constants of the tolerances.

@@ -55,7 +55,7 @@ __device__ __forceinline__ QRRes orth_gs(const T* W, T* Q, T* R) {
             }
         } else {
             const T eta = T(1) / sqrt(T(2));
-            T nold = safe_norm<D>(w);
+            T nold = nrm<D>(w);
             passes = 0;
             for (;;) {
                 passes += 1;
@@ -70,20 +70,20 @@ __device__ __forceinline__ QRRes orth_gs(const T* W, T* Q, T* R) {
 #pragma unroll
                     for (int l = 0; l < D; ++l) u[l] = u[l] - c * qi[l];
                 }
-                const T nnew = safe_norm<D>(u);
+                const T nnew = nrm<D>(u);
                 if (nnew >= nold * eta || !(isfin(nnew) && nnew > T(0))) break;
                 if (passes == MAX_PASSES) { passes = MAX_PASSES + 1; break; }
                 nold = nnew;
             }
         }
-        const T gamma = safe_norm<D>(u);
+        const T gamma = nrm<D>(u);
 #pragma unroll
         for (int i = 0; i < K; ++i) R[i + m * K] = i < m ? r[i] : (i == m ? gamma : T(0));
         if (passes > MAX_PASSES) { res.status = QR_PASSES; res.column = m + 1; }
         else if (!(isfin(gamma) && gamma > T(0))) { res.status = QR_PIVOT; res.column = m + 1; }
         if (res.status != QR_OK) break;
 #pragma unroll
-        for (int l = 0; l < D; ++l) Q[l + m * D] = u[l] / gamma;
+        for (int l = 0; l < D; ++l) Q[l + m * D] = dv(u[l], gamma);
         res.count = passes > res.count ? passes : res.count;
     }
     return res;
@@ -113,15 +113,15 @@ __device__ __forceinline__ int hh_sweep(T* A, T* U) {
         T a[D];
 #pragma unroll
         for (int i = 0; i < D; ++i) a[i] = i >= j ? A[i + j * D] : T(0);
-        const T c = safe_norm<D>(a);
+        const T c = nrm<D>(a);
         T rho;
         if (isfin(c) && c > T(0)) {
             const T s = a[j] < T(0) ? T(-1) : T(1);
             a[j] = a[j] + s * c;
-            const T nv = safe_norm<D>(a);
+            const T nv = nrm<D>(a);
             T u[D];
 #pragma unroll
-            for (int i = 0; i < D; ++i) u[i] = a[i] / nv;
+            for (int i = 0; i < D; ++i) u[i] = dv(a[i], nv);
             rho = -s * c;
             hh_reflect<D, MC>(A, u);
 #pragma unroll
@@ -204,9 +204,9 @@ __device__ __forceinline__ QRRes orth_givens(const T* W, T* Q, T* R) {        //
 #pragma unroll
         for (int i = D - 1; i >= j + 1; --i) {
             const T ab[2] = {rows[i - 1][j], rows[i][j]};
-            const T rho = safe_norm<2>(ab);
+            const T rho = nrm<2>(ab);
             if (isfin(rho) && rho > T(0)) {
-                const T c = ab[0] / rho, s = ab[1] / rho;
+                const T c = dv(ab[0], rho), s = dv(ab[1], rho);
 #pragma unroll
                 for (int l = 0; l < WD; ++l) {
                     const T ra = rows[i - 1][l], rb = rows[i][l];
@@ -244,24 +244,24 @@ __device__ __forceinline__ T window_Gw(const T* R0) {
     T R[K * K];
     T m = fabs(R0[0]);
 #pragma unroll
-    for (int l = 1; l < K * K; ++l) m = jl_max(m, static_cast<T>(fabs(R0[l])));
+    for (int l = 1; l < K * K; ++l) m = mx(m, static_cast<T>(fabs(R0[l])));
     // T(1e100) is Inf and T(1e-100) is 0 in Float32, so the rescale never fires there (as in the reference).
     bool rescale = false;
     if (sizeof(T) == 8) rescale = (m > T(1e100) || m < T(1e-100)) && isfin(m) && m > T(0);
 #pragma unroll
-    for (int l = 0; l < K * K; ++l) R[l] = rescale ? R0[l] / m : R0[l];
+    for (int l = 0; l < K * K; ++l) R[l] = rescale ? dv(R0[l], m) : R0[l];
     T Ri[K * K];
 #pragma unroll
     for (int l = 0; l < K * K; ++l) Ri[l] = T(0);
 #pragma unroll
     for (int j = 0; j < K; ++j) {
-        Ri[j + j * K] = T(1) / R[j + j * K];
+        Ri[j + j * K] = dv(T(1), R[j + j * K]);
 #pragma unroll
         for (int i = j - 1; i >= 0; --i) {
             T s = T(0);
 #pragma unroll
             for (int l = i + 1; l <= j; ++l) s = s + R[i + l * K] * Ri[l + j * K];
-            Ri[i + j * K] = -s / R[i + i * K];
+            Ri[i + j * K] = dv(-s, R[i + i * K]);
         }
     }
     T a = R[0] * R[0], b = Ri[0] * Ri[0];
@@ -291,7 +291,7 @@ __device__ __forceinline__ T orth_loss(const T* Q) {
             for (int q = 1; q < D; ++q) acc = fma(Q[q + i * D], Q[q + j * D], acc);
             if (i == j) acc = acc - T(1);
             const T a = fabs(acc);
-            m = (i == 0 && j == 0) ? a : jl_max(m, a);
+            m = (i == 0 && j == 0) ? a : mx(m, a);
         }
     return m;
 }

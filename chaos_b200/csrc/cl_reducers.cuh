@@ -61,7 +61,7 @@ struct RQR {
             return;
         }
 #pragma unroll
-        for (int i = 0; i < K; ++i) cs_add(st.sums[i], cl_log(static_cast<double>(R[i + i * K])));
+        for (int i = 0; i < K; ++i) cs_add(st.sums[i], lnr(R[i + i * K]));
         const T G = G_from_Gw<K>(Gw);
         st.n = n;
         st.G_max = jl_max(st.G_max, static_cast<double>(G));
@@ -85,12 +85,12 @@ struct RBenettin {
     template <int D, int K, typename T>
     static __device__ __forceinline__ void step(State<D, K>& st, i64 n, T* W, const RedParams&) {
         if (st.code != 0) return;
-        const T alpha = safe_norm<D>(W);
+        const T alpha = nrm<D>(W);
         if (!(isfin(alpha) && alpha > T(0))) { st.code = 1; st.value = static_cast<double>(alpha); st.step = n; return; }
-        cs_add(st.sum, cl_log(static_cast<double>(alpha)));
+        cs_add(st.sum, lnr(alpha));
         st.n = n;
 #pragma unroll
-        for (int l = 0; l < D * K; ++l) W[l] = W[l] / alpha;
+        for (int l = 0; l < D * K; ++l) W[l] = dv(W[l], alpha);
     }
     template <int D, int K>
     static __device__ __forceinline__ bool failed(const State<D, K>& st) { return st.code != 0; }
@@ -115,18 +115,18 @@ struct RSALI {
     template <int D, int K, typename T>
     static __device__ __forceinline__ void step(State<D, K>& st, i64 n, T* W, const RedParams&) {
         if (st.code != 0) return;
-        const T a1 = safe_norm<D>(W), a2 = safe_norm<D>(W + D);
+        const T a1 = nrm<D>(W), a2 = nrm<D>(W + D);
         if (!pair_norms(st, n, a1, a2)) return;
         T dm[D], dp[D];
 #pragma unroll
         for (int i = 0; i < D; ++i) {
-            const T u1 = W[i] / a1, u2 = W[D + i] / a2;
+            const T u1 = dv(W[i], a1), u2 = dv(W[D + i], a2);
             W[i] = u1; W[D + i] = u2;
             dm[i] = u1 - u2; dp[i] = u1 + u2;
         }
-        cs_add(st.s1, cl_log(static_cast<double>(a1)));
-        cs_add(st.s2, cl_log(static_cast<double>(a2)));
-        st.sali = static_cast<double>(jl_min(safe_norm<D>(dm), safe_norm<D>(dp)));
+        cs_add(st.s1, lnr(a1));
+        cs_add(st.s2, lnr(a2));
+        st.sali = static_cast<double>(jl_min(nrm<D>(dm), nrm<D>(dp)));
         st.n = n;
     }
     template <int D, int K>
@@ -154,7 +154,7 @@ struct RGALI {
         if (st.code != 0) return;
         T a[K];
 #pragma unroll
-        for (int j = 0; j < K; ++j) a[j] = safe_norm<D>(W + j * D);   // _norm_col
+        for (int j = 0; j < K; ++j) a[j] = nrm<D>(W + j * D);   // _norm_col
         bool sali_ok = true;
         if constexpr (WITH_SALI) sali_ok = S.s.code == 0 && pair_norms(S.s, n, a[0], a[1]);
         int bad = 0;
@@ -171,14 +171,14 @@ struct RGALI {
 #pragma unroll
         for (int j = 0; j < K; ++j) {
             CS acc{st.s[j], st.c[j]};
-            cs_add(acc, cl_log(static_cast<double>(a[j])));
+            cs_add(acc, lnr(a[j]));
             st.s[j] = acc.s; st.c[j] = acc.c;
         }
         T Q[D * K];
 #pragma unroll
         for (int j = 0; j < K; ++j)
 #pragma unroll
-            for (int i = 0; i < D; ++i) { const T u = W[i + j * D] / a[j]; W[i + j * D] = u; Q[i + j * D] = u; }
+            for (int i = 0; i < D; ++i) { const T u = dv(W[i + j * D], a[j]); W[i + j * D] = u; Q[i + j * D] = u; }
         if constexpr (WITH_SALI) {
             if (sali_ok) {   // sali.jl:107-110 on the unit columns 1-2
                 T dm[D], dp[D];
@@ -186,7 +186,7 @@ struct RGALI {
                 for (int i = 0; i < D; ++i) { dm[i] = W[i] - W[D + i]; dp[i] = W[i] + W[D + i]; }
                 S.s.s1 = CS{st.s[0], st.c[0]};
                 S.s.s2 = CS{st.s[1], st.c[1]};
-                S.s.sali = static_cast<double>(jl_min(safe_norm<D>(dm), safe_norm<D>(dp)));
+                S.s.sali = static_cast<double>(jl_min(nrm<D>(dm), nrm<D>(dp)));
                 S.s.n = n;
             }
         }
@@ -203,10 +203,10 @@ struct RGALI {
 #pragma unroll
                     for (int i = 0; i < D; ++i) Q[i + j * D] = Q[i + j * D] - cc * Q[i + p * D];
                 }
-            const T r = safe_norm<D>(Q + j * D);
+            const T r = nrm<D>(Q + j * D);
             const T sc = r == T(0) ? T(1) : r;
 #pragma unroll
-            for (int i = 0; i < D; ++i) Q[i + j * D] = Q[i + j * D] / sc;
+            for (int i = 0; i < D; ++i) Q[i + j * D] = dv(Q[i + j * D], sc);
             if (j > 0) { g = g * r; st.gali[j - 1] = static_cast<double>(g); }
         }
         st.n = n;
@@ -239,14 +239,14 @@ struct RMEGNO {
     template <int D, int K, typename T>
     static __device__ __forceinline__ void step(State<D, K>& st, i64 n, T* W, const RedParams&) {
         if (st.code != 0) return;
-        const T a1 = safe_norm<D>(W), a2 = safe_norm<D>(W + D);
+        const T a1 = nrm<D>(W), a2 = nrm<D>(W + D);
         if (!pair_norms(st, n, a1, a2)) return;
-        megno_add(st.c1, cl_log(static_cast<double>(a1)), n);
-        megno_add(st.c2, cl_log(static_cast<double>(a2)), n);
+        megno_add(st.c1, lnr(a1), n);
+        megno_add(st.c2, lnr(a2), n);
         st.n = n; st.K = st.K + 1;
         if (REPLACE) {
 #pragma unroll
-            for (int i = 0; i < D; ++i) { W[i] = W[i] / a1; W[D + i] = W[D + i] / a2; }
+            for (int i = 0; i < D; ++i) { W[i] = dv(W[i], a1); W[D + i] = dv(W[D + i], a2); }
         }
     }
     template <int D, int K>
@@ -264,10 +264,10 @@ struct RFLI {
     template <int D, int K, typename T>
     static __device__ __forceinline__ void step(State<D, K>& st, i64 n, T* W, const RedParams&) {
         if (st.code != 0) return;
-        const T a1 = safe_norm<D>(W), a2 = safe_norm<D>(W + D);
+        const T a1 = nrm<D>(W), a2 = nrm<D>(W + D);
         if (!pair_norms(st, n, a1, a2)) return;
-        cs_add(st.s1, cl_log(static_cast<double>(a1)));
-        cs_add(st.s2, cl_log(static_cast<double>(a2)));
+        cs_add(st.s1, lnr(a1));
+        cs_add(st.s2, lnr(a2));
         const double S1 = cs_total(st.s1), S2 = cs_total(st.s2);   // fli_maxima, fli.jl:187-193
         if (S1 > st.f1) { st.f1 = S1; st.step1 = n; }
         if (S1 > st.fB) { st.fB = S1; st.stepB = n; st.colB = 1; }
@@ -275,7 +275,7 @@ struct RFLI {
         st.n = n;
         if (REPLACE) {
 #pragma unroll
-            for (int i = 0; i < D; ++i) { W[i] = W[i] / a1; W[D + i] = W[D + i] / a2; }
+            for (int i = 0; i < D; ++i) { W[i] = dv(W[i], a1); W[D + i] = dv(W[D + i], a2); }
         }
     }
     template <int D, int K>

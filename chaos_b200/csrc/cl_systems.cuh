@@ -11,6 +11,8 @@
 //   forward(x, J)    the new point, Float64 in every kernel, operation for operation the reference's `forward`.
 #pragma once
 
+#include <type_traits>
+
 #include "cl_math.cuh"
 #include "cl_reducers.cuh"
 
@@ -56,14 +58,33 @@ __device__ __forceinline__ void fused_dense(const double* M, float* W) {   // mi
 
 // ---- StandardMap (standard_map.jl:8-44) and WrappedStandardMap (wrapped_standard_map.jl:12-57) -----------------
 struct StdJac { double s, c; };   // sin x, K cos x at the old x
+struct StdJacF { double s; float c; };   // mixed kernels: sin x in Float64 (orbit), K cos x in Float32 (tangent)
 
 struct SysStandard {
     static constexpr int D = 2, S = 2;
     using Jac = StdJac;
+    template <typename R> using JacR = typename std::conditional<sizeof(R) == 8, StdJac, StdJacF>::type;
     double K;
     __device__ __forceinline__ void jac(const double* x, StdJac& J) const {
         double sn, cs; cl_sincos(x[0], &sn, &cs);
         J.s = sn; J.c = K * cs;
+    }
+    __device__ __forceinline__ void jac(const double* x, StdJacF& J) const {
+        const Reduced w = cl_reduce(x[0]);
+        J.s = cl_sin_split(w);
+        float sf, cf;
+        cl_sincos32(w, &sf, &cf);
+        J.c = static_cast<float>(K) * cf;
+    }
+    template <int KK>
+    __device__ __forceinline__ void apply(const StdJacF& J, float* W) const {
+        const float c = J.c, opc = 1.0f + J.c;
+#pragma unroll
+        for (int j = 0; j < KK; ++j) {
+            const float w0 = W[2 * j], w1 = W[2 * j + 1];
+            W[2 * j] = __fmaf_rn(opc, w0, w1);
+            W[2 * j + 1] = __fmaf_rn(c, w0, w1);
+        }
     }
     // _dt: [[1 + c, 1], [c, 1]]
     template <int KK>
@@ -82,7 +103,8 @@ struct SysStandard {
             W[2 * j + 1] = __fmaf_rn(c, w0, w1);
         }
     }
-    __device__ __forceinline__ void forward(double* x, const StdJac& J) const {
+    template <class JJ>
+    __device__ __forceinline__ void forward(double* x, const JJ& J) const {
         const double p = x[1] + K * J.s;
         x[0] = x[0] + p;
         x[1] = p;
@@ -100,7 +122,8 @@ __device__ __forceinline__ void wrap_reduce(double u, double tp, double& r, doub
 struct SysWrapped : SysStandard {
     static constexpr int S = 4;
     // forward (wrapped_standard_map.jl:30-37) with _checked (:23-28)
-    __device__ __forceinline__ void forward(double* z, const StdJac& J) const {
+    template <class JJ>
+    __device__ __forceinline__ void forward(double* z, const JJ& J) const {
         const double tp = 2 * jl_pi();
         double p, a, x, b;
         wrap_reduce(z[1] + K * J.s, tp, p, a);
@@ -115,11 +138,31 @@ struct SysWrapped : SysStandard {
 
 // ---- FroeschleMap (froeschle_map.jl:9-58) ---------------------------------------------------------------------
 struct FroJac { double x1, x2, s1, s2, c12, a, b, c; };
+struct FroJacF { double x1, x2, s1, s2, c12; float a, b, c; };   // mixed: Float64 orbit terms, Float32 A
 
 struct SysFroeschle {
     static constexpr int D = 4, S = 4;
     using Jac = FroJac;
+    template <typename R> using JacR = typename std::conditional<sizeof(R) == 8, FroJac, FroJacF>::type;
     double nu, kappa, mu;
+    // mixed: sin x1', sin x2', cos(x1' + x2') in Float64 bit-identical to the plain kernel's (the orbit), the
+    // tangent's cos x1', cos x2', sin(x1' + x2') in Float32 from the same reductions
+    __device__ __forceinline__ void jac(const double* z, FroJacF& J) const {
+        J.x1 = z[0] + z[2];
+        J.x2 = z[1] + z[3];
+        const Reduced w1 = cl_reduce(J.x1), w2 = cl_reduce(J.x2), w12 = cl_reduce(J.x1 + J.x2);
+        J.s1 = cl_sin_split(w1);
+        J.s2 = cl_sin_split(w2);
+        J.c12 = cl_cos_split(w12);
+        float s1f, c1f, s2f, c2f, s12f, c12f;
+        cl_sincos32(w1, &s1f, &c1f);
+        cl_sincos32(w2, &s2f, &c2f);
+        cl_sincos32(w12, &s12f, &c12f);
+        const float t = static_cast<float>(mu) * s12f;
+        J.a = -static_cast<float>(nu) * c1f - t;
+        J.b = -t;
+        J.c = -static_cast<float>(kappa) * c2f - t;
+    }
     __device__ __forceinline__ void jac(const double* z, FroJac& J) const {
         J.x1 = z[0] + z[2];
         J.x2 = z[1] + z[3];
@@ -140,8 +183,8 @@ struct SysFroeschle {
         fused_dense<4, KK>(M, W);
     }
     // Float32: top = W_q + W_p, bottom = A (W_q + W_p) + W_p
-    template <int KK>
-    __device__ __forceinline__ void apply(const FroJac& J, float* W) const {
+    template <int KK, class JJ>
+    __device__ __forceinline__ void apply(const JJ& J, float* W) const {
         const float a = static_cast<float>(J.a), b = static_cast<float>(J.b), c = static_cast<float>(J.c);
 #pragma unroll
         for (int j = 0; j < KK; ++j) {
@@ -152,7 +195,8 @@ struct SysFroeschle {
             w[0] = t1; w[1] = t2; w[2] = b1; w[3] = b2;
         }
     }
-    __device__ __forceinline__ void forward(double* z, const FroJac& J) const {   // :20-25
+    template <class JJ>
+    __device__ __forceinline__ void forward(double* z, const JJ& J) const {   // :20-25
         const double f = mu * (1.0 - J.c12);
         const double p1 = z[2] - nu * J.s1 - f;
         const double p2 = z[3] - kappa * J.s2 - f;
@@ -166,6 +210,7 @@ struct SysLinear {
     static constexpr int D = DD, S = DD;
     double A[D * D];   // the d x d matrix (column-major), passed by value: kernel-parameter (constant bank) loads
     struct Jac {};
+    template <typename R> using JacR = Jac;
     __device__ __forceinline__ void jac(const double*, Jac&) const {}
     template <int KK, typename T>
     __device__ __forceinline__ void apply(const Jac&, T* W) const { fused_dense<D, KK>(A, W); }
@@ -184,42 +229,93 @@ struct SysLinear {
 };
 
 // ---- StandardMapChain with the banded ChainTangent (standard_map_chain.jl, chain_tangent.jl) -------------------
+// Neighbours are compile-time per boundary (the ring flag is uniform over a launch, so the branch on it costs
+// nothing and every index stays static, keeping the frame in registers). Each bond (j, j+1) is evaluated once:
+// sin(q_j - q_j+1) = -sin(q_j+1 - q_j) and cos(q_j - q_j+1) = cos(q_j+1 - q_j) hold bitwise for the portable
+// functions (the reduction and both polynomials are odd / even in the argument, and q_j+1 - q_j = -(q_j - q_j+1)
+// exactly); the only difference, the sign of a zero sine, is erased by `_force`'s 0 + s (standard_map_chain.jl:166).
 template <int NS>
 struct ChainJac { double g[NS], gl[NS], gr[NS], sq[NS], sl[NS], sr[NS]; };
+template <int NS>
+struct ChainJacF { float g[NS], gl[NS], gr[NS]; double sq[NS], sl[NS], sr[NS]; };
 
 template <int NS>
 struct SysChain {
     static constexpr int D = 2 * NS, S = 2 * NS;
     using Jac = ChainJac<NS>;
+    template <typename R> using JacR = typename std::conditional<sizeof(R) == 8, ChainJac<NS>, ChainJacF<NS>>::type;
     double K, eps;
     int ring;
-    __device__ __forceinline__ int left(int j) const { return j > 0 ? j - 1 : (ring ? NS - 1 : -1); }
-    __device__ __forceinline__ int right(int j) const { return j < NS - 1 ? j + 1 : (ring ? 0 : -1); }
-    // _chain_tangent (chain_tangent.jl:84-91) at the old positions, and the sines `_force` needs (:164-170)
-    __device__ __forceinline__ void jac(const double* z, ChainJac<NS>& J) const {
+    template <bool RING> static __device__ __forceinline__ constexpr int L(int j) { return j > 0 ? j - 1 : (RING ? NS - 1 : -1); }
+    template <bool RING> static __device__ __forceinline__ constexpr int R(int j) { return j < NS - 1 ? j + 1 : (RING ? 0 : -1); }
+
+    // _chain_tangent (chain_tangent.jl:84-91) at the old positions and the sines `_force` needs (:164-170).
+    template <bool RING, class JJ>
+    __device__ __forceinline__ void jac_impl(const double* z, JJ& J) const {
+        constexpr bool F32 = sizeof(J.g[0]) == 4;
+        double sb[NS], cb[NS];     // bond j: q_j - q_R(j), Float64 sine (orbit), cosine in the tangent's type
+        float cbf[NS];
 #pragma unroll
         for (int j = 0; j < NS; ++j) {
-            const int kl = left(j), kr = right(j);
-            double sq, cq; cl_sincos(z[j], &sq, &cq);
-            double sl = 0.0, cl_ = 0.0, sr = 0.0, cr = 0.0;
-            if (kl >= 0) { double s_, c_; cl_sincos(z[j] - z[kl], &s_, &c_); sl = s_; cl_ = eps * c_; }
-            if (kr >= 0) { double s_, c_; cl_sincos(z[j] - z[kr], &s_, &c_); sr = s_; cr = eps * c_; }
-            J.g[j] = (K * cq + cl_) + cr;
-            J.gl[j] = -cl_;
-            J.gr[j] = -cr;
+            if (R<RING>(j) < 0) continue;
+            const double y = z[j] - z[R<RING>(j)];
+            if constexpr (F32) {
+                const Reduced w = cl_reduce(y);
+                sb[j] = cl_sin_split(w);
+                float sf; cl_sincos32(w, &sf, &cbf[j]);
+                cb[j] = 0.0;
+            } else {
+                cl_sincos(y, &sb[j], &cb[j]);
+                cbf[j] = 0.0f;
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < NS; ++j) {
+            const int kl = L<RING>(j), kr = R<RING>(j);
+            double sq, cq = 0.0;
+            float cqf = 0.0f;
+            if constexpr (F32) {
+                const Reduced w = cl_reduce(z[j]);
+                sq = cl_sin_split(w);
+                float sf; cl_sincos32(w, &sf, &cqf);
+            } else {
+                cl_sincos(z[j], &sq, &cq);
+            }
+            // left neighbour kl = j - 1 (or N - 1 for j = 0 on a ring): bond kl, sine negated
+            const double sl = kl >= 0 ? -sb[kl] : 0.0;
+            const double sr = kr >= 0 ? sb[j] : 0.0;
             J.sq[j] = sq; J.sl[j] = sl; J.sr[j] = sr;
+            if constexpr (F32) {
+                const float e = static_cast<float>(eps);
+                const float cl_ = kl >= 0 ? e * cbf[kl] : 0.0f, cr = kr >= 0 ? e * cbf[j] : 0.0f;
+                J.g[j] = (static_cast<float>(K) * cqf + cl_) + cr;
+                J.gl[j] = -cl_;
+                J.gr[j] = -cr;
+            } else {
+                const double cl_ = kl >= 0 ? eps * cb[kl] : 0.0, cr = kr >= 0 ? eps * cb[j] : 0.0;
+                J.g[j] = (K * cq + cl_) + cr;
+                J.gl[j] = -cl_;
+                J.gr[j] = -cr;
+            }
         }
     }
+    template <class JJ>
+    __device__ __forceinline__ void jac(const double* z, JJ& J) const {
+        if (ring) jac_impl<true>(z, J); else jac_impl<false>(z, J);
+    }
+
     // `ChainTangent * W`: GW = _band(W_q); top = (W_q + GW) + W_p, bottom = GW + W_p (chain_tangent.jl:62-78)
-    template <int KK, typename T>
-    __device__ __forceinline__ void apply(const ChainJac<NS>& J, T* W) const {
+    template <bool RING, int KK, class JJ, typename T>
+    __device__ __forceinline__ void apply_impl(const JJ& J, T* W) const {
 #pragma unroll
         for (int col = 0; col < KK; ++col) {
             T* Wq = W + col * D;
             T v[NS];
 #pragma unroll
             for (int j = 0; j < NS; ++j) {
-                const int kl = left(j), kr = right(j);
+                constexpr int dummy = 0;
+                (void)dummy;
+                const int kl = L<RING>(j), kr = R<RING>(j);
                 T t = static_cast<T>(J.g[j]) * Wq[j];
                 if (kl >= 0) t = t + static_cast<T>(J.gl[j]) * Wq[kl];
                 if (kr >= 0) t = t + static_cast<T>(J.gr[j]) * Wq[kr];
@@ -233,18 +329,28 @@ struct SysChain {
             }
         }
     }
-    // forward: p_j' = p_j + (K sin q_j + eps s_j), s_j = 0 + sin(q_j - q_left) + sin(q_j - q_right); q_j' = q_j + p_j'
-    __device__ __forceinline__ void forward(double* z, const ChainJac<NS>& J) const {
+    template <int KK, class JJ, typename T>
+    __device__ __forceinline__ void apply(const JJ& J, T* W) const {
+        if (ring) apply_impl<true, KK>(J, W); else apply_impl<false, KK>(J, W);
+    }
+
+    // forward: p_j' = p_j + (K sin q_j + eps s_j), s_j = (0 + sin(q_j - q_left)) + sin(q_j - q_right); q_j' = q_j + p_j'
+    template <bool RING, class JJ>
+    __device__ __forceinline__ void forward_impl(double* z, const JJ& J) const {
         double p[NS];
 #pragma unroll
         for (int j = 0; j < NS; ++j) {
             double s = 0.0;
-            if (left(j) >= 0) s = s + J.sl[j];
-            if (right(j) >= 0) s = s + J.sr[j];
+            if (L<RING>(j) >= 0) s = s + J.sl[j];
+            if (R<RING>(j) >= 0) s = s + J.sr[j];
             p[j] = z[NS + j] + (K * J.sq[j] + eps * s);
         }
 #pragma unroll
         for (int j = 0; j < NS; ++j) { z[j] = z[j] + p[j]; z[NS + j] = p[j]; }
+    }
+    template <class JJ>
+    __device__ __forceinline__ void forward(double* z, const JJ& J) const {
+        if (ring) forward_impl<true>(z, J); else forward_impl<false>(z, J);
     }
 };
 

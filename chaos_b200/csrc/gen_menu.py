@@ -117,6 +117,26 @@ def menu():
     return groups
 
 
+# The batched uneven ensemble: (system kind, d, precision, k, chain, tau unrolled in the variants).
+ENSEMBLE = [(SYS_STANDARD, 2, p, 2, ["QR4"], 5) for p in (0, 1)] + \
+           [(SYS_CHAIN, 4, p, 4, ["QR4"], 10) for p in (0, 1)] + \
+           [(SYS_CHAIN, 8, p, 8, ["QR4"], 10) for p in (0, 1)] + \
+           [(SYS_CHAIN, 16, p, 8, ["QR4"], 20) for p in (0, 1)]
+
+
+def render_ensemble(entries):
+    out = ['// Generated by chaos_b200/csrc/gen_menu.py (do not edit): ensemble kernel instances.',
+           '#include "cl_ensemble.cuh"', '', 'namespace cl {', 'namespace {']
+    for idx, (kind, d, prec, k, ch, U) in enumerate(entries):
+        real = "double" if prec == 0 else "float"
+        ft = f"Frame<{k}{''.join(', ' + t for t in red_type(ch))}>"
+        out.append(f"cudaError_t E{idx}(const cl_run& r, const EArgs& a, int g, const ETune& t, cudaStream_t s, LaunchInfo* i) {{\n"
+                   f"    return launch_ensemble<{sys_type(kind, d)}, {real}, {ft}, {U}>(r, a, g, t, s, i);\n}}\n"
+                   f"const ERegistrar R{idx}(\"{key(kind, d, prec, [(k, ch)])}\", E{idx});")
+    out += ['}  // namespace', '}  // namespace cl', '']
+    return "\n".join(out)
+
+
 HEADER = """// Generated by chaos_b200/csrc/gen_menu.py (do not edit): compiled orbit-kernel instances, group "{group}".
 #include "cl_registry.cuh"
 {extra}
@@ -151,8 +171,15 @@ def main():
             with open(path, "w") as f:
                 f.write(text)
         written.append(path)
+    for prec in (0, 1):
+        path = os.path.join(HERE, f"cl_ens_menu_p{prec}.cu")
+        text = render_ensemble([e for e in ENSEMBLE if e[2] == prec])
+        if (open(path).read() if os.path.exists(path) else None) != text:
+            with open(path, "w") as f:
+                f.write(text)
+        written.append(path)
     for fn in os.listdir(HERE):   # drop stale groups
-        if fn.startswith("cl_menu_") and fn.endswith(".cu") and os.path.join(HERE, fn) not in written:
+        if fn.startswith(("cl_menu_", "cl_ens_menu_")) and fn.endswith(".cu") and os.path.join(HERE, fn) not in written:
             os.remove(os.path.join(HERE, fn))
     return written
 

@@ -209,6 +209,44 @@ CL_API const char* cl_b200_version(void);
 /* Number of orbit-kernel launches since the library was loaded (a device-launch counter for audits). */
 CL_API int64_t cl_b200_launch_count(void);
 
+/* ---- Batched uneven ensembles ------------------------------------------------------------------------------------
+ * One class = orbits of one system kind and dimension with one frame and chain; every orbit may carry its own map
+ * parameter K (K[i]), its own length N[i] (a multiple of tau) and an escape stop: at the first handoff where
+ * max_j |p_j| > escape the orbit stops with code 4 (STATUS_ESCAPED) and its records are those of the reference call
+ * `propagate_orbit(sys(K[i]), x0[i], W0[i], N', tau, reducers)` with N' that handoff (src/Tangent/orbit.jl:85-99).
+ * The reference has one N, one system and no escape per call, so an ensemble is the set of such calls. Orbits are
+ * taken from a device work queue in `order` (longest first balances the load) by persistent kernels, one per class,
+ * all classes concurrently. Buffers are orbit-major (frame 0 of each class's cl_buffers). */
+typedef struct cl_ensemble_class {
+    cl_run run;            /* system, d, s, tau, one frame, precision; run.N is the length when N is NULL      */
+    int64_t n_orbits;
+    const int64_t* order;  /* queue: n_orbits orbit indices (NULL: 0..n-1)                                     */
+    const double* K;       /* per-orbit K (NULL: run.sys.K); standard maps and chains                          */
+    const int64_t* N;      /* per-orbit lengths, multiples of tau, each <= run.N (NULL: run.N)                 */
+    double escape;         /* momentum bound of the escape stop; <= 0 disables it                              */
+    int32_t minb;          /* kernel variant: register cap as blocks per SM (1, 2 or 4); 0 = tuned/default     */
+    int32_t unroll;        /* kernel variant: tau loop unrolled (tau itself, when tau is 5, 10 or 20) or 1; 0 = tuned/default */
+    cl_buffers buf;        /* frame 0 only                                                                      */
+} cl_ensemble_class;
+
+/* Run the classes on device buffers, enqueued on `stream`; the queue heads are allocated and freed in stream
+ * order (cudaMallocAsync). No reference counterpart (see above). */
+CL_API int cl_b200_ensemble_device(const cl_ensemble_class* classes, int32_t n_classes, void* stream);
+
+/* The same on host buffers: copies in, runs, copies out (synchronous). */
+CL_API int cl_b200_ensemble(const cl_ensemble_class* classes, int32_t n_classes, cl_prov* prov);
+
+/* Autotune one class on its device buffers: times every kernel variant on a sample of the queue (at most
+ * `sample_orbits` orbits, `sample_steps` steps each) and writes the fastest (minb, unroll) into the class.
+ * The buffers' contents are overwritten. */
+CL_API int cl_b200_ensemble_tune(cl_ensemble_class* cls, int64_t sample_orbits, int64_t sample_steps, void* stream);
+
+/* Capture the classes' launches (queue resets included) into one CUDA graph on device buffers; launching the
+ * graph replays the whole ensemble. The graph owns its queue heads until destroyed. */
+CL_API int cl_b200_ensemble_graph_create(const cl_ensemble_class* classes, int32_t n_classes, void** graph);
+CL_API int cl_b200_ensemble_graph_launch(void* graph, void* stream);
+CL_API int cl_b200_ensemble_graph_destroy(void* graph);
+
 /* The compiled menu: number of kernel instances, and the key of instance i (NULL outside 0..size-1). A key reads
  * "s<system kind>d<d>p<precision>|k<k>:<reducer>,...|..." with reducers QR<alg>, BEN, SALI, GALI, MEGNO<replace>,
  * FLI<replace>, one "|"-terminated group per frame. No reference counterpart (Julia compiles on demand). */

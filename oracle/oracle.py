@@ -51,6 +51,9 @@ def lib() -> C.CDLL:
         L.oracle_seeded_frame.argtypes = [C.c_uint64, C.c_int64, C.c_int32, C.c_int32, dp]
         L.oracle_gauss3_step.argtypes = [dp, C.c_double, C.c_int32, C.c_double, dp]
         L.oracle_max_threads.restype = C.c_int32
+        L.oracle_ensemble.argtypes = [P(_abi.cl_run), C.c_int64, P(_abi.cl_buffers), dp, P(C.c_int64), C.c_double,
+                                      C.c_int32, C.c_int32]
+        L.oracle_ensemble.restype = C.c_int
         _lib = L
     return _lib
 
@@ -147,3 +150,33 @@ def oracle_frames(sys, x0, N, frames: list[FrameSpec], *, tau=1, seed=0, math="p
         done += run.steps
     return [dict(x=x, W=Ws[f].transpose(0, 2, 1), states=sts[f], code=codes[f], hstep=hs[f])
             for f in range(len(frames))]
+
+
+def oracle_ensemble(sys, x0, N, frame: FrameSpec, *, tau, K=None, lengths=None, escape=0.0, seed=0,
+                    math="portable", threads=0):
+    """One ensemble class on the oracle: per-orbit K and lengths, escape bound (see oracle_capi.cpp)."""
+    x0 = np.ascontiguousarray(np.asarray(x0, dtype=np.float64))
+    n, s = x0.shape
+    d = sys.d
+    run = build_run(sys, N, tau, [frame], "fp64", seed)
+    x = np.empty((n, s))
+    W0 = None if frame.W0 is None else np.ascontiguousarray(np.asarray(frame.W0, dtype=np.float64).transpose(0, 2, 1))
+    W = np.empty((n, frame.k, d))
+    dt = chain_dtype(tuple(frame.reducers), d, frame.k)
+    st = np.zeros(n, dtype=dt) if dt.itemsize else None
+    code = np.zeros(n, dtype=np.int8)
+    hs = np.zeros(n, dtype=np.int64)
+    b = _abi.cl_buffers()
+    b.x0, b.x = x0.ctypes.data, x.ctypes.data
+    b.W0[0] = None if W0 is None else W0.ctypes.data
+    b.W[0] = W.ctypes.data
+    b.states[0] = None if st is None else st.ctypes.data
+    b.code[0], b.hstep[0] = code.ctypes.data, hs.ctypes.data
+    Kc = None if K is None else np.ascontiguousarray(K, dtype=np.float64)
+    Nc = None if lengths is None else np.ascontiguousarray(lengths, dtype=np.int64)
+    rc = lib().oracle_ensemble(C.byref(run), n, C.byref(b), None if Kc is None else _dp(Kc),
+                               None if Nc is None else Nc.ctypes.data_as(C.POINTER(C.c_int64)), float(escape),
+                               MATH[math], threads)
+    if rc != 0:
+        raise ValueError(f"oracle_ensemble returned {rc}")
+    return dict(x=x, W=W.transpose(0, 2, 1), states=st, code=code, hstep=hs)

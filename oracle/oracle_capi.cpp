@@ -34,8 +34,23 @@ int8_t status_of(const double* x, int s, const double* W, int dk) {
     return STATUS_OK;
 }
 
+constexpr int8_t STATUS_ESCAPED = 4;
+
+// max_j |p_j| over the momenta (second half of the state; (x, p) for the standard map)
+double max_abs_p(const double* x, int d) {
+    double m = std::fabs(x[d / 2]);
+    for (int j = d / 2 + 1; j < d; ++j) m = std::fmax(m, std::fabs(x[j]));
+    return m;
+}
+
+// One orbit. Ensembles pass a per-orbit K (Kp), length (Np) and the escape bound: the orbit then stops after the
+// first handoff at which max |p_j| > escape with code 4, its records those of the run with N = that handoff.
 template <int MM>
-void run_orbit(const cl_run& run, int64_t i, const cl_buffers& b) {
+void run_orbit(const cl_run& run0, int64_t i, const cl_buffers& b, const double* Kp = nullptr,
+               const int64_t* Np = nullptr, double escape = 0.0) {
+    cl_run run = run0;
+    if (Kp) run.sys.K = Kp[i];
+    if (Np) { run.N = Np[i]; run.steps = 0; }
     const int d = run.d, s = run.s, nf = run.n_frames;
     const int64_t n0 = run.n0;
     const int64_t steps = run.steps > 0 ? run.steps : run.N - n0;
@@ -84,6 +99,7 @@ void run_orbit(const cl_run& run, int64_t i, const cl_buffers& b) {
     Chain<MM> chain{run.sys.n_sites, run.sys.K, run.sys.eps, run.sys.ring != 0};
     Gauss3 gauss(run.sys.gauss_maxiter, run.sys.gauss_tol);
     int64_t n = n0;
+    bool escaped = false;
     const int tau = run.tau;
     const int64_t handoffs = steps / tau;
     for (int64_t h = 0; h < handoffs; ++h) {
@@ -142,10 +158,12 @@ void run_orbit(const cl_run& run, int64_t i, const cl_buffers& b) {
             still = true;
         }
         if (!still) break;
+        if (escape > 0.0 && max_abs_p(x, d) > escape) { escaped = true; break; }
     }
     for (int f = 0; f < nf; ++f) {
-        if (alive[f]) {   // orbit.jl:58: the final status check runs only at step N
-            code[f] = n == run.N ? status_of(x, s, W[f], d * run.frames[f].k) : STATUS_OK;
+        if (alive[f]) {   // orbit.jl:58: the final status check runs only at step N (here: N or the escape handoff)
+            const int8_t c = status_of(x, s, W[f], d * run.frames[f].k);
+            code[f] = escaped ? (c == STATUS_OK ? STATUS_ESCAPED : c) : (n == run.N ? c : STATUS_OK);
             hstep[f] = n;
         }
     }
@@ -185,6 +203,30 @@ int oracle_propagate(const cl_run* run, int64_t n, const cl_buffers* b, int32_t 
             for (int64_t i = lo; i < hi; ++i) {
                 if (math_mode == MATH_LIBM) run_orbit<MATH_LIBM>(*run, i, *b);
                 else run_orbit<MATH_PORTABLE>(*run, i, *b);
+            }
+        }
+    };
+    std::vector<std::thread> pool;
+    for (int t = 1; t < nt; ++t) pool.emplace_back(worker);
+    worker();
+    for (auto& th : pool) th.join();
+    return 0;
+}
+
+// A batched uneven ensemble class (one frame): per-orbit K (may be NULL), lengths (may be NULL), escape bound.
+int oracle_ensemble(const cl_run* run, int64_t n, const cl_buffers* b, const double* K, const int64_t* N,
+                    double escape, int32_t math_mode, int32_t threads) {
+    if (run->n_frames != 1 || run->n0 != 0) return CL_EINVAL;
+    const int hw = static_cast<int>(std::max(1u, std::thread::hardware_concurrency()));
+    const int nt = static_cast<int>(std::min<int64_t>(threads > 0 ? threads : hw, std::max<int64_t>(n, 1)));
+    std::atomic<int64_t> next{0};
+    auto worker = [&]() {
+        for (;;) {
+            const int64_t lo = next.fetch_add(4);
+            if (lo >= n) return;
+            for (int64_t i = lo; i < std::min<int64_t>(lo + 4, n); ++i) {
+                if (math_mode == MATH_LIBM) run_orbit<MATH_LIBM>(*run, i, *b, K, N, escape);
+                else run_orbit<MATH_PORTABLE>(*run, i, *b, K, N, escape);
             }
         }
     };
