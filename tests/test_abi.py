@@ -65,6 +65,7 @@ def _run_from_key(key: str) -> _abi.cl_run:
     r.sys.kind = kind
     r.sys.n_sites = d // 2
     r.sys.gauss_maxiter = 50
+    r.sys.dt = 0.01
     for f, grp in enumerate(g for g in rest.split("|") if g):
         k, toks = grp.split(":")
         r.frames[f].k = int(k[1:])

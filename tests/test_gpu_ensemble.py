@@ -33,13 +33,15 @@ def _oracle(oracle, c):
 
 
 @pytest.mark.parametrize("d,tau", [(2, 5), (4, 10), (8, 10), (16, 20)])
-def test_ensemble_class_bitwise(oracle, d, tau):
-    c = _class(d, 300, tau, 100 + d)
+@pytest.mark.parametrize("escape", [1e3, 25.0])
+def test_ensemble_class_bitwise(oracle, d, tau, escape):
+    c = _class(d, 300, tau, 100 + d, escape=escape)
     dev = propagate_ensemble([c])[0]
     ref = _oracle(oracle, c)
     assert np.array_equal(dev.code, ref["code"]) and np.array_equal(dev.hstep, ref["hstep"])
     assert same_bits(dev.x, ref["x"]) and same_bits(dev.W, ref["W"]) and states_equal(dev.states, ref["states"])
-    assert (dev.code == 4).any() or d > 2   # K up to 3 escapes some standard-map orbits past |p| = 1e3
+    if escape == 25.0 and d == 2:
+        assert (dev.code == 4).any()   # a low bound: some standard-map orbits escape within a few thousand steps
 
 
 def test_ensemble_all_classes_concurrently(oracle):

@@ -250,3 +250,25 @@ def test_gauss3_order_and_symplecticity(oracle):
     _, T = oracle.gauss3_step(z0, 0.01, 50, 1e-14)
     J = np.block([[np.zeros((2, 2)), np.eye(2)], [-np.eye(2), np.zeros((2, 2))]])
     assert np.max(np.abs(T.T @ J @ T - J)) <= 1e-13
+
+
+def test_ensemble_orbit_is_a_reference_call(oracle):
+    """Each orbit of a batched uneven ensemble equals the reference call propagate_orbit(sys(K_i), x0_i, W0_i, N_i')
+    with N_i' its own length, or the escape handoff (code 4) when max |p| passes the bound first."""
+    rng = np.random.default_rng(3)
+    n, tau = 40, 5
+    x0 = uniform_starts(n, 2, 12)
+    K = rng.uniform(0.5, 3.0, n)
+    L = (rng.integers(1, 400, n) * tau).astype(np.int64)
+    W0 = identity_frames(n, 2, 2)
+    fr = FrameSpec(2, (QRSpectrum(HouseholderQR()),), W0)
+    ens = oracle.oracle_ensemble(StandardMap(1.0), x0, int(L.max()), fr, tau=tau, K=K, lengths=L, escape=50.0)
+    assert (ens["code"] == 4).any() and (ens["code"] == 0).any()
+    for i in range(n):
+        Ni = int(ens["hstep"][i])
+        assert Ni == L[i] or ens["code"][i] == 4
+        one = _one(oracle, StandardMap(float(K[i])), x0[i], Ni, 2, (QRSpectrum(HouseholderQR()),), W0[i:i + 1], tau=tau)
+        assert same_bits(one["W"][0], ens["W"][i]) and same_bits(one["x"][0], ens["x"][i])
+        assert states_equal(one["states"][:1], ens["states"][i:i + 1])
+        if ens["code"][i] == 4:
+            assert np.max(np.abs(ens["x"][i][1:])) > 50.0
