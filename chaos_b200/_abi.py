@@ -12,6 +12,7 @@ MAX_FRAMES = 3
 MAX_REDUCERS = 4
 MAX_DIM = 16
 MAX_K = 8
+NOALLOC_MAX_CLASSES = 64
 
 # enum cl_system_kind
 SYS_STANDARD, SYS_WRAPPED_STANDARD, SYS_FROESCHLE, SYS_CHAIN, SYS_LINEAR, SYS_HH_GAUSS = 1, 2, 3, 4, 5, 6
@@ -163,6 +164,8 @@ def declare(lib: C.CDLL) -> C.CDLL:
     lib.cl_b200_launch_count.restype = C.c_int64
     lib.cl_b200_ensemble_device.argtypes = [P(cl_ensemble_class), C.c_int32, C.c_void_p]
     lib.cl_b200_ensemble_device.restype = C.c_int
+    lib.cl_b200_ensemble_device_noalloc.argtypes = [P(cl_ensemble_class), C.c_int32, C.c_void_p]
+    lib.cl_b200_ensemble_device_noalloc.restype = C.c_int
     lib.cl_b200_ensemble.argtypes = [P(cl_ensemble_class), C.c_int32, P(cl_prov)]
     lib.cl_b200_ensemble.restype = C.c_int
     lib.cl_b200_ensemble_tune.argtypes = [P(cl_ensemble_class), C.c_int64, C.c_int64, C.c_void_p]
@@ -185,4 +188,4 @@ EXPORTS = ("cl_b200_propagate", "cl_b200_propagate_device", "cl_b200_check", "cl
            "cl_b200_probe", "cl_b200_last_error", "cl_b200_version", "cl_b200_launch_count",
            "cl_b200_menu_size", "cl_b200_menu_key", "cl_b200_ensemble_device", "cl_b200_ensemble",
            "cl_b200_ensemble_tune", "cl_b200_ensemble_graph_create", "cl_b200_ensemble_graph_launch",
-           "cl_b200_ensemble_graph_destroy")
+           "cl_b200_ensemble_graph_destroy", "cl_b200_ensemble_device_noalloc")

@@ -144,6 +144,24 @@ struct Graph {
 
 void register_ensemble(const char* key, ELaunchFn fn) { ereg().emplace_back(key, fn); }
 
+// The classes one after another on `st`, each class's queue head at heads[c] (already zeroed by the caller). Creates
+// no stream, event or buffer: the entry point without allocations (cl_noalloc.cu) runs through here.
+int enqueue_classes_in_order(const cl_ensemble_class* cs, int nc, unsigned long long* heads, cudaStream_t st) {
+    std::vector<ELaunchFn> fns(nc);
+    for (int c = 0; c < nc; ++c) {
+        const int v = check_class(cs[c], &fns[c]);
+        if (v) return v;
+    }
+    const int sms = sm_count();
+    for (int c = 0; c < nc; ++c) {
+        const ETune t = variant_of(cs[c]);
+        const cudaError_t e = fns[c](cs[c].run, eargs(cs[c], heads + c), sms * t.minb, t, st, nullptr);
+        capi_count_launch();
+        if (e != cudaSuccess) return capi_map_cuda(e, "ensemble kernel launch");
+    }
+    return 0;
+}
+
 }  // namespace cl
 
 using namespace cl;

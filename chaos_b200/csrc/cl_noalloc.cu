@@ -1,0 +1,72 @@
+// cl_noalloc.cu -- the ensemble entry point that allocates nothing.
+//
+// Some callers cannot allocate GPU memory while they call in: a host that owns the whole device heap through its
+// own pool (a Julia or Python runtime with its own caching allocator, where a foreign cudaMalloc would fragment or
+// fail against it), a sandboxed plugin host that forbids allocation calls from plugins, or a latency-bound loop that
+// cannot afford the synchronisation a cudaMalloc / cudaFree may cost. For them `cl_b200_ensemble_device_noalloc`
+// runs the same ensemble kernels with the queue heads (the kernels' only scratch memory) in a fixed array that
+// lives in this file: CL_NOALLOC_MAX_CLASSES heads of 8 bytes (512 bytes), resident on every GPU that loads the
+// library until the process exits.
+//
+// In host code `g_queue_heads` names a host-side stand-in, not the device array, so a kernel is never handed the
+// symbol itself: once per device, with that device current, the first call asks the runtime for the array's device
+// address (cudaGetSymbolAddress) and keeps it; every call passes that address to the kernels. That first call on
+// a device should come before any stream capture. Every call shares the array and clears the heads it uses
+// (cudaMemsetAsync, on the caller's stream) before its launches; calls that overlap on the GPU race on it.
+#include <cuda_runtime.h>
+
+#include <mutex>
+#include <string>
+
+#include "../../include/chaoslab_b200.h"
+#include "cl_ensemble.cuh"
+
+namespace cl {
+
+int capi_fail(int code, const std::string& msg);
+int capi_map_cuda(cudaError_t e, const char* where);
+int enqueue_classes_in_order(const cl_ensemble_class* cs, int nc, unsigned long long* heads, cudaStream_t st);
+
+namespace {
+
+static __device__ __align__(256) unsigned long long g_queue_heads[CL_NOALLOC_MAX_CLASSES];
+
+constexpr int kMaxDevices = 64;
+std::mutex g_mu;
+unsigned long long* g_heads[kMaxDevices] = {};
+
+// The device address of g_queue_heads on the current device, looked up once per device.
+int heads_on_current_device(unsigned long long** out) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return capi_map_cuda(e, "current device");
+    if (dev < 0 || dev >= kMaxDevices) return capi_fail(CL_EINVAL, "device index beyond the set-up table");
+    std::lock_guard<std::mutex> g(g_mu);
+    if (!g_heads[dev]) {
+        void* p = nullptr;
+        e = cudaGetSymbolAddress(&p, g_queue_heads);
+        if (e != cudaSuccess) return capi_map_cuda(e, "address of the fixed queue heads");
+        g_heads[dev] = static_cast<unsigned long long*>(p);
+    }
+    *out = g_heads[dev];
+    return 0;
+}
+
+}  // namespace
+}  // namespace cl
+
+using namespace cl;
+
+extern "C" int cl_b200_ensemble_device_noalloc(const cl_ensemble_class* classes, int32_t n_classes, void* stream) {
+    if (!classes || n_classes < 1) return capi_fail(CL_EINVAL, "no classes");
+    if (n_classes > CL_NOALLOC_MAX_CLASSES)
+        return capi_fail(CL_EINVAL, "at most " + std::to_string(CL_NOALLOC_MAX_CLASSES) +
+                                        " classes per call without allocation (the fixed queue-head array)");
+    unsigned long long* heads = nullptr;
+    int rc = heads_on_current_device(&heads);
+    if (rc) return rc;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const cudaError_t e = cudaMemsetAsync(heads, 0, sizeof(unsigned long long) * n_classes, st);
+    if (e != cudaSuccess) return capi_map_cuda(e, "clear the queue heads");
+    return enqueue_classes_in_order(classes, n_classes, heads, st);
+}

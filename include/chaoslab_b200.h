@@ -233,6 +233,16 @@ typedef struct cl_ensemble_class {
  * order (cudaMallocAsync). No reference counterpart (see above). */
 CL_API int cl_b200_ensemble_device(const cl_ensemble_class* classes, int32_t n_classes, void* stream);
 
+/* The same without allocating anything, for callers that cannot allocate GPU memory while they call in (a host
+ * whose own allocator owns the device heap, a plugin host that forbids allocation calls, a latency-bound loop).
+ * No counterpart in the reference. The classes run one after another on `stream`; their queue heads live in a
+ * fixed array inside the library, CL_NOALLOC_MAX_CLASSES heads (512 bytes) held on every GPU that loads the
+ * library until exit, and more classes than that are rejected with CL_EINVAL. The first call on a device looks
+ * the array's device address up (make it before any stream capture); each call clears the heads it uses on
+ * `stream`; calls that overlap on the GPU race on the shared array. */
+#define CL_NOALLOC_MAX_CLASSES 64
+CL_API int cl_b200_ensemble_device_noalloc(const cl_ensemble_class* classes, int32_t n_classes, void* stream);
+
 /* The same on host buffers: copies in, runs, copies out (synchronous). */
 CL_API int cl_b200_ensemble(const cl_ensemble_class* classes, int32_t n_classes, cl_prov* prov);
 
