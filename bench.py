@@ -228,8 +228,16 @@ def main() -> None:
     stream = torch.cuda.current_stream(dev)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)   # 256 MB > L2
 
+    tuned = {}
+
     def timed(precision: str, steps: int, warmup: int, sampler=None):
         r, cb = run_for(precision)
+        # the autotuner picks the register budget (resident blocks per SM) of this instance on a 2000-step sample
+        mb = C.c_int32(0)
+        rc = L.cl_b200_tune(C.byref(r), n, C.byref(cb), 1, 2000, C.c_void_p(stream.cuda_stream), C.byref(mb))
+        if rc != 0:
+            raise RuntimeError(f"cl_b200_tune: {rc} {last_error()}")
+        tuned[precision] = int(mb.value)
         for _ in range(warmup):
             rc = L.cl_b200_propagate_device(C.byref(r), n, C.byref(cb), 1, C.c_void_p(stream.cuda_stream))
             if rc != 0:
@@ -337,7 +345,8 @@ def main() -> None:
             dtype="f64 orbit + f32 frames", data="synthetic",
             config=dict(workload="froeschle-4d-65536x1e5-tau10-qr-householder+gali4+sali", orbits_per_gpu=n, N=N,
                         tau=TAU, frames="QRSpectrum(HouseholderQR) k=4 | GALI_4+SALI k=4", W0="I",
-                        l2="flushed between timed steps (256 MB write)", parallelism=f"dp{world} (orbit shards)"),
+                        l2="flushed between timed steps (256 MB write)", parallelism=f"dp{world} (orbit shards)",
+                        tuned_blocks_per_sm=tuned),
             fp64_kernel=dict(value=value64, ms_per_step=t64 / args.steps, mixed_over_fp64=value / value64,
                              max_abs_dlambda1=dl1, roofline_tflops=achieved64, frac_of_fp64_peak=achieved64 / fp64_peak),
             e2e=dict(value=e2e_value, unit="orbit-steps/s", h2d_bytes_per_step=int(h2d), d2h_bytes_per_step=int(d2h)),

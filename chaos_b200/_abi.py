@@ -150,6 +150,9 @@ def declare(lib: C.CDLL) -> C.CDLL:
     lib.cl_b200_propagate.restype = C.c_int
     lib.cl_b200_propagate_device.argtypes = [P(cl_run), C.c_int64, P(cl_buffers), C.c_int32, C.c_void_p]
     lib.cl_b200_propagate_device.restype = C.c_int
+    lib.cl_b200_tune.argtypes = [P(cl_run), C.c_int64, P(cl_buffers), C.c_int32, C.c_int64, C.c_void_p,
+                                 P(C.c_int32)]
+    lib.cl_b200_tune.restype = C.c_int
     lib.cl_b200_check.argtypes = [P(cl_run)]
     lib.cl_b200_check.restype = C.c_int
     lib.cl_b200_state_bytes.argtypes = [P(cl_run), C.c_int32]
@@ -188,4 +191,4 @@ EXPORTS = ("cl_b200_propagate", "cl_b200_propagate_device", "cl_b200_check", "cl
            "cl_b200_probe", "cl_b200_last_error", "cl_b200_version", "cl_b200_launch_count",
            "cl_b200_menu_size", "cl_b200_menu_key", "cl_b200_ensemble_device", "cl_b200_ensemble",
            "cl_b200_ensemble_tune", "cl_b200_ensemble_graph_create", "cl_b200_ensemble_graph_launch",
-           "cl_b200_ensemble_graph_destroy", "cl_b200_ensemble_device_noalloc")
+           "cl_b200_ensemble_graph_destroy", "cl_b200_ensemble_device_noalloc", "cl_b200_tune")

@@ -2,6 +2,7 @@
 // rules, the instance lookup, device buffers, launches and copies, and the error mapping onto FALLBACK_REASONS.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <atomic>
 #include <cmath>
 #include <cstdio>
@@ -174,7 +175,24 @@ struct DevBufs {
 
 }  // namespace
 
-void register_instance(const char* key, LaunchFn fn) { registry_list().push_back(Instance{key, fn}); }
+void register_instance(const char* key, LaunchFn fn, unsigned mask) { registry_list().push_back(Instance{key, fn, mask}); }
+
+namespace {
+std::mutex g_tuned_mu;
+std::vector<std::pair<std::string, int>> g_tuned_minb;   // run key + tau -> register budget picked by cl_b200_tune
+int tuned_minb(const cl_run& r) {
+    const std::string k = run_key(r) + "t" + std::to_string(r.tau);
+    std::lock_guard<std::mutex> g(g_tuned_mu);
+    for (auto& p : g_tuned_minb) if (p.first == k) return p.second;
+    return 0;
+}
+void set_tuned_minb(const cl_run& r, int m) {
+    const std::string k = run_key(r) + "t" + std::to_string(r.tau);
+    std::lock_guard<std::mutex> g(g_tuned_mu);
+    for (auto& p : g_tuned_minb) if (p.first == k) { p.second = m; return; }
+    g_tuned_minb.emplace_back(k, m);
+}
+}  // namespace
 
 // Shared with the ensemble entry points (cl_ensemble_capi.cu).
 int capi_fail(int code, const std::string& msg) { return fail(code, msg); }
@@ -262,7 +280,7 @@ int cl_b200_propagate_device(const cl_run* run, int64_t n_orbits, const cl_buffe
         if (run->n0 > 0 && !a.W_in[f]) return fail(CL_EINVAL, "carried W missing");
     }
     LaunchInfo info{};
-    cudaError_t e = in->fn(*run, a, nullptr, static_cast<cudaStream_t>(stream), &info);
+    cudaError_t e = in->fn(*run, a, nullptr, static_cast<cudaStream_t>(stream), &info, tuned_minb(*run));
     g_launches.fetch_add(1);
     if (e != cudaSuccess) return map_cuda(e, "orbit kernel launch");
     return 0;
@@ -341,7 +359,7 @@ int cl_b200_propagate(const cl_run* run, int64_t n, const cl_buffers* h, cl_prov
             a.code[f] = dcode[f];
             a.hstep[f] = dhs[f];
         }
-        e = in->fn(rr, a, nullptr, st, &info);
+        e = in->fn(rr, a, nullptr, st, &info, tuned_minb(*run));
         g_launches.fetch_add(1);
         ++launches;
         if (e != cudaSuccess) { cudaEventDestroy(e0); cudaEventDestroy(e1); return map_cuda(e, "orbit kernel launch"); }
@@ -377,6 +395,62 @@ int cl_b200_propagate(const cl_run* run, int64_t n, const cl_buffers* h, cl_prov
         prov->regs = info.regs;
         prov->orbits_per_block = info.block;
     }
+    return 0;
+}
+
+int cl_b200_tune(const cl_run* run, int64_t n_orbits, const cl_buffers* dev, int32_t soa, int64_t sample_steps,
+                 void* stream, int32_t* minb_out) {
+    if (!run || !dev || n_orbits <= 0) return fail(CL_EINVAL, "bad arguments");
+    int v = validate(*run);
+    if (v) return v;
+    const Instance* in = lookup(*run);
+    if (!in) return CL_EUNSUPPORTED;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    cl_run rr = *run;
+    const int64_t steps = std::max<int64_t>(rr.tau, (sample_steps > 0 ? sample_steps : 100 * rr.tau) / rr.tau * rr.tau);
+    rr.N = steps;
+    rr.n0 = 0;
+    rr.steps = steps;
+    KArgs a;
+    base_args(rr, n_orbits, a);
+    a.n0 = 0;
+    a.steps = steps;
+    a.soa = soa ? 1 : 0;
+    a.x_in = dev->x0;
+    a.x_out = dev->x;
+    for (int f = 0; f < rr.n_frames; ++f) {
+        a.W_in[f] = dev->W0[f];
+        a.W_out[f] = dev->W[f];
+        a.states[f] = static_cast<uint64_t*>(dev->states[f]);
+        a.code[f] = dev->code[f];
+        a.hstep[f] = dev->hstep[f];
+        if (!a.x_in || !a.x_out || !a.W_out[f] || !a.code[f] || (frame_bytes(rr.frames[f]) > 0 && !a.states[f]))
+            return fail(CL_EINVAL, "missing device buffer");
+    }
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    int best = 1;
+    float best_ms = 1e30f;
+    int rc = 0;
+    for (int m = 1; m <= 4 && rc == 0; ++m) {
+        if (!(in->minb_mask & (1u << (m - 1)))) continue;
+        float ms = 0.f;
+        for (int rep = 0; rep < 2; ++rep) {   // the first run warms up
+            cudaEventRecord(e0, st);
+            cudaError_t e = in->fn(rr, a, nullptr, st, nullptr, m);
+            cudaEventRecord(e1, st);
+            if (e != cudaSuccess) { rc = map_cuda(e, "tune launch"); break; }
+            cudaEventSynchronize(e1);
+            cudaEventElapsedTime(&ms, e0, e1);
+        }
+        if (rc == 0 && ms < best_ms) { best_ms = ms; best = m; }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (rc) return rc;
+    set_tuned_minb(*run, best);
+    if (minb_out) *minb_out = best;
     return 0;
 }
 

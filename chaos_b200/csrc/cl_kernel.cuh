@@ -203,8 +203,9 @@ __device__ __forceinline__ void frame_handoff(FrameRegs<D, Real, F>& fr, const d
 }
 
 // ---- the kernel ------------------------------------------------------------------------------------------------------
-template <class Sys, typename Real, class F0, class F1, class F2, int NF>
-__global__ void __launch_bounds__(128) orbit_kernel(const KArgs a, const Sys sys) {
+// MINB is the register budget as resident blocks of 128 threads per SM (1: no cap); the tuner picks it per run.
+template <class Sys, typename Real, class F0, class F1, class F2, int NF, int MINB>
+__global__ void __launch_bounds__(128, MINB) orbit_kernel(const KArgs a, const Sys sys) {
     constexpr int D = Sys::D, S = Sys::S;
     const i64 i = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (i >= a.n) return;

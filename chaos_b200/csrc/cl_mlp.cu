@@ -1,0 +1,408 @@
+// cl_mlp.cu -- the tensor-core kernels of the learned screen: a BF16 x BF16 -> FP32 GEMM on the 5th-generation
+// tensor cores (tcgen05.mma, accumulator in tensor memory) with fused epilogues, and the elementwise kernels of the
+// MLP's forward and backward passes (GELU, its derivative, the two-headed loss, bias gradients, Adam, transposes).
+// No reference counterpart: the reference has no learned component.
+//
+// GEMM: C[M x N] = A[M x K] . B[N x K]^T (+ bias[N]) (+ C when accumulating), A and B row-major BF16 (K contiguous:
+// both operands K-major). One CTA of 128 threads computes a 128 x NT tile (NT = 16..256): the CTA stages 128 x 32
+// and NT x 32 BF16 blocks of A and B in shared memory in the canonical K-major no-swizzle layout (8-row x 16-byte
+// core matrices, the two 8-element K halves of an MMA LBO = 128 B apart, consecutive 8-row groups SBO = 512 B
+// apart), one elected thread issues two tcgen05.mma (M = 128, N = NT, K = 16 each) per block into an FP32 tile in
+// tensor memory and commits them to an mbarrier, and after the last block each warp reads its 32 rows back with
+// tcgen05.ld (warp w owns TMEM lanes 32w..32w+31) for the epilogue. Every wait on the mbarrier is bounded: past
+// the limit the kernel records an error flag and returns instead of spinning on.
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstdio>
+#include <string>
+
+#include "../../include/chaoslab_b200.h"
+
+namespace cl {
+
+int capi_fail(int code, const std::string& msg);
+int capi_map_cuda(cudaError_t e, const char* where);
+void capi_count_launch();
+
+namespace {
+
+constexpr int BM = 128, BK = 32;
+constexpr unsigned kWaitLimit = 1u << 26;   // mbarrier polls before giving up (~seconds; a stuck MMA sets the flag)
+
+__device__ unsigned g_mlp_error;            // nonzero after a bounded wait gave up
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+// Shared-memory matrix descriptor (tcgen05): start >> 4 in bits 0-13, leading-dimension byte offset >> 4 in
+// 16-29, stride-dimension byte offset >> 4 in 32-45, version 1 in 46-47, base offset 0, layout SWIZZLE_NONE (0).
+__device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+    return (static_cast<uint64_t>((addr >> 4) & 0x3FFF)) | (static_cast<uint64_t>((lbo >> 4) & 0x3FFF) << 16) |
+           (static_cast<uint64_t>((sbo >> 4) & 0x3FFF) << 32) | (1ull << 46);
+}
+
+// Instruction descriptor, kind::f16: FP32 accumulator (bits 4-5 = 1), BF16 A and B (bits 7-9, 10-12 = 1), both
+// K-major (bits 15, 16 = 0), N >> 3 in bits 17-22, M >> 4 in bits 24-28.
+__host__ __device__ constexpr uint32_t idesc_bf16(int M, int N) {
+    return (1u << 4) | (1u << 7) | (1u << 10) | (static_cast<uint32_t>(N >> 3) << 17) | (static_cast<uint32_t>(M >> 4) << 24);
+}
+
+// Canonical K-major no-swizzle offset (bytes) of element (row, k) of a tile with 8 K-groups of 8 BF16 per block.
+__device__ __forceinline__ uint32_t kmajor_off(int row, int k) {
+    return static_cast<uint32_t>(((row >> 3) * (BK / 8) + (k >> 3)) * 128 + (row & 7) * 16 + (k & 7) * 2);
+}
+
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t phase) {
+    for (unsigned it = 0; it < kWaitLimit; ++it) {
+        uint32_t done;
+        asm volatile(
+            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+            : "=r"(done) : "r"(bar), "r"(phase) : "memory");
+        if (done) return true;
+    }
+    atomicExch(&g_mlp_error, 1u);
+    return false;
+}
+
+template <int NT>
+__global__ void __launch_bounds__(128, 1) gemm_bf16_tc(const __nv_bfloat16* __restrict__ A, int lda,
+                                                       const __nv_bfloat16* __restrict__ B, int ldb, int M, int N,
+                                                       int K, const float* __restrict__ bias, int epilogue,
+                                                       float* __restrict__ C32, __nv_bfloat16* __restrict__ Cb,
+                                                       int ldc, float* __restrict__ pre, int accumulate) {
+    constexpr int TCOLS = NT < 32 ? 32 : NT;   // TMEM allocation: a power of two, at least 32 columns
+    static_assert((NT % 16) == 0 && NT >= 16 && NT <= 256, "N tile");
+    __shared__ __align__(1024) uint8_t sA[BM * BK * 2];
+    __shared__ __align__(1024) uint8_t sB[NT * BK * 2];
+    __shared__ __align__(8) uint64_t mbar;
+    __shared__ uint32_t tmem_base;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int m0 = blockIdx.x * BM, n0 = blockIdx.y * NT;
+
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n"
+                     :: "r"(smem_u32(&tmem_base)), "r"(TCOLS) : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
+    }
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" :: "r"(smem_u32(&mbar)) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+    const uint32_t tmem = tmem_base;
+    const uint32_t bar = smem_u32(&mbar);
+    constexpr uint32_t idesc = idesc_bf16(BM, NT);
+    uint32_t phase = 0;
+    bool ok = true;
+
+    const int kblocks = (K + BK - 1) / BK;
+    for (int kb = 0; kb < kblocks && ok; ++kb) {
+        const int k0 = kb * BK;
+        // stage A (128 x 64) and B (NT x 64): 8-element (16-byte) chunks, zero outside the matrices
+        for (int c = tid; c < BM * (BK / 8); c += 128) {
+            const int row = c / (BK / 8), kc = (c % (BK / 8)) * 8;
+            const int gr = m0 + row, gk = k0 + kc;
+            uint4 v = make_uint4(0, 0, 0, 0);
+            if (gr < M && gk + 8 <= K) v = *reinterpret_cast<const uint4*>(A + static_cast<size_t>(gr) * lda + gk);
+            else if (gr < M && gk < K) {
+                __nv_bfloat16 t[8];
+                for (int e = 0; e < 8; ++e) t[e] = gk + e < K ? A[static_cast<size_t>(gr) * lda + gk + e] : __float2bfloat16(0.f);
+                v = *reinterpret_cast<uint4*>(t);
+            }
+            *reinterpret_cast<uint4*>(sA + kmajor_off(row, kc)) = v;
+        }
+        for (int c = tid; c < NT * (BK / 8); c += 128) {
+            const int row = c / (BK / 8), kc = (c % (BK / 8)) * 8;
+            const int gr = n0 + row, gk = k0 + kc;
+            uint4 v = make_uint4(0, 0, 0, 0);
+            if (gr < N && gk + 8 <= K) v = *reinterpret_cast<const uint4*>(B + static_cast<size_t>(gr) * ldb + gk);
+            else if (gr < N && gk < K) {
+                __nv_bfloat16 t[8];
+                for (int e = 0; e < 8; ++e) t[e] = gk + e < K ? B[static_cast<size_t>(gr) * ldb + gk + e] : __float2bfloat16(0.f);
+                v = *reinterpret_cast<uint4*>(t);
+            }
+            *reinterpret_cast<uint4*>(sB + kmajor_off(row, kc)) = v;
+        }
+        // the generic-proxy writes must be visible to the tensor core's async proxy
+        asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+        asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+        __syncthreads();
+        asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+        if (tid == 0) {
+#pragma unroll
+            for (int s = 0; s < BK / 16; ++s) {
+                const uint64_t da = smem_desc(smem_u32(sA) + s * 256, 128, (BK / 8) * 128);
+                const uint64_t db = smem_desc(smem_u32(sB) + s * 256, 128, (BK / 8) * 128);
+                const uint32_t acc = (kb > 0 || s > 0) ? 1u : 0u;
+                asm volatile(
+                    "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+                    " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n"
+                    :: "r"(tmem), "l"(da), "l"(db), "r"(idesc), "r"(acc) : "memory");
+            }
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n"
+                         :: "r"(bar) : "memory");
+        }
+        // every thread waits for the MMAs of this block before the tiles are overwritten (or read back)
+        ok = mbar_wait(bar, phase);
+        phase ^= 1u;
+        asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+    }
+
+    if (ok) {
+        // epilogue: warp w reads TMEM lanes 32w..32w+31 (its rows), 16 columns at a time
+        const int row = m0 + warp * 32 + lane;
+#pragma unroll 1
+        for (int c0 = 0; c0 < NT; c0 += 16) {
+            uint32_t r[16];
+            const uint32_t taddr = tmem + (static_cast<uint32_t>(warp * 32) << 16) + static_cast<uint32_t>(c0);
+            asm volatile(
+                "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];\n"
+                : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+                  "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+                : "r"(taddr));
+            asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+            if (row < M) {
+#pragma unroll
+                for (int j = 0; j < 16; ++j) {
+                    const int col = n0 + c0 + j;
+                    if (col >= N) continue;
+                    float v = __uint_as_float(r[j]);
+                    const size_t at = static_cast<size_t>(row) * ldc + col;
+                    if (accumulate && C32) v += C32[at];
+                    if (bias) v += bias[col];
+                    if (pre) pre[at] = v;
+                    if (epilogue == 1) v = 0.5f * v * (1.0f + erff(v * 0.70710678118654752f));   // GELU (erf form)
+                    if (C32) C32[at] = v;
+                    if (Cb) Cb[at] = __float2bfloat16(v);
+                }
+            }
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+    __syncthreads();
+    if (warp == 0) {
+        asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" :: "r"(tmem), "r"(TCOLS) : "memory");
+    }
+}
+
+// ---- elementwise kernels ---------------------------------------------------------------------------------------------
+__global__ void transpose_bf16(const __nv_bfloat16* __restrict__ src, int rows, int cols, int lds,
+                               __nv_bfloat16* __restrict__ dst, int ldd) {
+    __shared__ __nv_bfloat16 t[32][33];
+    const int bx = blockIdx.x * 32, by = blockIdx.y * 32;
+    for (int j = threadIdx.y; j < 32; j += blockDim.y) {
+        const int r = by + j, c = bx + threadIdx.x;
+        t[j][threadIdx.x] = (r < rows && c < cols) ? src[static_cast<size_t>(r) * lds + c] : __float2bfloat16(0.f);
+    }
+    __syncthreads();
+    for (int j = threadIdx.y; j < 32; j += blockDim.y) {
+        const int r = bx + j, c = by + threadIdx.x;   // dst is cols x rows
+        if (r < cols && c < rows) dst[static_cast<size_t>(r) * ldd + c] = t[threadIdx.x][j];
+    }
+}
+
+// dH = dY * GELU'(pre) (erf form), written in BF16 for the next GEMMs and FP32 for the bias gradient.
+__global__ void gelu_backward(const float* __restrict__ dY, const float* __restrict__ pre, int64_t n,
+                              __nv_bfloat16* __restrict__ dHb, float* __restrict__ dH32) {
+    const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float x = pre[i];
+    const float cdf = 0.5f * (1.0f + erff(x * 0.70710678118654752f));
+    const float pdf = 0.39894228040143268f * __expf(-0.5f * x * x);
+    const float g = dY[i] * (cdf + x * pdf);
+    if (dHb) dHb[i] = __float2bfloat16(g);
+    if (dH32) dH32[i] = g;
+}
+
+// Column sums of an FP32 matrix (bias gradients): db[j] = sum_i dH[i, j].
+__global__ void col_sum(const float* __restrict__ X, int rows, int cols, int ld, float* __restrict__ out) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= cols) return;
+    float s = 0.f;
+    for (int i = 0; i < rows; ++i) s += X[static_cast<size_t>(i) * ld + j];
+    out[j] = s;
+}
+
+// Head loss on logits [B x ld] (column 0: chaos logit, column 1: lambda_1 prediction): mean binary cross-entropy
+// plus w_reg times the mean squared error; the gradient dL/dlogits (columns 0, 1; zero elsewhere), FP32 and BF16,
+// and the per-row losses.
+__global__ void head_loss(const float* __restrict__ logits, int B, int ld, const float* __restrict__ label,
+                          const float* __restrict__ target, float w_reg, float* __restrict__ grad,
+                          __nv_bfloat16* __restrict__ gradb, float* __restrict__ row_loss) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= B) return;
+    const float z = logits[static_cast<size_t>(i) * ld], y = label[i];
+    const float p = 1.0f / (1.0f + __expf(-z));
+    const float bce = fmaxf(z, 0.f) - z * y + log1pf(__expf(-fabsf(z)));
+    const float e = logits[static_cast<size_t>(i) * ld + 1] - target[i];
+    row_loss[i] = bce + w_reg * e * e;
+    for (int j = 0; j < ld; ++j) {
+        float g = 0.f;
+        if (j == 0) g = (p - y) / B;
+        else if (j == 1) g = 2.0f * w_reg * e / B;
+        grad[static_cast<size_t>(i) * ld + j] = g;
+        if (gradb) gradb[static_cast<size_t>(i) * ld + j] = __float2bfloat16(g);
+    }
+}
+
+// Adam on FP32 master weights; refreshes the BF16 copy (and its transpose when given: W is rows x cols).
+__global__ void adam_step(float* __restrict__ w, const float* __restrict__ g, float* __restrict__ m,
+                          float* __restrict__ v, int64_t n, float lr, float b1, float b2, float eps, float c1,
+                          float c2, __nv_bfloat16* __restrict__ wb, __nv_bfloat16* __restrict__ wbt, int rows, int cols) {
+    const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float gi = g[i];
+    const float mi = b1 * m[i] + (1.0f - b1) * gi, vi = b2 * v[i] + (1.0f - b2) * gi * gi;
+    m[i] = mi;
+    v[i] = vi;
+    const float wi = w[i] - lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+    w[i] = wi;
+    if (wb) wb[i] = __float2bfloat16(wi);
+    if (wbt) {
+        const int r = static_cast<int>(i / cols), c = static_cast<int>(i % cols);
+        wbt[static_cast<size_t>(c) * rows + r] = __float2bfloat16(wi);
+    }
+}
+
+// Screening features from the reducer states of the chain (MEGNO(replace = false), SALI()) on a k = 2 frame, Julia
+// layout (MEGNOState 200 bytes, then SALIState 72 bytes, per orbit), read after the window ending at global step n:
+// feature 3w + 0: log-stretch rate of column 1, (s + c) / n; 3w + 1: log10(max(SALI, 1e-16)) / 8; 3w + 2: the running
+// MEGNO Y = 2 R1 / n of column 1, / 4. After the last window (w = windows - 1) also 60: the mean MEGNO Ybar / 4,
+// 61: the log-stretch rate of column 2, 62: log10 SALI / 8 again, 63: 0.
+__global__ void screen_features(const double* __restrict__ st, int64_t n_orbits, int64_t n, int w, int windows,
+                                float* __restrict__ f32, __nv_bfloat16* __restrict__ fb) {
+    const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= n_orbits) return;
+    const double* s = st + i * 34;       // 272 bytes
+    // MEGNOState: c1 {s, R1, R2, Q, Q2} (10 doubles), c2 (10), value, n, K, step, code|column
+    const double tn = static_cast<double>(n);
+    const double rate1 = (s[0] + s[1]) / tn, Y = 2.0 * (s[2] + s[3]) / tn;
+    const double* sali = s + 25;         // SALIState: s1 (2), s2 (2), sali, ...
+    const double lsal = log10(fmax(sali[4], 1e-16)) / 8.0;
+    float v[3] = {static_cast<float>(rate1), static_cast<float>(lsal), static_cast<float>(Y / 4.0)};
+    for (int j = 0; j < 3; ++j) {
+        const int64_t at = i * 64 + 3 * w + j;
+        if (f32) f32[at] = v[j];
+        if (fb) fb[at] = __float2bfloat16(v[j]);
+    }
+    if (w == windows - 1) {
+        const long long Kh = *reinterpret_cast<const long long*>(s + 22);
+        const double Ybar = Kh > 0 ? (s[6] + s[7]) / static_cast<double>(Kh) : 0.0;
+        const double rate2 = (s[10] + s[11]) / tn;
+        float e[4] = {static_cast<float>(Ybar / 4.0), static_cast<float>(rate2), static_cast<float>(lsal), 0.f};
+        for (int j = 0; j < 4; ++j) {
+            const int64_t at = i * 64 + 60 + j;
+            if (f32) f32[at] = e[j];
+            if (fb) fb[at] = __float2bfloat16(e[j]);
+        }
+    }
+}
+
+__global__ void f32_to_bf16(const float* __restrict__ x, int64_t n, __nv_bfloat16* __restrict__ y) {
+    const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i < n) y[i] = __float2bfloat16(x[i]);
+}
+
+template <int NT>
+cudaError_t launch_gemm(const void* A, int lda, const void* B, int ldb, int M, int N, int K, const float* bias,
+                        int epi, float* C32, void* Cb, int ldc, float* pre, int acc, cudaStream_t st) {
+    dim3 grid((M + BM - 1) / BM, (N + NT - 1) / NT);
+    gemm_bf16_tc<NT><<<grid, 128, 0, st>>>(static_cast<const __nv_bfloat16*>(A), lda,
+                                           static_cast<const __nv_bfloat16*>(B), ldb, M, N, K, bias, epi, C32,
+                                           static_cast<__nv_bfloat16*>(Cb), ldc, pre, acc);
+    return cudaGetLastError();
+}
+
+}  // namespace
+}  // namespace cl
+
+using namespace cl;
+
+extern "C" {
+
+int cl_b200_gemm_bf16(const void* A, int32_t lda, const void* B, int32_t ldb, int32_t M, int32_t N, int32_t K,
+                      const float* bias, int32_t epilogue, float* C32, void* Cbf16, int32_t ldc, float* pre,
+                      int32_t accumulate, void* stream) {
+    if (!A || !B || M <= 0 || N <= 0 || K <= 0 || (!C32 && !Cbf16)) return capi_fail(CL_EINVAL, "gemm: bad arguments");
+    if ((lda % 8) || (ldb % 8) || (reinterpret_cast<uintptr_t>(A) % 16) || (reinterpret_cast<uintptr_t>(B) % 16))
+        return capi_fail(CL_EINVAL, "gemm: operands need 16-byte aligned rows (ld a multiple of 8)");
+    if (epilogue != 0 && epilogue != 1) return capi_fail(CL_EINVAL, "gemm: epilogue 0 (none) or 1 (GELU)");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    cudaError_t e;
+    if (N <= 16) e = launch_gemm<16>(A, lda, B, ldb, M, N, K, bias, epilogue, C32, Cbf16, ldc, pre, accumulate, st);
+    else if (N <= 64) e = launch_gemm<64>(A, lda, B, ldb, M, N, K, bias, epilogue, C32, Cbf16, ldc, pre, accumulate, st);
+    else if (N <= 128) e = launch_gemm<128>(A, lda, B, ldb, M, N, K, bias, epilogue, C32, Cbf16, ldc, pre, accumulate, st);
+    else e = launch_gemm<256>(A, lda, B, ldb, M, N, K, bias, epilogue, C32, Cbf16, ldc, pre, accumulate, st);
+    capi_count_launch();
+    return e == cudaSuccess ? 0 : capi_map_cuda(e, "gemm launch");
+}
+
+int cl_b200_mlp_status(void) {
+    unsigned v = 0;
+    if (cudaMemcpyFromSymbol(&v, g_mlp_error, sizeof v) != cudaSuccess) return CL_EDEVICE_LOST;
+    return v ? CL_EDEVICE_LOST : 0;
+}
+
+int cl_b200_transpose_bf16(const void* src, int32_t rows, int32_t cols, int32_t lds, void* dst, int32_t ldd, void* stream) {
+    dim3 grid((cols + 31) / 32, (rows + 31) / 32), block(32, 8);
+    transpose_bf16<<<grid, block, 0, static_cast<cudaStream_t>(stream)>>>(
+        static_cast<const __nv_bfloat16*>(src), rows, cols, lds, static_cast<__nv_bfloat16*>(dst), ldd);
+    const cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? 0 : capi_map_cuda(e, "transpose");
+}
+
+int cl_b200_gelu_backward(const float* dY, const float* pre, int64_t n, void* dHb, float* dH32, void* stream) {
+    gelu_backward<<<static_cast<unsigned>((n + 255) / 256), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+        dY, pre, n, static_cast<__nv_bfloat16*>(dHb), dH32);
+    const cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? 0 : capi_map_cuda(e, "gelu backward");
+}
+
+int cl_b200_col_sum(const float* X, int32_t rows, int32_t cols, int32_t ld, float* out, void* stream) {
+    col_sum<<<(cols + 127) / 128, 128, 0, static_cast<cudaStream_t>(stream)>>>(X, rows, cols, ld, out);
+    const cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? 0 : capi_map_cuda(e, "column sums");
+}
+
+int cl_b200_head_loss(const float* logits, int32_t B, int32_t ld, const float* label, const float* target, float w_reg,
+                      float* grad, void* gradb, float* row_loss, void* stream) {
+    head_loss<<<(B + 127) / 128, 128, 0, static_cast<cudaStream_t>(stream)>>>(
+        logits, B, ld, label, target, w_reg, grad, static_cast<__nv_bfloat16*>(gradb), row_loss);
+    const cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? 0 : capi_map_cuda(e, "head loss");
+}
+
+int cl_b200_adam(float* w, const float* g, float* m, float* v, int64_t n, float lr, float b1, float b2, float eps,
+                 int32_t t, void* wb, void* wbt, int32_t rows, int32_t cols, void* stream) {
+    const float c1 = 1.0f - powf(b1, static_cast<float>(t)), c2 = 1.0f - powf(b2, static_cast<float>(t));
+    adam_step<<<static_cast<unsigned>((n + 255) / 256), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+        w, g, m, v, n, lr, b1, b2, eps, c1, c2, static_cast<__nv_bfloat16*>(wb), static_cast<__nv_bfloat16*>(wbt),
+        rows, cols);
+    const cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? 0 : capi_map_cuda(e, "adam");
+}
+
+int cl_b200_screen_features(const void* states, int64_t n_orbits, int64_t n, int32_t window, int32_t windows,
+                            float* f32, void* fbf16, void* stream) {
+    if (!states || n_orbits <= 0 || n <= 0 || window < 0 || window >= windows || 3 * windows + 4 > 64)
+        return capi_fail(CL_EINVAL, "screen features: bad arguments");
+    screen_features<<<static_cast<unsigned>((n_orbits + 127) / 128), 128, 0, static_cast<cudaStream_t>(stream)>>>(
+        static_cast<const double*>(states), n_orbits, n, window, windows, f32, static_cast<__nv_bfloat16*>(fbf16));
+    const cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? 0 : capi_map_cuda(e, "screen features");
+}
+
+int cl_b200_to_bf16(const float* x, int64_t n, void* y, void* stream) {
+    f32_to_bf16<<<static_cast<unsigned>((n + 255) / 256), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+        x, n, static_cast<__nv_bfloat16*>(y));
+    const cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? 0 : capi_map_cuda(e, "to bf16");
+}
+
+}  // extern "C"

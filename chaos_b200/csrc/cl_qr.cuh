@@ -278,14 +278,16 @@ __device__ __forceinline__ T G_from_Gw(T Gw) {
     return Gw;
 }
 
-// orth_loss (qr_spectrum.jl:4): maximum(abs, Q'Q - I) with Q'Q the fused StaticArrays product.
+// orth_loss (qr_spectrum.jl:4): maximum(abs, Q'Q - I) with Q'Q the fused StaticArrays product. Q'Q is symmetric bit
+// for bit (each entry's fma chain has the same operands in the same order, and a*b == b*a), so the maximum over the
+// upper triangle is the maximum over the matrix.
 template <int D, int K, typename T>
 __device__ __forceinline__ T orth_loss(const T* Q) {
     T m = T(0);
 #pragma unroll
     for (int j = 0; j < K; ++j)
 #pragma unroll
-        for (int i = 0; i < K; ++i) {
+        for (int i = 0; i <= j; ++i) {
             T acc = Q[i * D] * Q[j * D];
 #pragma unroll
             for (int q = 1; q < D; ++q) acc = fma(Q[q + i * D], Q[q + j * D], acc);

@@ -17,11 +17,12 @@ namespace cl {
 struct LaunchInfo { int block, grid, regs; };
 
 typedef cudaError_t (*LaunchFn)(const cl_run& run, const KArgs& a, const double* devA, cudaStream_t st,
-                                LaunchInfo* info);
+                                LaunchInfo* info, int minb);
 
-struct Instance { const char* key; LaunchFn fn; };
+// An instance and the register budgets it was compiled with (bit b set: blocks-per-SM cap b + 1 available).
+struct Instance { const char* key; LaunchFn fn; unsigned minb_mask; };
 
-void register_instance(const char* key, LaunchFn fn);
+void register_instance(const char* key, LaunchFn fn, unsigned minb_mask);
 const Instance* find_instance(const std::string& key);
 int instance_count();
 const Instance* instance_at(int i);
@@ -54,10 +55,10 @@ template <class Sys> struct SysMaker {
 
 constexpr int ORBIT_BLOCK = 128;
 
-template <class Sys, typename Real, class F0, class F1, class F2, int NF>
-cudaError_t launch_instance(const cl_run& run, const KArgs& a, const double* devA, cudaStream_t st, LaunchInfo* info) {
+template <class Sys, typename Real, class F0, class F1, class F2, int NF, int MINB>
+cudaError_t launch_variant(const cl_run& run, const KArgs& a, const double* devA, cudaStream_t st, LaunchInfo* info) {
     const Sys sys = SysMaker<Sys>::make(run, devA);
-    auto k = orbit_kernel<Sys, Real, F0, F1, F2, NF>;
+    auto k = orbit_kernel<Sys, Real, F0, F1, F2, NF, MINB>;
     const int block = ORBIT_BLOCK;
     const long long grid = (a.n + block - 1) / block;
     k<<<static_cast<unsigned>(grid), block, 0, st>>>(a, sys);
@@ -71,8 +72,24 @@ cudaError_t launch_instance(const cl_run& run, const KArgs& a, const double* dev
     return e;
 }
 
+// The compiled variants MB... of one instance; an unknown minb runs the first.
+template <class Sys, typename Real, class F0, class F1, class F2, int NF, int... MB>
+cudaError_t launch_instance(const cl_run& run, const KArgs& a, const double* devA, cudaStream_t st, LaunchInfo* info,
+                            int minb) {
+    cudaError_t e = cudaErrorInvalidValue;
+    bool done = false;
+    ((!done && MB == minb ? (e = launch_variant<Sys, Real, F0, F1, F2, NF, MB>(run, a, devA, st, info), done = true)
+                          : false), ...);
+    if (!done) {
+        constexpr int first[] = {MB...};
+        return launch_variant<Sys, Real, F0, F1, F2, NF, first[0]>(run, a, devA, st, info);
+    }
+    return e;
+}
+template <int... MB> constexpr unsigned minb_mask() { return ((1u << (MB - 1)) | ...); }
+
 struct Registrar {
-    Registrar(const char* key, LaunchFn fn) { register_instance(key, fn); }
+    Registrar(const char* key, LaunchFn fn, unsigned mask) { register_instance(key, fn, mask); }
 };
 
 }  // namespace cl

@@ -54,8 +54,8 @@ def menu():
     """The compiled menu, grouped into translation units (compiled in parallel)."""
     groups: dict[str, list] = {}
 
-    def add(group, kind, d, prec, frames):
-        groups.setdefault(group, []).append((kind, d, prec, frames))
+    def add(group, kind, d, prec, frames, minbs=(1,)):
+        groups.setdefault(group, []).append((kind, d, prec, frames, minbs))
 
     k2_chains = [[q] for q in QR] + [["SALI"], ["GALI"], ["MEGNO1"], ["FLI1"], ["MEGNO0", "FLI0", "QR6"],
                                      ["MEGNO0", "SALI"], ["FLI0", "SALI"], ["MEGNO0", "FLI0", "SALI"], []]
@@ -90,10 +90,11 @@ def menu():
     add("fro4", SYS_FROESCHLE, 4, 0, [(4, ["GALI", "SALI"])])
     # the fused QRSpectrum + GALI_4 + SALI ensemble (two frames, one orbit) in both precisions
     for prec in (0, 1):
-        add("fro_fused" if prec == 0 else "fro_mixed", SYS_FROESCHLE, 4, prec, [(4, ["QR4"]), (4, ["GALI", "SALI"])])
+        add("fro_fused" if prec == 0 else "fro_mixed", SYS_FROESCHLE, 4, prec, [(4, ["QR4"]), (4, ["GALI", "SALI"])],
+            minbs=(1, 2, 3) if prec == 0 else (1, 2, 3, 4))
     for ch in (["QR4"], ["QR2"], ["GALI", "SALI"], ["GALI"]):
         add("fro_mixed", SYS_FROESCHLE, 4, 1, [(4, ch)])
-    for ch in (["QR2"], ["SALI"], ["MEGNO1"]):
+    for ch in (["QR2"], ["SALI"], ["MEGNO1"], ["MEGNO0", "SALI"]):
         add("fro_mixed", SYS_FROESCHLE, 4, 1, [(2, ch)])
     # coupled standard-map lattices, N = 2..8 sites
     for N in range(2, 9):
@@ -148,14 +149,15 @@ namespace {{
 def render(group, entries):
     extra = '#include "cl_gauss.cuh"\n' if any(e[0] == SYS_HH for e in entries) else ""
     out = [HEADER.format(group=group, extra=extra)]
-    for idx, (kind, d, prec, frames) in enumerate(entries):
+    for idx, (kind, d, prec, frames, minbs) in enumerate(entries):
         real = "double" if prec == 0 else "float"
         ftypes = [f"Frame<{k}{''.join(', ' + t for t in red_type(ch))}>" for k, ch in frames]
         while len(ftypes) < 3:
             ftypes.append("NoFrame")
-        out.append(f"cudaError_t L{idx}(const cl_run& r, const KArgs& a, const double* A, cudaStream_t s, LaunchInfo* i) {{\n"
-                   f"    return launch_instance<{sys_type(kind, d)}, {real}, {', '.join(ftypes)}, {len(frames)}>(r, a, A, s, i);\n}}\n"
-                   f"const Registrar R{idx}(\"{key(kind, d, prec, frames)}\", L{idx});\n")
+        mb = ", ".join(str(m) for m in minbs)
+        out.append(f"cudaError_t L{idx}(const cl_run& r, const KArgs& a, const double* A, cudaStream_t s, LaunchInfo* i, int m) {{\n"
+                   f"    return launch_instance<{sys_type(kind, d)}, {real}, {', '.join(ftypes)}, {len(frames)}, {mb}>(r, a, A, s, i, m);\n}}\n"
+                   f"const Registrar R{idx}(\"{key(kind, d, prec, frames)}\", L{idx}, minb_mask<{mb}>());\n")
     out.append("}  // namespace\n}  // namespace cl\n")
     return "\n".join(out)
 

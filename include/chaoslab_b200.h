@@ -190,6 +190,13 @@ CL_API int cl_b200_propagate(const cl_run* run, int64_t n_orbits, const cl_buffe
  * orbit-major. Returns after the launch is enqueued. */
 CL_API int cl_b200_propagate_device(const cl_run* run, int64_t n_orbits, const cl_buffers* dev, int32_t soa, void* stream);
 
+/* Autotune the register budget of the instance that covers `run`: times each compiled variant (1, 2, 3 or 4
+ * resident blocks of 128 threads per SM) over `sample_steps` steps of the n_orbits orbits on the device buffers
+ * (whose contents are overwritten), remembers the fastest for this run's instance and tau in the process, and
+ * writes it to *minb_out. Later propagate calls of the same instance use it. No reference counterpart. */
+CL_API int cl_b200_tune(const cl_run* run, int64_t n_orbits, const cl_buffers* dev, int32_t soa, int64_t sample_steps,
+                        void* stream, int32_t* minb_out);
+
 /* 0 when a compiled kernel instance covers `run`, else CL_EINVAL (ill-formed run, message in cl_b200_last_error)
  * or CL_EUNSUPPORTED (well-formed, but not in the compiled menu: the caller falls back with reason 3). */
 CL_API int cl_b200_check(const cl_run* run);
