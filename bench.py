@@ -15,6 +15,19 @@ not installed) on the host cores.
 
 Multi-GPU: orbits are independent, so N ranks run N shards of the same size with no collective in the data path
 (weak scaling); the time is the max over ranks.
+
+`--workload` selects one of the other measured configurations (one GPU, one JSON line each, same keys):
+  standard  the Chirikov standard map K = 6, 4096 orbits, N = 1e5, k = 2, tau = 1, QRSpectrum(MGS), FP64 kernel
+            (bit-identical to the oracle);
+  gauss     IntegratorMap(Gauss-3, Henon-Heiles, dt = 0.01), 16384 starts on the E = 1/8 section, N = 1e6,
+            k = 2, tau = 10, chain MEGNO + FLI + QRSpectrum(Givens), FP64 kernel: Gauss steps/s;
+  lattice   the uneven ensemble: 1,048,576 orbits of standard-map lattices d in {2, 4, 8, 16}, K ~ U[0.5, 3],
+            lengths log-uniform in [1e3, 1e6], escape at |p| > 1e3, k = min(d, 8), tau in {5, 10, 20}, mixed
+            precision, one CUDA graph of persistent work-queue kernels with autotuned variants: executed
+            orbit-steps/s;
+  screen    the learned screen on the 2048 x 2048 (x1, p1) grid of Froeschle orbits (x2 = p2 = 0.1), N = 1e5:
+            screened orbits/s against the plain full integration of every orbit, with the misclassification
+            over the whole grid.
 """
 from __future__ import annotations
 
@@ -144,10 +157,14 @@ def main() -> None:
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--orbits", type=int, default=N_ORBITS)
+    ap.add_argument("--orbits", type=int, default=None, help="orbits per GPU (default: the workload's own)")
     ap.add_argument("--N", type=int, default=N_STEPS)
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
+    ap.add_argument("--workload", default="coupled", choices=["coupled", "standard", "gauss", "lattice", "screen"])
     args = ap.parse_args()
+    if args.workload != "coupled":
+        run_workload(args)
+        return
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -168,7 +185,7 @@ def main() -> None:
         line = dict(metric=METRIC, value=v, unit="orbit-steps/s", n_gpus=args.gpus, steps=args.steps,
                     warmup=args.warmup, ms_per_step=so * ss / v * 1e3, higher_is_better=True, scaling="weak",
                     vs_baseline=None, dtype="f64", data="synthetic", impl="reference",
-                    config=dict(workload="froeschle-4d-65536x1e5-tau10-qr-householder+gali4+sali", orbits=args.orbits,
+                    config=dict(workload="froeschle-4d-65536x1e5-tau10-qr-householder+gali4+sali", orbits=args.orbits or N_ORBITS,
                                 N=args.N, tau=TAU),
                     cpu_baseline=dict(value=v, unit="orbit-steps/s", cores=threads, kind="port",
                                       sample=f"{so} orbits x {ss} steps of the workload per step (oracle, all host threads; Julia absent)"),
@@ -191,7 +208,7 @@ def main() -> None:
     from chaos_b200.propagate import FrameSpec, build_run
     L = lib()
 
-    n, N = args.orbits, args.N
+    n, N = args.orbits or N_ORBITS, args.N
     sysm = FroeschleMap(NU, KAPPA, MU)
     # each rank its own shard of the same size (weak scaling): orbit ids rank*n+1 .. (rank+1)*n
     rng = np.random.default_rng(SEED + rank)
@@ -359,6 +376,282 @@ def main() -> None:
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
+
+# ---- the other measured configurations (--workload) --------------------------------------------------------------
+def _setup():
+    import torch
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    from chaos_b200._lib import lib
+    return torch, dev, lib()
+
+
+def _device_frames(torch, dev, L, sysm, x0_h, N, tau, frames, precision, seed=SEED):
+    """SoA device buffers for propagate_device: x0 (s, n), each frame's W0 = I[:, 1:k] as (d k, n), states, codes."""
+    from chaos_b200 import _abi
+    from chaos_b200.propagate import build_run
+    n = len(x0_h)
+    r = build_run(sysm, N, tau, frames, precision, seed)
+    b = dict(x0=torch.tensor(np.ascontiguousarray(x0_h.T), device=dev))
+    b["x"] = torch.empty_like(b["x0"])
+    cb = _abi.cl_buffers()
+    cb.x0, cb.x = b["x0"].data_ptr(), b["x"].data_ptr()
+    d = sysm.d
+    for f, fr in enumerate(frames):
+        W0 = torch.zeros((d * fr.k, n), dtype=torch.float64, device=dev)
+        for j in range(fr.k):
+            W0[j * d + j] = 1.0
+        sb = L.cl_b200_state_bytes(C.byref(r), f)
+        b[f"W0{f}"], b[f"W{f}"] = W0, torch.empty_like(W0)
+        b[f"st{f}"] = torch.zeros(max(1, n * sb // 8), dtype=torch.int64, device=dev)
+        b[f"code{f}"] = torch.zeros(n, dtype=torch.int8, device=dev)
+        b[f"hs{f}"] = torch.zeros(n, dtype=torch.int64, device=dev)
+        cb.W0[f], cb.W[f] = W0.data_ptr(), b[f"W{f}"].data_ptr()
+        cb.states[f] = b[f"st{f}"].data_ptr() if sb else None
+        cb.code[f], cb.hstep[f] = b[f"code{f}"].data_ptr(), b[f"hs{f}"].data_ptr()
+    return r, cb, b
+
+
+def _event_times(torch, dev, stream, fn, steps, warmup, flush, sampler=None):
+    for _ in range(warmup):
+        fn()
+    torch.cuda.synchronize(dev)
+    ms = []
+    with (sampler if sampler is not None else _Null()):
+        for _ in range(steps):
+            flush.fill_(1.0)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            fn()
+            e1.record(stream)
+            e1.synchronize()
+            ms.append(e0.elapsed_time(e1))
+    return ms
+
+
+def _line(metric, value, unit, args, ms, config, **extra):
+    out = dict(metric=metric, value=value, unit=unit, n_gpus=1, steps=len(ms), warmup=args.warmup,
+               ms_per_step=float(np.mean(ms)) if ms else None, higher_is_better=True, scaling="weak",
+               vs_baseline=None, data="synthetic", config=config)
+    out.update(extra)
+    print(json.dumps(out), flush=True)
+
+
+def _propagate_workload(args, name, sysm, x0_h, N, tau, frames, unit_name, cpu_fn, config):
+    """A plain / mixed pair of propagate_device timings (value = the mixed kernel when compiled, else FP64)."""
+    torch, dev, L = _setup()
+    from chaos_b200._lib import last_error
+    stream = torch.cuda.current_stream(dev)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    n = len(x0_h)
+    res = {}
+    launches = 0
+    sampler = ClockSampler(0)
+    for prec in ("fp64", "mixed"):
+        r, cb, b = _device_frames(torch, dev, L, sysm, x0_h, N, tau, frames, prec)
+        if L.cl_b200_check(C.byref(r)) != 0:
+            continue
+        mb = C.c_int32(0)
+        rc = L.cl_b200_tune(C.byref(r), n, C.byref(cb), 1, min(N, 2000), C.c_void_p(stream.cuda_stream), C.byref(mb))
+        if rc != 0:
+            raise RuntimeError(f"cl_b200_tune: {rc} {last_error()}")
+
+        def go():
+            rc_ = L.cl_b200_propagate_device(C.byref(r), n, C.byref(cb), 1, C.c_void_p(stream.cuda_stream))
+            if rc_ != 0:
+                raise RuntimeError(f"cl_b200_propagate_device: {rc_} {last_error()}")
+        l0 = L.cl_b200_launch_count()
+        ms = _event_times(torch, dev, stream, go, args.steps, args.warmup, flush, sampler if prec == "mixed" else None)
+        launches = L.cl_b200_launch_count() - l0 - args.warmup
+        st = b["st0"].view(torch.float64).reshape(n, -1).cpu().numpy()
+        res[prec] = dict(ms=ms, value=n * N / (np.mean(ms) / 1e3), minb=int(mb.value), st=st,
+                         code=b["code0"].cpu().numpy())
+    head = res.get("mixed", res["fp64"])
+    extra = dict(fp64_kernel=dict(value=res["fp64"]["value"], ms_per_step=float(np.mean(res["fp64"]["ms"]))))
+    if "mixed" in res:
+        extra["fp64_kernel"]["mixed_over_fp64"] = res["mixed"]["value"] / res["fp64"]["value"]
+    cpu = None if args.no_cpu else cpu_fn()
+    config = dict(config, tuned_blocks_per_sm={k: v["minb"] for k, v in res.items()},
+                  l2="flushed between timed steps (256 MB write)")
+    _line(f"{unit_name}/s ({name})", head["value"], f"{unit_name}/s", args, head["ms"], config,
+          dtype="f64 orbit + f32 frames" if "mixed" in res else "f64", cpu_baseline=cpu, clocks=sampler.summary(),
+          gpu_launches=int(launches), **extra)
+    return res
+
+
+def _cpu_port(sysm, x0, N, tau, frames, unit, sample):
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    threads = os.cpu_count() or 1
+    t = time.perf_counter()
+    O.oracle_frames(sysm, x0, N, frames, tau=tau, math="portable", threads=threads)
+    dt = time.perf_counter() - t
+    return dict(value=len(x0) * N / dt, unit=unit, cores=threads, kind="port", sample=sample)
+
+
+def workload_standard(args):
+    from chaos_b200 import MGS, QRSpectrum, WrappedStandardMap, torus_state
+    from chaos_b200.propagate import FrameSpec
+    n, N = 4096, 100_000
+    xp = np.random.default_rng(SEED).uniform(0, 2 * np.pi, (n, 2))
+    x0 = np.array([torus_state(z) for z in xp])
+    sysm = WrappedStandardMap(6.0)
+    frames = [FrameSpec(2, (QRSpectrum(MGS()),))]
+
+    def cpu():
+        W0 = np.broadcast_to(np.eye(2), (512, 2, 2)).copy()
+        return _cpu_port(sysm, x0[:512], 20_000, 1, [FrameSpec(2, (QRSpectrum(MGS()),), W0)], "orbit-steps/s",
+                         "512 orbits x 20000 steps of the workload (oracle, all host threads)")
+    res = _propagate_workload(args, "Chirikov standard map K=6 mod 2pi, QRSpectrum(MGS) k=2 tau=1", sysm, x0, N, 1,
+                              frames, "orbit-steps", cpu,
+                              dict(workload="standard-map-k6-4096x1e5-tau1-mgs", orbits=n, N=N, tau=1, W0="I"))
+    st = res["fp64"]["st"]
+    lam = (st[:, 0:4:2] + st[:, 1:4:2]) / st[:, [4]].view(np.int64)
+    print(json.dumps(dict(check="sum of the two exponents", max_abs=float(np.max(np.abs(lam.sum(axis=1)))))),
+          file=sys.stderr)
+
+
+def workload_gauss(args):
+    from chaos_b200 import FLI, MEGNO, Gauss, GivensQR, HenonHeilesFlow, IntegratorMap, QRSpectrum, random_energy_starts
+    from chaos_b200.propagate import FrameSpec
+    n = 16384
+    N = args.N if args.N != N_STEPS else 1_000_000
+    x0 = random_energy_starts(1 / 8, n, seed=SEED)
+    sysm = IntegratorMap(Gauss(3, tol=1e-14), HenonHeilesFlow(), 0.01)
+    chain = (MEGNO(replace=False), FLI(replace=False), QRSpectrum(GivensQR()))
+    frames = [FrameSpec(2, chain)]
+
+    def cpu():
+        W0 = np.broadcast_to(np.eye(4)[:, :2], (256, 4, 2)).copy()
+        return _cpu_port(sysm, x0[:256], 2000, 10, [FrameSpec(2, chain, W0)], "gauss-steps/s",
+                         "256 orbits x 2000 Gauss steps of the workload (oracle, all host threads)")
+    _propagate_workload(args, "Henon-Heiles E=1/8, Gauss-3 tol 1e-14 dt 0.01, MEGNO+FLI+QRSpectrum(Givens) k=2 "
+                        "tau=10", sysm, x0, N, 10, frames, "gauss-steps", cpu,
+                        dict(workload=f"henon-heiles-gauss3-16384x{N:.0e}-tau10", orbits=n, N=N, tau=10, W0="I[:, 1:2]"))
+
+
+def workload_lattice(args):
+    torch, dev, L = _setup()
+    from chaos_b200._lib import last_error
+    from chaos_b200.ensemble import DeviceClass, device_classes_array, lattice_workload
+    stream = torch.cuda.current_stream(dev)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    n_total = args.orbits or 1 << 20
+    classes = lattice_workload(n_total, seed=SEED, precision="mixed")
+    dcs = [DeviceClass(c, torch, dev) for c in classes]
+    tuned = []
+    for dc in dcs:
+        rc = L.cl_b200_ensemble_tune(C.byref(dc.cls), 4096, 2000, C.c_void_p(stream.cuda_stream))
+        if rc != 0:
+            raise RuntimeError(f"cl_b200_ensemble_tune: {rc} {last_error()}")
+        tuned.append(dict(d=dc.c.sys.d, blocks_per_sm=int(dc.cls.minb), tau_unroll=int(dc.cls.unroll)))
+    arr = device_classes_array(dcs)
+    g = C.c_void_p()
+    if L.cl_b200_ensemble_graph_create(arr, len(dcs), C.byref(g)) != 0:
+        raise RuntimeError(last_error())
+    sampler = ClockSampler(0)
+    try:
+        def go():
+            if L.cl_b200_ensemble_graph_launch(g, C.c_void_p(stream.cuda_stream)) != 0:
+                raise RuntimeError(last_error())
+        ms = _event_times(torch, dev, stream, go, args.steps, args.warmup, flush, sampler)
+    finally:
+        L.cl_b200_ensemble_graph_destroy(g)
+    executed, escaped, per_d = 0, 0, {}
+    for dc in dcs:
+        code = dc.t["code"].cpu().numpy()
+        hs = dc.t["hs"].cpu().numpy()
+        steps = np.where(code != 0, hs, dc.c.lengths)
+        executed += int(steps.sum())
+        escaped += int((code == 4).sum())
+        per_d[str(dc.c.sys.d)] = int(steps.sum())
+    value = executed / (np.mean(ms) / 1e3)
+    cpu = None
+    if not args.no_cpu:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle as O
+        threads = os.cpu_count() or 1
+        m, work, t = 24, 0, 0.0
+        for c in classes:
+            W0 = c.frame.W0[:m]
+            from chaos_b200.propagate import FrameSpec
+            t0 = time.perf_counter()
+            r = O.oracle_ensemble(c.sys, c.x0[:m], c.N, FrameSpec(c.frame.k, c.frame.reducers, W0), tau=c.tau,
+                                  K=c.K[:m], lengths=c.lengths[:m], escape=c.escape, threads=threads)
+            t += time.perf_counter() - t0
+            work += int(np.where(r["code"] != 0, r["hstep"], c.lengths[:m]).sum())
+        cpu = dict(value=work / t, unit="orbit-steps/s", cores=threads, kind="port",
+                   sample=f"the first {m} orbits of each d class ({work:.3g} executed orbit-steps; oracle, FP64, all host threads)")
+    _line("executed orbit-steps/s (uneven lattice ensemble, one CUDA graph of persistent work-queue kernels)", value,
+          "orbit-steps/s", args, ms,
+          dict(workload=f"lattice-ensemble-{n_total}-d2/4/8/16-N1e3..1e6-escape1e3", orbits=n_total,
+               executed_orbit_steps=executed, escaped=escaped, executed_by_d=per_d, tuned=tuned,
+               l2="flushed between timed steps (256 MB write)"),
+          dtype="f64 orbit + f32 frames", cpu_baseline=cpu, clocks=sampler.summary(),
+          gpu_launches=len(dcs) * len(ms))
+
+
+def workload_screen(args):
+    torch, dev, L = _setup()
+    from chaos_b200.screen import FEATURE_STEPS, N_FULL, Screen
+    G = int(os.environ.get("SCREEN_GRID", "2048"))
+    n_train = int(os.environ.get("SCREEN_TRAIN", "200000"))
+    sc = Screen(torch, dev)
+    t0 = time.perf_counter()
+    X, label, lam = sc.training_set(n_train, N=N_FULL)
+    torch.cuda.synchronize(dev)
+    t_label = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    net, info = sc.train(X, label, lam, epochs=12, batch=4096)
+    torch.cuda.synchronize(dev)
+    t_train = time.perf_counter() - t0
+    # warm-up of both paths on a small grid, then one timed run each on the full grid
+    sc.screen_grid(net, 128, N=N_FULL)
+    sc.full_grid(128, N=N_FULL)
+    sampler = ClockSampler(0)
+    l0 = L.cl_b200_launch_count()
+    with sampler:
+        res = sc.screen_grid(net, G, N=N_FULL)
+    launches = L.cl_b200_launch_count() - l0
+    plain, t_full = sc.full_grid(G, N=N_FULL)
+    mis = float((res["labels"] != plain).mean())
+    value = res["n"] / res["seconds"]
+    base = res["n"] / t_full
+    cpu = None
+    if not args.no_cpu:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle as O
+        from chaos_b200.propagate import FrameSpec
+        m = 48
+        rng = np.random.default_rng(SEED)
+        x0 = np.stack([rng.uniform(0, 2 * np.pi, m), np.full(m, 0.1), rng.uniform(0, 2 * np.pi, m),
+                       np.full(m, 0.1)], axis=1)
+        W0 = np.broadcast_to(np.eye(4)[:, :2], (m, 4, 2)).copy()
+        threads = os.cpu_count() or 1
+        t0 = time.perf_counter()
+        O.oracle_frames(sc.sys, x0, N_FULL, [FrameSpec(2, sc.frame.reducers, W0)], tau=10, threads=threads)
+        cpu = dict(value=m / (time.perf_counter() - t0), unit="orbits/s", cores=threads, kind="port",
+                   sample=f"{m} grid orbits classified by full FP64 integration to N = 1e5 (oracle, all host threads)")
+    _line("screened orbits/s (learned BF16 MLP screen, 4D coupled-map grid, label final MEGNO > 2.2)", value,
+          "orbits/s", args, [res["seconds"] * 1e3],
+          dict(workload=f"screen-froeschle-grid{G}x{G}-N1e5", grid=G, N=N_FULL, feature_steps=FEATURE_STEPS,
+               training_orbits=n_train, audit=0.05, band=[0.05, 0.95]),
+          dtype="bf16 mlp (f32 accumulate) + f64/f32 orbits", e2e=dict(value=value, unit="orbits/s",
+                                                                       h2d_bytes_per_step=int(res["n"] * 32),
+                                                                       d2h_bytes_per_step=int(res["n"] * 64)),
+          plain_full_integration=dict(value=base, seconds=t_full), speedup_over_full=value / base,
+          misclassification_whole_grid=mis, audit_misclassification=res["audit_misclassification"],
+          unsure=res["unsure"], audited=res["audited"], chaotic_fraction=float(plain.mean()),
+          orbit_steps_screen=res["orbit_steps"], orbit_steps_full=res["full_orbit_steps"],
+          training=dict(label_seconds=t_label, train_seconds=t_train, **{k: v for k, v in info.items() if k != "loss"},
+                        final_loss=info["loss"][-1], positives=float(np.mean(label))),
+          cpu_baseline=cpu, clocks=sampler.summary(), gpu_launches=int(launches))
+
+
+def run_workload(args):
+    {"standard": workload_standard, "gauss": workload_gauss, "lattice": workload_lattice,
+     "screen": workload_screen}[args.workload](args)
+
 
 
 class _Null:

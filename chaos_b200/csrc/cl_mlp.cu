@@ -29,7 +29,8 @@ void capi_count_launch();
 namespace {
 
 constexpr int BM = 128, BK = 32;
-constexpr unsigned kWaitLimit = 1u << 26;   // mbarrier polls before giving up (~seconds; a stuck MMA sets the flag)
+constexpr unsigned kWaitLimit = 1u << 26;   // mbarrier polls before giving up (a stuck MMA sets the flag)
+constexpr uint64_t kWaitNs = 2000000000ull; // and at most 2 s of wall time per wait
 
 __device__ unsigned g_mlp_error;            // nonzero after a bounded wait gave up
 
@@ -55,13 +56,22 @@ __device__ __forceinline__ uint32_t kmajor_off(int row, int k) {
     return static_cast<uint32_t>(((row >> 3) * (BK / 8) + (k >> 3)) * 128 + (row & 7) * 16 + (k & 7) * 2);
 }
 
+__device__ __forceinline__ uint64_t global_ns() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Waits for the mbarrier phase `phase`; gives up after kWaitLimit polls or kWaitNs nanoseconds, whichever first.
 __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t phase) {
+    const uint64_t t0 = global_ns();
     for (unsigned it = 0; it < kWaitLimit; ++it) {
         uint32_t done;
         asm volatile(
             "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
             : "=r"(done) : "r"(bar), "r"(phase) : "memory");
         if (done) return true;
+        if ((it & 255u) == 255u && global_ns() - t0 > kWaitNs) break;
     }
     atomicExch(&g_mlp_error, 1u);
     return false;

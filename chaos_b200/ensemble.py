@@ -139,3 +139,48 @@ def lattice_workload(n_total: int, seed: int = 1, n_max: int = 10 ** 6, n_min: i
         classes.append(EnsembleClass(sysm, x0, FrameSpec(k, (QRSpectrum(HouseholderQR()),), W0), tau, Nmax, K=K,
                                      lengths=L, escape=escape, precision=precision, seed=seed))
     return classes
+
+
+class DeviceClass:
+    """One class's buffers resident on a CUDA device (torch tensors) and its `cl_ensemble_class` pointing at them,
+    for `cl_b200_ensemble_device`, `cl_b200_ensemble_tune` and the graph entry points. x and W come back
+    orbit-major (W as k columns of d, the C side's layout)."""
+
+    def __init__(self, c: EnsembleClass, torch, device):
+        keep: list = []
+        self.c = c
+        self.cls = make_class_struct(c, keep)
+        n, s, d, k = len(c.x0), c.sys.s, c.sys.d, c.frame.k
+        t = torch
+        W0 = keep[1]
+        if W0 is None:
+            raise ValueError("a device class needs an explicit W0")
+        sb = keep[5]["states"].dtype.itemsize if keep[5]["states"] is not None else 0
+        self.t = dict(x0=t.tensor(keep[0], device=device), x=t.empty((n, s), dtype=t.float64, device=device),
+                      W0=t.tensor(W0, device=device), W=t.empty((n, d * k), dtype=t.float64, device=device),
+                      st=t.zeros(max(1, n * sb // 8), dtype=t.int64, device=device),
+                      code=t.zeros(n, dtype=t.int8, device=device), hs=t.zeros(n, dtype=t.int64, device=device),
+                      order=t.tensor(keep[3], device=device))
+        if keep[4] is not None:
+            self.t["K"] = t.tensor(keep[4], device=device)
+        if keep[2] is not None:
+            self.t["N"] = t.tensor(keep[2], device=device)
+        self.state_dtype = keep[5]["states"].dtype if sb else None
+        b = self.cls.buf
+        b.x0, b.x = self.t["x0"].data_ptr(), self.t["x"].data_ptr()
+        b.W0[0], b.W[0] = self.t["W0"].data_ptr(), self.t["W"].data_ptr()
+        b.states[0] = self.t["st"].data_ptr() if sb else None
+        b.code[0], b.hstep[0] = self.t["code"].data_ptr(), self.t["hs"].data_ptr()
+        self.cls.order = self.t["order"].data_ptr()
+        self.cls.K = self.t["K"].data_ptr() if "K" in self.t else None
+        self.cls.N = self.t["N"].data_ptr() if "N" in self.t else None
+        self.orbit_steps = int(np.sum(c.lengths)) if c.lengths is not None else len(c.x0) * int(c.N)
+
+    def states(self) -> np.ndarray | None:
+        if self.state_dtype is None:
+            return None
+        return self.t["st"].cpu().numpy().view(self.state_dtype)[: len(self.c.x0)]
+
+
+def device_classes_array(dcs: list[DeviceClass]):
+    return (_abi.cl_ensemble_class * len(dcs))(*[dc.cls for dc in dcs])

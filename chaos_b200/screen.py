@@ -113,8 +113,17 @@ class Screen:
                        code=b.code.index_select(0, ii), hstep=b.hstep.index_select(0, ii), n=len(idx))
 
     # ---- the pipeline -----------------------------------------------------------------------------------------------
-    def training_set(self, n: int, N: int = N_FULL, seed: int = 11):
-        x0 = np.random.default_rng(seed).uniform(0, 2 * math.pi, (n, 4))
+    def training_set(self, n: int, N: int = N_FULL, seed: int = 11, plane: bool = True):
+        """n labelled orbits: (x1, p1) uniform on [0, 2 pi)^2 with x2 = p2 = 0.1 (the plane the grid screens; on this
+        map ~85 % of it is chaotic), or, with plane = False, all four coordinates uniform (~97 % chaotic: the
+        coupling's mu (1 - cos) term leaves few regular orbits in the full torus). Returns the BF16 features of
+        the orbits that finished without a failure, their labels and their final lambda_1."""
+        rng = np.random.default_rng(seed)
+        if plane:
+            x0 = np.stack([rng.uniform(0, 2 * math.pi, n), np.full(n, 0.1), rng.uniform(0, 2 * math.pi, n),
+                           np.full(n, 0.1)], axis=1)
+        else:
+            x0 = rng.uniform(0, 2 * math.pi, (n, 4))
         b = self.buffers(x0)
         fb, f32 = self.features(b, N)
         label, lam, code = self.finish(b, N)

@@ -264,6 +264,35 @@ CL_API int cl_b200_ensemble_graph_create(const cl_ensemble_class* classes, int32
 CL_API int cl_b200_ensemble_graph_launch(void* graph, void* stream);
 CL_API int cl_b200_ensemble_graph_destroy(void* graph);
 
+/* ---- The learned screen's kernels (no reference counterpart: the reference has no learned component) ---------------
+ * All enqueue on `stream` and take device pointers. BF16 matrices are row-major with 16-byte aligned rows. */
+
+/* C[M x N] = A[M x K] . B[N x K]^T on the tcgen05 tensor cores (BF16 operands, FP32 accumulator in tensor memory),
+ * + bias[N] (NULL: none), epilogue 0 none / 1 GELU (erf form); C32 (FP32) and/or Cbf16 written with row stride ldc;
+ * pre (FP32, NULL: none) receives the value before the epilogue; accumulate adds the old C32. */
+CL_API int cl_b200_gemm_bf16(const void* A, int32_t lda, const void* B, int32_t ldb, int32_t M, int32_t N, int32_t K,
+                             const float* bias, int32_t epilogue, float* C32, void* Cbf16, int32_t ldc, float* pre,
+                             int32_t accumulate, void* stream);
+/* 0, or CL_EDEVICE_LOST after a GEMM's bounded wait on its MMA barrier gave up. */
+CL_API int cl_b200_mlp_status(void);
+CL_API int cl_b200_transpose_bf16(const void* src, int32_t rows, int32_t cols, int32_t lds, void* dst, int32_t ldd,
+                                  void* stream);
+/* dH = dY * GELU'(pre), to BF16 (dHb) and / or FP32 (dH32). */
+CL_API int cl_b200_gelu_backward(const float* dY, const float* pre, int64_t n, void* dHb, float* dH32, void* stream);
+/* out[j] = sum_i X[i, j] (bias gradients). */
+CL_API int cl_b200_col_sum(const float* X, int32_t rows, int32_t cols, int32_t ld, float* out, void* stream);
+/* Per-row loss BCE(logit = column 0, label) + w_reg (column 1 - target)^2 and the mean-loss gradient dL/dlogits. */
+CL_API int cl_b200_head_loss(const float* logits, int32_t B, int32_t ld, const float* label, const float* target,
+                             float w_reg, float* grad, void* gradb, float* row_loss, void* stream);
+/* Adam on FP32 weights (step t >= 1), refreshing their BF16 copy wb and its transpose wbt (rows x cols) if given. */
+CL_API int cl_b200_adam(float* w, const float* g, float* m, float* v, int64_t n, float lr, float b1, float b2, float eps,
+                        int32_t t, void* wb, void* wbt, int32_t rows, int32_t cols, void* stream);
+CL_API int cl_b200_to_bf16(const float* x, int64_t n, void* y, void* stream);
+/* Screening features of window `window` (ending at global step n) from the reducer states of the chain
+ * (MEGNO(replace = false), SALI()) on a k = 2 frame: 3 per window, 4 more after the last; 64 per orbit. */
+CL_API int cl_b200_screen_features(const void* states, int64_t n_orbits, int64_t n, int32_t window, int32_t windows,
+                                   float* f32, void* fbf16, void* stream);
+
 /* The compiled menu: number of kernel instances, and the key of instance i (NULL outside 0..size-1). A key reads
  * "s<system kind>d<d>p<precision>|k<k>:<reducer>,...|..." with reducers QR<alg>, BEN, SALI, GALI, MEGNO<replace>,
  * FLI<replace>, one "|"-terminated group per frame. No reference counterpart (Julia compiles on demand). */
