@@ -27,7 +27,8 @@ Multi-GPU: orbits are independent, so N ranks run N shards of the same size with
             orbit-steps/s;
   screen    the learned screen on the 2048 x 2048 (x1, p1) grid of Froeschle orbits (x2 = p2 = 0.1), N = 1e5:
             screened orbits/s against the plain full integration of every orbit, with the misclassification
-            over the whole grid.
+            over the whole grid;
+  mlp       the screen's network alone: inference rows/s at a batch of 262144 against the BF16 tensor peak.
 """
 from __future__ import annotations
 
@@ -160,7 +161,9 @@ def main() -> None:
     ap.add_argument("--orbits", type=int, default=None, help="orbits per GPU (default: the workload's own)")
     ap.add_argument("--N", type=int, default=N_STEPS)
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
-    ap.add_argument("--workload", default="coupled", choices=["coupled", "standard", "gauss", "lattice", "screen"])
+    ap.add_argument("--only", choices=["fp64", "mixed"], default=None,
+                    help="time one kernel of the default workload and print a short line (a small case for ncu)")
+    ap.add_argument("--workload", default="coupled", choices=["coupled", "standard", "gauss", "lattice", "screen", "mlp"])
     args = ap.parse_args()
     if args.workload != "coupled":
         run_workload(args)
@@ -293,6 +296,16 @@ def main() -> None:
         return ((s1 + c1) / nn).cpu().numpy(), bufs["code"][0].cpu().numpy().copy()
 
     # plain Float64 kernel (the reference's arithmetic), then the mixed kernel
+    if args.only:
+        tk, msk, launches = timed(args.only, args.steps, args.warmup)
+        if rank == 0:
+            print(json.dumps(dict(metric=METRIC, kernel=args.only, value=n * N * world * args.steps / (tk / 1e3),
+                                  unit="orbit-steps/s", ms_per_step=tk / args.steps, orbits=n, N=N,
+                                  tuned_blocks_per_sm=tuned, gpu_launches=int(launches))), flush=True)
+        if world > 1:
+            dist.barrier()
+            dist.destroy_process_group()
+        return
     t64, ms64, _ = timed("fp64", args.steps, args.warmup)
     lam64, code64 = lambdas()
     sampler = ClockSampler(dev.index if world == 1 else local)
@@ -541,10 +554,12 @@ def workload_lattice(args):
     dcs = [DeviceClass(c, torch, dev) for c in classes]
     tuned = []
     for dc in dcs:
-        rc = L.cl_b200_ensemble_tune(C.byref(dc.cls), 4096, 2000, C.c_void_p(stream.cuda_stream))
+        # every queue slot, lengths scaled to 1 % (the longest orbit keeps its share of the class's time)
+        rc = L.cl_b200_ensemble_tune(C.byref(dc.cls), 0, max(dc.c.tau, dc.c.N // 100), C.c_void_p(stream.cuda_stream))
         if rc != 0:
             raise RuntimeError(f"cl_b200_ensemble_tune: {rc} {last_error()}")
-        tuned.append(dict(d=dc.c.sys.d, blocks_per_sm=int(dc.cls.minb), tau_unroll=int(dc.cls.unroll)))
+        tuned.append(dict(d=dc.c.sys.d, blocks_per_sm=int(dc.cls.minb), tau_unroll=int(dc.cls.unroll),
+                          lanes_per_orbit=int(dc.cls.lanes)))
     arr = device_classes_array(dcs)
     g = C.c_void_p()
     if L.cl_b200_ensemble_graph_create(arr, len(dcs), C.byref(g)) != 0:
@@ -647,10 +662,54 @@ def workload_screen(args):
                         final_loss=info["loss"][-1], positives=float(np.mean(label))),
           cpu_baseline=cpu, clocks=sampler.summary(), gpu_launches=int(launches))
 
+def workload_mlp(args):
+    """The learned screen's network on the tensor cores: inference (4 GEMMs with fused bias / GELU epilogues) and one
+    training step (forward, loss, backward GEMMs, Adam) at a batch of 262144 rows."""
+    torch, dev, L = _setup()
+    from chaos_b200.mlp import DIMS, MLP, OUT_PAD
+    B = args.orbits or 262144
+    net = MLP(torch, dev, seed=0)
+    rng = np.random.default_rng(SEED)
+    X = torch.tensor(rng.standard_normal((B, 64)).astype(np.float32), device=dev).to(torch.bfloat16)
+    label = torch.tensor((rng.random(B) < 0.5).astype(np.float32), device=dev)
+    target = torch.tensor(rng.standard_normal(B).astype(np.float32), device=dev)
+    stream = torch.cuda.current_stream(dev)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    # algorithmic FLOPs of one forward: 2 B (64*256 + 256*256 + 256*256 + 256*16), the last layer padded to 16
+    # outputs as the kernel computes it; a training step adds the weight-gradient GEMM of every layer and the
+    # input-gradient GEMM of every layer but the first
+    fin = list(DIMS[:-1])
+    fout = [DIMS[1], DIMS[2], DIMS[3], OUT_PAD]
+    fwd = sum(2 * B * a * b for a, b in zip(fin, fout))
+    bwd = sum(2 * B * a * b for a, b in zip(fin, fout)) + sum(2 * B * a * b for a, b in zip(fin[1:], fout[1:]))
+    sampler = ClockSampler(0)
+    l0 = L.cl_b200_launch_count()
+    ms_fwd = _event_times(torch, dev, stream, lambda: net.forward(X), args.steps, args.warmup, flush, sampler)
+    n_fwd = L.cl_b200_launch_count() - l0
+    ms_train = _event_times(torch, dev, stream, lambda: net.train_step(X, label, target), args.steps, args.warmup,
+                            flush)
+    peaks = {}
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            peaks = json.load(f)
+    except OSError:
+        pass
+    peak = peaks.get("bf16_tflops", 1590.0)
+    achieved = fwd / (np.mean(ms_fwd) / 1e3) / 1e12
+    _line("screen-MLP inference rows/s (BF16 tcgen05 GEMMs, FP32 accumulate, fused bias+GELU)",
+          B / (np.mean(ms_fwd) / 1e3), "rows/s", args, ms_fwd,
+          dict(workload=f"mlp-64x256x256x256x2-batch{B}", batch=B, layers=list(DIMS),
+               l2="flushed between timed steps (256 MB write)"),
+          dtype="bf16 (f32 accumulate)",
+          roofline=dict(bound="tensor", achieved=achieved, peak=peak, unit="TFLOP/s", frac=achieved / peak,
+                        traffic=None, peak_source="MEASURED_PEAKS.json bf16_tflops (burst)" if peaks else "fallback"),
+          training_step=dict(ms=float(np.mean(ms_train)), tflops=(fwd + bwd) / (np.mean(ms_train) / 1e3) / 1e12),
+          clocks=sampler.summary(), gpu_launches=int(n_fwd))
+
 
 def run_workload(args):
     {"standard": workload_standard, "gauss": workload_gauss, "lattice": workload_lattice,
-     "screen": workload_screen}[args.workload](args)
+     "screen": workload_screen, "mlp": workload_mlp}[args.workload](args)
 
 
 

@@ -130,6 +130,8 @@ class cl_ensemble_class(C.Structure):
         ("minb", C.c_int32),
         ("unroll", C.c_int32),
         ("buf", cl_buffers),
+        ("lanes", C.c_int32),
+        ("reserved", C.c_int32),
     ]
 
 

@@ -125,7 +125,7 @@ __global__ void __launch_bounds__(128, MINB) ensemble_kernel(const EArgs a, Sys 
     }
 }
 
-struct ETune { int block, minb, unroll; };
+struct ETune { int block, minb, unroll, lanes; };   // lanes: per orbit (1 = one orbit per thread)
 
 typedef cudaError_t (*ELaunchFn)(const cl_run& run, const EArgs& a, int grid, const ETune& t, cudaStream_t st,
                                  LaunchInfo* info);
@@ -149,6 +149,7 @@ cudaError_t launch_ensemble_v(const cl_run& run, const EArgs& a, int grid, cudaS
 template <class Sys, typename Real, class F, int U>
 cudaError_t launch_ensemble(const cl_run& run, const EArgs& a, int grid, const ETune& t, cudaStream_t st,
                             LaunchInfo* info) {
+    if (t.lanes > 1) return cudaErrorNotSupported;
     const bool unrolled = U > 1 && t.unroll == U && a.tau == U;
     if (unrolled) {
         if (t.minb == 1) return launch_ensemble_v<Sys, Real, F, U, 1>(run, a, grid, st, info);

@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdio>
+#include <algorithm>
 #include <cstring>
 #include <map>
 #include <mutex>
@@ -10,7 +11,7 @@
 #include <vector>
 
 #include "../../include/chaoslab_b200.h"
-#include "cl_ensemble.cuh"
+#include "cl_coop.cuh"
 
 namespace cl {
 
@@ -42,7 +43,7 @@ int sm_count() {
 std::string tune_key(const cl_run& r) { return run_key(r) + "t" + std::to_string(r.tau); }
 
 ETune variant_of(const cl_ensemble_class& c) {
-    ETune t{128, 2, 1};
+    ETune t{128, 2, 1, 1};
     {
         std::lock_guard<std::mutex> g(g_tune_mu);
         auto it = g_tuned.find(tune_key(c.run));
@@ -50,7 +51,9 @@ ETune variant_of(const cl_ensemble_class& c) {
     }
     if (c.minb > 0) t.minb = c.minb;
     if (c.unroll > 0) t.unroll = c.unroll;
+    if (c.lanes > 0) t.lanes = c.lanes;
     if (t.unroll != 1 && t.unroll != c.run.tau) t.unroll = 1;
+    if (t.lanes > 1 && (t.lanes != coop_lanes(c.run) || !c.buf.W0[0])) t.lanes = 1;
     return t;
 }
 
@@ -61,6 +64,9 @@ int check_class(const cl_ensemble_class& c, ELaunchFn* fn) {
     if (c.run.n0 != 0 || (c.run.steps != 0 && c.run.steps != c.run.N)) return capi_fail(CL_EINVAL, "ensembles start fresh and run whole");
     if (c.minb != 0 && c.minb != 1 && c.minb != 2 && c.minb != 4) return capi_fail(CL_EINVAL, "minb must be 0, 1, 2 or 4");
     if (c.unroll < 0) return capi_fail(CL_EINVAL, "unroll must be >= 0");
+    if (c.lanes != 0 && c.lanes != 1 && c.lanes != coop_lanes(c.run))
+        return capi_fail(CL_EINVAL, "lanes must be 0, 1 or, for this class, " + std::to_string(coop_lanes(c.run)));
+    if (c.lanes > 1 && !c.buf.W0[0]) return capi_fail(CL_EINVAL, "lanes > 1 needs an explicit W0");
     *fn = find_ensemble(run_key(c.run));
     if (!*fn) return capi_fail(CL_EUNSUPPORTED, "no compiled ensemble kernel for " + run_key(c.run));
     return 0;
@@ -88,6 +94,22 @@ EArgs eargs(const cl_ensemble_class& c, unsigned long long* counter, int64_t n_l
     a.orbit_base = c.run.orbit_base;
     for (int r = 0; r < c.run.frames[0].n_reducers; ++r) a.prm[r].orthogonality_tol = c.run.frames[0].reducers[r].orthogonality_tol;
     return a;
+}
+
+// The tuner's sample: m queue slots taken at stride n / m (the length distribution and the longest-first order
+// kept), each orbit's length scaled by steps / Nmax (at least tau, a multiple of tau), so the sample's longest
+// orbit against its total work stays what it is in the whole class.
+__global__ void tune_sample(const i64* order, const i64* N, i64 n, i64 m, i64 Nmax, i64 steps, int tau,
+                            i64* order_out, i64* N_out) {
+    const i64 t = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (t >= m) return;
+    const i64 slot = t * n / m;
+    const i64 i = order ? order[slot] : slot;
+    order_out[t] = i;
+    const i64 L = N ? N[i] : Nmax;
+    i64 s = L / Nmax * steps + (L % Nmax) * steps / Nmax;   // L * steps / Nmax without overflow
+    s = s / tau * tau;
+    N_out[i] = s < tau ? tau : s;
 }
 
 struct Forks {   // side streams and events of one enqueue; released after the work (or the capture) ends
@@ -270,40 +292,66 @@ int cl_b200_ensemble_tune(cl_ensemble_class* cls, int64_t sample_orbits, int64_t
     if (rc) return rc;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     const int tau = cls->run.tau;
+    const int64_t n = cls->n_orbits;
     int64_t steps = sample_steps > 0 ? sample_steps : 20 * tau;
-    steps = (steps + tau - 1) / tau * tau;
+    steps = std::max<int64_t>(tau, (std::min<int64_t>(steps, cls->run.N) + tau - 1) / tau * tau);
+    const int64_t m = sample_orbits > 0 && sample_orbits < n ? sample_orbits : n;
+    // device scratch: the queue head, the sample's queue and its scaled lengths (indexed by orbit)
     unsigned long long* counter = nullptr;
+    i64 *ord = nullptr, *len = nullptr;
     cudaError_t e = cudaMalloc(reinterpret_cast<void**>(&counter), sizeof(unsigned long long));
-    if (e != cudaSuccess) return capi_map_cuda(e, "queue head");
+    if (e == cudaSuccess) e = cudaMalloc(reinterpret_cast<void**>(&ord), sizeof(i64) * m);
+    if (e == cudaSuccess) e = cudaMalloc(reinterpret_cast<void**>(&len), sizeof(i64) * n);
+    if (e != cudaSuccess) {
+        cudaFree(counter); cudaFree(ord); cudaFree(len);
+        return capi_map_cuda(e, "tuner scratch");
+    }
+    tune_sample<<<static_cast<unsigned>((m + 255) / 256), 256, 0, st>>>(reinterpret_cast<const i64*>(cls->order),
+        reinterpret_cast<const i64*>(cls->N), n, m, cls->run.N, steps, tau, ord, len);
+    if ((e = cudaGetLastError()) != cudaSuccess) rc = capi_map_cuda(e, "tuner sample");
     const int sms = sm_count();
-    ETune best{128, 2, 1};
+    ETune best{128, 2, 1, 1};
     float best_ms = 1e30f;
+    const int coop = cls->buf.W0[0] ? coop_lanes(cls->run) : 1;
     const int unrolls[2] = {1, (tau == 5 || tau == 10 || tau == 20) ? tau : 1};
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
-    for (int minb : {1, 2, 4})
-        for (int u = 0; u < 2; ++u) {
-            if (u == 1 && unrolls[1] == 1) continue;
-            ETune t{128, minb, unrolls[u]};
-            EArgs a = eargs(*cls, counter, sample_orbits, steps);
-            a.escape = 0.0;
-            float ms = 0.f;
-            for (int rep = 0; rep < 2; ++rep) {   // the first run warms up
+    const int lane_opts[2] = {1, coop};
+    for (int li = 0; li < (coop > 1 ? 2 : 1) && rc == 0; ++li)
+        for (int minb : {1, 2, 4})
+            for (int u = 0; u < 2 && rc == 0; ++u) {
+                if (u == 1 && unrolls[1] == 1) continue;
+                const ETune t{128, minb, unrolls[u], lane_opts[li]};
+                EArgs a = eargs(*cls, counter, m);
+                a.order = ord;
+                a.Np = len;
+                a.N = steps;
+                a.escape = 0.0;
+                // warm-up on a few orbits (module load, attributes), then the timed sample
+                EArgs w = a;
+                w.n = std::min<int64_t>(m, 256);
+                w.Np = nullptr;
+                w.N = tau;
                 cudaMemsetAsync(counter, 0, sizeof(unsigned long long), st);
-                cudaEventRecord(e0, st);
-                e = fn(cls->run, a, sms * minb, t, st, nullptr);
-                cudaEventRecord(e1, st);
-                if (e != cudaSuccess) break;
-                cudaEventSynchronize(e1);
+                e = fn(cls->run, w, sms * minb, t, st, nullptr);
+                if (e == cudaSuccess) {
+                    cudaMemsetAsync(counter, 0, sizeof(unsigned long long), st);
+                    cudaEventRecord(e0, st);
+                    e = fn(cls->run, a, sms * minb, t, st, nullptr);
+                    cudaEventRecord(e1, st);
+                }
+                if (e != cudaSuccess) { rc = capi_map_cuda(e, "tune launch"); break; }
+                float ms = 0.f;
+                if ((e = cudaEventSynchronize(e1)) != cudaSuccess) { rc = capi_map_cuda(e, "tune"); break; }
                 cudaEventElapsedTime(&ms, e0, e1);
+                if (ms < best_ms) { best_ms = ms; best = t; }
             }
-            if (e != cudaSuccess) { rc = capi_map_cuda(e, "tune launch"); break; }
-            if (ms < best_ms) { best_ms = ms; best = t; }
-        }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     cudaFree(counter);
+    cudaFree(ord);
+    cudaFree(len);
     if (rc) return rc;
     {
         std::lock_guard<std::mutex> g(g_tune_mu);
@@ -311,6 +359,7 @@ int cl_b200_ensemble_tune(cl_ensemble_class* cls, int64_t sample_orbits, int64_t
     }
     cls->minb = best.minb;
     cls->unroll = best.unroll;
+    cls->lanes = best.lanes;
     return 0;
 }
 

@@ -14,6 +14,7 @@
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdint>
 #include <cstdio>
 #include <string>
@@ -230,13 +231,22 @@ __global__ void gelu_backward(const float* __restrict__ dY, const float* __restr
     if (dH32) dH32[i] = g;
 }
 
-// Column sums of an FP32 matrix (bias gradients): db[j] = sum_i dH[i, j].
+// Column sums of an FP32 matrix (bias gradients): db[j] = sum_i dH[i, j]. Blocks of 32 columns x 8 row lanes
+// stride over the rows, fold their 8 partial sums in shared memory and add them to the (zeroed) output atomically,
+// so the last bits of a sum depend on the order the blocks finish in.
 __global__ void col_sum(const float* __restrict__ X, int rows, int cols, int ld, float* __restrict__ out) {
-    const int j = blockIdx.x * blockDim.x + threadIdx.x;
-    if (j >= cols) return;
+    __shared__ float part[8][33];
+    const int j = blockIdx.x * 32 + threadIdx.x;
     float s = 0.f;
-    for (int i = 0; i < rows; ++i) s += X[static_cast<size_t>(i) * ld + j];
-    out[j] = s;
+    if (j < cols)
+        for (int i = blockIdx.y * 8 + threadIdx.y; i < rows; i += gridDim.y * 8) s += X[static_cast<size_t>(i) * ld + j];
+    part[threadIdx.y][threadIdx.x] = s;
+    __syncthreads();
+    if (threadIdx.y == 0 && j < cols) {
+        float t = part[0][threadIdx.x];
+        for (int r = 1; r < 8; ++r) t += part[r][threadIdx.x];
+        atomicAdd(out + j, t);
+    }
 }
 
 // Head loss on logits [B x ld] (column 0: chaos logit, column 1: lambda_1 prediction): mean binary cross-entropy
@@ -375,8 +385,13 @@ int cl_b200_gelu_backward(const float* dY, const float* pre, int64_t n, void* dH
 }
 
 int cl_b200_col_sum(const float* X, int32_t rows, int32_t cols, int32_t ld, float* out, void* stream) {
-    col_sum<<<(cols + 127) / 128, 128, 0, static_cast<cudaStream_t>(stream)>>>(X, rows, cols, ld, out);
-    const cudaError_t e = cudaGetLastError();
+    if (!X || !out || rows < 0 || cols <= 0 || ld < cols) return capi_fail(CL_EINVAL, "column sums: bad arguments");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    cudaError_t e = cudaMemsetAsync(out, 0, sizeof(float) * static_cast<size_t>(cols), st);
+    if (e != cudaSuccess) return capi_map_cuda(e, "column sums");
+    const unsigned gy = static_cast<unsigned>(std::min(1024, std::max(1, (rows + 255) / 256)));
+    col_sum<<<dim3((cols + 31) / 32, gy), dim3(32, 8), 0, st>>>(X, rows, cols, ld, out);
+    e = cudaGetLastError();
     return e == cudaSuccess ? 0 : capi_map_cuda(e, "column sums");
 }
 

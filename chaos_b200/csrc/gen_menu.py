@@ -127,12 +127,12 @@ ENSEMBLE = [(SYS_STANDARD, 2, p, 2, ["QR4"], 5) for p in (0, 1)] + \
 
 def render_ensemble(entries):
     out = ['// Generated by chaos_b200/csrc/gen_menu.py (do not edit): ensemble kernel instances.',
-           '#include "cl_ensemble.cuh"', '', 'namespace cl {', 'namespace {']
+           '#include "cl_coop.cuh"', '', 'namespace cl {', 'namespace {']
     for idx, (kind, d, prec, k, ch, U) in enumerate(entries):
         real = "double" if prec == 0 else "float"
         ft = f"Frame<{k}{''.join(', ' + t for t in red_type(ch))}>"
         out.append(f"cudaError_t E{idx}(const cl_run& r, const EArgs& a, int g, const ETune& t, cudaStream_t s, LaunchInfo* i) {{\n"
-                   f"    return launch_ensemble<{sys_type(kind, d)}, {real}, {ft}, {U}>(r, a, g, t, s, i);\n}}\n"
+                   f"    return launch_ensemble_any<{sys_type(kind, d)}, {real}, {ft}, {U}>(r, a, g, t, s, i);\n}}\n"
                    f"const ERegistrar R{idx}(\"{key(kind, d, prec, [(k, ch)])}\", E{idx});")
     out += ['}  // namespace', '}  // namespace cl', '']
     return "\n".join(out)

@@ -38,6 +38,7 @@ class EnsembleClass:
     seed: int = 0
     minb: int = 0
     unroll: int = 0
+    lanes: int = 0       # lanes per orbit: 1, or the lattice's site count (cooperative kernel); 0 = tuned/default
 
 
 @dataclass
@@ -75,7 +76,7 @@ def make_class_struct(c: EnsembleClass, keep: list) -> _abi.cl_ensemble_class:
     cs.run = run
     cs.n_orbits = n
     cs.escape = float(c.escape)
-    cs.minb, cs.unroll = c.minb, c.unroll
+    cs.minb, cs.unroll, cs.lanes = c.minb, c.unroll, c.lanes
     W0 = None if c.frame.W0 is None else np.ascontiguousarray(np.asarray(c.frame.W0, dtype=np.float64).transpose(0, 2, 1))
     lengths = None if c.lengths is None else np.ascontiguousarray(c.lengths, dtype=np.int64)
     order = queue_order(lengths if lengths is not None else np.full(n, c.N))

@@ -234,6 +234,11 @@ typedef struct cl_ensemble_class {
     int32_t minb;          /* kernel variant: register cap as blocks per SM (1, 2 or 4); 0 = tuned/default     */
     int32_t unroll;        /* kernel variant: tau loop unrolled (tau itself, when tau is 5, 10 or 20) or 1; 0 = tuned/default */
     cl_buffers buf;        /* frame 0 only                                                                      */
+    int32_t lanes;         /* kernel variant: lanes per orbit, 1 (one orbit per thread) or, for lattices of
+                              2, 4 or 8 sites reduced by QRSpectrum(HouseholderQR) with k a multiple of the sites and
+                              an explicit W0, the number of sites (the sites and the frame's columns spread over
+                              that many lanes); 0 = tuned/default                                               */
+    int32_t reserved;      /* 0                                                                                 */
 } cl_ensemble_class;
 
 /* Run the classes on device buffers, enqueued on `stream`; the queue heads are allocated and freed in stream
@@ -253,9 +258,10 @@ CL_API int cl_b200_ensemble_device_noalloc(const cl_ensemble_class* classes, int
 /* The same on host buffers: copies in, runs, copies out (synchronous). */
 CL_API int cl_b200_ensemble(const cl_ensemble_class* classes, int32_t n_classes, cl_prov* prov);
 
-/* Autotune one class on its device buffers: times every kernel variant on a sample of the queue (at most
- * `sample_orbits` orbits, `sample_steps` steps each) and writes the fastest (minb, unroll) into the class.
- * The buffers' contents are overwritten. */
+/* Autotune one class on its device buffers: times every kernel variant (register cap, tau unrolling, lanes per
+ * orbit) on a sample of the queue and writes the fastest (minb, unroll, lanes) into the class. The sample is
+ * `sample_orbits` queue slots at an even stride (all of them when <= 0 or >= n_orbits) with every length scaled by
+ * sample_steps / run.N, so the longest orbit keeps its share of the work. The buffers' contents are overwritten. */
 CL_API int cl_b200_ensemble_tune(cl_ensemble_class* cls, int64_t sample_orbits, int64_t sample_steps, void* stream);
 
 /* Capture the classes' launches (queue resets included) into one CUDA graph on device buffers; launching the
