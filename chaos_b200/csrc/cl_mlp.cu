@@ -4,13 +4,15 @@
 // No reference counterpart: the reference has no learned component.
 //
 // GEMM: C[M x N] = A[M x K] . B[N x K]^T (+ bias[N]) (+ C when accumulating), A and B row-major BF16 (K contiguous:
-// both operands K-major). One CTA of 128 threads computes a 128 x NT tile (NT = 16..256): the CTA stages 128 x 32
-// and NT x 32 BF16 blocks of A and B in shared memory in the canonical K-major no-swizzle layout (8-row x 16-byte
-// core matrices, the two 8-element K halves of an MMA LBO = 128 B apart, consecutive 8-row groups SBO = 512 B
-// apart), one elected thread issues two tcgen05.mma (M = 128, N = NT, K = 16 each) per block into an FP32 tile in
-// tensor memory and commits them to an mbarrier, and after the last block each warp reads its 32 rows back with
-// tcgen05.ld (warp w owns TMEM lanes 32w..32w+31) for the epilogue. Every wait on the mbarrier is bounded: past
-// the limit the kernel records an error flag and returns instead of spinning on.
+// both operands K-major). One CTA of 128 threads computes a 128 x NT tile (NT = 16..256) over its K range: a ring
+// of 3-4 shared-memory stages, each a 128 x 64 block of A and an NT x 64 block of B in the canonical K-major
+// no-swizzle layout (8-row x 16-byte core matrices, the two 8-element K halves of an MMA LBO = 128 B apart,
+// consecutive 8-row groups SBO = 1024 B apart), filled by cp.async; one thread issues four tcgen05.mma (M = 128,
+// N = NT, K = 16) per stage into an FP32 tile in tensor memory and commits them to the stage's mbarrier; after the
+// last block each warp reads its 32 rows back with tcgen05.ld (warp w owns TMEM lanes 32w..32w+31) for the fused
+// epilogue. Long-K products with few output tiles (weight gradients) split K over CTAs and add their partial tiles
+// atomically. Every wait on an mbarrier is bounded: past the limit the kernel records an error flag and returns
+// instead of spinning on.
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
@@ -29,7 +31,7 @@ void capi_count_launch();
 
 namespace {
 
-constexpr int BM = 128, BK = 32;
+constexpr int BM = 128, BK = 64;
 constexpr unsigned kWaitLimit = 1u << 26;   // mbarrier polls before giving up (a stuck MMA sets the flag)
 constexpr uint64_t kWaitNs = 2000000000ull; // and at most 2 s of wall time per wait
 
@@ -78,20 +80,57 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t phase) {
     return false;
 }
 
-template <int NT>
+// Async 16-byte global -> shared copy; src_bytes < 16 zero-fills the rest (0: nothing is read).
+__device__ __forceinline__ void cp_async16(uint32_t dst, const void* src, uint32_t src_bytes) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" :: "r"(dst), "l"(src), "r"(src_bytes) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" :: "n"(N) : "memory"); }
+
+// Stages one BM x BK (or NT x BK) block of a K-major BF16 matrix into the canonical no-swizzle layout. Chunk c of
+// the tile (16 bytes = 8 elements) is row (c >> 6) * 8 + (c & 7), K-chunk (c >> 3) & 7: the 32 lanes of a warp
+// cover 8 rows x 4 K-chunks, i.e. 64 contiguous bytes of each row in global memory and 8 distinct 16-byte bank
+// groups in shared memory (4 wavefronts per 512 bytes, no conflicts).
+template <int ROWS>
+__device__ __forceinline__ void stage_tile(uint32_t dst, const __nv_bfloat16* __restrict__ G, int ld, int r0,
+                                           int rows, int k0, int K, int tid) {
+#pragma unroll
+    for (int c = tid; c < ROWS * (BK / 8); c += 128) {
+        const int r = (c >> 6) * 8 + (c & 7), kc = (c >> 3) & 7;
+        const int gr = r0 + r, gk = k0 + kc * 8;
+        const int valid = gr < rows ? max(0, min(8, K - gk)) : 0;
+        const __nv_bfloat16* src = valid ? G + static_cast<size_t>(gr) * ld + gk : G;
+        cp_async16(dst + kmajor_off(r, kc * 8), src, static_cast<uint32_t>(valid * 2));
+    }
+}
+
+// C[M x N] (+)= A . B^T: one CTA of 128 threads per 128 x NT output tile and K range (split-K over gridDim.z).
+// STAGES-deep ring of shared-memory stages filled by cp.async; one thread issues the stage's BK / 16 MMAs and
+// commits them to the stage's mbarrier, which the copies into that stage wait on before it is refilled, so the
+// loads of the next STAGES - 1 blocks overlap the tensor cores. With split-K (gridDim.z > 1) the partial tiles are
+// added to C32 with atomics (C32 zeroed by the caller; no bias, epilogue or BF16 output).
+template <int NT, int STAGES>
 __global__ void __launch_bounds__(128, 1) gemm_bf16_tc(const __nv_bfloat16* __restrict__ A, int lda,
                                                        const __nv_bfloat16* __restrict__ B, int ldb, int M, int N,
                                                        int K, const float* __restrict__ bias, int epilogue,
                                                        float* __restrict__ C32, __nv_bfloat16* __restrict__ Cb,
                                                        int ldc, float* __restrict__ pre, int accumulate) {
     constexpr int TCOLS = NT < 32 ? 32 : NT;   // TMEM allocation: a power of two, at least 32 columns
+    constexpr int A_BYTES = BM * BK * 2, B_BYTES = NT * BK * 2, STAGE_BYTES = A_BYTES + B_BYTES;
     static_assert((NT % 16) == 0 && NT >= 16 && NT <= 256, "N tile");
-    __shared__ __align__(1024) uint8_t sA[BM * BK * 2];
-    __shared__ __align__(1024) uint8_t sB[NT * BK * 2];
-    __shared__ __align__(8) uint64_t mbar;
+    extern __shared__ __align__(1024) uint8_t gsm[];
+    __shared__ __align__(8) uint64_t mbar[STAGES];
     __shared__ uint32_t tmem_base;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int m0 = blockIdx.x * BM, n0 = blockIdx.y * NT;
+    const int kblocks_all = (K + BK - 1) / BK;
+    const int per = (kblocks_all + gridDim.z - 1) / gridDim.z;
+    const int kb0 = blockIdx.z * per, kb1 = min(kblocks_all, kb0 + per), nkb = max(0, kb1 - kb0);
+    const bool split = gridDim.z > 1;
+    // vector epilogue: rows of C / pre start 32-byte aligned (ldc % 8 == 0 and 32-byte aligned bases)
+    const bool vec = (ldc % 8) == 0 && (reinterpret_cast<uintptr_t>(C32) & 31) == 0 &&
+                     (reinterpret_cast<uintptr_t>(Cb) & 15) == 0 && (reinterpret_cast<uintptr_t>(pre) & 31) == 0;
 
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n"
@@ -99,72 +138,70 @@ __global__ void __launch_bounds__(128, 1) gemm_bf16_tc(const __nv_bfloat16* __re
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
     }
     if (tid == 0) {
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" :: "r"(smem_u32(&mbar)) : "memory");
+        for (int s = 0; s < STAGES; ++s)
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" :: "r"(smem_u32(&mbar[s])) : "memory");
         asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
     }
     asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
     const uint32_t tmem = tmem_base;
-    const uint32_t bar = smem_u32(&mbar);
+    const uint32_t sbase = smem_u32(gsm);
     constexpr uint32_t idesc = idesc_bf16(BM, NT);
-    uint32_t phase = 0;
     bool ok = true;
 
-    const int kblocks = (K + BK - 1) / BK;
-    for (int kb = 0; kb < kblocks && ok; ++kb) {
-        const int k0 = kb * BK;
-        // stage A (128 x 64) and B (NT x 64): 8-element (16-byte) chunks, zero outside the matrices
-        for (int c = tid; c < BM * (BK / 8); c += 128) {
-            const int row = c / (BK / 8), kc = (c % (BK / 8)) * 8;
-            const int gr = m0 + row, gk = k0 + kc;
-            uint4 v = make_uint4(0, 0, 0, 0);
-            if (gr < M && gk + 8 <= K) v = *reinterpret_cast<const uint4*>(A + static_cast<size_t>(gr) * lda + gk);
-            else if (gr < M && gk < K) {
-                __nv_bfloat16 t[8];
-                for (int e = 0; e < 8; ++e) t[e] = gk + e < K ? A[static_cast<size_t>(gr) * lda + gk + e] : __float2bfloat16(0.f);
-                v = *reinterpret_cast<uint4*>(t);
-            }
-            *reinterpret_cast<uint4*>(sA + kmajor_off(row, kc)) = v;
+    // prologue: the first STAGES - 1 blocks in flight (one commit group per block, empty past the end)
+#pragma unroll
+    for (int s = 0; s < STAGES - 1; ++s) {
+        if (s < nkb) {
+            const uint32_t st = sbase + s * STAGE_BYTES;
+            stage_tile<BM>(st, A, lda, m0, M, (kb0 + s) * BK, K, tid);
+            stage_tile<NT>(st + A_BYTES, B, ldb, n0, N, (kb0 + s) * BK, K, tid);
         }
-        for (int c = tid; c < NT * (BK / 8); c += 128) {
-            const int row = c / (BK / 8), kc = (c % (BK / 8)) * 8;
-            const int gr = n0 + row, gk = k0 + kc;
-            uint4 v = make_uint4(0, 0, 0, 0);
-            if (gr < N && gk + 8 <= K) v = *reinterpret_cast<const uint4*>(B + static_cast<size_t>(gr) * ldb + gk);
-            else if (gr < N && gk < K) {
-                __nv_bfloat16 t[8];
-                for (int e = 0; e < 8; ++e) t[e] = gk + e < K ? B[static_cast<size_t>(gr) * ldb + gk + e] : __float2bfloat16(0.f);
-                v = *reinterpret_cast<uint4*>(t);
-            }
-            *reinterpret_cast<uint4*>(sB + kmajor_off(row, kc)) = v;
-        }
-        // the generic-proxy writes must be visible to the tensor core's async proxy
-        asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
-        asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
-        __syncthreads();
+        cp_async_commit();
+    }
+    for (int i = 0; i < nkb && ok; ++i) {
+        const int s = i % STAGES;
+        cp_async_wait<STAGES - 2>();          // this thread's copies of block i have landed
+        asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");   // visible to the tensor cores
+        __syncthreads();                       // ... and every other thread's
         asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
         if (tid == 0) {
+            const uint32_t st = sbase + s * STAGE_BYTES;
 #pragma unroll
-            for (int s = 0; s < BK / 16; ++s) {
-                const uint64_t da = smem_desc(smem_u32(sA) + s * 256, 128, (BK / 8) * 128);
-                const uint64_t db = smem_desc(smem_u32(sB) + s * 256, 128, (BK / 8) * 128);
-                const uint32_t acc = (kb > 0 || s > 0) ? 1u : 0u;
+            for (int k = 0; k < BK / 16; ++k) {
+                const uint64_t da = smem_desc(st + k * 256, 128, (BK / 8) * 128);
+                const uint64_t db = smem_desc(st + A_BYTES + k * 256, 128, (BK / 8) * 128);
+                const uint32_t acc = (i > 0 || k > 0) ? 1u : 0u;
                 asm volatile(
                     "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
                     " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n"
                     :: "r"(tmem), "l"(da), "l"(db), "r"(idesc), "r"(acc) : "memory");
             }
             asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n"
-                         :: "r"(bar) : "memory");
+                         :: "r"(smem_u32(&mbar[s])) : "memory");
         }
-        // every thread waits for the MMAs of this block before the tiles are overwritten (or read back)
-        ok = mbar_wait(bar, phase);
-        phase ^= 1u;
-        asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+        // refill the stage of block i - 1 with block i + STAGES - 1, once block i - 1's MMAs are done with it
+        const int nx = i + STAGES - 1;
+        if (nx < nkb) {
+            if (i >= 1) {
+                const int ps = (i - 1) % STAGES;
+                ok = mbar_wait(smem_u32(&mbar[ps]), static_cast<uint32_t>(((i - 1) / STAGES) & 1));
+            }
+            if (ok) {
+                const uint32_t st = sbase + (nx % STAGES) * STAGE_BYTES;
+                stage_tile<BM>(st, A, lda, m0, M, (kb0 + nx) * BK, K, tid);
+                stage_tile<NT>(st + A_BYTES, B, ldb, n0, N, (kb0 + nx) * BK, K, tid);
+            }
+        }
+        cp_async_commit();
     }
+    cp_async_wait<0>();
+    // the last block's commit completes after every earlier MMA
+    if (ok && nkb > 0) ok = mbar_wait(smem_u32(&mbar[(nkb - 1) % STAGES]), static_cast<uint32_t>(((nkb - 1) / STAGES) & 1));
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
 
-    if (ok) {
+    if (ok && nkb > 0) {
         // epilogue: warp w reads TMEM lanes 32w..32w+31 (its rows), 16 columns at a time
         const int row = m0 + warp * 32 + lane;
 #pragma unroll 1
@@ -178,18 +215,66 @@ __global__ void __launch_bounds__(128, 1) gemm_bf16_tc(const __nv_bfloat16* __re
                 : "r"(taddr));
             asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
             if (row < M) {
+                const int colb = n0 + c0;
+                const size_t at0 = static_cast<size_t>(row) * ldc + colb;
+                if (split) {
 #pragma unroll
-                for (int j = 0; j < 16; ++j) {
-                    const int col = n0 + c0 + j;
-                    if (col >= N) continue;
-                    float v = __uint_as_float(r[j]);
-                    const size_t at = static_cast<size_t>(row) * ldc + col;
-                    if (accumulate && C32) v += C32[at];
-                    if (bias) v += bias[col];
-                    if (pre) pre[at] = v;
-                    if (epilogue == 1) v = 0.5f * v * (1.0f + erff(v * 0.70710678118654752f));   // GELU (erf form)
-                    if (C32) C32[at] = v;
-                    if (Cb) Cb[at] = __float2bfloat16(v);
+                    for (int j = 0; j < 16; ++j)
+                        if (colb + j < N) atomicAdd(C32 + at0 + j, __uint_as_float(r[j]));
+                } else if (vec && colb + 16 <= N) {
+                    // a whole 16-column chunk: 16-byte loads and stores (rows 32-byte aligned: ldc % 8 == 0)
+                    float v[16];
+#pragma unroll
+                    for (int j = 0; j < 16; ++j) v[j] = __uint_as_float(r[j]);
+                    if (accumulate && C32) {
+#pragma unroll
+                        for (int q = 0; q < 4; ++q) {
+                            const float4 c = reinterpret_cast<const float4*>(C32 + at0)[q];
+                            v[4 * q] += c.x; v[4 * q + 1] += c.y; v[4 * q + 2] += c.z; v[4 * q + 3] += c.w;
+                        }
+                    }
+                    if (bias) {
+#pragma unroll
+                        for (int j = 0; j < 16; ++j) v[j] += bias[colb + j];
+                    }
+                    if (pre) {
+#pragma unroll
+                        for (int q = 0; q < 4; ++q)
+                            reinterpret_cast<float4*>(pre + at0)[q] = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+                    }
+                    if (epilogue == 1) {
+#pragma unroll
+                        for (int j = 0; j < 16; ++j) v[j] = 0.5f * v[j] * (1.0f + erff(v[j] * 0.70710678118654752f));
+                    }
+                    if (C32) {
+#pragma unroll
+                        for (int q = 0; q < 4; ++q)
+                            reinterpret_cast<float4*>(C32 + at0)[q] = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+                    }
+                    if (Cb) {
+                        uint32_t w[8];
+#pragma unroll
+                        for (int q = 0; q < 8; ++q) {
+                            const __nv_bfloat162 h = __floats2bfloat162_rn(v[2 * q], v[2 * q + 1]);
+                            w[q] = *reinterpret_cast<const uint32_t*>(&h);
+                        }
+                        reinterpret_cast<uint4*>(Cb + at0)[0] = make_uint4(w[0], w[1], w[2], w[3]);
+                        reinterpret_cast<uint4*>(Cb + at0)[1] = make_uint4(w[4], w[5], w[6], w[7]);
+                    }
+                } else {
+#pragma unroll
+                    for (int j = 0; j < 16; ++j) {
+                        const int col = colb + j;
+                        if (col >= N) continue;
+                        float v = __uint_as_float(r[j]);
+                        const size_t at = at0 + j;
+                        if (accumulate && C32) v += C32[at];
+                        if (bias) v += bias[col];
+                        if (pre) pre[at] = v;
+                        if (epilogue == 1) v = 0.5f * v * (1.0f + erff(v * 0.70710678118654752f));   // GELU (erf form)
+                        if (C32) C32[at] = v;
+                        if (Cb) Cb[at] = __float2bfloat16(v);
+                    }
                 }
             }
         }
@@ -331,11 +416,19 @@ __global__ void f32_to_bf16(const float* __restrict__ x, int64_t n, __nv_bfloat1
 
 template <int NT>
 cudaError_t launch_gemm(const void* A, int lda, const void* B, int ldb, int M, int N, int K, const float* bias,
-                        int epi, float* C32, void* Cb, int ldc, float* pre, int acc, cudaStream_t st) {
-    dim3 grid((M + BM - 1) / BM, (N + NT - 1) / NT);
-    gemm_bf16_tc<NT><<<grid, 128, 0, st>>>(static_cast<const __nv_bfloat16*>(A), lda,
-                                           static_cast<const __nv_bfloat16*>(B), ldb, M, N, K, bias, epi, C32,
-                                           static_cast<__nv_bfloat16*>(Cb), ldc, pre, acc);
+                        int epi, float* C32, void* Cb, int ldc, float* pre, int acc, int splits, cudaStream_t st) {
+    constexpr int STAGES = NT >= 256 ? 3 : 4;
+    constexpr int smem = STAGES * (BM + NT) * BK * 2;
+    auto k = gemm_bf16_tc<NT, STAGES>;
+    static bool attr = false;   // one attribute call per instantiation (idempotent)
+    if (!attr) {
+        const cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        if (e != cudaSuccess) return e;
+        attr = true;
+    }
+    dim3 grid((M + BM - 1) / BM, (N + NT - 1) / NT, splits);
+    k<<<grid, 128, smem, st>>>(static_cast<const __nv_bfloat16*>(A), lda, static_cast<const __nv_bfloat16*>(B), ldb,
+                               M, N, K, bias, epi, C32, static_cast<__nv_bfloat16*>(Cb), ldc, pre, acc);
     return cudaGetLastError();
 }
 
@@ -349,16 +442,34 @@ extern "C" {
 int cl_b200_gemm_bf16(const void* A, int32_t lda, const void* B, int32_t ldb, int32_t M, int32_t N, int32_t K,
                       const float* bias, int32_t epilogue, float* C32, void* Cbf16, int32_t ldc, float* pre,
                       int32_t accumulate, void* stream) {
-    if (!A || !B || M <= 0 || N <= 0 || K <= 0 || (!C32 && !Cbf16)) return capi_fail(CL_EINVAL, "gemm: bad arguments");
-    if ((lda % 8) || (ldb % 8) || (reinterpret_cast<uintptr_t>(A) % 16) || (reinterpret_cast<uintptr_t>(B) % 16))
-        return capi_fail(CL_EINVAL, "gemm: operands need 16-byte aligned rows (ld a multiple of 8)");
+    if (!A || !B || M <= 0 || N <= 0 || K <= 0 || (!C32 && !Cbf16) || ldc < N)
+        return capi_fail(CL_EINVAL, "gemm: bad arguments");
+    if ((lda % 8) || (ldb % 8) || lda < K || ldb < K || (reinterpret_cast<uintptr_t>(A) % 16) ||
+        (reinterpret_cast<uintptr_t>(B) % 16))
+        return capi_fail(CL_EINVAL, "gemm: operands need 16-byte aligned rows (ld a multiple of 8, at least K)");
     if (epilogue != 0 && epilogue != 1) return capi_fail(CL_EINVAL, "gemm: epilogue 0 (none) or 1 (GELU)");
     cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const int nt = N <= 16 ? 16 : N <= 64 ? 64 : N <= 128 ? 128 : 256;
+    // split-K when the output tiles cannot fill the GPU and K is long (weight gradients: K = the batch); only
+    // for a plain FP32 result, which the partial tiles are added into
+    const int64_t tiles = static_cast<int64_t>((M + BM - 1) / BM) * ((N + nt - 1) / nt);
+    const int kblocks = (K + BK - 1) / BK;
+    int splits = 1;
+    if (C32 && !Cbf16 && !bias && !pre && epilogue == 0 && tiles < 148 && kblocks >= 16) {
+        splits = static_cast<int>(std::min<int64_t>(kblocks / 8, (2 * 148 + tiles - 1) / tiles));
+        splits = std::max(1, std::min(splits, 1024));
+        // the partial sums start from zero, or from C when accumulating
+        if (!accumulate) {
+            const cudaError_t e = cudaMemset2DAsync(C32, sizeof(float) * static_cast<size_t>(ldc), 0,
+                                                    sizeof(float) * static_cast<size_t>(N), static_cast<size_t>(M), st);
+            if (e != cudaSuccess) return capi_map_cuda(e, "gemm zero");
+        }
+    }
     cudaError_t e;
-    if (N <= 16) e = launch_gemm<16>(A, lda, B, ldb, M, N, K, bias, epilogue, C32, Cbf16, ldc, pre, accumulate, st);
-    else if (N <= 64) e = launch_gemm<64>(A, lda, B, ldb, M, N, K, bias, epilogue, C32, Cbf16, ldc, pre, accumulate, st);
-    else if (N <= 128) e = launch_gemm<128>(A, lda, B, ldb, M, N, K, bias, epilogue, C32, Cbf16, ldc, pre, accumulate, st);
-    else e = launch_gemm<256>(A, lda, B, ldb, M, N, K, bias, epilogue, C32, Cbf16, ldc, pre, accumulate, st);
+    if (nt == 16) e = launch_gemm<16>(A, lda, B, ldb, M, N, K, bias, epilogue, C32, Cbf16, ldc, pre, accumulate, splits, st);
+    else if (nt == 64) e = launch_gemm<64>(A, lda, B, ldb, M, N, K, bias, epilogue, C32, Cbf16, ldc, pre, accumulate, splits, st);
+    else if (nt == 128) e = launch_gemm<128>(A, lda, B, ldb, M, N, K, bias, epilogue, C32, Cbf16, ldc, pre, accumulate, splits, st);
+    else e = launch_gemm<256>(A, lda, B, ldb, M, N, K, bias, epilogue, C32, Cbf16, ldc, pre, accumulate, splits, st);
     capi_count_launch();
     return e == cudaSuccess ? 0 : capi_map_cuda(e, "gemm launch");
 }

@@ -40,6 +40,26 @@ def test_gemm_matches_fp64(torch_dev, M, N, K, gelu, bias):
     assert np.max(np.abs(C32.cpu().numpy() - want)) <= 2e-5 * scale
 
 
+@pytest.mark.parametrize("M,N,K,accumulate", [(256, 64, 8192, False), (16, 256, 4096, True), (256, 256, 20000, False)])
+def test_gemm_split_k_matches_fp64(torch_dev, M, N, K, accumulate):
+    """Weight-gradient shapes (few output tiles, K = the batch): K is split over CTAs whose partial tiles are added
+    into the FP32 result (zeroed first, or added to C when accumulating)."""
+    torch, dev = torch_dev
+    from chaos_b200.mlp import gemm
+    rng = np.random.default_rng(M * 7 + K)
+    A = MO.bf16_round(rng.standard_normal((M, K)))
+    B = MO.bf16_round(rng.standard_normal((N, K)))
+    C0 = rng.standard_normal((M, N)).astype(np.float32)
+    At = torch.tensor(A.astype(np.float32), device=dev).to(torch.bfloat16)
+    Bt = torch.tensor(B.astype(np.float32), device=dev).to(torch.bfloat16)
+    C32 = torch.tensor(C0, device=dev) if accumulate else torch.full((M, N), 7.0, dtype=torch.float32, device=dev)
+    gemm(At, Bt, M, N, K, C32=C32, accumulate=accumulate, stream=torch.cuda.current_stream(dev).cuda_stream)
+    torch.cuda.synchronize(dev)
+    Z = A @ B.T + (C0.astype(np.float64) if accumulate else 0.0)
+    scale = np.max(np.abs(A @ B.T))
+    assert np.max(np.abs(C32.cpu().numpy() - Z)) <= 2e-5 * scale
+
+
 def test_forward_backward_match_oracle(torch_dev):
     torch, dev = torch_dev
     from chaos_b200.mlp import MLP
