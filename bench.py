@@ -52,6 +52,9 @@ TAU = 10
 NU = KAPPA = 1.5
 MU = 0.05
 SEED = 1
+# DRAM bytes per orbit of one launch of the mixed kernel (ncu capture of 32768 orbits: 5.376 MB read, 4.6 KB
+# written; the records written stay in the 126 MB L2 at that size)
+TRAFFIC_PER_ORBIT = (5.376256e6 + 4.608e3) / 32768
 METRIC = "orbit-steps/s (4D coupled standard maps, QRSpectrum(Householder) + GALI_4 + SALI, mixed-precision kernel)"
 
 
@@ -381,7 +384,11 @@ def main() -> None:
                              max_abs_dlambda1=dl1, roofline_tflops=achieved64, frac_of_fp64_peak=achieved64 / fp64_peak),
             e2e=dict(value=e2e_value, unit="orbit-steps/s", h2d_bytes_per_step=int(h2d), d2h_bytes_per_step=int(d2h)),
             roofline=dict(bound="fp64", achieved=achieved, peak=fp64_peak, unit="TFLOP/s", frac=achieved / fp64_peak,
-                          traffic=None, peak_source="cuBLAS DGEMM 8192^3 measured here (burst)",
+                          traffic=TRAFFIC_PER_ORBIT * n,
+                          traffic_source="ncu dram__bytes_read + dram__bytes_write of the mixed kernel on 32768 orbits "
+                                         "x 2000 steps (5.38e6 B), scaled by orbits: DRAM bytes grow with the orbits "
+                                         "loaded and stored, not with the steps",
+                          peak_source="cuBLAS DGEMM 8192^3 measured here (burst)",
                           flops_per_orbit_step=fl),
             cpu_baseline=cpu, clocks=clocks, gpu_launches=int(launches),
         )
@@ -702,7 +709,9 @@ def workload_mlp(args):
                l2="flushed between timed steps (256 MB write)"),
           dtype="bf16 (f32 accumulate)",
           roofline=dict(bound="tensor", achieved=achieved, peak=peak, unit="TFLOP/s", frac=achieved / peak,
-                        traffic=None, peak_source="MEASURED_PEAKS.json bf16_tflops (burst)" if peaks else "fallback"),
+                        traffic=None, peak_source="MEASURED_PEAKS.json bf16_tflops (burst)" if peaks else "fallback",
+                        dram_read_per_layer_b=33.8e6 * B / 65536,
+                        dram_source="ncu: 256x256 layer at 65536 rows reads 33.8 MB (its input once), scaled by rows"),
           training_step=dict(ms=float(np.mean(ms_train)), tflops=(fwd + bwd) / (np.mean(ms_train) / 1e3) / 1e12),
           clocks=sampler.summary(), gpu_launches=int(n_fwd))
 

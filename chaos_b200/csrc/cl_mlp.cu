@@ -5,7 +5,7 @@
 //
 // GEMM: C[M x N] = A[M x K] . B[N x K]^T (+ bias[N]) (+ C when accumulating), A and B row-major BF16 (K contiguous:
 // both operands K-major). One CTA of 128 threads computes a 128 x NT tile (NT = 16..256) over its K range: a ring
-// of 3-4 shared-memory stages, each a 128 x 64 block of A and an NT x 64 block of B in the canonical K-major
+// of 2-3 shared-memory stages, each a 128 x 64 block of A and an NT x 64 block of B in the canonical K-major
 // no-swizzle layout (8-row x 16-byte core matrices, the two 8-element K halves of an MMA LBO = 128 B apart,
 // consecutive 8-row groups SBO = 1024 B apart), filled by cp.async; one thread issues four tcgen05.mma (M = 128,
 // N = NT, K = 16) per stage into an FP32 tile in tensor memory and commits them to the stage's mbarrier; after the
@@ -417,7 +417,8 @@ __global__ void f32_to_bf16(const float* __restrict__ x, int64_t n, __nv_bfloat1
 template <int NT>
 cudaError_t launch_gemm(const void* A, int lda, const void* B, int ldb, int M, int N, int K, const float* bias,
                         int epi, float* C32, void* Cb, int ldc, float* pre, int acc, int splits, cudaStream_t st) {
-    constexpr int STAGES = NT >= 256 ? 3 : 4;
+    // two CTAs per SM (one's epilogue overlaps the other's main loop): 96 KB of stages at NT = 256 and 128
+    constexpr int STAGES = NT >= 256 ? 2 : 3;
     constexpr int smem = STAGES * (BM + NT) * BK * 2;
     auto k = gemm_bf16_tc<NT, STAGES>;
     static bool attr = false;   // one attribute call per instantiation (idempotent)
