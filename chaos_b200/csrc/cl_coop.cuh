@@ -73,7 +73,7 @@ __device__ __forceinline__ T window_Gw_sm(const T* R0, T* ri) {
 #pragma unroll 1
         for (int i = 0; i < K; ++i) b = (jc == 0 && i == 0) ? ri[0] * ri[0] : b + ri[i] * ri[i];
     }
-    return sqrt(a) * sqrt(b);
+    return sqt(a) * sqt(b);
 }
 
 // One lane's part of QRState<K>: the sums of its own columns; the scalars are kept identical in every lane.

@@ -115,22 +115,13 @@ __device__ __forceinline__ double cl_cos_split(const Reduced& w) {
     const double v = cl_poly(w, (w.q & 1) != 0 ? false : true);
     return (w.q == 1 || w.q == 2) ? -v : v;
 }
-// Float32 sin / cos from the same reduction.
+// Float32 sin / cos from the same reduction: the hardware sine and cosine (special-function unit, absolute error
+// below 2^-21.4 on [-pi, pi]) of the reduced argument |r| <= pi/4, then the quadrant. Two issue slots instead of
+// two polynomials: the tangent's trigonometry is Float32 in the mixed kernels, and the orbit's stays Float64.
 __device__ __forceinline__ void cl_sincos32(const Reduced& w, float* sn, float* cs) {
     if (!isfin(w.x)) { const float nan = __int_as_float(0x7fc00000); *sn = nan; *cs = nan; return; }
-    const float r = static_cast<float>(w.r), z = r * r;
-    float ps = static_cast<float>(CL_SIN_T11);
-    ps = __fmaf_rn(ps, z, static_cast<float>(CL_SIN_T9));
-    ps = __fmaf_rn(ps, z, static_cast<float>(CL_SIN_T7));
-    ps = __fmaf_rn(ps, z, static_cast<float>(CL_SIN_T5));
-    ps = __fmaf_rn(ps, z, static_cast<float>(CL_SIN_T3));
-    const float s = __fmaf_rn(r * z, ps, r);
-    float pc = static_cast<float>(CL_COS_T10);
-    pc = __fmaf_rn(pc, z, static_cast<float>(CL_COS_T8));
-    pc = __fmaf_rn(pc, z, static_cast<float>(CL_COS_T6));
-    pc = __fmaf_rn(pc, z, static_cast<float>(CL_COS_T4));
-    pc = __fmaf_rn(pc, z, static_cast<float>(CL_COS_T2));
-    const float c = __fmaf_rn(z, pc, 1.0f);
+    float s, c;
+    __sincosf(static_cast<float>(w.r), &s, &c);
     switch (w.q) {
         case 0: *sn = s; *cs = c; break;
         case 1: *sn = c; *cs = -s; break;
@@ -199,8 +190,8 @@ __device__ __forceinline__ T safe_norm(const T* v) {
 
 // Norm, division and maximum of the reducers and the QR family. Float64: the reference's safe_norm, IEEE division
 // and Julia's NaN-propagating max, so the plain kernels stay operation-for-operation. Float32 (mixed kernels): the
-// unscaled norm sqrt(sum v^2) when the sum is a normal float (the scaled safe_norm otherwise), the fast reciprocal
-// division (2 ulp) and fmaxf; the frames are renormalised every handoff, so their entries stay far inside the
+// unscaled norm sqrt(sum v^2) by the hardware reciprocal square root when the sum is a normal float (the scaled
+// safe_norm otherwise), the fast reciprocal division (2 ulp) and fmaxf; the frames are renormalised every handoff, so their entries stay far inside the
 // float range, and non-finite values are caught by the status check before any reducer runs.
 template <int N, typename T>
 __device__ __forceinline__ T nrm(const T* v) {
@@ -210,8 +201,17 @@ __device__ __forceinline__ T nrm(const T* v) {
         float s = v[0] * v[0];
 #pragma unroll
         for (int i = 1; i < N; ++i) s = __fmaf_rn(v[i], v[i], s);
-        if (s >= 1e-30f && s <= 1e30f) return __fsqrt_rn(s);
+        if (s >= 1e-30f && s <= 1e30f) return s * rsqrtf(s);   // hardware reciprocal square root (2 ulp)
         return safe_norm<N>(v);
+    }
+}
+// Square root: IEEE in Float64; in Float32 the hardware reciprocal square root for positive finite x.
+template <typename T>
+__device__ __forceinline__ T sqt(T x) {
+    if constexpr (sizeof(T) == 8) {
+        return sqrt(x);
+    } else {
+        return (x > 0.0f && x < __int_as_float(0x7f800000)) ? x * rsqrtf(x) : sqrtf(x);
     }
 }
 template <typename T>

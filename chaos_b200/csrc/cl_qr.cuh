@@ -267,7 +267,7 @@ __device__ __forceinline__ T window_Gw(const T* R0) {
     T a = R[0] * R[0], b = Ri[0] * Ri[0];
 #pragma unroll
     for (int l = 1; l < K * K; ++l) { a = a + R[l] * R[l]; b = b + Ri[l] * Ri[l]; }
-    return sqrt(a) * sqrt(b);
+    return sqt(a) * sqt(b);
 }
 
 // _G_from_Gw (orthonormalize.jl:130-132).
