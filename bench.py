@@ -28,7 +28,9 @@ Multi-GPU: orbits are independent, so N ranks run N shards of the same size with
   screen    the learned screen on the 2048 x 2048 (x1, p1) grid of Froeschle orbits (x2 = p2 = 0.1), N = 1e5:
             screened orbits/s against the plain full integration of every orbit, with the misclassification
             over the whole grid;
-  mlp       the screen's network alone: inference rows/s at a batch of 262144 against the BF16 tensor peak.
+  mlp       the screen's network alone: inference rows/s at a batch of 262144 against the BF16 tensor peak;
+  split     IntegratorMap(KahanLi(8), Henon-Heiles, dt = 0.05), 16384 starts on the E = 1/8 section, N = 2e5
+            (t = 1e4), k = 2, tau = 10, chain MEGNO + FLI + QRSpectrum(Givens), FP64 kernel: steps/s.
 """
 from __future__ import annotations
 
@@ -166,7 +168,7 @@ def main() -> None:
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
     ap.add_argument("--only", choices=["fp64", "mixed"], default=None,
                     help="time one kernel of the default workload and print a short line (a small case for ncu)")
-    ap.add_argument("--workload", default="coupled", choices=["coupled", "standard", "gauss", "lattice", "screen", "mlp"])
+    ap.add_argument("--workload", default="coupled", choices=["coupled", "standard", "gauss", "lattice", "screen", "mlp", "split"])
     args = ap.parse_args()
     if args.workload != "coupled":
         run_workload(args)
@@ -467,10 +469,10 @@ def _propagate_workload(args, name, sysm, x0_h, N, tau, frames, unit_name, cpu_f
     res = {}
     launches = 0
     sampler = ClockSampler(0)
-    for prec in ("fp64", "mixed"):
+    from chaos_b200.propagate import build_run
+    precs = [p for p in ("fp64", "mixed") if L.cl_b200_check(C.byref(build_run(sysm, N, tau, frames, p, SEED))) == 0]
+    for prec in precs:
         r, cb, b = _device_frames(torch, dev, L, sysm, x0_h, N, tau, frames, prec)
-        if L.cl_b200_check(C.byref(r)) != 0:
-            continue
         mb = C.c_int32(0)
         rc = L.cl_b200_tune(C.byref(r), n, C.byref(cb), 1, min(N, 2000), C.c_void_p(stream.cuda_stream), C.byref(mb))
         if rc != 0:
@@ -481,7 +483,7 @@ def _propagate_workload(args, name, sysm, x0_h, N, tau, frames, unit_name, cpu_f
             if rc_ != 0:
                 raise RuntimeError(f"cl_b200_propagate_device: {rc_} {last_error()}")
         l0 = L.cl_b200_launch_count()
-        ms = _event_times(torch, dev, stream, go, args.steps, args.warmup, flush, sampler if prec == "mixed" else None)
+        ms = _event_times(torch, dev, stream, go, args.steps, args.warmup, flush, sampler if prec == precs[-1] else None)
         launches = L.cl_b200_launch_count() - l0 - args.warmup
         st = b["st0"].view(torch.float64).reshape(n, -1).cpu().numpy()
         res[prec] = dict(ms=ms, value=n * N / (np.mean(ms) / 1e3), minb=int(mb.value), st=st,
@@ -548,6 +550,25 @@ def workload_gauss(args):
     _propagate_workload(args, "Henon-Heiles E=1/8, Gauss-3 tol 1e-14 dt 0.01, MEGNO+FLI+QRSpectrum(Givens) k=2 "
                         "tau=10", sysm, x0, N, 10, frames, "gauss-steps", cpu,
                         dict(workload=f"henon-heiles-gauss3-16384x{N:.0e}-tau10", orbits=n, N=N, tau=10, W0="I[:, 1:2]"))
+
+
+def workload_split(args):
+    from chaos_b200 import FLI, MEGNO, GivensQR, HenonHeilesFlow, IntegratorMap, KahanLi, QRSpectrum, random_energy_starts
+    from chaos_b200.propagate import FrameSpec
+    n = 16384
+    N = args.N if args.N != N_STEPS else 200_000
+    x0 = random_energy_starts(1 / 8, n, seed=SEED)
+    sysm = IntegratorMap(KahanLi(8), HenonHeilesFlow(), 0.05)
+    chain = (MEGNO(replace=False), FLI(replace=False), QRSpectrum(GivensQR()))
+
+    def cpu():
+        W0 = np.broadcast_to(np.eye(4)[:, :2], (256, 4, 2)).copy()
+        return _cpu_port(sysm, x0[:256], 4000, 10, [FrameSpec(2, chain, W0)], "steps/s",
+                         "256 orbits x 4000 KahanLi-8 steps of the workload (oracle, all host threads)")
+    _propagate_workload(args, "Henon-Heiles E=1/8, KahanLi(8) splitting dt 0.05, MEGNO+FLI+QRSpectrum(Givens) k=2 "
+                        "tau=10", sysm, x0, N, 10, [FrameSpec(2, chain)], "steps", cpu,
+                        dict(workload=f"henon-heiles-kahanli8-16384x{N:.0e}-tau10", orbits=n, N=N, tau=10,
+                             W0="I[:, 1:2]", stages=18))
 
 
 def workload_lattice(args):
@@ -718,7 +739,7 @@ def workload_mlp(args):
 
 def run_workload(args):
     {"standard": workload_standard, "gauss": workload_gauss, "lattice": workload_lattice,
-     "screen": workload_screen, "mlp": workload_mlp}[args.workload](args)
+     "screen": workload_screen, "mlp": workload_mlp, "split": workload_split}[args.workload](args)
 
 
 

@@ -9,9 +9,9 @@ from .foundation import FALLBACK_REASONS, DeviceError, NumericalHealthError
 from .propagate import FrameSpec, PropagationResult, build_run, bytes_per_orbit, chunk_size, probe, propagate, propagate_frames
 from .reducers import (CGS, FLI, GALI, MEGNO, MGS, RGS, SALI, AugmentedQR, Benettin, GivensQR, HouseholderQR,
                        QRSpectrum)
-from .systems import (FroeschleMap, Gauss, HenonHeilesFlow, IntegratorMap, LinearSymplecticMap, StandardMap,
-                      StandardMapChain, WrappedStandardMap, energy_start, lift, random_energy_starts, section_interval,
-                      torus_state)
+from .systems import (FroeschleMap, Gauss, HenonHeilesFlow, IntegratorMap, KahanLi, Leapfrog, LinearSymplecticMap,
+                      SplittingMethod, StandardMap, StandardMapChain, WrappedStandardMap, energy_start, lift,
+                      random_energy_starts, section_interval, torus_state)
 
 __all__ = [
     "propagate", "propagate_frames", "FrameSpec", "PropagationResult", "build_run", "bytes_per_orbit", "chunk_size",
@@ -19,5 +19,5 @@ __all__ = [
     "QRSpectrum", "CGS", "MGS", "RGS", "HouseholderQR", "AugmentedQR", "GivensQR", "Benettin", "SALI", "GALI",
     "MEGNO", "FLI",
     "StandardMap", "WrappedStandardMap", "FroeschleMap", "StandardMapChain", "LinearSymplecticMap", "IntegratorMap",
-    "Gauss", "HenonHeilesFlow", "torus_state", "lift", "energy_start", "random_energy_starts", "section_interval",
+    "Gauss", "SplittingMethod", "KahanLi", "Leapfrog", "HenonHeilesFlow", "torus_state", "lift", "energy_start", "random_energy_starts", "section_interval",
 ]

@@ -7,15 +7,16 @@ from __future__ import annotations
 
 import ctypes as C
 
-ABI_VERSION = 1
+ABI_VERSION = 2
 MAX_FRAMES = 3
 MAX_REDUCERS = 4
+MAX_STAGES = 64
 MAX_DIM = 16
 MAX_K = 8
 NOALLOC_MAX_CLASSES = 64
 
 # enum cl_system_kind
-SYS_STANDARD, SYS_WRAPPED_STANDARD, SYS_FROESCHLE, SYS_CHAIN, SYS_LINEAR, SYS_HH_GAUSS = 1, 2, 3, 4, 5, 6
+SYS_STANDARD, SYS_WRAPPED_STANDARD, SYS_FROESCHLE, SYS_CHAIN, SYS_LINEAR, SYS_HH_GAUSS, SYS_HH_SPLIT = 1, 2, 3, 4, 5, 6, 7
 # enum cl_reducer_kind
 RED_QR, RED_BENETTIN, RED_SALI, RED_GALI, RED_MEGNO, RED_FLI = 1, 2, 3, 4, 5, 6
 # enum cl_qr_alg
@@ -40,6 +41,10 @@ class cl_system(C.Structure):
         ("gauss_tol", C.c_double),
         ("dt", C.c_double),
         ("A", C.c_double * (MAX_DIM * MAX_DIM)),
+        ("n_stages", C.c_int32),
+        ("reserved", C.c_int32),
+        ("stage_c", C.c_double * MAX_STAGES),
+        ("stage_d", C.c_double * MAX_STAGES),
     ]
 
 

@@ -57,7 +57,7 @@ const char* red_token(const cl_reducer& r, char* buf) {
 int sys_dim(const cl_system& s, int d) {
     switch (s.kind) {
         case CL_SYS_STANDARD: case CL_SYS_WRAPPED_STANDARD: return 2;
-        case CL_SYS_FROESCHLE: case CL_SYS_HH_GAUSS: return 4;
+        case CL_SYS_FROESCHLE: case CL_SYS_HH_GAUSS: case CL_SYS_HH_SPLIT: return 4;
         case CL_SYS_CHAIN: return 2 * s.n_sites;
         case CL_SYS_LINEAR: return d;
     }
@@ -109,6 +109,14 @@ int validate(const cl_run& r) {
     if (r.sys.kind == CL_SYS_HH_GAUSS) {
         if (r.sys.gauss_maxiter < 2) return fail(CL_EINVAL, "maxiter must be at least 2");
         if (!(std::isfinite(r.sys.dt) && r.sys.dt != 0.0)) return fail(CL_EINVAL, "the step dt must be finite and nonzero");
+    }
+    if (r.sys.kind == CL_SYS_HH_SPLIT) {
+        if (!(r.sys.n_stages >= 1 && r.sys.n_stages <= CL_MAX_STAGES))
+            return fail(CL_EUNSUPPORTED, "a splitting table needs 1..64 stages");
+        if (!(std::isfinite(r.sys.dt) && r.sys.dt != 0.0)) return fail(CL_EINVAL, "the step dt must be finite and nonzero");
+        for (int i = 0; i < r.sys.n_stages; ++i)
+            if (!(std::isfinite(r.sys.stage_c[i]) && std::isfinite(r.sys.stage_d[i])))
+                return fail(CL_EINVAL, "the splitting table has a non-finite weight");
     }
     if (r.n_frames < 1 || r.n_frames > CL_MAX_FRAMES) return fail(CL_EINVAL, "n_frames must be in 1..3");
     if (r.precision != CL_PREC_FP64 && r.precision != CL_PREC_MIXED) return fail(CL_EINVAL, "unknown precision");

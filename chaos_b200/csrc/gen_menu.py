@@ -10,7 +10,7 @@ import os
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 
-SYS_STANDARD, SYS_WRAPPED, SYS_FROESCHLE, SYS_CHAIN, SYS_LINEAR, SYS_HH = 1, 2, 3, 4, 5, 6
+SYS_STANDARD, SYS_WRAPPED, SYS_FROESCHLE, SYS_CHAIN, SYS_LINEAR, SYS_HH, SYS_SPLIT = 1, 2, 3, 4, 5, 6, 7
 QR = [f"QR{a}" for a in range(1, 7)]   # CGS, MGS, RGS, Householder, augmented, Givens
 
 
@@ -43,7 +43,8 @@ def red_type(tokens):
 
 def sys_type(kind, d):
     return {SYS_STANDARD: "SysStandard", SYS_WRAPPED: "SysWrapped", SYS_FROESCHLE: "SysFroeschle",
-            SYS_CHAIN: f"SysChain<{d // 2}>", SYS_LINEAR: f"SysLinear<{d}>", SYS_HH: "SysGauss3HH"}[kind]
+            SYS_CHAIN: f"SysChain<{d // 2}>", SYS_LINEAR: f"SysLinear<{d}>", SYS_HH: "SysGauss3HH",
+            SYS_SPLIT: "SysSplitHH"}[kind]
 
 
 def key(kind, d, prec, frames):
@@ -115,6 +116,12 @@ def menu():
     add("hh", SYS_HH, 4, 0, [(1, ["BEN"])])
     add("hh_mixed", SYS_HH, 4, 1, [(2, ["MEGNO0", "FLI0", "QR6"])])
     add("hh_mixed", SYS_HH, 4, 1, [(2, ["QR2"])])
+    # IntegratorMap(SplittingMethod(c, d), HenonHeilesFlow(), dt): any table of at most 64 stages
+    for ch in (["MEGNO0", "FLI0", "QR6"], ["QR2"], ["QR6"], ["MEGNO1"], ["FLI1"], ["SALI"], ["GALI"]):
+        add("split", SYS_SPLIT, 4, 0, [(2, ch)])
+    for ch in (["QR2"], ["QR4"], ["GALI"]):
+        add("split", SYS_SPLIT, 4, 0, [(4, ch)])
+    add("split", SYS_SPLIT, 4, 0, [(1, ["BEN"])])
     return groups
 
 
@@ -147,7 +154,8 @@ namespace {{
 
 
 def render(group, entries):
-    extra = '#include "cl_gauss.cuh"\n' if any(e[0] == SYS_HH for e in entries) else ""
+    extra = ('#include "cl_gauss.cuh"\n' if any(e[0] == SYS_HH for e in entries) else "") + \
+            ('#include "cl_split.cuh"\n' if any(e[0] == SYS_SPLIT for e in entries) else "")
     out = [HEADER.format(group=group, extra=extra)]
     for idx, (kind, d, prec, frames, minbs) in enumerate(entries):
         real = "double" if prec == 0 else "float"

@@ -25,6 +25,8 @@ struct ClSystem
     kind::Int32; n_sites::Int32; ring::Int32; gauss_maxiter::Int32
     K::Float64; eps::Float64; nu::Float64; kappa::Float64; mu::Float64; gauss_tol::Float64; dt::Float64
     A::NTuple{256, Float64}
+    n_stages::Int32; reserved::Int32
+    stage_c::NTuple{64, Float64}; stage_d::NTuple{64, Float64}
 end
 struct ClReducer
     kind::Int32; alg::Int32; replace::Int32; pad::Int32; orthogonality_tol::Float64
@@ -59,15 +61,23 @@ Foundation.is_device_lost(e::ClB200Error) = e.code == -9
 
 # ---- the menu: system and reducer records ----------------------------------------------------------------------
 const ZA = ntuple(_ -> 0.0, 256)
-clsys(m::StandardMap{Float64}) = ClSystem(1, 0, 0, 0, m.K, 0, 0, 0, 0, NaN, 0, ZA)
-clsys(m::WrappedStandardMap{Float64}) = ClSystem(2, 0, 0, 0, m.K, 0, 0, 0, 0, NaN, 0, ZA)
-clsys(m::FroeschleMap{Float64}) = ClSystem(3, 0, 0, 0, 0, 0, m.nu, m.kappa, m.mu, NaN, 0, ZA)
-clsys(m::StandardMapChain{Float64}) = ClSystem(4, m.N, m.ring, 0, m.K, m.eps, 0, 0, 0, NaN, 0, ZA)
+const ZS = ntuple(_ -> 0.0, 64)
+clsys(m::StandardMap{Float64}) = ClSystem(1, 0, 0, 0, m.K, 0, 0, 0, 0, NaN, 0, ZA, 0, 0, ZS, ZS)
+clsys(m::WrappedStandardMap{Float64}) = ClSystem(2, 0, 0, 0, m.K, 0, 0, 0, 0, NaN, 0, ZA, 0, 0, ZS, ZS)
+clsys(m::FroeschleMap{Float64}) = ClSystem(3, 0, 0, 0, 0, 0, m.nu, m.kappa, m.mu, NaN, 0, ZA, 0, 0, ZS, ZS)
+clsys(m::StandardMapChain{Float64}) = ClSystem(4, m.N, m.ring, 0, m.K, m.eps, 0, 0, 0, NaN, 0, ZA, 0, 0, ZS, ZS)
 function clsys(m::LinearSymplecticMap{Float64, D}) where {D}
-    return ClSystem(5, 0, 0, 0, 0, 0, 0, 0, 0, NaN, 0, ntuple(l -> l <= D * D ? m.A[l] : 0.0, 256))
+    return ClSystem(5, 0, 0, 0, 0, 0, 0, 0, 0, NaN, 0, ntuple(l -> l <= D * D ? m.A[l] : 0.0, 256), 0, 0, ZS, ZS)
 end
 clsys(m::IntegratorMap{<:Gauss{Float64, 3}, HenonHeilesFlow, Float64}) =
-    ClSystem(6, 0, 0, m.method.maxiter, 0, 0, 0, 0, 0, m.method.tol, m.tau, ZA)
+    ClSystem(6, 0, 0, m.method.maxiter, 0, 0, 0, 0, 0, m.method.tol, m.tau, ZA, 0, 0, ZS, ZS)
+# a table method's weights travel as they are (Integrators/splitting.jl:16-21), at most 64 stages
+function clsys(m::IntegratorMap{<:SplittingMethod{Float64, K}, HenonHeilesFlow, Float64}) where {K}
+    K <= 64 || throw(ClB200Error(-3, "a splitting table of $K stages is above the compiled limit (64)"))
+    c, d = coefficients(m.method)
+    return ClSystem(7, 0, 0, 0, 0, 0, 0, 0, 0, NaN, m.tau, ZA, K, 0, ntuple(i -> i <= K ? c[i] : 0.0, 64),
+                    ntuple(i -> i <= K ? d[i] : 0.0, 64))
+end
 clsys(m) = throw(ClB200Error(-3, "system $(typeof(m)) is not in the compiled menu"))
 
 qralg(::CGS) = 1; qralg(::MGS) = 2; qralg(::RGS) = 3
@@ -85,7 +95,7 @@ function clrun(sys, d, s, k, tau, N, n0, steps, reducers, seed, base)
     rs = map(clred, reducers)
     length(rs) <= 4 || throw(ClB200Error(-3, "more than four reducers"))
     fr = ClFrame(k, length(rs), ntuple(i -> i <= length(rs) ? rs[i] : ClReducer(0, 0, 0, 0, 0), 4))
-    return ClRun(1, d, s, tau, N, n0, steps, 1, 0, seed % UInt64, base, clsys(sys), (fr, NOFRAME, NOFRAME))
+    return ClRun(2, d, s, tau, N, n0, steps, 1, 0, seed % UInt64, base, clsys(sys), (fr, NOFRAME, NOFRAME))
 end
 
 function last_error()

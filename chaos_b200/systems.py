@@ -137,18 +137,131 @@ class Gauss:
             raise ValueError("maxiter must be at least 2")
 
 
-class IntegratorMap(System):
-    """IntegratorMap(method, flow, tau), src/Integrators/integrator_map.jl:12-23: one Gauss step of the flow as
-    a map; the tangent is the exact Jacobian of the step (gauss.jl:176-192)."""
+class SplittingMethod:
+    """A table method (src/Integrators/splitting.jl:16-36): drift weights c, kick weights d, k stages, one step =
+    drift(c_1 tau), kick(d_1 tau), ..., first stage first. Construction checks the reference's conditions: k >= 1,
+    as many kick as drift weights, finite weights, |sum c - 1| and |sum d - 1| at most 4 k max(eps, 10^-digits),
+    and for a palindromic table c_i = c_(k+1-i), d_i = d_(k-i), d_k = 0."""
 
-    def __init__(self, method: Gauss, flow: HenonHeilesFlow, tau: float):
+    def __init__(self, c, d, *, order: int, palindromic: bool, name: str, digits: float = math.inf):
+        c = [float(v) for v in c]
+        d = [float(v) for v in d]
+        k = len(c)
+        if not (k >= 1 and len(d) == k):
+            raise ValueError(f"a splitting table needs k >= 1 stages and as many kick as drift weights, got {k} and {len(d)}")
+        if not all(math.isfinite(v) for v in c + d):
+            raise ValueError(f"table {name} has a non-finite weight")
+        tol = 4 * k * max(2.0 ** -52, 10.0 ** (-digits))
+        if not (abs(_jl_sum(c) - 1.0) <= tol and abs(_jl_sum(d) - 1.0) <= tol):
+            raise ValueError(f"table {name} violates the sum conditions sum c = sum d = 1 (bound {tol})")
+        if palindromic and not (all(c[i] == c[k - 1 - i] for i in range(k)) and
+                                all(d[i] == d[k - 2 - i] for i in range(k - 1)) and d[k - 1] == 0.0):
+            raise ValueError(f"table {name} is declared palindromic but is not (c_i = c_(k+1-i), d_i = d_(k-i), d_k = 0)")
+        self.c, self.d, self.order, self.palindromic, self.name, self.digits = tuple(c), tuple(d), order, palindromic, name, digits
+
+    @property
+    def stages(self) -> int:
+        return len(self.c)
+
+    def __repr__(self):
+        return f"SplittingMethod({self.name}, {self.stages} stages, order {self.order})"
+
+
+def _jl_sum(v):
+    """Julia's `sum` of a short Float64 vector: pairwise blocks of 1024 degenerate to a left fold below 1024."""
+    s = 0.0
+    for x in v:
+        s = s + x
+    return s
+
+
+def _normalize(cs, ds, trailing: bool):
+    """Merge the drifts between consecutive kicks and drop empty stages (splitting.jl:109-120)."""
+    c, d, acc = [], [], 0.0
+    for ci, di in zip(cs, ds):
+        acc = acc + ci
+        if di != 0.0:
+            c.append(acc)
+            d.append(di)
+            acc = 0.0
+    if acc != 0.0:
+        c.append(acc)
+        d.append(0.0)
+    if trailing and d[-1] != 0.0:
+        c.append(0.0)
+        d.append(0.0)
+    return c, d
+
+
+def Leapfrog(order: str = "DKD") -> SplittingMethod:
+    """Leapfrog(Float64, order), src/Integrators/tables.jl:15-20: DKD (c = (1/2, 1/2), d = (1, 0)) or KDK."""
+    if order == "DKD":
+        c, d = [0.5, 0.5], [1.0, 0.0]
+    elif order == "KDK":
+        c, d = [0.0, 1.0, 0.0], [0.5, 0.5, 0.0]
+    else:
+        raise ValueError(f"Leapfrog order must be :DKD or :KDK, got :{order}")
+    return SplittingMethod(c, d, order=2, palindromic=True, name=f"leapfrog {order}")
+
+
+# Kahan and Li (1997), Appendix A: the step fractions gamma_1.. of the palindromic compositions of leapfrogs
+# (the middle one last), 20 digits as published; scheme 6 is s9odr6a, 8 is s17odr8a.
+_KAHANLI_GAMMA = {
+    "s7odr6": (6, ("0.78451361047755726382", "0.23557321335935813368", "-1.1776799841788710069",
+                   "1.3151863206839112189")),
+    "s9odr6a": (6, ("0.39216144400731413928", "0.33259913678935943860", "-0.70624617255763935981",
+                    "0.082213596293550800230", "0.79854399093482996340")),
+    "s17odr8a": (8, ("0.13020248308889008088", "0.56116298177510838456", "-0.38947496264484728641",
+                     "0.15884190655515560090", "-0.39590389413323757734", "0.18453964097831570709",
+                     "0.25837438768632204729", "0.29501172360931029887", "-0.60550853383003451170")),
+}
+
+
+def KahanLi(scheme=6) -> SplittingMethod:
+    """KahanLi(Float64, scheme), src/Integrators/tables.jl:74-86: the leapfrog (DKD) composed with the step fractions
+    gamma_1..gamma_m..gamma_1 (splitting.jl:174-177, 126-134); the decimal constants are rounded to Float64 once
+    (Julia's `parse`, correctly rounded, as Python's `float`)."""
+    key = scheme if isinstance(scheme, str) else {6: "s9odr6a", 8: "s17odr8a"}.get(scheme)
+    if key not in _KAHANLI_GAMMA:
+        raise ValueError("KahanLi: scheme 6, 8 or 's7odr6'")
+    order, g = _KAHANLI_GAMMA[key]
+    half = [float(v) for v in g]
+    gammas = half + half[-2::-1]
+    lf = Leapfrog("DKD")
+    cs, ds = [], []
+    for gm in gammas:
+        for ci, di in zip(lf.c, lf.d):
+            cs.append(gm * ci)
+            ds.append(gm * di)
+    c, d = _normalize(cs, ds, lf.palindromic)
+    return SplittingMethod(c, d, order=order, palindromic=True, name=f"Kahan-Li {key}", digits=20)
+
+
+class IntegratorMap(System):
+    """IntegratorMap(method, flow, tau), src/Integrators/integrator_map.jl:12-23: one step of the flow as a map, by
+    Gauss (gauss.jl:49-192) or a table method (stepper.jl:27-48); the tangent is the exact Jacobian of the step
+    (gauss.jl:176-192; stepper.jl:108-118, the product of the stage Jacobians)."""
+
+    def __init__(self, method, flow: HenonHeilesFlow, tau: float):
         if not isinstance(flow, HenonHeilesFlow):
             raise TypeError("the compiled menu integrates HenonHeilesFlow")
+        if not isinstance(method, (Gauss, SplittingMethod)):
+            raise TypeError("the compiled menu integrates with Gauss(3) or a SplittingMethod table")
+        if isinstance(method, SplittingMethod) and method.stages > _abi.MAX_STAGES:
+            raise ValueError(f"a table of {method.stages} stages is above the compiled limit ({_abi.MAX_STAGES})")
         self.method, self.flow, self.tau = method, flow, float(tau)
         self.d = self.s = 4
-        self.name = "IntegratorMap{Gauss3,HenonHeilesFlow}"
+        kind = "Gauss3" if isinstance(method, Gauss) else "SplittingMethod"
+        self.name = f"IntegratorMap{{{kind},HenonHeilesFlow}}"
 
     def to_cl(self):
+        if isinstance(self.method, SplittingMethod):
+            k = self.method.stages
+            cs = _abi.cl_system(kind=_abi.SYS_HH_SPLIT, dt=self.tau, n_stages=k, gauss_tol=math.nan)
+            for i in range(k):
+                cs.stage_c[i] = self.method.c[i]
+                cs.stage_d[i] = self.method.d[i]
+            return cs
         tol = math.nan if self.method.tol is None else float(self.method.tol)
         return _abi.cl_system(kind=_abi.SYS_HH_GAUSS, gauss_maxiter=self.method.maxiter, gauss_tol=tol, dt=self.tau)
 

@@ -44,11 +44,12 @@ extern "C" {
 #define CL_API
 #endif
 
-#define CL_B200_ABI_VERSION 1
+#define CL_B200_ABI_VERSION 2
 #define CL_MAX_FRAMES 3
 #define CL_MAX_REDUCERS 4
 #define CL_MAX_DIM 16
 #define CL_MAX_K 8
+#define CL_MAX_STAGES 64
 
 /* Systems (src/Systems): the fixed menu the compiled kernels cover. */
 enum cl_system_kind {
@@ -57,8 +58,11 @@ enum cl_system_kind {
     CL_SYS_FROESCHLE = 3,        /* FroeschleMap(nu, kappa, mu), d = s = 4           froeschle_map.jl:9-58       */
     CL_SYS_CHAIN = 4,            /* StandardMapChain(N, K, eps), d = s = 2N          standard_map_chain.jl:11-31 */
     CL_SYS_LINEAR = 5,           /* LinearSymplecticMap(A), d = s                    linear_symplectic.jl:1-40   */
-    CL_SYS_HH_GAUSS = 6          /* IntegratorMap(Gauss(Float64, 3; tol), HenonHeilesFlow(), dt), d = s = 4
+    CL_SYS_HH_GAUSS = 6,         /* IntegratorMap(Gauss(Float64, 3; tol), HenonHeilesFlow(), dt), d = s = 4
                                     integrator_map.jl:12-23, gauss.jl:49-192, flow_models.jl:101-103        */
+    CL_SYS_HH_SPLIT = 7          /* IntegratorMap(SplittingMethod(c, d), HenonHeilesFlow(), dt), d = s = 4: a table
+                                    method (drift c_i dt, then kick d_i dt), forward with merged kicks, tangent the
+                                    product of the stage Jacobians; stepper.jl:27-48,108-118, flow_core.jl:59-72  */
 };
 
 /* Reducers (src/Lyapunov, src/Indicators). */
@@ -107,6 +111,10 @@ typedef struct cl_system {
     double gauss_tol;      /* absolute stage tolerance; NaN = the reference's 8 eps max(1, |Y|) bound   */
     double dt;             /* IntegratorMap step tau of the flow                                        */
     double A[CL_MAX_DIM * CL_MAX_DIM]; /* CL_SYS_LINEAR: d x d matrix, column-major                     */
+    int32_t n_stages;      /* CL_SYS_HH_SPLIT: stages k of the table, 1..CL_MAX_STAGES                          */
+    int32_t reserved;      /* 0                                                                          */
+    double stage_c[CL_MAX_STAGES]; /* CL_SYS_HH_SPLIT: drift weights c_1..c_k (splitting.jl:16-21)      */
+    double stage_d[CL_MAX_STAGES]; /* CL_SYS_HH_SPLIT: kick weights d_1..d_k                            */
 } cl_system;
 
 typedef struct cl_reducer {

@@ -408,6 +408,82 @@ struct Gauss3 {
     }
 };
 
+// ---- a table method on the Henon-Heiles flow: IntegratorMap(SplittingMethod(c, d), HenonHeilesFlow(), dt) ----
+// force (flow_models.jl:102): (q1 + 2 q1 q2, q2 + q1^2 - q2^2), each as Julia evaluates it left to right.
+inline void hh_force(double q1, double q2, double* F) {
+    F[0] = q1 + (2 * q1) * q2;
+    F[1] = (q2 + q1 * q1) - q2 * q2;
+}
+// drift (flow_core.jl:59): q += t p; kick (flow_core.jl:60): p -= t grad V(q).
+inline void hh_drift(double* z, double t) { z[0] = z[0] + t * z[2]; z[1] = z[1] + t * z[3]; }
+inline void hh_kick(double* z, double t) {
+    double F[2];
+    hh_force(z[0], z[1], F);
+    z[2] = z[2] - t * F[0];
+    z[3] = z[3] - t * F[1];
+}
+// drift_jacobian (flow_core.jl:64-67): [[I, t I], [0, I]], entries as built (t * 1, t * 0); column-major 4 x 4.
+inline void hh_drift_jacobian(double t, double* J) {
+    const double Jv[16] = {1, 0, 0, 0, 0, 1, 0, 0, t * 1.0, t * 0.0, 1, 0, t * 0.0, t * 1.0, 0, 1};
+    std::memcpy(J, Jv, sizeof Jv);
+}
+// kick_jacobian (flow_core.jl:68-72) at the pre-kick point: [[I, 0], [-t Hs, I]], Hs = force_jacobian
+// (flow_models.jl:103) = [[1 + 2 q2, 2 q1], [2 q1, 1 - 2 q2]], -t Hs formed as (-t) * Hs.
+inline void hh_kick_jacobian(const double* z, double t, double* J) {
+    const double h11 = 1 + 2 * z[1], h21 = 2 * z[0], h12 = 2 * z[0], h22 = 1 - 2 * z[1];
+    const double mt = -t;
+    const double Jv[16] = {1, 0, mt * h11, mt * h21, 0, 1, mt * h12, mt * h22, 0, 0, 1, 0, 0, 0, 0, 1};
+    std::memcpy(J, Jv, sizeof Jv);
+}
+
+struct SplitHH {
+    int n;
+    const double* c;
+    const double* d;
+    // tangent_advance with the identity frame (stepper.jl:108-118): per stage, drift then kick where the weight is
+    // nonzero, each Jacobian (at the point before the sub-step) multiplied onto the frame by the StaticArrays
+    // product (the fused chain of fused_product); the state advanced without merging kicks.
+    void tangent(const double* x, double dt, double* T) const {
+        double z[4] = {x[0], x[1], x[2], x[3]};
+        double W[16] = {1, 0, 0, 0, 0, 1, 0, 0, 0, 0, 1, 0, 0, 0, 0, 1}, J[16], Wn[16];
+        for (int i = 0; i < n; ++i) {
+            if (c[i] != 0.0) {
+                const double t = c[i] * dt;
+                hh_drift_jacobian(t, J);
+                fused_product(J, W, Wn, 4, 4, 4);
+                std::memcpy(W, Wn, sizeof W);
+                hh_drift(z, t);
+            }
+            if (d[i] != 0.0) {
+                const double t = d[i] * dt;
+                hh_kick_jacobian(z, t, J);
+                fused_product(J, W, Wn, 4, 4, 4);
+                std::memcpy(W, Wn, sizeof W);
+                hh_kick(z, t);
+            }
+        }
+        std::memcpy(T, W, sizeof W);
+    }
+    // advance_n(m, flow, z, dt, 1) (stepper.jl:27-48): kicks with no drift between them merged into one.
+    void forward(double* z, double dt) const {
+        double pend = 0.0;
+        for (int i = 0; i < n; ++i) {
+            const double ci = c[i];
+            if (ci != 0.0) {
+                if (pend != 0.0) { hh_kick(z, pend * dt); pend = 0.0; }
+                hh_drift(z, ci * dt);
+            }
+            pend = pend + d[i];
+        }
+        if (pend != 0.0) hh_kick(z, pend * dt);
+    }
+    // the orbit body's map step: the tangent at the old point, then forward (orbit.jl:44-50)
+    void step(double* x, double dt, double* T) const {
+        tangent(x, dt, T);
+        forward(x, dt);
+    }
+};
+
 // ---- Orthonormalisers (src/Lyapunov/orthonormalize.jl, householder.jl) ---------------------------------------------
 enum { QR_OK = 0, QR_PIVOT = 1, QR_PASSES = 2 };
 constexpr int MAX_PASSES = 4;

@@ -50,6 +50,7 @@ def lib() -> C.CDLL:
         L.oracle_orth_loss.restype = C.c_double
         L.oracle_seeded_frame.argtypes = [C.c_uint64, C.c_int64, C.c_int32, C.c_int32, dp]
         L.oracle_gauss3_step.argtypes = [dp, C.c_double, C.c_int32, C.c_double, dp]
+        L.oracle_split_step.argtypes = [dp, C.c_double, C.c_int32, dp, dp, dp]
         L.oracle_max_threads.restype = C.c_int32
         L.oracle_ensemble.argtypes = [P(_abi.cl_run), C.c_int64, P(_abi.cl_buffers), dp, P(C.c_int64), C.c_double,
                                       C.c_int32, C.c_int32]
@@ -110,6 +111,16 @@ def gauss3_step(z, h, maxiter=50, tol=float("nan")):
     z = np.ascontiguousarray(z, dtype=np.float64).copy()
     T = np.zeros((4, 4), order="F")
     lib().oracle_gauss3_step(_dp(z), h, maxiter, tol, _dp(T))
+    return z, T
+
+
+def split_step(z, h, method):
+    """One step of the table method `method` (a SplittingMethod) on the Henon-Heiles flow: (z', 4 x 4 tangent)."""
+    z = np.ascontiguousarray(z, dtype=np.float64).copy()
+    T = np.zeros((4, 4), order="F")
+    c = np.ascontiguousarray(method.c, dtype=np.float64)
+    d = np.ascontiguousarray(method.d, dtype=np.float64)
+    lib().oracle_split_step(_dp(z), h, len(c), _dp(c), _dp(d), _dp(T))
     return z, T
 
 

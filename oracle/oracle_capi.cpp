@@ -98,6 +98,7 @@ void run_orbit(const cl_run& run0, int64_t i, const cl_buffers& b, const double*
     (void)sysf;
     Chain<MM> chain{run.sys.n_sites, run.sys.K, run.sys.eps, run.sys.ring != 0};
     Gauss3 gauss(run.sys.gauss_maxiter, run.sys.gauss_tol);
+    const SplitHH split{run.sys.n_stages, run.sys.stage_c, run.sys.stage_d};
     int64_t n = n0;
     bool escaped = false;
     const int tau = run.tau;
@@ -121,6 +122,7 @@ void run_orbit(const cl_run& run0, int64_t i, const cl_buffers& b, const double*
                     case CL_SYS_FROESCHLE: Systems<MM>::froeschle(run.sys.nu, run.sys.kappa, run.sys.mu, x, M); break;
                     case CL_SYS_LINEAR: Systems<MM>::linear(run.sys.A, d, x, M); break;
                     case CL_SYS_HH_GAUSS: gauss.step(x, run.sys.dt, M); break;
+                    case CL_SYS_HH_SPLIT: split.step(x, run.sys.dt, M); break;
                 }
                 for (int f = 0; f < nf; ++f) {
                     if (!alive[f]) continue;
@@ -272,6 +274,13 @@ void oracle_seeded_frame(uint64_t seed, int64_t orbit, int32_t d, int32_t k, dou
 int32_t oracle_gauss3_step(double* z, double h, int32_t maxiter, double tol, double* T) {
     Gauss3 g(maxiter, tol);
     g.step(z, h, T);
+    return 0;
+}
+
+// One step of a table method on the Henon-Heiles flow: advances z (4) and writes the 4 x 4 tangent T.
+int32_t oracle_split_step(double* z, double h, int32_t n_stages, const double* c, const double* d, double* T) {
+    const SplitHH s{n_stages, c, d};
+    s.step(z, h, T);
     return 0;
 }
 

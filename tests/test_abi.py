@@ -66,6 +66,9 @@ def _run_from_key(key: str) -> _abi.cl_run:
     r.sys.n_sites = d // 2
     r.sys.gauss_maxiter = 50
     r.sys.dt = 0.01
+    r.sys.n_stages = 2                      # a table method: the DKD leapfrog
+    r.sys.stage_c[0] = r.sys.stage_c[1] = 0.5
+    r.sys.stage_d[0] = 1.0
     for f, grp in enumerate(g for g in rest.split("|") if g):
         k, toks = grp.split(":")
         r.frames[f].k = int(k[1:])

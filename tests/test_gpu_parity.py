@@ -159,3 +159,18 @@ def test_henon_heiles_gauss3(oracle, k, chain, tol):
     x0 = random_energy_starts(1 / 8, n, seed=5)
     sysm = IntegratorMap(Gauss(3, tol=tol), HenonHeilesFlow(), 0.01)
     _compare(sysm, x0, 600, [FrameSpec(k, chain, haar_frames(n, 4, k, 6))], 10, oracle)
+
+
+@pytest.mark.parametrize("k,chain", [(2, (MEGNO(replace=False), FLI(replace=False), QRSpectrum(GivensQR()))),
+                                     (2, (QRSpectrum(MGS()),)), (2, (SALI(),)), (4, (QRSpectrum(HouseholderQR()),)),
+                                     (4, (GALI(),)), (1, (Benettin(),))], ids=repr)
+@pytest.mark.parametrize("method", ["KahanLi8", "KahanLi6", "LeapfrogKDK"])
+def test_henon_heiles_splitting(oracle, k, chain, method):
+    """IntegratorMap(SplittingMethod, HenonHeilesFlow(), 0.05): merged-kick forward, the stage-Jacobian tangent and the
+    reducers, bit for bit against the oracle on E = 1/8 energy-shell starts."""
+    from chaos_b200 import HenonHeilesFlow, IntegratorMap, KahanLi, Leapfrog, random_energy_starts
+    m = {"KahanLi8": KahanLi(8), "KahanLi6": KahanLi(6), "LeapfrogKDK": Leapfrog("KDK")}[method]
+    n = 160
+    x0 = random_energy_starts(1 / 8, n, seed=12)
+    sysm = IntegratorMap(m, HenonHeilesFlow(), 0.05)
+    _compare(sysm, x0, 800, [FrameSpec(k, chain, haar_frames(n, 4, k, 13))], 10, oracle)

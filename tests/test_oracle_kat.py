@@ -272,3 +272,79 @@ def test_ensemble_orbit_is_a_reference_call(oracle):
         assert states_equal(one["states"][:1], ens["states"][i:i + 1])
         if ens["code"][i] == 4:
             assert np.max(np.abs(ens["x"][i][1:])) > 50.0
+
+
+# ---- table methods on the Henon-Heiles flow (src/Integrators/stepper.jl, tables.jl; test/henon-heiles) -------------
+def _hh_starts(n, seed):
+    from chaos_b200 import random_energy_starts
+    return random_energy_starts(1 / 8, n, seed=seed)
+
+
+def test_kahanli_table_shapes():
+    """KahanLi(Float64, 8) is the palindromic composition of 17 leapfrogs (18 stages, the last kick weight zero);
+    both sums are 1 to rounding; Leapfrog(:DKD) is (1/2, 1/2 | 1, 0)."""
+    from chaos_b200 import KahanLi, Leapfrog
+    m = KahanLi(8)
+    assert m.stages == 18 and m.d[-1] == 0.0 and m.order == 8
+    assert abs(sum(m.c) - 1) < 1e-14 and abs(sum(m.d) - 1) < 1e-14
+    assert m.c == m.c[::-1] and m.d[:-1] == m.d[-2::-1]
+    assert KahanLi(6).stages == 10 and KahanLi("s7odr6").stages == 8
+    lf = Leapfrog("DKD")
+    assert lf.c == (0.5, 0.5) and lf.d == (1.0, 0.0)
+
+
+def test_split_step_commutes_with_reflection(oracle):
+    """hh_ac01_05.jl AC3b: one KahanLi-8 step commutes with q1 -> -q1, p1 -> -p1 bit for bit (1000 random states)."""
+    from chaos_b200 import KahanLi
+    m = KahanLi(8)
+    rng = np.random.default_rng(33)
+    flip = np.array([-1.0, 1.0, -1.0, 1.0])
+    for _ in range(1000):
+        z = 2 * rng.random(4) - 1
+        a, _ = oracle.split_step(z, 0.05, m)
+        b, _ = oracle.split_step(z * flip, 0.05, m)
+        assert np.array_equal(a * flip, b)
+
+
+def test_split_energy_conservation(oracle):
+    """hh_ac06_09.jl AC6: KahanLi-8 at tau = 1/20 keeps |H - H0| <= 1e-8 along E = 1/8 orbits (no drift)."""
+    from chaos_b200 import HenonHeilesFlow, KahanLi
+    m = KahanLi(8)
+    H = HenonHeilesFlow.hamiltonian
+    worst = 0.0
+    for z0 in _hh_starts(4, 6):
+        z, H0 = z0.copy(), H(z0)
+        for _ in range(2000):
+            z, _ = oracle.split_step(z, 1 / 20, m)
+            worst = max(worst, abs(H(z) - H0))
+    assert worst <= 1e-8
+
+
+def test_split_time_reversal(oracle):
+    """hh_ac01_05.jl AC3d: n steps, p -> -p, n steps, p -> -p returns to the start (regular E = 1/20 orbits)."""
+    from chaos_b200 import KahanLi, Leapfrog, random_energy_starts
+    flipp = np.array([1.0, 1.0, -1.0, -1.0])
+    for m in (KahanLi(8), Leapfrog("DKD")):
+        for z0 in random_energy_starts(1 / 20, 3, seed=8):
+            z = z0.copy()
+            for _ in range(2000):
+                z, _ = oracle.split_step(z, 0.05, m)
+            z = z * flipp
+            for _ in range(2000):
+                z, _ = oracle.split_step(z, 0.05, m)
+            assert np.max(np.abs(z * flipp - z0)) <= 1e-11
+
+
+def test_split_tangent_is_the_step_jacobian(oracle):
+    """tangent_advance (stepper.jl:108-118): the tangent is symplectic (T' Omega T = Omega to rounding) and equals
+    central differences of the step."""
+    from chaos_b200 import KahanLi
+    m = KahanLi(8)
+    Om = np.block([[np.zeros((2, 2)), np.eye(2)], [-np.eye(2), np.zeros((2, 2))]])
+    for z0 in _hh_starts(3, 9):
+        _, T = oracle.split_step(z0, 0.05, m)
+        assert np.max(np.abs(T.T @ Om @ T - Om)) <= 1e-14
+        e = 1e-6
+        fd = np.column_stack([(oracle.split_step(z0 + e * np.eye(4)[j], 0.05, m)[0] -
+                               oracle.split_step(z0 - e * np.eye(4)[j], 0.05, m)[0]) / (2 * e) for j in range(4)])
+        assert np.max(np.abs(T - fd)) <= 1e-8
