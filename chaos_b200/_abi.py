@@ -179,6 +179,14 @@ def declare(lib: C.CDLL) -> C.CDLL:
     lib.cl_b200_ensemble.argtypes = [P(cl_ensemble_class), C.c_int32, P(cl_prov)]
     lib.cl_b200_ensemble.restype = C.c_int
     lib.cl_b200_ensemble_tune.argtypes = [P(cl_ensemble_class), C.c_int64, C.c_int64, C.c_void_p]
+    lib.cl_b200_shadow_bytes.argtypes = [C.c_int32]
+    lib.cl_b200_shadow_bytes.restype = C.c_int64
+    lib.cl_b200_shadow_device.argtypes = [P(cl_run), C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_double,
+                                          C.c_void_p]
+    lib.cl_b200_shadow_device.restype = C.c_int
+    lib.cl_b200_shadow.argtypes = [P(cl_run), C.c_int64, P(C.c_double), P(C.c_double), C.c_void_p, C.c_double,
+                                   P(cl_prov)]
+    lib.cl_b200_shadow.restype = C.c_int
     lib.cl_b200_ensemble_tune.restype = C.c_int
     lib.cl_b200_ensemble_graph_create.argtypes = [P(cl_ensemble_class), C.c_int32, P(C.c_void_p)]
     lib.cl_b200_ensemble_graph_create.restype = C.c_int
@@ -200,4 +208,5 @@ EXPORTS = ("cl_b200_propagate", "cl_b200_propagate_device", "cl_b200_check", "cl
            "cl_b200_ensemble_tune", "cl_b200_ensemble_graph_create", "cl_b200_ensemble_graph_launch",
            "cl_b200_ensemble_graph_destroy", "cl_b200_ensemble_device_noalloc", "cl_b200_tune",
            "cl_b200_gemm_bf16", "cl_b200_mlp_status", "cl_b200_transpose_bf16", "cl_b200_gelu_backward",
-           "cl_b200_col_sum", "cl_b200_head_loss", "cl_b200_adam", "cl_b200_to_bf16", "cl_b200_screen_features")
+           "cl_b200_col_sum", "cl_b200_head_loss", "cl_b200_adam", "cl_b200_to_bf16", "cl_b200_screen_features",
+           "cl_b200_shadow_bytes", "cl_b200_shadow_device", "cl_b200_shadow")

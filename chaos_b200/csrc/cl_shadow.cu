@@ -1,0 +1,311 @@
+// cl_shadow.cu -- the two-trajectory estimator (src/Lyapunov/two_trajectory.jl): per orbit a shadow started at
+// distance d0 from the reference along a unit direction u0, both advanced by the map's `forward`, and every tau steps
+// the separation d is measured, log(d / d_prev) added to a Neumaier sum and the shadow put back at distance d0 along
+// the separation (Algorithm 1 to 3). One orbit per thread, the states in registers; a launch covers a window of
+// steps and carries the end record, which is written in the isbits layout of the reference's `ShadowEnd{s, Float64}`
+// (x, y, sum, dprev, code, step, value).
+//
+// `separation` and `displaced` (src/Lyapunov/separation.jl) are the plain difference and sum on lifted states, and
+// for WrappedStandardMap the minimal image in (-pi, pi] and the reduction with carried winding counts.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <type_traits>
+
+#include "../../include/chaoslab_b200.h"
+#include "cl_gauss.cuh"
+#include "cl_split.cuh"
+
+namespace cl {
+
+int capi_fail(int code, const std::string& msg);      // cl_capi.cu
+int capi_map_cuda(cudaError_t e, const char* where);  // cl_capi.cu
+int capi_validate(const cl_run& r);                   // cl_capi.cu
+void capi_count_launch();                             // cl_capi.cu
+
+namespace {
+
+struct ShArgs {
+    i64 n, n0, steps, N;
+    int tau;
+    double d0;
+    const double* x0;   // n x S (orbit-major)
+    const double* u0;   // n x D, or NULL: the seeded direction (first column of the seeded frame)
+    uint64_t* ends;     // n records of ShadowEnd{S, Float64}
+    uint64_t seed;
+    i64 orbit_base;
+};
+
+template <class Sys> struct Wrapped { static constexpr bool value = false; };
+template <> struct Wrapped<SysWrapped> { static constexpr bool value = true; };
+
+// separation (separation.jl:9, :25-28)
+template <class Sys>
+__device__ __forceinline__ void separation(const double* x, const double* y, double* delta) {
+    constexpr int D = Sys::D;
+    if constexpr (Wrapped<Sys>::value) {
+        const double tp = 2 * jl_pi(), h = tp / 2;
+#pragma unroll
+        for (int i = 0; i < 2; ++i) {
+            const double u = y[i] - x[i];
+            delta[i] = u > h ? u - tp : (u <= -h ? u + tp : u);
+        }
+    } else {
+#pragma unroll
+        for (int i = 0; i < D; ++i) delta[i] = y[i] - x[i];
+    }
+}
+
+// displaced (separation.jl:17, :30-35): y = x + delta; wrapped: reduce both coordinates, add the counts
+template <class Sys>
+__device__ __forceinline__ void displaced(const double* x, const double* delta, double* y) {
+    constexpr int D = Sys::D;
+    if constexpr (Wrapped<Sys>::value) {
+        const double tp = 2 * jl_pi();
+        double xr, a, pr, b;
+        wrap_reduce(x[0] + delta[0], tp, xr, a);
+        wrap_reduce(x[1] + delta[1], tp, pr, b);
+        y[0] = xr; y[1] = pr; y[2] = x[2] + a; y[3] = x[3] + b;
+    } else {
+#pragma unroll
+        for (int i = 0; i < D; ++i) y[i] = x[i] + delta[i];
+    }
+}
+
+// forward (the map's own, without its tangent where the system separates them)
+template <class Sys>
+__device__ __forceinline__ void fwd(const Sys& sys, double* z) {
+    if constexpr (std::is_same<Sys, SysSplitHH>::value) {
+        SplitJac unused;
+        sys.forward(z, unused);
+    } else {
+        typename Sys::Jac J;
+        sys.jac(z, J);
+        sys.forward(z, J);
+    }
+}
+
+template <int S>
+__device__ __forceinline__ void store_end(uint64_t* e, const double* x, const double* y, const CS& acc, double dprev,
+                                          int8_t code, i64 step, double value) {
+#pragma unroll
+    for (int c = 0; c < S; ++c) { e[c] = __double_as_longlong(x[c]); e[S + c] = __double_as_longlong(y[c]); }
+    e[2 * S] = __double_as_longlong(acc.s);
+    e[2 * S + 1] = __double_as_longlong(acc.c);
+    e[2 * S + 2] = __double_as_longlong(dprev);
+    e[2 * S + 3] = static_cast<uint64_t>(static_cast<uint8_t>(code));
+    e[2 * S + 4] = static_cast<uint64_t>(step);
+    e[2 * S + 5] = __double_as_longlong(value);
+}
+
+// _shadow_body (two_trajectory.jl:59-80) for one launch window of one orbit
+template <class Sys>
+__global__ void __launch_bounds__(128) shadow_kernel(const ShArgs a, const Sys sys) {
+    constexpr int D = Sys::D, S = Sys::S, W = 2 * S + 6;
+    const i64 i = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= a.n) return;
+    uint64_t* e = a.ends + i * W;
+    double x[S], y[S], delta[D];
+    CS acc{0.0, 0.0};
+    double dprev;
+    const double d0 = a.d0;
+    if (a.n0 == 0) {
+        // _shadow_start (two_trajectory.jl:31-36): y = displaced(x0, d0 u0), its realised separation, a code
+#pragma unroll
+        for (int c = 0; c < S; ++c) x[c] = a.x0[i * S + c];
+        double u[D];
+        if (a.u0) {
+#pragma unroll
+            for (int c = 0; c < D; ++c) u[c] = a.u0[i * D + c];
+        } else {
+            seeded_frame<D, 1>(a.seed, a.orbit_base + i + 1, u);
+        }
+#pragma unroll
+        for (int c = 0; c < D; ++c) delta[c] = d0 * u[c];
+        displaced<Sys>(x, delta, y);
+        separation<Sys>(x, y, delta);
+        dprev = safe_norm<D>(delta);
+        const int8_t code = !(isfin(dprev) && dprev > 0) ? 2 : (dprev < d0 / 2 || dprev > 2 * d0 ? 3 : 0);
+        if (code != 0) { store_end<S>(e, x, y, acc, dprev, code, 0, dprev); return; }
+    } else {
+        if (static_cast<int8_t>(e[2 * S + 3] & 0xff) != 0) return;   // failed in an earlier launch: frozen
+#pragma unroll
+        for (int c = 0; c < S; ++c) { x[c] = __longlong_as_double(e[c]); y[c] = __longlong_as_double(e[S + c]); }
+        acc.s = __longlong_as_double(e[2 * S]);
+        acc.c = __longlong_as_double(e[2 * S + 1]);
+        dprev = __longlong_as_double(e[2 * S + 2]);
+    }
+    i64 n = a.n0;
+    const i64 handoffs = a.steps / a.tau;
+    for (i64 h = 0; h < handoffs; ++h) {
+        for (int t = 0; t < a.tau; ++t) {
+            fwd(sys, x);
+            fwd(sys, y);
+        }
+        n += a.tau;
+        bool fin = true;
+        double bad = 0.0;
+#pragma unroll
+        for (int c = S - 1; c >= 0; --c) if (!isfin(y[c])) { fin = false; bad = y[c]; }
+#pragma unroll
+        for (int c = S - 1; c >= 0; --c) if (!isfin(x[c])) { fin = false; bad = x[c]; }
+        if (!fin) { store_end<S>(e, x, y, acc, dprev, 1, n, bad); return; }
+        separation<Sys>(x, y, delta);
+        const double d = safe_norm<D>(delta);
+        if (!(isfin(d) && d > 0)) { store_end<S>(e, x, y, acc, dprev, 2, n, d); return; }
+        cs_add(acc, cl_log(d / dprev));
+        const double f = d0 / d;
+#pragma unroll
+        for (int c = 0; c < D; ++c) delta[c] = delta[c] * f;
+        displaced<Sys>(x, delta, y);
+        separation<Sys>(x, y, delta);
+        dprev = safe_norm<D>(delta);
+        if (!(dprev >= d0 / 2 && dprev <= 2 * d0)) {
+            store_end<S>(e, x, y, acc, dprev, (isfin(dprev) && dprev > 0) ? 3 : 2, n, dprev);
+            return;
+        }
+    }
+    store_end<S>(e, x, y, acc, dprev, 0, n, dprev);
+}
+
+typedef cudaError_t (*ShadowFn)(const cl_run& run, const ShArgs& a, cudaStream_t st);
+
+template <class Sys>
+cudaError_t launch_shadow(const cl_run& run, const ShArgs& a, cudaStream_t st) {
+    const Sys sys = SysMaker<Sys>::make(run, nullptr);
+    shadow_kernel<Sys><<<static_cast<unsigned>((a.n + 127) / 128), 128, 0, st>>>(a, sys);
+    return cudaGetLastError();
+}
+
+ShadowFn shadow_fn(const cl_run& r) {
+    switch (r.sys.kind) {
+        case CL_SYS_STANDARD: return launch_shadow<SysStandard>;
+        case CL_SYS_WRAPPED_STANDARD: return launch_shadow<SysWrapped>;
+        case CL_SYS_FROESCHLE: return launch_shadow<SysFroeschle>;
+        case CL_SYS_HH_GAUSS: return launch_shadow<SysGauss3HH>;
+        case CL_SYS_HH_SPLIT: return launch_shadow<SysSplitHH>;
+        case CL_SYS_LINEAR:
+            if (r.d == 2) return launch_shadow<SysLinear<2>>;
+            if (r.d == 4) return launch_shadow<SysLinear<4>>;
+            if (r.d == 6) return launch_shadow<SysLinear<6>>;
+            return nullptr;
+        case CL_SYS_CHAIN:
+            switch (r.sys.n_sites) {
+                case 2: return launch_shadow<SysChain<2>>;
+                case 3: return launch_shadow<SysChain<3>>;
+                case 4: return launch_shadow<SysChain<4>>;
+                case 5: return launch_shadow<SysChain<5>>;
+                case 6: return launch_shadow<SysChain<6>>;
+                case 7: return launch_shadow<SysChain<7>>;
+                case 8: return launch_shadow<SysChain<8>>;
+            }
+            return nullptr;
+    }
+    return nullptr;
+}
+
+// The run's checks (system, tau, N, launch window) through propagate's validation with a placeholder frame.
+int check_shadow(const cl_run& run, double d0, ShadowFn* fn) {
+    cl_run r = run;
+    r.n_frames = 1;
+    std::memset(&r.frames[0], 0, sizeof r.frames[0]);
+    r.frames[0].k = 1;
+    r.precision = CL_PREC_FP64;
+    const int v = capi_validate(r);
+    if (v) return v;
+    if (!(std::isfinite(d0) && d0 > 0)) return capi_fail(CL_EINVAL, "d0 must be finite and positive");
+    *fn = shadow_fn(run);
+    if (!*fn) return capi_fail(CL_EUNSUPPORTED, "no compiled two-trajectory kernel for this system");
+    return 0;
+}
+
+ShArgs shargs(const cl_run& run, int64_t n, const double* x0, const double* u0, void* ends, double d0, int64_t n0,
+              int64_t steps) {
+    ShArgs a;
+    a.n = n; a.n0 = n0; a.steps = steps; a.N = run.N; a.tau = run.tau; a.d0 = d0;
+    a.x0 = x0; a.u0 = u0; a.ends = static_cast<uint64_t*>(ends);
+    a.seed = run.seed; a.orbit_base = run.orbit_base;
+    return a;
+}
+
+}  // namespace
+}  // namespace cl
+
+using namespace cl;
+
+extern "C" {
+
+int64_t cl_b200_shadow_bytes(int32_t s) { return s > 0 ? 8 * (2 * static_cast<int64_t>(s) + 6) : -1; }
+
+int cl_b200_shadow_device(const cl_run* run, int64_t n, const double* x0, const double* u0, void* ends, double d0,
+                          void* stream) {
+    if (!run || n <= 0 || !ends || (run->n0 == 0 && !x0)) return capi_fail(CL_EINVAL, "bad arguments");
+    ShadowFn fn;
+    const int v = check_shadow(*run, d0, &fn);
+    if (v) return v;
+    const int64_t steps = run->steps > 0 ? run->steps : run->N - run->n0;
+    const cudaError_t e = fn(*run, shargs(*run, n, x0, u0, ends, d0, run->n0, steps), static_cast<cudaStream_t>(stream));
+    capi_count_launch();
+    return e == cudaSuccess ? 0 : capi_map_cuda(e, "two-trajectory launch");
+}
+
+int cl_b200_shadow(const cl_run* run, int64_t n, const double* x0, const double* u0, void* ends, double d0,
+                   cl_prov* prov) {
+    if (!run || n <= 0 || !x0 || !ends) return capi_fail(CL_EINVAL, "bad arguments");
+    ShadowFn fn;
+    int rc = check_shadow(*run, d0, &fn);
+    if (rc) return rc;
+    const int S = run->s, D = run->d;
+    const size_t xb = sizeof(double) * S * n, ub = sizeof(double) * D * n, eb = static_cast<size_t>(cl_b200_shadow_bytes(S)) * n;
+    double *dx = nullptr, *du = nullptr;
+    void* de = nullptr;
+    cudaStream_t st = nullptr;
+    cudaError_t e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaMalloc(reinterpret_cast<void**>(&dx), xb);
+    if (e == cudaSuccess && u0) e = cudaMalloc(reinterpret_cast<void**>(&du), ub);
+    if (e == cudaSuccess) e = cudaMalloc(&de, eb);
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    int launches = 0;
+    if (e == cudaSuccess) {
+        cudaMemcpyAsync(dx, x0, xb, cudaMemcpyHostToDevice, st);
+        if (u0) cudaMemcpyAsync(du, u0, ub, cudaMemcpyHostToDevice, st);
+        if (run->n0 > 0) cudaMemcpyAsync(de, ends, eb, cudaMemcpyHostToDevice, st);
+        cudaEventCreate(&e0);
+        cudaEventCreate(&e1);
+        cudaEventRecord(e0, st);
+        // windows of run.steps steps (the whole remaining run when 0), each a launch carrying the end records
+        const int64_t L = run->steps > 0 ? run->steps : run->N - run->n0;
+        for (int64_t n0 = run->n0; n0 < run->N && e == cudaSuccess; n0 += L) {
+            const int64_t steps = std::min<int64_t>(L, run->N - n0);
+            e = fn(*run, shargs(*run, n, dx, du, de, d0, n0, steps), st);
+            capi_count_launch();
+            ++launches;
+        }
+        cudaEventRecord(e1, st);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(ends, de, eb, cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    }
+    if (e != cudaSuccess) rc = capi_map_cuda(e, "two-trajectory");
+    if (rc == 0 && prov) {
+        std::memset(prov, 0, sizeof *prov);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        prov->gpu_ms = ms;
+        prov->launches = launches;
+        prov->launch_steps = run->steps > 0 ? run->steps : run->N - run->n0;
+        std::snprintf(prov->variant, sizeof prov->variant, "two-trajectory s%d d%d", S, D);
+    }
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    cudaFree(dx);
+    cudaFree(du);
+    cudaFree(de);
+    if (st) cudaStreamDestroy(st);
+    return rc;
+}
+
+}  // extern "C"

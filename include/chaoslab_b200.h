@@ -278,6 +278,23 @@ CL_API int cl_b200_ensemble_graph_create(const cl_ensemble_class* classes, int32
 CL_API int cl_b200_ensemble_graph_launch(void* graph, void* stream);
 CL_API int cl_b200_ensemble_graph_destroy(void* graph);
 
+/* ---- The two-trajectory estimator (src/Lyapunov/two_trajectory.jl:40-96, separation.jl) ---------------------------
+ * Per orbit a shadow started at displaced(x0, d0 u0) (u0 a unit vector of the d tangent coordinates), both orbits
+ * advanced by `forward`; every tau steps the separation d is measured, log(d / d_prev) is added to a Neumaier sum and
+ * the shadow is put back at distance d0 along the separation. `ends` holds one record per orbit in the isbits layout
+ * of the reference's ShadowEnd{s, Float64}: x[s], y[s], sum (s, c), dprev, code (Int8 in an 8-byte slot: 0 ok,
+ * 1 non-finite state, 2 separation zero or non-finite, 3 realised separation outside [d0/2, 2 d0]), step (Int64),
+ * value; X2 = (sum.s + sum.c) / N. run.n0 == 0 starts the shadows (u0 NULL: the first column of the seeded frame of
+ * the run's seed and orbit_base + i + 1), a later window continues from `ends` and leaves failed orbits untouched.
+ * run.frames are not used. Replaces the launch loop of `_shadow_chunk!` (two_trajectory.jl:123-143). */
+CL_API int64_t cl_b200_shadow_bytes(int32_t s);
+/* One launch window [run.n0, run.n0 + run.steps) (run.steps 0: to run.N) on device buffers, enqueued on `stream`. */
+CL_API int cl_b200_shadow_device(const cl_run* run, int64_t n, const double* x0, const double* u0, void* ends,
+                                 double d0, void* stream);
+/* The same from run.n0 to run.N on host buffers, in windows of run.steps steps (synchronous). */
+CL_API int cl_b200_shadow(const cl_run* run, int64_t n, const double* x0, const double* u0, void* ends, double d0,
+                          cl_prov* prov);
+
 /* ---- The learned screen's kernels (no reference counterpart: the reference has no learned component) ---------------
  * All enqueue on `stream` and take device pointers. BF16 matrices are row-major with 16-byte aligned rows. */
 

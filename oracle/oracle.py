@@ -51,6 +51,8 @@ def lib() -> C.CDLL:
         L.oracle_seeded_frame.argtypes = [C.c_uint64, C.c_int64, C.c_int32, C.c_int32, dp]
         L.oracle_gauss3_step.argtypes = [dp, C.c_double, C.c_int32, C.c_double, dp]
         L.oracle_split_step.argtypes = [dp, C.c_double, C.c_int32, dp, dp, dp]
+        L.oracle_shadow.argtypes = [P(_abi.cl_run), C.c_int64, dp, C.c_void_p, C.c_void_p, C.c_double, C.c_int32,
+                                    C.c_int32]
         L.oracle_max_threads.restype = C.c_int32
         L.oracle_ensemble.argtypes = [P(_abi.cl_run), C.c_int64, P(_abi.cl_buffers), dp, P(C.c_int64), C.c_double,
                                       C.c_int32, C.c_int32]
@@ -122,6 +124,26 @@ def split_step(z, h, method):
     d = np.ascontiguousarray(method.d, dtype=np.float64)
     lib().oracle_split_step(_dp(z), h, len(c), _dp(c), _dp(d), _dp(T))
     return z, T
+
+
+def oracle_shadow(sys, x0, N, *, d0, tau=1, seed=0, U0=None, math="portable", threads=0, launch_steps=None,
+                  orbit_base=0):
+    """The two-trajectory estimator on the oracle: the end records (structured array, ShadowEnd layout)."""
+    from chaos_b200.shadow import end_dtype
+    x0 = np.ascontiguousarray(np.asarray(x0, dtype=np.float64))
+    n, s = x0.shape
+    run = build_run(sys, N, tau, [FrameSpec(1, ())], "fp64", seed, orbit_base=orbit_base)
+    ends = np.zeros(n, dtype=end_dtype(s))
+    u = None if U0 is None else np.ascontiguousarray(np.asarray(U0, dtype=np.float64))
+    total, L, done = int(N), int(launch_steps) if launch_steps else int(N), 0
+    while done < total:
+        run.n0, run.steps = done, min(L, total - done)
+        rc = lib().oracle_shadow(C.byref(run), n, _dp(x0), None if u is None else u.ctypes.data, ends.ctypes.data,
+                                 float(d0), MATH[math], threads)
+        if rc != 0:
+            raise ValueError(f"oracle_shadow returned {rc}")
+        done += run.steps
+    return ends
 
 
 def oracle_frames(sys, x0, N, frames: list[FrameSpec], *, tau=1, seed=0, math="portable", threads=0,

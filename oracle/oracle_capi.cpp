@@ -182,6 +182,125 @@ void run_orbit(const cl_run& run0, int64_t i, const cl_buffers& b, const double*
     }
 }
 
+// ---- the two-trajectory estimator (src/Lyapunov/two_trajectory.jl:31-80, separation.jl) ------------------------
+// forward of the run's system (the tangent the system computes alongside is dropped)
+template <int MM>
+void forward_only(const cl_run& run, const Chain<MM>& chain, Gauss3& gauss, const SplitHH& split, double* x) {
+    double M[CL_MAX_DIM * CL_MAX_DIM];
+    switch (run.sys.kind) {
+        case CL_SYS_STANDARD: Systems<MM>::standard(run.sys.K, x, M); break;
+        case CL_SYS_WRAPPED_STANDARD: Systems<MM>::wrapped(run.sys.K, x, M); break;
+        case CL_SYS_FROESCHLE: Systems<MM>::froeschle(run.sys.nu, run.sys.kappa, run.sys.mu, x, M); break;
+        case CL_SYS_LINEAR: Systems<MM>::linear(run.sys.A, run.d, x, M); break;
+        case CL_SYS_HH_GAUSS: gauss.step(x, run.sys.dt, M); break;
+        case CL_SYS_HH_SPLIT: split.forward(x, run.sys.dt); break;
+        case CL_SYS_CHAIN: {
+            double g[CL_MAX_DIM / 2], gl[CL_MAX_DIM / 2], gr[CL_MAX_DIM / 2];
+            chain.band(x, g, gl, gr);
+            chain.forward(x);
+            break;
+        }
+    }
+}
+// separation: y - x on lifted states; WrappedStandardMap: the minimal image in (-pi, pi] of both coordinates
+void shadow_separation(const cl_run& run, const double* x, const double* y, double* delta) {
+    if (run.sys.kind == CL_SYS_WRAPPED_STANDARD) {
+        const double tp = 2 * jl_pi(), h = tp / 2;
+        for (int i = 0; i < 2; ++i) {
+            const double u = y[i] - x[i];
+            delta[i] = u > h ? u - tp : (u <= -h ? u + tp : u);
+        }
+    } else {
+        for (int i = 0; i < run.d; ++i) delta[i] = y[i] - x[i];
+    }
+}
+// displaced: x + delta; WrappedStandardMap: both coordinates reduced, the reduction counts added to x's
+void shadow_displaced(const cl_run& run, const double* x, const double* delta, double* y) {
+    if (run.sys.kind == CL_SYS_WRAPPED_STANDARD) {
+        const double tp = 2 * jl_pi();
+        double xr, a, pr, b;
+        wrap_reduce(x[0] + delta[0], tp, &xr, &a);
+        wrap_reduce(x[1] + delta[1], tp, &pr, &b);
+        y[0] = xr; y[1] = pr; y[2] = x[2] + a; y[3] = x[3] + b;
+    } else {
+        for (int i = 0; i < run.d; ++i) y[i] = x[i] + delta[i];
+    }
+}
+void shadow_store(uint8_t* e, int s, const double* x, const double* y, CS acc, double dprev, int8_t code, int64_t step,
+                  double value) {
+    std::memset(e, 0, 8 * (2 * s + 6));
+    std::memcpy(e, x, 8 * s);
+    std::memcpy(e + 8 * s, y, 8 * s);
+    std::memcpy(e + 8 * (2 * s), &acc.s, 8);
+    std::memcpy(e + 8 * (2 * s + 1), &acc.c, 8);
+    std::memcpy(e + 8 * (2 * s + 2), &dprev, 8);
+    std::memcpy(e + 8 * (2 * s + 3), &code, 1);
+    std::memcpy(e + 8 * (2 * s + 4), &step, 8);
+    std::memcpy(e + 8 * (2 * s + 5), &value, 8);
+}
+template <int MM>
+void shadow_orbit(const cl_run& run, int64_t i, const double* x0, const double* u0, uint8_t* ends, double d0,
+                  int64_t n0, int64_t steps) {
+    using Mth = Math<MM>;
+    const int s = run.s, d = run.d;
+    uint8_t* e = ends + i * 8 * (2 * s + 6);
+    double x[CL_MAX_DIM] = {}, y[CL_MAX_DIM] = {}, delta[CL_MAX_DIM] = {};
+    CS acc{0.0, 0.0};
+    double dprev;
+    const Chain<MM> chain{run.sys.n_sites, run.sys.K, run.sys.eps, run.sys.ring != 0};
+    Gauss3 gauss(run.sys.gauss_maxiter, run.sys.gauss_tol);
+    const SplitHH split{run.sys.n_stages, run.sys.stage_c, run.sys.stage_d};
+    if (n0 == 0) {
+        std::memcpy(x, x0 + i * s, 8 * s);
+        double u[CL_MAX_DIM];
+        if (u0) std::memcpy(u, u0 + i * d, 8 * d);
+        else seeded_frame<MM>(run.seed, run.orbit_base + i + 1, d, 1, u);
+        for (int c = 0; c < d; ++c) delta[c] = d0 * u[c];
+        shadow_displaced(run, x, delta, y);
+        shadow_separation(run, x, y, delta);
+        dprev = safe_norm(delta, d);
+        const int8_t code = !(std::isfinite(dprev) && dprev > 0) ? 2 : (dprev < d0 / 2 || dprev > 2 * d0 ? 3 : 0);
+        if (code != 0) { shadow_store(e, s, x, y, acc, dprev, code, 0, dprev); return; }
+    } else {
+        int8_t code;
+        std::memcpy(&code, e + 8 * (2 * s + 3), 1);
+        if (code != 0) return;
+        std::memcpy(x, e, 8 * s);
+        std::memcpy(y, e + 8 * s, 8 * s);
+        std::memcpy(&acc.s, e + 8 * (2 * s), 8);
+        std::memcpy(&acc.c, e + 8 * (2 * s + 1), 8);
+        std::memcpy(&dprev, e + 8 * (2 * s + 2), 8);
+    }
+    int64_t n = n0;
+    for (int64_t h = 0; h < steps / run.tau; ++h) {
+        for (int t = 0; t < run.tau; ++t) {
+            forward_only<MM>(run, chain, gauss, split, x);
+            forward_only<MM>(run, chain, gauss, split, y);
+        }
+        n += run.tau;
+        // _first_bad_value: the first non-finite entry of x, else of y
+        bool fin = true;
+        double bad = 0.0;
+        for (int c = 0; c < s && fin; ++c) if (!std::isfinite(x[c])) { fin = false; bad = x[c]; }
+        for (int c = 0; c < s && fin; ++c) if (!std::isfinite(y[c])) { fin = false; bad = y[c]; }
+        if (!fin) { shadow_store(e, s, x, y, acc, dprev, 1, n, bad); return; }
+        shadow_separation(run, x, y, delta);
+        const double dd = safe_norm(delta, d);
+        if (!(std::isfinite(dd) && dd > 0)) { shadow_store(e, s, x, y, acc, dprev, 2, n, dd); return; }
+        acc = cs_add(acc, Mth::log(dd / dprev));
+        const double f = d0 / dd;
+        for (int c = 0; c < d; ++c) delta[c] = delta[c] * f;
+        shadow_displaced(run, x, delta, y);
+        shadow_separation(run, x, y, delta);
+        dprev = safe_norm(delta, d);
+        if (!(dprev >= d0 / 2 && dprev <= 2 * d0)) {
+            shadow_store(e, s, x, y, acc, dprev, (std::isfinite(dprev) && dprev > 0) ? 3 : 2, n, dprev);
+            return;
+        }
+    }
+    shadow_store(e, s, x, y, acc, dprev, 0, n, dprev);
+}
+
 }  // namespace
 
 extern "C" {
@@ -281,6 +400,33 @@ int32_t oracle_gauss3_step(double* z, double h, int32_t maxiter, double tol, dou
 int32_t oracle_split_step(double* z, double h, int32_t n_stages, const double* c, const double* d, double* T) {
     const SplitHH s{n_stages, c, d};
     s.step(z, h, T);
+    return 0;
+}
+
+// The two-trajectory estimator on the CPU: one window [run.n0, run.n0 + steps) of n orbits (see the C ABI).
+int oracle_shadow(const cl_run* run, int64_t n, const double* x0, const double* u0, void* ends, double d0,
+                  int32_t math_mode, int32_t threads) {
+    const int64_t steps = run->steps > 0 ? run->steps : run->N - run->n0;
+    if (run->tau <= 0 || steps % run->tau != 0 || run->n0 + steps > run->N) return CL_EINVAL;
+    const int hw = static_cast<int>(std::max(1u, std::thread::hardware_concurrency()));
+    const int nt = static_cast<int>(std::min<int64_t>(threads > 0 ? threads : hw, std::max<int64_t>(n, 1)));
+    std::atomic<int64_t> next{0};
+    auto worker = [&]() {
+        for (;;) {
+            const int64_t lo = next.fetch_add(16);
+            if (lo >= n) return;
+            for (int64_t i = lo; i < std::min<int64_t>(lo + 16, n); ++i) {
+                if (math_mode == MATH_LIBM)
+                    shadow_orbit<MATH_LIBM>(*run, i, x0, u0, static_cast<uint8_t*>(ends), d0, run->n0, steps);
+                else
+                    shadow_orbit<MATH_PORTABLE>(*run, i, x0, u0, static_cast<uint8_t*>(ends), d0, run->n0, steps);
+            }
+        }
+    };
+    std::vector<std::thread> pool;
+    for (int t = 1; t < nt; ++t) pool.emplace_back(worker);
+    worker();
+    for (auto& th : pool) th.join();
     return 0;
 }
 
