@@ -30,7 +30,10 @@ Multi-GPU: orbits are independent, so N ranks run N shards of the same size with
             over the whole grid;
   mlp       the screen's network alone: inference rows/s at a batch of 262144 against the BF16 tensor peak;
   split     IntegratorMap(KahanLi(8), Henon-Heiles, dt = 0.05), 16384 starts on the E = 1/8 section, N = 2e5
-            (t = 1e4), k = 2, tau = 10, chain MEGNO + FLI + QRSpectrum(Givens), FP64 kernel: steps/s.
+            (t = 1e4), k = 2, tau = 10, chain MEGNO + FLI + QRSpectrum(Givens), FP64 kernel: steps/s;
+  shadow    the two-trajectory estimator on the coupled-map workload's orbits (65536 x 1e5, tau = 10, d0 = 1e-8);
+  record    the study recorder: the wrapped standard map K = 6, 4096 orbits x 1e5 steps, QRSpectrum(MGS), tau = 1,
+            100 log-spaced grid rows.
 """
 from __future__ import annotations
 
@@ -168,7 +171,8 @@ def main() -> None:
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
     ap.add_argument("--only", choices=["fp64", "mixed"], default=None,
                     help="time one kernel of the default workload and print a short line (a small case for ncu)")
-    ap.add_argument("--workload", default="coupled", choices=["coupled", "standard", "gauss", "lattice", "screen", "mlp", "split"])
+    ap.add_argument("--workload", default="coupled", choices=["coupled", "standard", "gauss", "lattice", "screen", "mlp", "split", "shadow",
+                                                             "record"])
     args = ap.parse_args()
     if args.workload != "coupled":
         run_workload(args)
@@ -737,9 +741,115 @@ def workload_mlp(args):
           clocks=sampler.summary(), gpu_launches=int(n_fwd))
 
 
+def _host_call_workload(args, metric, unit, units_per_call, call, config, cpu, dtype="f64"):
+    """Steps of the public host entry point: `value` from the device events around its launches (inputs resident),
+    `e2e` from the wall clock around the whole call (copies in and out included)."""
+    torch, dev, L = _setup()
+    sampler = ClockSampler(0)
+    for _ in range(args.warmup):
+        call()
+    gpu, wall = [], []
+    with sampler:
+        for _ in range(args.steps):
+            t0 = time.perf_counter()
+            ms, h2d, d2h = call()
+            wall.append(time.perf_counter() - t0)
+            gpu.append(ms)
+    l0 = L.cl_b200_launch_count()
+    call()
+    launches = L.cl_b200_launch_count() - l0
+    value = units_per_call / (np.mean(gpu) / 1e3)
+    e2e = units_per_call / np.mean(wall)
+    _line(metric, value, unit, args, gpu, config, dtype=dtype,
+          e2e=dict(value=e2e, unit=unit, h2d_bytes_per_step=int(h2d), d2h_bytes_per_step=int(d2h)),
+          cpu_baseline=None if args.no_cpu else cpu(), clocks=sampler.summary(), gpu_launches=int(launches))
+
+
+def workload_shadow(args):
+    from chaos_b200 import FroeschleMap
+    from chaos_b200.propagate import build_run, FrameSpec
+    from chaos_b200.shadow import end_dtype
+    import ctypes as C_
+    from chaos_b200 import _abi
+    torch, dev, L = _setup()
+    n, N, tau, d0 = args.orbits or 65536, args.N if args.N != N_STEPS else 100_000, 10, 1e-8
+    sysm = FroeschleMap(NU, KAPPA, MU)
+    x0 = np.random.default_rng(SEED).uniform(0, 2 * np.pi, (n, 4))
+    run = build_run(sysm, N, tau, [FrameSpec(1, ())], "fp64", SEED)
+
+    def call():
+        ends = np.zeros(n, dtype=end_dtype(4))
+        prov = _abi.cl_prov()
+        rc = L.cl_b200_shadow(C_.byref(run), n, x0.ctypes.data_as(C_.POINTER(C_.c_double)), None, ends.ctypes.data,
+                              d0, C_.byref(prov))
+        if rc != 0:
+            raise RuntimeError(rc)
+        return prov.gpu_ms, x0.nbytes, ends.nbytes
+
+    def cpu():
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle as O
+        threads = os.cpu_count() or 1
+        t = time.perf_counter()
+        O.oracle_shadow(sysm, x0[:1024], 4000, d0=d0, tau=tau, seed=SEED, threads=threads)
+        return dict(value=1024 * 4000 / (time.perf_counter() - t), unit="orbit-steps/s", cores=threads, kind="port",
+                    sample="1024 orbits x 4000 steps (oracle, all host threads)")
+    _host_call_workload(args, "orbit-steps/s (two-trajectory estimator, 4D coupled standard maps, reference and "
+                        "shadow orbits)", "orbit-steps/s", n * N, call,
+                        dict(workload=f"shadow-froeschle-{n}x{N:.0e}-tau10-d0-1e-8", orbits=n, N=N, tau=tau, d0=d0),
+                        cpu)
+
+
+def workload_record(args):
+    from chaos_b200 import MGS, QRSpectrum, WrappedStandardMap, torus_state
+    from chaos_b200.propagate import build_run, FrameSpec
+    import ctypes as C_
+    from chaos_b200 import _abi
+    torch, dev, L = _setup()
+    n, N, tau = args.orbits or 4096, args.N if args.N != N_STEPS else 100_000, 1
+    sysm = WrappedStandardMap(6.0)
+    xp = np.random.default_rng(SEED).uniform(0, 2 * np.pi, (n, 2))
+    x0 = np.array([torus_state(z) for z in xp])
+    grid = np.unique(np.round(np.logspace(0, np.log10(N), 100)).astype(np.int64))
+    run = build_run(sysm, N, tau, [FrameSpec(2, (QRSpectrum(MGS()),))], "fp64", SEED)
+    ncol = L.cl_b200_record_columns(C_.byref(run))
+    sb = L.cl_b200_record_state_bytes(C_.byref(run))
+
+    def call():
+        x = x0.copy()
+        W = np.broadcast_to(np.eye(2), (n, 2, 2)).copy()
+        st = np.zeros((n, sb), np.uint8)
+        code = np.zeros(n, np.int8)
+        hs = np.zeros(n, np.int64)
+        R = np.zeros((n, len(grid), ncol))
+        fail = np.zeros(n, np.int64)
+        prov = _abi.cl_prov()
+        rc = L.cl_b200_record(C_.byref(run), n, x.ctypes.data, W.ctypes.data, st.ctypes.data, code.ctypes.data,
+                              hs.ctypes.data, grid.ctypes.data, len(grid), R.ctypes.data, fail.ctypes.data,
+                              C_.byref(prov))
+        if rc != 0:
+            raise RuntimeError(rc)
+        return prov.gpu_ms, x.nbytes + W.nbytes + grid.nbytes + R.nbytes, R.nbytes + x.nbytes + W.nbytes + st.nbytes
+
+    def cpu():
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle as O
+        threads = os.cpu_count() or 1
+        g = grid[grid <= 20000]
+        t = time.perf_counter()
+        O.oracle_record(sysm, x0[:512], 20000, tau, QRSpectrum(MGS()), g, threads=threads)
+        return dict(value=512 * 20000 / (time.perf_counter() - t), unit="orbit-steps/s", cores=threads, kind="port",
+                    sample="512 orbits x 20000 steps with the grid rows up to 20000 (oracle, all host threads)")
+    _host_call_workload(args, "orbit-steps/s (study recorder, wrapped standard map K=6, QRSpectrum(MGS), 100 grid "
+                        "rows)", "orbit-steps/s", n * N, call,
+                        dict(workload=f"record-wrapped-k6-{n}x{N:.0e}-tau1-mgs-{len(grid)}rows", orbits=n, N=N, tau=tau,
+                             grid_rows=int(len(grid))), cpu)
+
+
 def run_workload(args):
     {"standard": workload_standard, "gauss": workload_gauss, "lattice": workload_lattice,
-     "screen": workload_screen, "mlp": workload_mlp, "split": workload_split}[args.workload](args)
+     "screen": workload_screen, "mlp": workload_mlp, "split": workload_split, "shadow": workload_shadow,
+     "record": workload_record}[args.workload](args)
 
 
 

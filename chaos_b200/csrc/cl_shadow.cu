@@ -102,22 +102,22 @@ __device__ __forceinline__ void store_end(uint64_t* e, const double* x, const do
     e[2 * S + 5] = __double_as_longlong(value);
 }
 
-// _shadow_body (two_trajectory.jl:59-80) for one launch window of one orbit
+// One orbit's end record in registers (ShadowEnd{S, Float64}).
 template <class Sys>
-__global__ void __launch_bounds__(128) shadow_kernel(const ShArgs a, const Sys sys) {
-    constexpr int D = Sys::D, S = Sys::S, W = 2 * S + 6;
-    const i64 i = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (i >= a.n) return;
-    uint64_t* e = a.ends + i * W;
-    double x[S], y[S], delta[D];
-    CS acc{0.0, 0.0};
+struct ShadowOrbit {
+    static constexpr int D = Sys::D, S = Sys::S, W = 2 * S + 6;
+    double x[S], y[S];
+    CS acc;
     double dprev;
-    const double d0 = a.d0;
-    if (a.n0 == 0) {
-        // _shadow_start (two_trajectory.jl:31-36): y = displaced(x0, d0 u0), its realised separation, a code
+    int8_t code;
+    i64 step;
+    double value;
+
+    // _shadow_start (two_trajectory.jl:31-36): y = displaced(x0, d0 u0), its realised separation, a code
+    __device__ __forceinline__ void start(const ShArgs& a, i64 i) {
+        double delta[D], u[D];
 #pragma unroll
         for (int c = 0; c < S; ++c) x[c] = a.x0[i * S + c];
-        double u[D];
         if (a.u0) {
 #pragma unroll
             for (int c = 0; c < D; ++c) u[c] = a.u0[i * D + c];
@@ -125,59 +125,139 @@ __global__ void __launch_bounds__(128) shadow_kernel(const ShArgs a, const Sys s
             seeded_frame<D, 1>(a.seed, a.orbit_base + i + 1, u);
         }
 #pragma unroll
-        for (int c = 0; c < D; ++c) delta[c] = d0 * u[c];
+        for (int c = 0; c < D; ++c) delta[c] = a.d0 * u[c];
         displaced<Sys>(x, delta, y);
         separation<Sys>(x, y, delta);
         dprev = safe_norm<D>(delta);
-        const int8_t code = !(isfin(dprev) && dprev > 0) ? 2 : (dprev < d0 / 2 || dprev > 2 * d0 ? 3 : 0);
-        if (code != 0) { store_end<S>(e, x, y, acc, dprev, code, 0, dprev); return; }
-    } else {
-        if (static_cast<int8_t>(e[2 * S + 3] & 0xff) != 0) return;   // failed in an earlier launch: frozen
+        acc = CS{0.0, 0.0};
+        code = !(isfin(dprev) && dprev > 0) ? 2 : (dprev < a.d0 / 2 || dprev > 2 * a.d0 ? 3 : 0);
+        step = 0;
+        value = dprev;
+    }
+    __device__ __forceinline__ void load(const uint64_t* e) {
 #pragma unroll
         for (int c = 0; c < S; ++c) { x[c] = __longlong_as_double(e[c]); y[c] = __longlong_as_double(e[S + c]); }
         acc.s = __longlong_as_double(e[2 * S]);
         acc.c = __longlong_as_double(e[2 * S + 1]);
         dprev = __longlong_as_double(e[2 * S + 2]);
+        code = static_cast<int8_t>(e[2 * S + 3] & 0xff);
+        step = static_cast<i64>(e[2 * S + 4]);
+        value = __longlong_as_double(e[2 * S + 5]);
     }
-    i64 n = a.n0;
-    const i64 handoffs = a.steps / a.tau;
-    for (i64 h = 0; h < handoffs; ++h) {
-        for (int t = 0; t < a.tau; ++t) {
-            fwd(sys, x);
-            fwd(sys, y);
+    __device__ __forceinline__ void store(uint64_t* e) const { store_end<S>(e, x, y, acc, dprev, code, step, value); }
+
+    // _shadow_body (two_trajectory.jl:59-80) over `steps` steps from global step n; sets code / step / value
+    __device__ __forceinline__ void body(const Sys& sys, i64 n, i64 steps, int tau, double d0) {
+        double delta[D];
+        for (i64 h = 0; h < steps / tau; ++h) {
+            for (int t = 0; t < tau; ++t) {
+                fwd(sys, x);
+                fwd(sys, y);
+            }
+            n += tau;
+            bool fin = true;
+            double bad = 0.0;
+#pragma unroll
+            for (int c = S - 1; c >= 0; --c) if (!isfin(y[c])) { fin = false; bad = y[c]; }
+#pragma unroll
+            for (int c = S - 1; c >= 0; --c) if (!isfin(x[c])) { fin = false; bad = x[c]; }
+            if (!fin) { code = 1; step = n; value = bad; return; }
+            separation<Sys>(x, y, delta);
+            const double d = safe_norm<D>(delta);
+            if (!(isfin(d) && d > 0)) { code = 2; step = n; value = d; return; }
+            cs_add(acc, cl_log(d / dprev));
+            const double f = d0 / d;
+#pragma unroll
+            for (int c = 0; c < D; ++c) delta[c] = delta[c] * f;
+            displaced<Sys>(x, delta, y);
+            separation<Sys>(x, y, delta);
+            dprev = safe_norm<D>(delta);
+            if (!(dprev >= d0 / 2 && dprev <= 2 * d0)) {
+                code = (isfin(dprev) && dprev > 0) ? 3 : 2;
+                step = n;
+                value = dprev;
+                return;
+            }
         }
-        n += a.tau;
-        bool fin = true;
-        double bad = 0.0;
-#pragma unroll
-        for (int c = S - 1; c >= 0; --c) if (!isfin(y[c])) { fin = false; bad = y[c]; }
-#pragma unroll
-        for (int c = S - 1; c >= 0; --c) if (!isfin(x[c])) { fin = false; bad = x[c]; }
-        if (!fin) { store_end<S>(e, x, y, acc, dprev, 1, n, bad); return; }
-        separation<Sys>(x, y, delta);
-        const double d = safe_norm<D>(delta);
-        if (!(isfin(d) && d > 0)) { store_end<S>(e, x, y, acc, dprev, 2, n, d); return; }
-        cs_add(acc, cl_log(d / dprev));
-        const double f = d0 / d;
-#pragma unroll
-        for (int c = 0; c < D; ++c) delta[c] = delta[c] * f;
-        displaced<Sys>(x, delta, y);
-        separation<Sys>(x, y, delta);
-        dprev = safe_norm<D>(delta);
-        if (!(dprev >= d0 / 2 && dprev <= 2 * d0)) {
-            store_end<S>(e, x, y, acc, dprev, (isfin(dprev) && dprev > 0) ? 3 : 2, n, dprev);
-            return;
-        }
+        code = 0;
+        step = n;
+        value = dprev;
     }
-    store_end<S>(e, x, y, acc, dprev, 0, n, dprev);
+};
+
+// One launch window of one orbit (the estimator: _shadow_kernel!, two_trajectory.jl:108-115)
+template <class Sys>
+__global__ void __launch_bounds__(128) shadow_kernel(const ShArgs a, const Sys sys) {
+    using O = ShadowOrbit<Sys>;
+    const i64 i = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= a.n) return;
+    uint64_t* e = a.ends + i * O::W;
+    O o;
+    if (a.n0 == 0) {
+        o.start(a, i);
+        if (o.code != 0) { o.store(e); return; }
+    } else {
+        o.load(e);
+        if (o.code != 0) return;   // failed in an earlier launch: frozen
+    }
+    o.body(sys, a.n0, a.steps, a.tau, a.d0);
+    o.store(e);
 }
 
-typedef cudaError_t (*ShadowFn)(const cl_run& run, const ShArgs& a, cudaStream_t st);
+// The recorder's two-trajectory method (_shadow_record_kernel!, src/Experiments/run_device.jl:80-100): segments
+// between the grid steps of the window; row g of R[col, g, orbit] (1 + 7 + S columns) gets X2 so far in column 1
+// and the reference state in the state columns; a failure stores its 1-based grid index in fail[orbit].
+template <class Sys>
+__global__ void __launch_bounds__(128) shadow_record_kernel(const ShArgs a, const Sys sys, const i64* grid, int n_grid,
+                                                            double* R, i64* fail) {
+    using O = ShadowOrbit<Sys>;
+    constexpr int S = O::S, NCOL = 1 + 7 + S;
+    const i64 i = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= a.n) return;
+    uint64_t* e = a.ends + i * O::W;
+    O o;
+    if (a.n0 == 0) {
+        o.start(a, i);
+        // _blank_end: the start is made in the first segment; a bad start fails that segment
+    } else {
+        o.load(e);
+        if (o.code != 0) return;
+    }
+    int glo = 0;
+    while (glo < n_grid && grid[glo] <= a.n0) ++glo;
+    int ghi = glo - 1;
+    while (ghi + 1 < n_grid && grid[ghi + 1] <= a.n0 + a.steps) ++ghi;
+    i64 n = a.n0;
+    double* Ri = R + i * static_cast<i64>(NCOL) * n_grid;
+    for (int g = glo; g <= ghi; ++g) {
+        const i64 target = grid[g];
+        if (o.code == 0) o.body(sys, n, target - n, a.tau, a.d0);
+        if (o.code != 0) { fail[i] = g + 1; o.store(e); return; }
+        n = target;
+        double* row = Ri + static_cast<i64>(g) * NCOL;
+        row[0] = cs_total(o.acc) / static_cast<double>(target);
+#pragma unroll
+        for (int j = 0; j < S; ++j) row[8 + j] = o.x[j];
+    }
+    if (o.code == 0 && n < a.n0 + a.steps) {
+        o.body(sys, n, a.n0 + a.steps - n, a.tau, a.d0);
+        if (o.code != 0) fail[i] = ghi + 2;
+    } else if (o.code != 0 && glo > ghi) {
+        fail[i] = ghi + 2;   // a bad start in a window with no grid step
+    }
+    o.store(e);
+}
+
+struct RecOut { const i64* grid; int n_grid; double* R; i64* fail; };   // grid records (NULL grid: none)
+
+typedef cudaError_t (*ShadowFn)(const cl_run& run, const ShArgs& a, const RecOut& r, cudaStream_t st);
 
 template <class Sys>
-cudaError_t launch_shadow(const cl_run& run, const ShArgs& a, cudaStream_t st) {
+cudaError_t launch_shadow(const cl_run& run, const ShArgs& a, const RecOut& r, cudaStream_t st) {
     const Sys sys = SysMaker<Sys>::make(run, nullptr);
-    shadow_kernel<Sys><<<static_cast<unsigned>((a.n + 127) / 128), 128, 0, st>>>(a, sys);
+    const unsigned grid = static_cast<unsigned>((a.n + 127) / 128);
+    if (r.grid) shadow_record_kernel<Sys><<<grid, 128, 0, st>>>(a, sys, r.grid, r.n_grid, r.R, r.fail);
+    else shadow_kernel<Sys><<<grid, 128, 0, st>>>(a, sys);
     return cudaGetLastError();
 }
 
@@ -248,45 +328,76 @@ int cl_b200_shadow_device(const cl_run* run, int64_t n, const double* x0, const 
     const int v = check_shadow(*run, d0, &fn);
     if (v) return v;
     const int64_t steps = run->steps > 0 ? run->steps : run->N - run->n0;
-    const cudaError_t e = fn(*run, shargs(*run, n, x0, u0, ends, d0, run->n0, steps), static_cast<cudaStream_t>(stream));
+    const cudaError_t e = fn(*run, shargs(*run, n, x0, u0, ends, d0, run->n0, steps), RecOut{nullptr, 0, nullptr, nullptr},
+                             static_cast<cudaStream_t>(stream));
     capi_count_launch();
     return e == cudaSuccess ? 0 : capi_map_cuda(e, "two-trajectory launch");
 }
 
-int cl_b200_shadow(const cl_run* run, int64_t n, const double* x0, const double* u0, void* ends, double d0,
-                   cl_prov* prov) {
-    if (!run || n <= 0 || !x0 || !ends) return capi_fail(CL_EINVAL, "bad arguments");
+int cl_b200_shadow_record_device(const cl_run* run, int64_t n, const double* x0, const double* u0, void* ends,
+                                 double d0, const int64_t* grid, int32_t n_grid, double* R, int64_t* fail,
+                                 void* stream) {
+    if (!run || n <= 0 || !ends || (run->n0 == 0 && !x0) || !grid || n_grid < 1 || !R || !fail)
+        return capi_fail(CL_EINVAL, "bad arguments");
+    ShadowFn fn;
+    const int v = check_shadow(*run, d0, &fn);
+    if (v) return v;
+    const int64_t steps = run->steps > 0 ? run->steps : run->N - run->n0;
+    const cudaError_t e = fn(*run, shargs(*run, n, x0, u0, ends, d0, run->n0, steps),
+                             RecOut{reinterpret_cast<const i64*>(grid), n_grid, R, reinterpret_cast<i64*>(fail)},
+                             static_cast<cudaStream_t>(stream));
+    capi_count_launch();
+    return e == cudaSuccess ? 0 : capi_map_cuda(e, "two-trajectory record launch");
+}
+
+// Host buffers: copies in, windows of run.steps steps from run.n0 to run.N, copies out; with `grid`, the records.
+static int shadow_host(const cl_run* run, int64_t n, const double* x0, const double* u0, void* ends, double d0,
+                       const int64_t* grid, int32_t n_grid, double* R, int64_t* fail, cl_prov* prov) {
+    if (!run || n <= 0 || !x0 || !ends || (grid && (n_grid < 1 || !R || !fail))) return capi_fail(CL_EINVAL, "bad arguments");
     ShadowFn fn;
     int rc = check_shadow(*run, d0, &fn);
     if (rc) return rc;
-    const int S = run->s, D = run->d;
+    const int S = run->s, D = run->d, ncol = 1 + 7 + S;
     const size_t xb = sizeof(double) * S * n, ub = sizeof(double) * D * n, eb = static_cast<size_t>(cl_b200_shadow_bytes(S)) * n;
-    double *dx = nullptr, *du = nullptr;
+    const size_t gb = grid ? sizeof(int64_t) * n_grid : 0, rb = grid ? sizeof(double) * ncol * n_grid * n : 0,
+                 fb = grid ? sizeof(int64_t) * n : 0;
+    double *dx = nullptr, *du = nullptr, *dr = nullptr;
+    int64_t *dg = nullptr, *df = nullptr;
     void* de = nullptr;
     cudaStream_t st = nullptr;
     cudaError_t e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaMalloc(reinterpret_cast<void**>(&dx), xb);
     if (e == cudaSuccess && u0) e = cudaMalloc(reinterpret_cast<void**>(&du), ub);
     if (e == cudaSuccess) e = cudaMalloc(&de, eb);
+    if (e == cudaSuccess && grid) e = cudaMalloc(reinterpret_cast<void**>(&dg), gb);
+    if (e == cudaSuccess && grid) e = cudaMalloc(reinterpret_cast<void**>(&dr), rb);
+    if (e == cudaSuccess && grid) e = cudaMalloc(reinterpret_cast<void**>(&df), fb);
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     int launches = 0;
     if (e == cudaSuccess) {
         cudaMemcpyAsync(dx, x0, xb, cudaMemcpyHostToDevice, st);
         if (u0) cudaMemcpyAsync(du, u0, ub, cudaMemcpyHostToDevice, st);
         if (run->n0 > 0) cudaMemcpyAsync(de, ends, eb, cudaMemcpyHostToDevice, st);
+        if (grid) {
+            cudaMemcpyAsync(dg, grid, gb, cudaMemcpyHostToDevice, st);
+            cudaMemcpyAsync(dr, R, rb, cudaMemcpyHostToDevice, st);
+            cudaMemcpyAsync(df, fail, fb, cudaMemcpyHostToDevice, st);
+        }
         cudaEventCreate(&e0);
         cudaEventCreate(&e1);
         cudaEventRecord(e0, st);
-        // windows of run.steps steps (the whole remaining run when 0), each a launch carrying the end records
         const int64_t L = run->steps > 0 ? run->steps : run->N - run->n0;
         for (int64_t n0 = run->n0; n0 < run->N && e == cudaSuccess; n0 += L) {
             const int64_t steps = std::min<int64_t>(L, run->N - n0);
-            e = fn(*run, shargs(*run, n, dx, du, de, d0, n0, steps), st);
+            e = fn(*run, shargs(*run, n, dx, du, de, d0, n0, steps),
+                   RecOut{reinterpret_cast<const i64*>(dg), n_grid, dr, reinterpret_cast<i64*>(df)}, st);
             capi_count_launch();
             ++launches;
         }
         cudaEventRecord(e1, st);
         if (e == cudaSuccess) e = cudaMemcpyAsync(ends, de, eb, cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess && grid) e = cudaMemcpyAsync(R, dr, rb, cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess && grid) e = cudaMemcpyAsync(fail, df, fb, cudaMemcpyDeviceToHost, st);
         if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     }
     if (e != cudaSuccess) rc = capi_map_cuda(e, "two-trajectory");
@@ -297,15 +408,29 @@ int cl_b200_shadow(const cl_run* run, int64_t n, const double* x0, const double*
         prov->gpu_ms = ms;
         prov->launches = launches;
         prov->launch_steps = run->steps > 0 ? run->steps : run->N - run->n0;
-        std::snprintf(prov->variant, sizeof prov->variant, "two-trajectory s%d d%d", S, D);
+        std::snprintf(prov->variant, sizeof prov->variant, "two-trajectory s%d d%d%s", S, D, grid ? " records" : "");
     }
     if (e0) cudaEventDestroy(e0);
     if (e1) cudaEventDestroy(e1);
     cudaFree(dx);
     cudaFree(du);
     cudaFree(de);
+    cudaFree(dg);
+    cudaFree(dr);
+    cudaFree(df);
     if (st) cudaStreamDestroy(st);
     return rc;
+}
+
+int cl_b200_shadow(const cl_run* run, int64_t n, const double* x0, const double* u0, void* ends, double d0,
+                   cl_prov* prov) {
+    return shadow_host(run, n, x0, u0, ends, d0, nullptr, 0, nullptr, nullptr, prov);
+}
+
+int cl_b200_shadow_record(const cl_run* run, int64_t n, const double* x0, const double* u0, void* ends, double d0,
+                          const int64_t* grid, int32_t n_grid, double* R, int64_t* fail, cl_prov* prov) {
+    if (!grid) return capi_fail(CL_EINVAL, "bad arguments");
+    return shadow_host(run, n, x0, u0, ends, d0, grid, n_grid, R, fail, prov);
 }
 
 }  // extern "C"

@@ -1,0 +1,125 @@
+"""The study recorder on the B200: `record` runs the variational methods with grid records, the device form of
+`_variational_batch!` (src/Experiments/run_device.jl:167-189) over the library's `cl_b200_record`
+(chaos_b200/csrc/cl_record.cu).
+
+At every grid step the record holds the estimator's exponents, the monitor's running maxima of the determinant and
+symplecticity residuals of the tangent and of max|M|, the orthogonality loss, the running maxima of the sum and
+pairing residuals (k = 2), G_max and the state (run_device.jl:10-35). An orbit that fails stops; its failing grid
+index (1-based) is in `fail` and, as `_unpack!` does (run_device.jl:126-139), only the rows before it are
+meaningful.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _abi
+from ._lib import last_error, lib
+from .foundation import DeviceError
+from .propagate import FrameSpec, build_run
+from .reducers import Benettin, QRSpectrum
+
+COLUMNS = ("lambda", "det", "symp", "orth", "sum", "pair", "G_max", "M_max", "state")
+
+
+@dataclass
+class RecordResult:
+    R: np.ndarray          # (n, n_grid, k + 7 + s): R[i, g] is the row of orbit i at grid step g
+    grid: np.ndarray
+    fail: np.ndarray       # 1-based failing grid index per orbit, 0 = none
+    x: np.ndarray
+    W: np.ndarray          # (n, d, k)
+    states: np.ndarray     # the estimator's state then MonState, per orbit (raw bytes)
+    code: np.ndarray
+    hstep: np.ndarray
+    k: int
+    gpu_ms: float = 0.0
+
+    def column(self, name: str) -> np.ndarray:
+        """A named field of every row: "lambda" (n, n_grid, k), "state" (n, n_grid, s), else (n, n_grid)."""
+        k = self.k
+        if name == "lambda":
+            return self.R[:, :, :k]
+        if name == "state":
+            return self.R[:, :, k + 7:]
+        return self.R[:, :, k + COLUMNS.index(name) - 1]
+
+
+def record(sys, x0, N: int, tau: int, estimator, grid, *, W0=None, launch_steps: int | None = None) -> RecordResult:
+    """Record n orbits of `sys` (StandardMap, WrappedStandardMap or a 2 x 2 LinearSymplecticMap) with `estimator`
+    (Benettin() with k = 1, or QRSpectrum(CGS / MGS / RGS / HouseholderQR / AugmentedQR) with k = 2) at the step
+    counts `grid` (increasing multiples of tau, at most N). W0 defaults to I[:, 1:k]; `launch_steps` splits the run
+    into launches that carry everything (the grid rows of a launch are written by it)."""
+    x0 = np.ascontiguousarray(np.asarray(x0, dtype=np.float64))
+    n, s = x0.shape
+    d = sys.d
+    k = 1 if isinstance(estimator, Benettin) else 2
+    if not isinstance(estimator, (Benettin, QRSpectrum)):
+        raise ValueError("the recorder's estimators are Benettin and QRSpectrum")
+    grid = np.ascontiguousarray(np.asarray(grid, dtype=np.int64))
+    if grid.ndim != 1 or len(grid) < 1 or np.any(np.diff(grid) <= 0) or grid[0] < tau or grid[-1] > N or \
+            np.any(grid % tau):
+        raise ValueError("grid: increasing multiples of tau in tau..N")
+    L = int(launch_steps) if launch_steps else int(N)
+    if L % tau:
+        raise ValueError("launch_steps must be a multiple of tau")
+    run = build_run(sys, N, tau, [FrameSpec(k, (estimator,))], "fp64", 0, steps=L)
+    Lb = lib()
+    ncol = Lb.cl_b200_record_columns(C.byref(run))
+    sb = Lb.cl_b200_record_state_bytes(C.byref(run))
+    if W0 is None:
+        W0 = np.broadcast_to(np.eye(d)[:, :k], (n, d, k))
+    Wc = np.ascontiguousarray(np.asarray(W0, dtype=np.float64).transpose(0, 2, 1))   # columns of d contiguous
+    x = x0.copy()
+    states = np.zeros((n, sb), np.uint8)
+    code = np.zeros(n, np.int8)
+    hstep = np.zeros(n, np.int64)
+    R = np.zeros((n, len(grid), ncol))
+    fail = np.zeros(n, np.int64)
+    prov = _abi.cl_prov()
+    rc = Lb.cl_b200_record(C.byref(run), n, x.ctypes.data, Wc.ctypes.data, states.ctypes.data, code.ctypes.data,
+                           hstep.ctypes.data, grid.ctypes.data, len(grid), R.ctypes.data, fail.ctypes.data,
+                           C.byref(prov))
+    if rc != 0:
+        msg = last_error()
+        if rc == _abi.EINVAL:
+            raise ValueError(msg)
+        raise DeviceError(rc, msg)
+    return RecordResult(R=R, grid=grid, fail=fail, x=x, W=Wc.transpose(0, 2, 1), states=states, code=code,
+                        hstep=hstep, k=k, gpu_ms=prov.gpu_ms)
+
+
+def record_shadow(sys, x0, N: int, tau: int, grid, *, d0: float, seed: int = 0, U0=None,
+                  launch_steps: int | None = None):
+    """The recorder's two-trajectory method (`_shadow_batch!`, run_device.jl:191-214): at the grid steps, X2 so far
+    and the reference state (R (n, n_grid, 8 + s): column 0 and columns 8..), the 1-based failing grid index per
+    orbit (`fail`), and the end records (ShadowEnd layout). U0 rows are normalised by safe_norm as
+    `propagate_shadow` does; without U0 the directions are the seeded frames' first columns."""
+    from .shadow import _safe_norm, end_dtype
+    x0 = np.ascontiguousarray(np.asarray(x0, dtype=np.float64))
+    n, s = x0.shape
+    grid = np.ascontiguousarray(np.asarray(grid, dtype=np.int64))
+    if grid.ndim != 1 or len(grid) < 1 or np.any(np.diff(grid) <= 0) or grid[0] < tau or grid[-1] > N or \
+            np.any(grid % tau):
+        raise ValueError("grid: increasing multiples of tau in tau..N")
+    L = int(launch_steps) if launch_steps else int(N)
+    u = None
+    if U0 is not None:
+        U0 = np.asarray(U0, dtype=np.float64)
+        u = np.ascontiguousarray([[float(v) / _safe_norm(row) for v in row] for row in U0])
+    run = build_run(sys, N, tau, [FrameSpec(1, ())], "fp64", seed, steps=L)
+    ends = np.zeros(n, dtype=end_dtype(s))
+    R = np.zeros((n, len(grid), 8 + s))
+    fail = np.zeros(n, np.int64)
+    prov = _abi.cl_prov()
+    rc = lib().cl_b200_shadow_record(C.byref(run), n, x0.ctypes.data, None if u is None else u.ctypes.data,
+                                     ends.ctypes.data, float(d0), grid.ctypes.data, len(grid), R.ctypes.data,
+                                     fail.ctypes.data, C.byref(prov))
+    if rc != 0:
+        msg = last_error()
+        if rc == _abi.EINVAL:
+            raise ValueError(msg)
+        raise DeviceError(rc, msg)
+    return R, fail, ends

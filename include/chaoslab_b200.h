@@ -294,6 +294,38 @@ CL_API int cl_b200_shadow_device(const cl_run* run, int64_t n, const double* x0,
 /* The same from run.n0 to run.N on host buffers, in windows of run.steps steps (synchronous). */
 CL_API int cl_b200_shadow(const cl_run* run, int64_t n, const double* x0, const double* u0, void* ends, double d0,
                           cl_prov* prov);
+/* The recorder's two-trajectory method (src/Experiments/run_device.jl:80-100): segments between the grid steps
+ * (increasing multiples of run.tau); at each grid step g of the window, row g of R[col, g, orbit] (8 + s columns,
+ * zeroed by the caller) gets X2 so far (sum / step) in column 1 and the reference state in columns 9..8+s; a failure
+ * stores the 1-based grid index whose segment holds it in fail[orbit] (zeroed by the caller). Replaces
+ * `_shadow_record_kernel!` launches. Device buffers, enqueued on `stream`; the host form runs every window. */
+CL_API int cl_b200_shadow_record_device(const cl_run* run, int64_t n, const double* x0, const double* u0, void* ends,
+                                        double d0, const int64_t* grid, int32_t n_grid, double* R, int64_t* fail,
+                                        void* stream);
+CL_API int cl_b200_shadow_record(const cl_run* run, int64_t n, const double* x0, const double* u0, void* ends,
+                                 double d0, const int64_t* grid, int32_t n_grid, double* R, int64_t* fail,
+                                 cl_prov* prov);
+
+/* ---- The study recorder (src/Experiments/run_device.jl:43-78, run_record.jl:24-40) ------------------------------
+ * One launch window [run.n0, run.n0 + run.steps) of the variational methods with grid records: the orbit body runs
+ * segment by segment between the grid steps (`grid`, increasing multiples of run.tau) and at every grid step inside
+ * the window writes one row of R[col, g, orbit] (Julia column-major, Float64), cl_b200_record_columns(run) =
+ * k + 7 + s columns: lambda (k), det_max, symp_max, orth_max, running max of eps_sum, running max of eps_pair,
+ * G_max, M_max, the state (s); det / symp / M are the running maxima of the non-raising monitor (|det M - 1|,
+ * max|M' Omega M - Omega|, max|M|, M the tangent at the handoff point). For k = 1 the sum and pair columns are left
+ * as they are. A failure stores the 1-based grid index whose segment holds it in fail[orbit] and stops the orbit.
+ * x, W, states (the estimator's state then MonState{Float64}: cl_b200_record_state_bytes(run) bytes per orbit),
+ * code and hstep are carried in place; x and W hold x0 and W0 before the first window, R and fail must be zero.
+ * Systems: StandardMap, WrappedStandardMap, 2 x 2 LinearSymplecticMap; run.frames[0]: Benettin with k = 1 or
+ * QRSpectrum(CGS, MGS, RGS, Householder, augmented) with k = 2; Float64. Replaces `_record_kernel!` launches. */
+CL_API int32_t cl_b200_record_columns(const cl_run* run);
+CL_API int64_t cl_b200_record_state_bytes(const cl_run* run);
+CL_API int cl_b200_record_device(const cl_run* run, int64_t n, double* x, double* W, void* states, int8_t* code,
+                                 int64_t* hstep, const int64_t* grid, int32_t n_grid, double* R, int64_t* fail,
+                                 void* stream);
+/* The same from run.n0 to run.N on host buffers, in windows of run.steps steps (synchronous). */
+CL_API int cl_b200_record(const cl_run* run, int64_t n, double* x, double* W, void* states, int8_t* code,
+                          int64_t* hstep, const int64_t* grid, int32_t n_grid, double* R, int64_t* fail, cl_prov* prov);
 
 /* ---- The learned screen's kernels (no reference counterpart: the reference has no learned component) ---------------
  * All enqueue on `stream` and take device pointers. BF16 matrices are row-major with 16-byte aligned rows. */

@@ -51,8 +51,10 @@ def lib() -> C.CDLL:
         L.oracle_seeded_frame.argtypes = [C.c_uint64, C.c_int64, C.c_int32, C.c_int32, dp]
         L.oracle_gauss3_step.argtypes = [dp, C.c_double, C.c_int32, C.c_double, dp]
         L.oracle_split_step.argtypes = [dp, C.c_double, C.c_int32, dp, dp, dp]
+        L.oracle_record.argtypes = [P(_abi.cl_run), C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                    C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_int32, C.c_int32]
         L.oracle_shadow.argtypes = [P(_abi.cl_run), C.c_int64, dp, C.c_void_p, C.c_void_p, C.c_double, C.c_int32,
-                                    C.c_int32]
+                                    C.c_int32, C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p]
         L.oracle_max_threads.restype = C.c_int32
         L.oracle_ensemble.argtypes = [P(_abi.cl_run), C.c_int64, P(_abi.cl_buffers), dp, P(C.c_int64), C.c_double,
                                       C.c_int32, C.c_int32]
@@ -126,24 +128,61 @@ def split_step(z, h, method):
     return z, T
 
 
+def oracle_record(sys, x0, N, tau, estimator, grid, *, W0=None, launch_steps=None, math="portable", threads=0):
+    """The recorder on the oracle: dict R (n, n_grid, ncol), fail, x, W (n, d, k), states (raw), code, hstep."""
+    from chaos_b200.reducers import Benettin
+    x = np.ascontiguousarray(np.asarray(x0, dtype=np.float64)).copy()
+    n, s = x.shape
+    d = sys.d
+    k = 1 if isinstance(estimator, Benettin) else 2
+    run = build_run(sys, N, tau, [FrameSpec(k, (estimator,))], "fp64", 0)
+    ncol = k + 7 + s
+    sb = (48 if k == 1 else 16 * k + 72) + 24
+    if W0 is None:
+        W0 = np.broadcast_to(np.eye(d)[:, :k], (n, d, k))
+    W = np.ascontiguousarray(np.asarray(W0, dtype=np.float64).transpose(0, 2, 1))
+    grid = np.ascontiguousarray(np.asarray(grid, dtype=np.int64))
+    states = np.zeros((n, sb), np.uint8)
+    code = np.zeros(n, np.int8)
+    hstep = np.zeros(n, np.int64)
+    R = np.zeros((n, len(grid), ncol))
+    fail = np.zeros(n, np.int64)
+    total, L, done = int(N), int(launch_steps) if launch_steps else int(N), 0
+    while done < total:
+        run.n0, run.steps = done, min(L, total - done)
+        rc = lib().oracle_record(C.byref(run), n, x.ctypes.data, W.ctypes.data, states.ctypes.data, code.ctypes.data,
+                                 hstep.ctypes.data, grid.ctypes.data, len(grid), R.ctypes.data, fail.ctypes.data,
+                                 MATH[math], threads)
+        if rc != 0:
+            raise ValueError(f"oracle_record returned {rc}")
+        done += run.steps
+    return dict(R=R, fail=fail, x=x, W=W.transpose(0, 2, 1), states=states, code=code, hstep=hstep)
+
+
 def oracle_shadow(sys, x0, N, *, d0, tau=1, seed=0, U0=None, math="portable", threads=0, launch_steps=None,
-                  orbit_base=0):
-    """The two-trajectory estimator on the oracle: the end records (structured array, ShadowEnd layout)."""
+                  orbit_base=0, grid=None):
+    """The two-trajectory estimator on the oracle: the end records (structured array, ShadowEnd layout); with
+    `grid`, (ends, R (n, n_grid, 8 + s), fail) of the recorder's two-trajectory method."""
     from chaos_b200.shadow import end_dtype
     x0 = np.ascontiguousarray(np.asarray(x0, dtype=np.float64))
     n, s = x0.shape
     run = build_run(sys, N, tau, [FrameSpec(1, ())], "fp64", seed, orbit_base=orbit_base)
     ends = np.zeros(n, dtype=end_dtype(s))
     u = None if U0 is None else np.ascontiguousarray(np.asarray(U0, dtype=np.float64))
+    g = None if grid is None else np.ascontiguousarray(np.asarray(grid, dtype=np.int64))
+    R = None if g is None else np.zeros((n, len(g), 8 + s))
+    fail = None if g is None else np.zeros(n, np.int64)
     total, L, done = int(N), int(launch_steps) if launch_steps else int(N), 0
     while done < total:
         run.n0, run.steps = done, min(L, total - done)
         rc = lib().oracle_shadow(C.byref(run), n, _dp(x0), None if u is None else u.ctypes.data, ends.ctypes.data,
-                                 float(d0), MATH[math], threads)
+                                 float(d0), MATH[math], threads, None if g is None else g.ctypes.data,
+                                 0 if g is None else len(g), None if R is None else R.ctypes.data,
+                                 None if fail is None else fail.ctypes.data)
         if rc != 0:
             raise ValueError(f"oracle_shadow returned {rc}")
         done += run.steps
-    return ends
+    return ends if g is None else (ends, R, fail)
 
 
 def oracle_frames(sys, x0, N, frames: list[FrameSpec], *, tau=1, seed=0, math="portable", threads=0,

@@ -238,67 +238,236 @@ void shadow_store(uint8_t* e, int s, const double* x, const double* y, CS acc, d
     std::memcpy(e + 8 * (2 * s + 4), &step, 8);
     std::memcpy(e + 8 * (2 * s + 5), &value, 8);
 }
+// One orbit's ShadowEnd in the oracle's hands: start (_shadow_start), load / store, body over a segment.
 template <int MM>
-void shadow_orbit(const cl_run& run, int64_t i, const double* x0, const double* u0, uint8_t* ends, double d0,
-                  int64_t n0, int64_t steps) {
-    using Mth = Math<MM>;
-    const int s = run.s, d = run.d;
-    uint8_t* e = ends + i * 8 * (2 * s + 6);
-    double x[CL_MAX_DIM] = {}, y[CL_MAX_DIM] = {}, delta[CL_MAX_DIM] = {};
+struct ShOrb {
+    const cl_run& run;
+    double x[CL_MAX_DIM] = {}, y[CL_MAX_DIM] = {};
     CS acc{0.0, 0.0};
-    double dprev;
-    const Chain<MM> chain{run.sys.n_sites, run.sys.K, run.sys.eps, run.sys.ring != 0};
-    Gauss3 gauss(run.sys.gauss_maxiter, run.sys.gauss_tol);
-    const SplitHH split{run.sys.n_stages, run.sys.stage_c, run.sys.stage_d};
-    if (n0 == 0) {
+    double dprev = 0.0, value = 0.0;
+    int8_t code = 0;
+    int64_t step = 0;
+    explicit ShOrb(const cl_run& r) : run(r) {}
+    void start(int64_t i, const double* x0, const double* u0, double d0) {
+        const int s = run.s, d = run.d;
+        double delta[CL_MAX_DIM] = {}, u[CL_MAX_DIM] = {};
         std::memcpy(x, x0 + i * s, 8 * s);
-        double u[CL_MAX_DIM];
         if (u0) std::memcpy(u, u0 + i * d, 8 * d);
         else seeded_frame<MM>(run.seed, run.orbit_base + i + 1, d, 1, u);
         for (int c = 0; c < d; ++c) delta[c] = d0 * u[c];
         shadow_displaced(run, x, delta, y);
         shadow_separation(run, x, y, delta);
         dprev = safe_norm(delta, d);
-        const int8_t code = !(std::isfinite(dprev) && dprev > 0) ? 2 : (dprev < d0 / 2 || dprev > 2 * d0 ? 3 : 0);
-        if (code != 0) { shadow_store(e, s, x, y, acc, dprev, code, 0, dprev); return; }
-    } else {
-        int8_t code;
-        std::memcpy(&code, e + 8 * (2 * s + 3), 1);
-        if (code != 0) return;
+        code = !(std::isfinite(dprev) && dprev > 0) ? 2 : (dprev < d0 / 2 || dprev > 2 * d0 ? 3 : 0);
+        step = 0;
+        value = dprev;
+    }
+    void load(const uint8_t* e) {
+        const int s = run.s;
         std::memcpy(x, e, 8 * s);
         std::memcpy(y, e + 8 * s, 8 * s);
         std::memcpy(&acc.s, e + 8 * (2 * s), 8);
         std::memcpy(&acc.c, e + 8 * (2 * s + 1), 8);
         std::memcpy(&dprev, e + 8 * (2 * s + 2), 8);
+        std::memcpy(&code, e + 8 * (2 * s + 3), 1);
+        std::memcpy(&step, e + 8 * (2 * s + 4), 8);
+        std::memcpy(&value, e + 8 * (2 * s + 5), 8);
     }
+    void store(uint8_t* e) const { shadow_store(e, run.s, x, y, acc, dprev, code, step, value); }
+    void body(int64_t n, int64_t steps, double d0) {
+        using Mth = Math<MM>;
+        const int s = run.s, d = run.d;
+        const Chain<MM> chain{run.sys.n_sites, run.sys.K, run.sys.eps, run.sys.ring != 0};
+        Gauss3 gauss(run.sys.gauss_maxiter, run.sys.gauss_tol);
+        const SplitHH split{run.sys.n_stages, run.sys.stage_c, run.sys.stage_d};
+        double delta[CL_MAX_DIM] = {};
+        for (int64_t h = 0; h < steps / run.tau; ++h) {
+            for (int t = 0; t < run.tau; ++t) {
+                forward_only<MM>(run, chain, gauss, split, x);
+                forward_only<MM>(run, chain, gauss, split, y);
+            }
+            n += run.tau;
+            // _first_bad_value: the first non-finite entry of x, else of y
+            bool fin = true;
+            double bad = 0.0;
+            for (int c = 0; c < s && fin; ++c) if (!std::isfinite(x[c])) { fin = false; bad = x[c]; }
+            for (int c = 0; c < s && fin; ++c) if (!std::isfinite(y[c])) { fin = false; bad = y[c]; }
+            if (!fin) { code = 1; step = n; value = bad; return; }
+            shadow_separation(run, x, y, delta);
+            const double dd = safe_norm(delta, d);
+            if (!(std::isfinite(dd) && dd > 0)) { code = 2; step = n; value = dd; return; }
+            acc = cs_add(acc, Mth::log(dd / dprev));
+            const double f = d0 / dd;
+            for (int c = 0; c < d; ++c) delta[c] = delta[c] * f;
+            shadow_displaced(run, x, delta, y);
+            shadow_separation(run, x, y, delta);
+            dprev = safe_norm(delta, d);
+            if (!(dprev >= d0 / 2 && dprev <= 2 * d0)) {
+                code = (std::isfinite(dprev) && dprev > 0) ? 3 : 2;
+                step = n;
+                value = dprev;
+                return;
+            }
+        }
+        code = 0;
+        step = n;
+        value = dprev;
+    }
+};
+
+template <int MM>
+void shadow_orbit(const cl_run& run, int64_t i, const double* x0, const double* u0, uint8_t* ends, double d0,
+                  int64_t n0, int64_t steps, const int64_t* grid = nullptr, int n_grid = 0, double* R = nullptr,
+                  int64_t* fail = nullptr) {
+    const int s = run.s;
+    uint8_t* e = ends + i * 8 * (2 * s + 6);
+    ShOrb<MM> o(run);
+    if (n0 == 0) {
+        o.start(i, x0, u0, d0);
+        if (!grid && o.code != 0) { o.store(e); return; }
+    } else {
+        o.load(e);
+        if (o.code != 0) return;
+    }
+    if (!grid) {
+        o.body(n0, steps, d0);
+        o.store(e);
+        return;
+    }
+    // _shadow_record_kernel! (src/Experiments/run_device.jl:80-100)
+    const int ncol = 1 + 7 + s;
+    int glo = 0;
+    while (glo < n_grid && grid[glo] <= n0) ++glo;
+    int ghi = glo - 1;
+    while (ghi + 1 < n_grid && grid[ghi + 1] <= n0 + steps) ++ghi;
     int64_t n = n0;
+    double* Ri = R + i * static_cast<int64_t>(ncol) * n_grid;
+    for (int g = glo; g <= ghi; ++g) {
+        if (o.code == 0) o.body(n, grid[g] - n, d0);
+        if (o.code != 0) { fail[i] = g + 1; o.store(e); return; }
+        n = grid[g];
+        double* row = Ri + static_cast<int64_t>(g) * ncol;
+        row[0] = (o.acc.s + o.acc.c) / static_cast<double>(grid[g]);
+        for (int j = 0; j < s; ++j) row[8 + j] = o.x[j];
+    }
+    if (o.code == 0 && n < n0 + steps) {
+        o.body(n, n0 + steps - n, d0);
+        if (o.code != 0) fail[i] = ghi + 2;
+    } else if (o.code != 0 && glo > ghi) {
+        fail[i] = ghi + 2;
+    }
+    o.store(e);
+}
+
+// ---- the study recorder (src/Experiments/run_device.jl:43-78, run_record.jl:24-40) ----------------------------
+// map step of a recorder system: the tangent M at x (column-major 2 x 2), then x advanced
+template <int MM>
+void rec_map(const cl_run& run, double* x, double* M) {
+    switch (run.sys.kind) {
+        case CL_SYS_STANDARD: Systems<MM>::standard(run.sys.K, x, M); break;
+        case CL_SYS_WRAPPED_STANDARD: Systems<MM>::wrapped(run.sys.K, x, M); break;
+        case CL_SYS_LINEAR: Systems<MM>::linear(run.sys.A, run.d, x, M); break;
+    }
+}
+// RunMonitor's step: |det M - 1|, max|M' Omega M - Omega| (StaticArrays products, the fused chain), max|M|
+template <int MM>
+void rec_monitor(const cl_run& run, const double* x, double* mon) {
+    double xc[CL_MAX_DIM], M[4];
+    std::memcpy(xc, x, sizeof(double) * run.s);
+    rec_map<MM>(run, xc, M);
+    const double edet = std::fabs((M[0] * M[3] - M[2] * M[1]) - 1.0);
+    const double Om[4] = {0.0, -1.0, 1.0, 0.0};
+    double P[4], Q[4];
+    for (int j = 0; j < 2; ++j)
+        for (int i = 0; i < 2; ++i) P[i + 2 * j] = std::fma(M[1 + 2 * i], Om[1 + 2 * j], M[2 * i] * Om[2 * j]);
+    for (int j = 0; j < 2; ++j)
+        for (int i = 0; i < 2; ++i) Q[i + 2 * j] = std::fma(P[i + 2], M[1 + 2 * j], P[i] * M[2 * j]);
+    double es = std::fabs(Q[0] - Om[0]);
+    for (int l = 1; l < 4; ++l) es = jl_max(es, std::fabs(Q[l] - Om[l]));
+    double mm = std::fabs(M[0]);
+    for (int l = 1; l < 4; ++l) mm = jl_max(mm, std::fabs(M[l]));
+    mon[0] = jl_max(mon[0], edet);
+    mon[1] = jl_max(mon[1], es);
+    mon[2] = jl_max(mon[2], mm);
+}
+// _orbit_body (orbit.jl:44-60) with the chain (estimator, monitor); est the estimator's bytes, mon its 3 doubles
+template <int MM>
+int8_t rec_body(const cl_run& run, double* x, double* W, uint8_t* est, double* mon, int64_t& n, int64_t steps) {
+    const int d = run.d, k = run.frames[0].k, s = run.s;
+    const cl_reducer& rd = run.frames[0].reducers[0];
     for (int64_t h = 0; h < steps / run.tau; ++h) {
         for (int t = 0; t < run.tau; ++t) {
-            forward_only<MM>(run, chain, gauss, split, x);
-            forward_only<MM>(run, chain, gauss, split, y);
+            double M[4], Wn[4];
+            rec_map<MM>(run, x, M);
+            fused_product(M, W, Wn, d, d, k);
+            std::memcpy(W, Wn, sizeof(double) * d * k);
         }
         n += run.tau;
-        // _first_bad_value: the first non-finite entry of x, else of y
-        bool fin = true;
-        double bad = 0.0;
-        for (int c = 0; c < s && fin; ++c) if (!std::isfinite(x[c])) { fin = false; bad = x[c]; }
-        for (int c = 0; c < s && fin; ++c) if (!std::isfinite(y[c])) { fin = false; bad = y[c]; }
-        if (!fin) { shadow_store(e, s, x, y, acc, dprev, 1, n, bad); return; }
-        shadow_separation(run, x, y, delta);
-        const double dd = safe_norm(delta, d);
-        if (!(std::isfinite(dd) && dd > 0)) { shadow_store(e, s, x, y, acc, dprev, 2, n, dd); return; }
-        acc = cs_add(acc, Mth::log(dd / dprev));
-        const double f = d0 / dd;
-        for (int c = 0; c < d; ++c) delta[c] = delta[c] * f;
-        shadow_displaced(run, x, delta, y);
-        shadow_separation(run, x, y, delta);
-        dprev = safe_norm(delta, d);
-        if (!(dprev >= d0 / 2 && dprev <= 2 * d0)) {
-            shadow_store(e, s, x, y, acc, dprev, (std::isfinite(dprev) && dprev > 0) ? 3 : 2, n, dprev);
-            return;
-        }
+        const int8_t c = status_of(x, s, W, d * k);
+        if (c != STATUS_OK) return c;
+        Reducers<MM>::step(rd, est, n, W, d, k);
+        rec_monitor<MM>(run, x, mon);
+        if (Reducers<MM>::failed(rd, est, k)) return STATUS_REDUCER;
     }
-    shadow_store(e, s, x, y, acc, dprev, 0, n, dprev);
+    return n == run.N ? status_of(x, s, W, d * k) : STATUS_OK;
+}
+template <int MM>
+void rec_orbit(const cl_run& run, int64_t i, double* xs, double* Ws, uint8_t* sts, int8_t* code, int64_t* hstep,
+               const int64_t* grid, int n_grid, double* R, int64_t* fail, int64_t n0, int64_t steps) {
+    if (!(n0 == 0 || code[i] == STATUS_OK)) return;
+    const int d = run.d, k = run.frames[0].k, s = run.s, ncol = k + 7 + s;
+    const cl_reducer& rd = run.frames[0].reducers[0];
+    const int64_t eb = state_bytes_of(rd, k), sb = eb + 24;
+    double* x = xs + i * s;
+    double* W = Ws + i * d * k;
+    uint8_t* est = sts + i * sb;
+    double mon[3];
+    if (n0 == 0) { std::memset(est, 0, sb); mon[0] = mon[1] = mon[2] = 0.0; }
+    else std::memcpy(mon, est + eb, 24);
+    int64_t n = n0, h = n0;
+    int8_t c = STATUS_OK;
+    int glo = 0;
+    while (glo < n_grid && grid[glo] <= n0) ++glo;
+    int ghi = glo - 1;
+    while (ghi + 1 < n_grid && grid[ghi + 1] <= n0 + steps) ++ghi;
+    double* Ri = R + i * static_cast<int64_t>(ncol) * n_grid;
+    for (int g = glo; g <= ghi; ++g) {
+        c = rec_body<MM>(run, x, W, est, mon, n, grid[g] - n);
+        h = n;
+        if (c != STATUS_OK) { fail[i] = g + 1; break; }
+        double lam[2], orth, gmax;
+        int64_t sn;
+        if (rd.kind == CL_RED_BENETTIN) {
+            CS sum; std::memcpy(&sum, est, 16); std::memcpy(&sn, est + 16, 8);
+            lam[0] = sn == 0 ? 0.0 : (sum.s + sum.c) / static_cast<double>(sn);
+            orth = 0.0; gmax = 1.0;
+        } else {
+            CS sums[2]; std::memcpy(sums, est, 32); std::memcpy(&sn, est + 32, 8);
+            std::memcpy(&gmax, est + 40, 8); std::memcpy(&orth, est + 48, 8);
+            for (int j = 0; j < 2; ++j) lam[j] = sn == 0 ? 0.0 : (sums[j].s + sums[j].c) / static_cast<double>(sn);
+        }
+        double* row = Ri + static_cast<int64_t>(g) * ncol;
+        for (int j = 0; j < k; ++j) row[j] = lam[j];
+        row[k] = mon[0];
+        row[k + 1] = mon[1];
+        row[k + 2] = orth;
+        if (k == 2) {
+            const double sp = std::fabs(lam[0] + lam[1]);
+            row[k + 3] = g > 0 ? jl_max(row[k + 3 - ncol], sp) : sp;
+            row[k + 4] = g > 0 ? jl_max(row[k + 4 - ncol], sp) : sp;
+        }
+        row[k + 5] = gmax;
+        row[k + 6] = mon[2];
+        for (int j = 0; j < s; ++j) row[k + 7 + j] = x[j];
+    }
+    if (c == STATUS_OK && n < n0 + steps) {
+        c = rec_body<MM>(run, x, W, est, mon, n, n0 + steps - n);
+        h = n;
+        if (c != STATUS_OK) fail[i] = ghi + 2;
+    }
+    std::memcpy(est + eb, mon, 24);
+    code[i] = c;
+    if (hstep) hstep[i] = h;
 }
 
 }  // namespace
@@ -403,9 +572,10 @@ int32_t oracle_split_step(double* z, double h, int32_t n_stages, const double* c
     return 0;
 }
 
-// The two-trajectory estimator on the CPU: one window [run.n0, run.n0 + steps) of n orbits (see the C ABI).
+// The two-trajectory estimator on the CPU: one window [run.n0, run.n0 + steps) of n orbits (see the C ABI); with
+// `grid`, the recorder's rows and failing grid indices as well.
 int oracle_shadow(const cl_run* run, int64_t n, const double* x0, const double* u0, void* ends, double d0,
-                  int32_t math_mode, int32_t threads) {
+                  int32_t math_mode, int32_t threads, const int64_t* grid, int32_t n_grid, double* R, int64_t* fail) {
     const int64_t steps = run->steps > 0 ? run->steps : run->N - run->n0;
     if (run->tau <= 0 || steps % run->tau != 0 || run->n0 + steps > run->N) return CL_EINVAL;
     const int hw = static_cast<int>(std::max(1u, std::thread::hardware_concurrency()));
@@ -417,9 +587,40 @@ int oracle_shadow(const cl_run* run, int64_t n, const double* x0, const double* 
             if (lo >= n) return;
             for (int64_t i = lo; i < std::min<int64_t>(lo + 16, n); ++i) {
                 if (math_mode == MATH_LIBM)
-                    shadow_orbit<MATH_LIBM>(*run, i, x0, u0, static_cast<uint8_t*>(ends), d0, run->n0, steps);
+                    shadow_orbit<MATH_LIBM>(*run, i, x0, u0, static_cast<uint8_t*>(ends), d0, run->n0, steps, grid,
+                                            n_grid, R, fail);
                 else
-                    shadow_orbit<MATH_PORTABLE>(*run, i, x0, u0, static_cast<uint8_t*>(ends), d0, run->n0, steps);
+                    shadow_orbit<MATH_PORTABLE>(*run, i, x0, u0, static_cast<uint8_t*>(ends), d0, run->n0, steps, grid,
+                                                n_grid, R, fail);
+            }
+        }
+    };
+    std::vector<std::thread> pool;
+    for (int t = 1; t < nt; ++t) pool.emplace_back(worker);
+    worker();
+    for (auto& th : pool) th.join();
+    return 0;
+}
+
+// The recorder on the CPU: one window [run.n0, run.n0 + steps) of n orbits, buffers in place (see the C ABI).
+int oracle_record(const cl_run* run, int64_t n, double* x, double* W, void* states, int8_t* code, int64_t* hstep,
+                  const int64_t* grid, int32_t n_grid, double* R, int64_t* fail, int32_t math_mode, int32_t threads) {
+    const int64_t steps = run->steps > 0 ? run->steps : run->N - run->n0;
+    if (run->tau <= 0 || steps % run->tau != 0 || run->n0 + steps > run->N || run->n_frames != 1) return CL_EINVAL;
+    const int hw = static_cast<int>(std::max(1u, std::thread::hardware_concurrency()));
+    const int nt = static_cast<int>(std::min<int64_t>(threads > 0 ? threads : hw, std::max<int64_t>(n, 1)));
+    std::atomic<int64_t> next{0};
+    auto worker = [&]() {
+        for (;;) {
+            const int64_t lo = next.fetch_add(16);
+            if (lo >= n) return;
+            for (int64_t i = lo; i < std::min<int64_t>(lo + 16, n); ++i) {
+                if (math_mode == MATH_LIBM)
+                    rec_orbit<MATH_LIBM>(*run, i, x, W, static_cast<uint8_t*>(states), code, hstep, grid, n_grid, R, fail,
+                                         run->n0, steps);
+                else
+                    rec_orbit<MATH_PORTABLE>(*run, i, x, W, static_cast<uint8_t*>(states), code, hstep, grid, n_grid, R,
+                                             fail, run->n0, steps);
             }
         }
     };

@@ -1,0 +1,95 @@
+"""The study recorder on the B200 against the oracle, bit for bit: every row of R, the failing grid index, the
+carried state, frame, estimator and monitor states, status and failing step, for the lifted and wrapped standard
+maps and a linear map, Benettin and the five QR estimators, tau 1 and 5, in one launch and in windows."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from chaos_b200 import (CGS, MGS, RGS, AugmentedQR, Benettin, HouseholderQR, LinearSymplecticMap, QRSpectrum,
+                        StandardMap, WrappedStandardMap, record, torus_state)
+from helpers import same_bits
+
+pytestmark = pytest.mark.gpu
+
+ESTS = [Benettin(), QRSpectrum(CGS()), QRSpectrum(MGS()), QRSpectrum(RGS()), QRSpectrum(HouseholderQR()),
+        QRSpectrum(AugmentedQR())]
+
+
+def _system(name):
+    z = np.random.default_rng(31).uniform(0, 2 * np.pi, (200, 2))
+    if name == "standard":
+        return StandardMap(2.5), z
+    if name == "wrapped":
+        return WrappedStandardMap(6.0), np.array([torus_state(v) for v in z])
+    return LinearSymplecticMap([[2.0, 1.0], [1.0, 1.0]]), z * 1e-6
+
+
+def _words(a):
+    """The 8-byte words of a record, every NaN pattern made one (NaN sign and payload are not IEEE-defined: the
+    device's and the host CPU's arithmetic may differ there, as the other parity tests allow)."""
+    w = np.ascontiguousarray(a).view(np.uint64).copy()
+    f = w.view(np.float64)
+    w[np.isnan(f)] = 0x7FF8000000000000
+    return w
+
+
+def _same(dev, ref):
+    assert same_bits(dev.R, ref["R"]), "R"
+    assert same_bits(dev.x, ref["x"]) and same_bits(dev.W, ref["W"]), "x / W"
+    assert np.array_equal(_words(dev.states), _words(ref["states"])), "states"
+    for key in ("fail", "code", "hstep"):
+        assert np.array_equal(getattr(dev, key), ref[key]), key
+
+
+@pytest.mark.parametrize("est", ESTS, ids=repr)
+@pytest.mark.parametrize("name", ["standard", "wrapped", "linear"])
+@pytest.mark.parametrize("tau", [1, 5])
+def test_record_matches_oracle(oracle, est, name, tau):
+    sys, x0 = _system(name)
+    N = 300 if name != "linear" else 30
+    grid = [g for g in (tau, 2 * tau, 10 * tau, 20 * tau, N) if g <= N]
+    grid = sorted(set(grid))
+    dev = record(sys, x0, N, tau, est, grid)
+    ref = oracle.oracle_record(sys, x0, N, tau, est, grid)
+    _same(dev, ref)
+
+
+@pytest.mark.parametrize("L", [10, 60])
+def test_record_windows(oracle, L):
+    sys, x0 = _system("wrapped")
+    grid = [5, 20, 40, 100, 240]
+    dev = record(sys, x0, 240, 5, QRSpectrum(HouseholderQR()), grid, launch_steps=L)
+    ref = oracle.oracle_record(sys, x0, 240, 5, QRSpectrum(HouseholderQR()), grid, launch_steps=L)
+    _same(dev, ref)
+    whole = record(sys, x0, 240, 5, QRSpectrum(HouseholderQR()), grid)
+    assert whole.R.tobytes() == dev.R.tobytes()
+
+
+def test_record_failures(oracle):
+    """A non-finite start fails at the first segment (fail = 1); an overflowing orbit fails in a later segment; the
+    rows before the failing one are kept, and everything equals the oracle."""
+    sys, x0 = _system("standard")
+    x = x0[:40].copy()
+    x[3, 0] = np.nan
+    x[9, 1] = 1e306
+    grid = [1, 5, 50, 100]
+    dev = record(sys, x, 100, 1, QRSpectrum(MGS()), grid)
+    ref = oracle.oracle_record(sys, x, 100, 1, QRSpectrum(MGS()), grid)
+    _same(dev, ref)
+    assert dev.fail[3] == 1 and dev.fail[9] >= 1 and (np.delete(dev.fail, [3, 9]) == 0).all()
+
+
+@pytest.mark.parametrize("name", ["standard", "wrapped"])
+@pytest.mark.parametrize("L", [None, 40])
+def test_shadow_record_matches_oracle(oracle, name, L):
+    from chaos_b200 import record_shadow
+    sys, x0 = _system(name)
+    x0 = x0.copy()
+    x0[5, 0] = np.nan            # fails at the start: the first segment
+    grid = [5, 20, 100, 200]
+    R, fail, ends = record_shadow(sys, x0, 200, 5, grid, d0=1e-8, seed=3, launch_steps=L)
+    rends, rR, rfail = oracle.oracle_shadow(sys, x0, 200, d0=1e-8, tau=5, seed=3, grid=grid, launch_steps=L)
+    assert same_bits(R, rR) and np.array_equal(fail, rfail)
+    assert np.array_equal(_words(ends), _words(rends))
+    assert fail[5] == 1
