@@ -33,7 +33,9 @@ Multi-GPU: orbits are independent, so N ranks run N shards of the same size with
             (t = 1e4), k = 2, tau = 10, chain MEGNO + FLI + QRSpectrum(Givens), FP64 kernel: steps/s;
   shadow    the two-trajectory estimator on the coupled-map workload's orbits (65536 x 1e5, tau = 10, d0 = 1e-8);
   record    the study recorder: the wrapped standard map K = 6, 4096 orbits x 1e5 steps, QRSpectrum(MGS), tau = 1,
-            100 log-spaced grid rows.
+            100 log-spaced grid rows;
+  indicators the indicator recorder's tangent kind: the chain FLI, MEGNO, SALI with the monitor on the wrapped
+            standard map K = 6, 4096 orbits x 1e5 steps, tau = 1, 100 log-spaced grid rows.
 """
 from __future__ import annotations
 
@@ -172,7 +174,7 @@ def main() -> None:
     ap.add_argument("--only", choices=["fp64", "mixed"], default=None,
                     help="time one kernel of the default workload and print a short line (a small case for ncu)")
     ap.add_argument("--workload", default="coupled", choices=["coupled", "standard", "gauss", "lattice", "screen", "mlp", "split", "shadow",
-                                                             "record"])
+                                                             "record", "indicators"])
     args = ap.parse_args()
     if args.workload != "coupled":
         run_workload(args)
@@ -846,10 +848,58 @@ def workload_record(args):
                              grid_rows=int(len(grid))), cpu)
 
 
+def workload_indicators(args):
+    from chaos_b200 import WrappedStandardMap, torus_state
+    from chaos_b200.propagate import build_run, FrameSpec
+    from chaos_b200.record import indicator_chain
+    import ctypes as C_
+    from chaos_b200 import _abi
+    torch, dev, L = _setup()
+    n, N, tau, ns = args.orbits or 4096, args.N if args.N != N_STEPS else 100_000, 1, 2
+    members = ["FLI", "MEGNO", "SALI"]
+    sysm = WrappedStandardMap(6.0)
+    xp = np.random.default_rng(SEED).uniform(0, 2 * np.pi, (n, 2))
+    x0 = np.array([torus_state(z) for z in xp])
+    grid = np.unique(np.round(np.logspace(0, np.log10(N), 100)).astype(np.int64))
+    run = build_run(sysm, N, tau, [FrameSpec(2, indicator_chain(members))], "fp64", SEED)
+    ncol = L.cl_b200_indicator_columns(C_.byref(run), ns)
+    sb = L.cl_b200_indicator_state_bytes(C_.byref(run))
+
+    def call():
+        x = x0.copy()
+        W = np.broadcast_to(np.eye(2), (n, 2, 2)).copy()
+        st = np.zeros((n, sb), np.uint8)
+        code = np.zeros(n, np.int8)
+        hs = np.zeros(n, np.int64)
+        R = np.zeros((n, len(grid), ncol))
+        fail = np.zeros(n, np.int64)
+        prov = _abi.cl_prov()
+        rc = L.cl_b200_indicator(C_.byref(run), n, ns, x.ctypes.data, W.ctypes.data, st.ctypes.data,
+                                 code.ctypes.data, hs.ctypes.data, grid.ctypes.data, len(grid), R.ctypes.data,
+                                 fail.ctypes.data, C_.byref(prov))
+        if rc != 0:
+            raise RuntimeError(rc)
+        return prov.gpu_ms, x.nbytes + W.nbytes + grid.nbytes + R.nbytes, R.nbytes + x.nbytes + W.nbytes + st.nbytes
+
+    def cpu():
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle as O
+        threads = os.cpu_count() or 1
+        g = grid[grid <= 20000]
+        t = time.perf_counter()
+        O.oracle_indicators(sysm, x0[:512], 20000, tau, members, g, ns=ns, threads=threads)
+        return dict(value=512 * 20000 / (time.perf_counter() - t), unit="orbit-steps/s", cores=threads, kind="port",
+                    sample="512 orbits x 20000 steps with the grid rows up to 20000 (oracle, all host threads)")
+    _host_call_workload(args, "orbit-steps/s (indicator recorder, tangent kind, chain FLI, MEGNO, SALI + monitor, "
+                        "wrapped standard map K=6, 100 grid rows)", "orbit-steps/s", n * N, call,
+                        dict(workload=f"indicators-wrapped-k6-{n}x{N:.0e}-tau1-fli-megno-sali-{len(grid)}rows",
+                             orbits=n, N=N, tau=tau, grid_rows=int(len(grid))), cpu)
+
+
 def run_workload(args):
     {"standard": workload_standard, "gauss": workload_gauss, "lattice": workload_lattice,
      "screen": workload_screen, "mlp": workload_mlp, "split": workload_split, "shadow": workload_shadow,
-     "record": workload_record}[args.workload](args)
+     "record": workload_record, "indicators": workload_indicators}[args.workload](args)
 
 
 

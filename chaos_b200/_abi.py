@@ -203,6 +203,18 @@ def declare(lib: C.CDLL) -> C.CDLL:
     lib.cl_b200_shadow_record.argtypes = [P(cl_run), C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_double,
                                           C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, P(cl_prov)]
     lib.cl_b200_shadow_record.restype = C.c_int
+    lib.cl_b200_indicator_columns.argtypes = [P(cl_run), C.c_int32]
+    lib.cl_b200_indicator_columns.restype = C.c_int32
+    lib.cl_b200_indicator_state_bytes.argtypes = [P(cl_run)]
+    lib.cl_b200_indicator_state_bytes.restype = C.c_int64
+    lib.cl_b200_indicator_device.argtypes = [P(cl_run), C.c_int64, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p,
+                                             C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p,
+                                             C.c_void_p]
+    lib.cl_b200_indicator_device.restype = C.c_int
+    lib.cl_b200_indicator.argtypes = [P(cl_run), C.c_int64, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p,
+                                      C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p,
+                                      P(cl_prov)]
+    lib.cl_b200_indicator.restype = C.c_int
     lib.cl_b200_ensemble_tune.restype = C.c_int
     lib.cl_b200_ensemble_graph_create.argtypes = [P(cl_ensemble_class), C.c_int32, P(C.c_void_p)]
     lib.cl_b200_ensemble_graph_create.restype = C.c_int
@@ -227,4 +239,5 @@ EXPORTS = ("cl_b200_propagate", "cl_b200_propagate_device", "cl_b200_check", "cl
            "cl_b200_col_sum", "cl_b200_head_loss", "cl_b200_adam", "cl_b200_to_bf16", "cl_b200_screen_features",
            "cl_b200_shadow_bytes", "cl_b200_shadow_device", "cl_b200_shadow", "cl_b200_record_columns",
            "cl_b200_record_state_bytes", "cl_b200_record_device", "cl_b200_record",
-           "cl_b200_shadow_record_device", "cl_b200_shadow_record")
+           "cl_b200_shadow_record_device", "cl_b200_shadow_record", "cl_b200_indicator_columns",
+           "cl_b200_indicator_state_bytes", "cl_b200_indicator_device", "cl_b200_indicator")

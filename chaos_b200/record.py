@@ -1,6 +1,8 @@
 """The study recorder on the B200: `record` runs the variational methods with grid records, the device form of
 `_variational_batch!` (src/Experiments/run_device.jl:167-189) over the library's `cl_b200_record`
-(chaos_b200/csrc/cl_record.cu).
+(chaos_b200/csrc/cl_record.cu); `record_shadow` the two-trajectory method; `record_indicators` the indicator
+recorder's tangent kind (src/Experiments/run_indicator_device.jl:31-60) over `cl_b200_indicator`
+(chaos_b200/csrc/cl_indicator.cu).
 
 At every grid step the record holds the estimator's exponents, the monitor's running maxima of the determinant and
 symplecticity residuals of the tangent and of max|M|, the orthogonality loss, the running maxima of the sum and
@@ -19,7 +21,7 @@ from . import _abi
 from ._lib import last_error, lib
 from .foundation import DeviceError
 from .propagate import FrameSpec, build_run
-from .reducers import Benettin, QRSpectrum
+from .reducers import FLI, MEGNO, SALI, Benettin, QRSpectrum
 
 COLUMNS = ("lambda", "det", "symp", "orth", "sum", "pair", "G_max", "M_max", "state")
 
@@ -123,3 +125,88 @@ def record_shadow(sys, x0, N: int, tau: int, grid, *, d0: float, seed: int = 0, 
             raise ValueError(msg)
         raise DeviceError(rc, msg)
     return R, fail, ends
+
+
+# The columns of each member (IND_MEMBER_COLUMNS, src/Experiments/run_indicator_chain.jl:16-17)
+MEMBER_COLUMNS = {"SALI": ("SALI.sali", "SALI.L"), "FLI": ("FLI.fli", "FLI.fli1"),
+                  "MEGNO": ("MEGNO.Y1", "MEGNO.Ybar1", "MEGNO.Ybar20_1", "MEGNO.Y2", "MEGNO.Ybar2", "MEGNO.Ybar20_2")}
+
+
+def indicator_chain(members) -> tuple:
+    """`chain_members` (run_indicator_chain.jl:27-28): the reducers in order, every member but the last
+    non-replacing, the last replacing (SALI has one form)."""
+    members = [str(m) for m in members]
+    if not members or any(m not in MEMBER_COLUMNS for m in members):
+        raise ValueError(f"members must be a non-empty list of SALI, FLI, MEGNO, got {members}")
+    out = []
+    for i, m in enumerate(members):
+        last = i == len(members) - 1
+        out.append(SALI() if m == "SALI" else FLI(replace=last) if m == "FLI" else MEGNO(replace=last))
+    return tuple(out)
+
+
+@dataclass
+class IndicatorRecord:
+    R: np.ndarray          # (n, n_grid, ncol): the members' columns, det_max, symp_max, M_max, x[:ns]
+    columns: tuple
+    grid: np.ndarray
+    fail: np.ndarray       # 1-based failing grid index per orbit, 0 = none
+    x: np.ndarray
+    W: np.ndarray          # (n, d, 2)
+    states: np.ndarray     # the members' states then the monitor's maxima, per orbit (raw bytes)
+    code: np.ndarray
+    hstep: np.ndarray
+    gpu_ms: float = 0.0
+
+    def column(self, name: str) -> np.ndarray:
+        return self.R[:, :, self.columns.index(name)]
+
+
+def record_indicators(sys, x0, N: int, tau: int, members, grid, *, ns: int = 2, W0=None,
+                      launch_steps: int | None = None) -> IndicatorRecord:
+    """The indicator recorder's tangent kind for n orbits of `sys` (StandardMap, WrappedStandardMap or a 2 x 2
+    LinearSymplecticMap): the chain of `members` (names, e.g. ["MEGNO", "SALI"]) on the frame W0 (default I) with
+    the non-raising monitor after it; at the step counts `grid` (increasing multiples of tau, at most N) one row of
+    the members' series columns (E24 order), det_max, symp_max, M_max and the first `ns` coordinates. An orbit that
+    fails stops; its failing grid index (1-based) is in `fail` and only the rows before it are meaningful."""
+    x0 = np.ascontiguousarray(np.asarray(x0, dtype=np.float64))
+    n, s = x0.shape
+    d = sys.d
+    chain = indicator_chain(members)
+    grid = np.ascontiguousarray(np.asarray(grid, dtype=np.int64))
+    if grid.ndim != 1 or len(grid) < 1 or np.any(np.diff(grid) <= 0) or grid[0] < tau or grid[-1] > N or \
+            np.any(grid % tau):
+        raise ValueError("grid: increasing multiples of tau in tau..N")
+    if not 0 <= ns <= s:
+        raise ValueError(f"ns must lie in 0..{s}")
+    L = int(launch_steps) if launch_steps else int(N)
+    if L % tau:
+        raise ValueError("launch_steps must be a multiple of tau")
+    run = build_run(sys, N, tau, [FrameSpec(2, chain)], "fp64", 0, steps=L)
+    Lb = lib()
+    ncol = Lb.cl_b200_indicator_columns(C.byref(run), ns)
+    if ncol < 0:
+        raise ValueError(f"member chain {members} is outside the compiled menu")
+    sb = Lb.cl_b200_indicator_state_bytes(C.byref(run))
+    if W0 is None:
+        W0 = np.broadcast_to(np.eye(d)[:, :2], (n, d, 2))
+    Wc = np.ascontiguousarray(np.asarray(W0, dtype=np.float64).transpose(0, 2, 1))
+    x = x0.copy()
+    states = np.zeros((n, sb), np.uint8)
+    code = np.zeros(n, np.int8)
+    hstep = np.zeros(n, np.int64)
+    R = np.zeros((n, len(grid), ncol))
+    fail = np.zeros(n, np.int64)
+    prov = _abi.cl_prov()
+    rc = Lb.cl_b200_indicator(C.byref(run), n, ns, x.ctypes.data, Wc.ctypes.data, states.ctypes.data,
+                              code.ctypes.data, hstep.ctypes.data, grid.ctypes.data, len(grid), R.ctypes.data,
+                              fail.ctypes.data, C.byref(prov))
+    if rc != 0:
+        msg = last_error()
+        if rc == _abi.EINVAL:
+            raise ValueError(msg)
+        raise DeviceError(rc, msg)
+    cols = tuple(c for m in members for c in MEMBER_COLUMNS[m]) + ("det_max", "symp_max", "M_max") + \
+        tuple(f"x{j + 1}" for j in range(ns))
+    return IndicatorRecord(R=R, columns=cols, grid=grid, fail=fail, x=x, W=Wc.transpose(0, 2, 1), states=states,
+                           code=code, hstep=hstep, gpu_ms=prov.gpu_ms)

@@ -327,6 +327,26 @@ CL_API int cl_b200_record_device(const cl_run* run, int64_t n, double* x, double
 CL_API int cl_b200_record(const cl_run* run, int64_t n, double* x, double* W, void* states, int8_t* code,
                           int64_t* hstep, const int64_t* grid, int32_t n_grid, double* R, int64_t* fail, cl_prov* prov);
 
+/* ---- The indicator recorder, tangent kind (src/Experiments/run_indicator_device.jl:13-60) ---------------------------
+ * One launch window of a chain of indicator members on a k = 2 frame (run.frames[0]: SALI, MEGNO, FLI in one of the
+ * compiled orders, every member but the last non-replacing, the last replacing) followed by the non-raising monitor.
+ * At every grid step inside the window one row of R[col, g, orbit] (column-major, Float64) of
+ * cl_b200_indicator_columns(run, ns) columns: the members' columns in chain order (SALI: sali, L; FLI: fli, fli1;
+ * MEGNO: Y, Ybar, Ybar20 of column 1, then of column 2; run_indicator_record.jl:40-56), then det_max, symp_max,
+ * M_max of the monitor, then x[0 .. ns-1]. fail[orbit] = the 1-based grid index whose segment holds the failure.
+ * states = the members' states (cl_b200_state_bytes layout) then MonState{Float64} (24 bytes):
+ * cl_b200_indicator_state_bytes(run) per orbit. Systems: StandardMap, WrappedStandardMap, 2 x 2 LinearSymplecticMap;
+ * Float64. Replaces `_ind_series_kernel!` launches. cl_b200_indicator_columns is -1 for a chain outside the menu. */
+CL_API int32_t cl_b200_indicator_columns(const cl_run* run, int32_t ns);
+CL_API int64_t cl_b200_indicator_state_bytes(const cl_run* run);
+CL_API int cl_b200_indicator_device(const cl_run* run, int64_t n, int32_t ns, double* x, double* W, void* states,
+                                    int8_t* code, int64_t* hstep, const int64_t* grid, int32_t n_grid, double* R,
+                                    int64_t* fail, void* stream);
+/* The same from run.n0 to run.N on host buffers, in windows of run.steps steps (synchronous). */
+CL_API int cl_b200_indicator(const cl_run* run, int64_t n, int32_t ns, double* x, double* W, void* states,
+                             int8_t* code, int64_t* hstep, const int64_t* grid, int32_t n_grid, double* R,
+                             int64_t* fail, cl_prov* prov);
+
 /* ---- The learned screen's kernels (no reference counterpart: the reference has no learned component) ---------------
  * All enqueue on `stream` and take device pointers. BF16 matrices are row-major with 16-byte aligned rows. */
 

@@ -53,6 +53,11 @@ def lib() -> C.CDLL:
         L.oracle_split_step.argtypes = [dp, C.c_double, C.c_int32, dp, dp, dp]
         L.oracle_record.argtypes = [P(_abi.cl_run), C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                     C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_int32, C.c_int32]
+        L.oracle_state_bytes.argtypes = [P(_abi.cl_run), C.c_int32]
+        L.oracle_state_bytes.restype = C.c_int64
+        L.oracle_indicator.argtypes = [P(_abi.cl_run), C.c_int64, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p,
+                                       C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p,
+                                       C.c_int32, C.c_int32]
         L.oracle_shadow.argtypes = [P(_abi.cl_run), C.c_int64, dp, C.c_void_p, C.c_void_p, C.c_double, C.c_int32,
                                     C.c_int32, C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p]
         L.oracle_max_threads.restype = C.c_int32
@@ -155,6 +160,40 @@ def oracle_record(sys, x0, N, tau, estimator, grid, *, W0=None, launch_steps=Non
                                  MATH[math], threads)
         if rc != 0:
             raise ValueError(f"oracle_record returned {rc}")
+        done += run.steps
+    return dict(R=R, fail=fail, x=x, W=W.transpose(0, 2, 1), states=states, code=code, hstep=hstep)
+
+
+def oracle_indicators(sys, x0, N, tau, members, grid, *, ns=2, W0=None, launch_steps=None, math="portable",
+                      threads=0):
+    """The indicator recorder (tangent kind) on the oracle: dict R (n, n_grid, cols + 3 + ns), fail, x, W (n, d, 2),
+    states (raw: the members' states then the monitor's three maxima), code, hstep."""
+    from chaos_b200.record import indicator_chain
+    x = np.ascontiguousarray(np.asarray(x0, dtype=np.float64)).copy()
+    n, s = x.shape
+    d = sys.d
+    chain = indicator_chain(members)
+    run = build_run(sys, N, tau, [FrameSpec(2, chain)], "fp64", 0)
+    cols = sum(6 if m == "MEGNO" else 2 for m in members)
+    ncol = cols + 3 + ns
+    sb = lib().oracle_state_bytes(C.byref(run), 0) + 24
+    if W0 is None:
+        W0 = np.broadcast_to(np.eye(d)[:, :2], (n, d, 2))
+    W = np.ascontiguousarray(np.asarray(W0, dtype=np.float64).transpose(0, 2, 1))
+    grid = np.ascontiguousarray(np.asarray(grid, dtype=np.int64))
+    states = np.zeros((n, sb), np.uint8)
+    code = np.zeros(n, np.int8)
+    hstep = np.zeros(n, np.int64)
+    R = np.zeros((n, len(grid), ncol))
+    fail = np.zeros(n, np.int64)
+    total, L, done = int(N), int(launch_steps) if launch_steps else int(N), 0
+    while done < total:
+        run.n0, run.steps = done, min(L, total - done)
+        rc = lib().oracle_indicator(C.byref(run), n, ns, x.ctypes.data, W.ctypes.data, states.ctypes.data,
+                                    code.ctypes.data, hstep.ctypes.data, grid.ctypes.data, len(grid), R.ctypes.data,
+                                    fail.ctypes.data, MATH[math], threads)
+        if rc != 0:
+            raise ValueError(f"oracle_indicator returned {rc}")
         done += run.steps
     return dict(R=R, fail=fail, x=x, W=W.transpose(0, 2, 1), states=states, code=code, hstep=hstep)
 

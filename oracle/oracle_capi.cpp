@@ -435,7 +435,7 @@ void rec_orbit(const cl_run& run, int64_t i, double* xs, double* Ws, uint8_t* st
         c = rec_body<MM>(run, x, W, est, mon, n, grid[g] - n);
         h = n;
         if (c != STATUS_OK) { fail[i] = g + 1; break; }
-        double lam[2], orth, gmax;
+        double lam[2] = {0.0, 0.0}, orth, gmax;
         int64_t sn;
         if (rd.kind == CL_RED_BENETTIN) {
             CS sum; std::memcpy(&sum, est, 16); std::memcpy(&sn, est + 16, 8);
@@ -466,6 +466,124 @@ void rec_orbit(const cl_run& run, int64_t i, double* xs, double* Ws, uint8_t* st
         if (c != STATUS_OK) fail[i] = ghi + 2;
     }
     std::memcpy(est + eb, mon, 24);
+    code[i] = c;
+    if (hstep) hstep[i] = h;
+}
+
+// ---- the indicator recorder, tangent kind (src/Experiments/run_indicator_device.jl:13-60) -----------------------
+// _orbit_body (orbit.jl:44-60) with the chain (members..., RunMonitor): every member steps on the W the one before
+// returned, then the monitor; a failure of any member stops the segment
+template <int MM>
+int8_t ind_body(const cl_run& run, double* x, double* W, uint8_t* st, double* mon, int64_t& n, int64_t steps) {
+    const cl_frame& fr = run.frames[0];
+    const int d = run.d, k = fr.k, s = run.s;
+    for (int64_t h = 0; h < steps / run.tau; ++h) {
+        for (int t = 0; t < run.tau; ++t) {
+            double M[4], Wn[4];
+            rec_map<MM>(run, x, M);
+            fused_product(M, W, Wn, d, d, k);
+            std::memcpy(W, Wn, sizeof(double) * d * k);
+        }
+        n += run.tau;
+        const int8_t c = status_of(x, s, W, d * k);
+        if (c != STATUS_OK) return c;
+        uint8_t* p = st;
+        for (int r = 0; r < fr.n_reducers; ++r) {
+            Reducers<MM>::step(fr.reducers[r], p, n, W, d, k);
+            p += state_bytes_of(fr.reducers[r], k);
+        }
+        rec_monitor<MM>(run, x, mon);
+        p = st;
+        bool failed = false;
+        for (int r = 0; r < fr.n_reducers; ++r) {
+            failed = failed || Reducers<MM>::failed(fr.reducers[r], p, k);
+            p += state_bytes_of(fr.reducers[r], k);
+        }
+        if (failed) return STATUS_REDUCER;
+    }
+    return n == run.N ? status_of(x, s, W, d * k) : STATUS_OK;
+}
+// megno_series (megno.jl:97-102): Y = 2 R1 / n, Ybar = Q / K, Ybar20 = (n / K) Q2 / n^3; zeros before the first handoff
+void ind_megno_series(const MegnoSumsJ& m, int64_t n, int64_t K, double* out) {
+    if (K == 0) { out[0] = out[1] = out[2] = 0.0; return; }
+    const double tn = static_cast<double>(n);
+    out[0] = 2 * (m.R1.s + m.R1.c) / tn;
+    out[1] = (m.Q.s + m.Q.c) / static_cast<double>(K);
+    out[2] = static_cast<double>(n / K) * (m.Q2.s + m.Q2.c) / (tn * tn * tn);
+}
+// _put! (run_indicator_record.jl:40-56) of one member from its state: SALI sali, L (sali.jl:62-66); FLI fli = fB,
+// fli1 = f1 (fli.jl:91-94); MEGNO Y, Ybar, Ybar20 of column 1 then of column 2. Returns the columns written.
+int ind_put(const cl_reducer& rd, const uint8_t* b, double* row) {
+    switch (rd.kind) {
+        case CL_RED_SALI: {
+            SALIStateJ st; std::memcpy(&st, b, sizeof st);
+            row[0] = st.sali;
+            row[1] = st.n == 0 ? 0.0 : -((st.s1.s + st.s2.s) + (st.s1.c + st.s2.c));
+            return 2;
+        }
+        case CL_RED_FLI: {
+            FLIStateJ st; std::memcpy(&st, b, sizeof st);
+            row[0] = st.fB;
+            row[1] = st.f1;
+            return 2;
+        }
+        case CL_RED_MEGNO: {
+            MEGNOStateJ st; std::memcpy(&st, b, sizeof st);
+            ind_megno_series(st.c1, st.n, st.K, row);
+            ind_megno_series(st.c2, st.n, st.K, row + 3);
+            return 6;
+        }
+    }
+    return 0;
+}
+int ind_cols(const cl_frame& fr) {
+    int c = 0;
+    for (int r = 0; r < fr.n_reducers; ++r) c += fr.reducers[r].kind == CL_RED_MEGNO ? 6 : 2;
+    return c;
+}
+// _ind_series_kernel! (run_indicator_device.jl:31-60) for one orbit over one launch window
+template <int MM>
+void ind_orbit(const cl_run& run, int64_t i, int ns, double* xs, double* Ws, uint8_t* sts, int8_t* code, int64_t* hstep,
+               const int64_t* grid, int n_grid, double* R, int64_t* fail, int64_t n0, int64_t steps) {
+    if (!(n0 == 0 || code[i] == STATUS_OK)) return;
+    const cl_frame& fr = run.frames[0];
+    const int d = run.d, k = fr.k, s = run.s, ncol = ind_cols(fr) + 3 + ns;
+    const int64_t cb = frame_state_bytes(fr), sb = cb + 24;
+    double* x = xs + i * s;
+    double* W = Ws + i * d * k;
+    uint8_t* st = sts + i * sb;
+    double mon[3];
+    if (n0 == 0) { std::memset(st, 0, sb); mon[0] = mon[1] = mon[2] = 0.0; }
+    else std::memcpy(mon, st + cb, 24);
+    int64_t n = n0, h = n0;
+    int8_t c = STATUS_OK;
+    int glo = 0;
+    while (glo < n_grid && grid[glo] <= n0) ++glo;
+    int ghi = glo - 1;
+    while (ghi + 1 < n_grid && grid[ghi + 1] <= n0 + steps) ++ghi;
+    double* Ri = R + i * static_cast<int64_t>(ncol) * n_grid;
+    for (int g = glo; g <= ghi; ++g) {
+        c = ind_body<MM>(run, x, W, st, mon, n, grid[g] - n);
+        h = n;
+        if (c != STATUS_OK) { fail[i] = g + 1; break; }
+        double* row = Ri + static_cast<int64_t>(g) * ncol;
+        const uint8_t* p = st;
+        int off = 0;
+        for (int r = 0; r < fr.n_reducers; ++r) {
+            off += ind_put(fr.reducers[r], p, row + off);
+            p += state_bytes_of(fr.reducers[r], k);
+        }
+        row[off] = mon[0];
+        row[off + 1] = mon[1];
+        row[off + 2] = mon[2];
+        for (int j = 0; j < ns; ++j) row[off + 3 + j] = x[j];
+    }
+    if (c == STATUS_OK && n < n0 + steps) {
+        c = ind_body<MM>(run, x, W, st, mon, n, n0 + steps - n);
+        h = n;
+        if (c != STATUS_OK) fail[i] = ghi + 2;
+    }
+    std::memcpy(st + cb, mon, 24);
     code[i] = c;
     if (hstep) hstep[i] = h;
 }
@@ -621,6 +739,39 @@ int oracle_record(const cl_run* run, int64_t n, double* x, double* W, void* stat
                 else
                     rec_orbit<MATH_PORTABLE>(*run, i, x, W, static_cast<uint8_t*>(states), code, hstep, grid, n_grid, R,
                                              fail, run->n0, steps);
+            }
+        }
+    };
+    std::vector<std::thread> pool;
+    for (int t = 1; t < nt; ++t) pool.emplace_back(worker);
+    worker();
+    for (auto& th : pool) th.join();
+    return 0;
+}
+
+// The indicator recorder on the CPU: one window [run.n0, run.n0 + steps) of n orbits, buffers in place (see the
+// C ABI's cl_b200_indicator_device); R has ncols(chain) + 3 + ns columns per row.
+int oracle_indicator(const cl_run* run, int64_t n, int32_t ns, double* x, double* W, void* states, int8_t* code,
+                     int64_t* hstep, const int64_t* grid, int32_t n_grid, double* R, int64_t* fail, int32_t math_mode,
+                     int32_t threads) {
+    const int64_t steps = run->steps > 0 ? run->steps : run->N - run->n0;
+    if (run->tau <= 0 || steps % run->tau != 0 || run->n0 + steps > run->N || run->n_frames != 1 ||
+        run->frames[0].k != 2 || ns < 0 || ns > run->s)
+        return CL_EINVAL;
+    const int hw = static_cast<int>(std::max(1u, std::thread::hardware_concurrency()));
+    const int nt = static_cast<int>(std::min<int64_t>(threads > 0 ? threads : hw, std::max<int64_t>(n, 1)));
+    std::atomic<int64_t> next{0};
+    auto worker = [&]() {
+        for (;;) {
+            const int64_t lo = next.fetch_add(16);
+            if (lo >= n) return;
+            for (int64_t i = lo; i < std::min<int64_t>(lo + 16, n); ++i) {
+                if (math_mode == MATH_LIBM)
+                    ind_orbit<MATH_LIBM>(*run, i, ns, x, W, static_cast<uint8_t*>(states), code, hstep, grid, n_grid,
+                                         R, fail, run->n0, steps);
+                else
+                    ind_orbit<MATH_PORTABLE>(*run, i, ns, x, W, static_cast<uint8_t*>(states), code, hstep, grid,
+                                             n_grid, R, fail, run->n0, steps);
             }
         }
     };
