@@ -34,6 +34,8 @@ Multi-GPU: orbits are independent, so N ranks run N shards of the same size with
   shadow    the two-trajectory estimator on the coupled-map workload's orbits (65536 x 1e5, tau = 10, d0 = 1e-8);
   record    the study recorder: the wrapped standard map K = 6, 4096 orbits x 1e5 steps, QRSpectrum(MGS), tau = 1,
             100 log-spaced grid rows;
+  advance   advance_ensemble(KahanLi(8), Henon-Heiles, tau = 0.05): 65536 starts on the E = 1/8 section x 2e4 steps,
+            states only;
   indicators the indicator recorder's tangent kind: the chain FLI, MEGNO, SALI with the monitor on the wrapped
             standard map K = 6, 4096 orbits x 1e5 steps, tau = 1, 100 log-spaced grid rows.
 """
@@ -174,7 +176,7 @@ def main() -> None:
     ap.add_argument("--only", choices=["fp64", "mixed"], default=None,
                     help="time one kernel of the default workload and print a short line (a small case for ncu)")
     ap.add_argument("--workload", default="coupled", choices=["coupled", "standard", "gauss", "lattice", "screen", "mlp", "split", "shadow",
-                                                             "record", "indicators"])
+                                                             "record", "indicators", "advance"])
     args = ap.parse_args()
     if args.workload != "coupled":
         run_workload(args)
@@ -896,10 +898,44 @@ def workload_indicators(args):
                              orbits=n, N=N, tau=tau, grid_rows=int(len(grid))), cpu)
 
 
+def workload_advance(args):
+    from chaos_b200 import HenonHeilesFlow, KahanLi, _abi
+    from chaos_b200.systems import IntegratorMap, random_energy_starts
+    import ctypes as C_
+    torch, dev, L = _setup()
+    n, N, tau = args.orbits or 65536, args.N if args.N != N_STEPS else 20_000, 0.05
+    m, flow = KahanLi(8), HenonHeilesFlow()
+    x0 = np.ascontiguousarray(random_energy_starts(0.125, n, SEED))
+    cs = IntegratorMap(m, flow, tau).to_cl()
+
+    def call():
+        out = np.empty_like(x0)
+        ok = np.zeros(n, np.uint8)
+        prov = _abi.cl_prov()
+        rc = L.cl_b200_advance_ensemble(C_.byref(cs), n, x0.ctypes.data, out.ctypes.data, ok.ctypes.data, N, 0,
+                                        C_.byref(prov))
+        if rc != 0:
+            raise RuntimeError(rc)
+        return prov.gpu_ms, x0.nbytes, out.nbytes + ok.nbytes
+
+    def cpu():
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle as O
+        threads = os.cpu_count() or 1
+        t = time.perf_counter()
+        O.oracle_advance(m, flow, x0[:4096], tau, 2000, threads=threads)
+        return dict(value=4096 * 2000 / (time.perf_counter() - t), unit="orbit-steps/s", cores=threads, kind="port",
+                    sample="4096 orbits x 2000 steps (oracle, all host threads)")
+    _host_call_workload(args, "orbit-steps/s (advance_ensemble, KahanLi(8) on the Henon-Heiles flow, states only)",
+                        "orbit-steps/s", n * N, call,
+                        dict(workload=f"advance-kahanli8-hh-{n}x{N:.0e}-dt0.05", orbits=n, N=N, tau=tau,
+                             stages=m.stages), cpu)
+
+
 def run_workload(args):
     {"standard": workload_standard, "gauss": workload_gauss, "lattice": workload_lattice,
      "screen": workload_screen, "mlp": workload_mlp, "split": workload_split, "shadow": workload_shadow,
-     "record": workload_record, "indicators": workload_indicators}[args.workload](args)
+     "record": workload_record, "indicators": workload_indicators, "advance": workload_advance}[args.workload](args)
 
 
 

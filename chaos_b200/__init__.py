@@ -9,6 +9,7 @@ from .foundation import FALLBACK_REASONS, DeviceError, NumericalHealthError
 from .propagate import FrameSpec, PropagationResult, build_run, bytes_per_orbit, chunk_size, probe, propagate, propagate_frames
 from .reducers import (CGS, FLI, GALI, MEGNO, MGS, RGS, SALI, AugmentedQR, Benettin, GivensQR, HouseholderQR,
                        QRSpectrum)
+from .advance import advance_ensemble
 from .record import record, record_indicators, record_shadow
 from .shadow import propagate_shadow
 from .systems import (FroeschleMap, Gauss, HenonHeilesFlow, IntegratorMap, KahanLi, Leapfrog, LinearSymplecticMap,
@@ -16,7 +17,7 @@ from .systems import (FroeschleMap, Gauss, HenonHeilesFlow, IntegratorMap, Kahan
                       random_energy_starts, section_interval, torus_state)
 
 __all__ = [
-    "propagate", "propagate_frames", "propagate_shadow", "record", "record_indicators", "record_shadow", "FrameSpec", "PropagationResult", "build_run", "bytes_per_orbit", "chunk_size",
+    "propagate", "propagate_frames", "propagate_shadow", "record", "record_indicators", "record_shadow", "advance_ensemble", "FrameSpec", "PropagationResult", "build_run", "bytes_per_orbit", "chunk_size",
     "probe", "NumericalHealthError", "DeviceError", "FALLBACK_REASONS",
     "QRSpectrum", "CGS", "MGS", "RGS", "HouseholderQR", "AugmentedQR", "GivensQR", "Benettin", "SALI", "GALI",
     "MEGNO", "FLI",

@@ -203,6 +203,12 @@ def declare(lib: C.CDLL) -> C.CDLL:
     lib.cl_b200_shadow_record.argtypes = [P(cl_run), C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_double,
                                           C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, P(cl_prov)]
     lib.cl_b200_shadow_record.restype = C.c_int
+    lib.cl_b200_advance_ensemble_device.argtypes = [P(cl_system), C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p,
+                                                    C.c_int64, C.c_void_p]
+    lib.cl_b200_advance_ensemble_device.restype = C.c_int
+    lib.cl_b200_advance_ensemble.argtypes = [P(cl_system), C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64,
+                                             C.c_int64, P(cl_prov)]
+    lib.cl_b200_advance_ensemble.restype = C.c_int
     lib.cl_b200_indicator_columns.argtypes = [P(cl_run), C.c_int32]
     lib.cl_b200_indicator_columns.restype = C.c_int32
     lib.cl_b200_indicator_state_bytes.argtypes = [P(cl_run)]
@@ -240,4 +246,5 @@ EXPORTS = ("cl_b200_propagate", "cl_b200_propagate_device", "cl_b200_check", "cl
            "cl_b200_shadow_bytes", "cl_b200_shadow_device", "cl_b200_shadow", "cl_b200_record_columns",
            "cl_b200_record_state_bytes", "cl_b200_record_device", "cl_b200_record",
            "cl_b200_shadow_record_device", "cl_b200_shadow_record", "cl_b200_indicator_columns",
-           "cl_b200_indicator_state_bytes", "cl_b200_indicator_device", "cl_b200_indicator")
+           "cl_b200_indicator_state_bytes", "cl_b200_indicator_device", "cl_b200_indicator",
+           "cl_b200_advance_ensemble_device", "cl_b200_advance_ensemble")

@@ -327,6 +327,18 @@ CL_API int cl_b200_record_device(const cl_run* run, int64_t n, double* x, double
 CL_API int cl_b200_record(const cl_run* run, int64_t n, double* x, double* W, void* states, int8_t* code,
                           int64_t* hstep, const int64_t* grid, int32_t n_grid, double* R, int64_t* fail, cl_prov* prov);
 
+/* ---- advance_ensemble (src/Integrators/ensemble.jl:13-45) ---------------------------------------------------------
+ * `steps` steps of size sys->dt of the integrator of an IntegratorMap system (CL_SYS_HH_SPLIT: a table method,
+ * advanced by advance_n with the pending kick carried across step boundaries, stepper.jl:27-48; CL_SYS_HH_GAUSS:
+ * Gauss(3), advance_checked per step, a failed step leaving the all-NaN state and ok = 0) on the Henon-Heiles flow,
+ * from every state of x0 (n x 4 doubles, orbit-major, 32-byte aligned on the device) into out, ok one byte per
+ * orbit. No tangent. Replaces `_ensemble_kernel!` launches; the result does not depend on the chunking. */
+CL_API int cl_b200_advance_ensemble_device(const cl_system* sys, int64_t n, const double* x0, double* out,
+                                           uint8_t* ok, int64_t steps, void* stream);
+/* The same on host buffers, `chunk` orbits per launch (<= 0: all), synchronous. */
+CL_API int cl_b200_advance_ensemble(const cl_system* sys, int64_t n, const double* x0, double* out, uint8_t* ok,
+                                    int64_t steps, int64_t chunk, cl_prov* prov);
+
 /* ---- The indicator recorder, tangent kind (src/Experiments/run_indicator_device.jl:13-60) ---------------------------
  * One launch window of a chain of indicator members on a k = 2 frame (run.frames[0]: SALI, MEGNO, FLI in one of the
  * compiled orders, every member but the last non-replacing, the last replacing) followed by the non-raising monitor.

@@ -53,6 +53,8 @@ def lib() -> C.CDLL:
         L.oracle_split_step.argtypes = [dp, C.c_double, C.c_int32, dp, dp, dp]
         L.oracle_record.argtypes = [P(_abi.cl_run), C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                     C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_int32, C.c_int32]
+        L.oracle_advance.argtypes = [P(_abi.cl_system), C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64,
+                                     C.c_int32]
         L.oracle_state_bytes.argtypes = [P(_abi.cl_run), C.c_int32]
         L.oracle_state_bytes.restype = C.c_int64
         L.oracle_indicator.argtypes = [P(_abi.cl_run), C.c_int64, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p,
@@ -162,6 +164,20 @@ def oracle_record(sys, x0, N, tau, estimator, grid, *, W0=None, launch_steps=Non
             raise ValueError(f"oracle_record returned {rc}")
         done += run.steps
     return dict(R=R, fail=fail, x=x, W=W.transpose(0, 2, 1), states=states, code=code, hstep=hstep)
+
+
+def oracle_advance(m, flow, x0, tau, n, threads=0):
+    """advance_ensemble on the oracle: (states (len, 4), ok (len,) bool) of `n` steps of size tau of IntegratorMap's
+    integrator `m` (a SplittingMethod or Gauss) on the Henon-Heiles flow."""
+    from chaos_b200.systems import IntegratorMap
+    x0 = np.ascontiguousarray(np.asarray(x0, dtype=np.float64).reshape(-1, 4))
+    out = np.empty_like(x0)
+    ok = np.zeros(len(x0), np.uint8)
+    cs = IntegratorMap(m, flow, tau).to_cl()
+    rc = lib().oracle_advance(C.byref(cs), len(x0), x0.ctypes.data, out.ctypes.data, ok.ctypes.data, int(n), threads)
+    if rc != 0:
+        raise ValueError(f"oracle_advance returned {rc}")
+    return out, ok.astype(bool)
 
 
 def oracle_indicators(sys, x0, N, tau, members, grid, *, ns=2, W0=None, launch_steps=None, math="portable",

@@ -11,6 +11,7 @@
 #include <thread>
 #include <cstdio>
 #include <cstring>
+#include <limits>
 #include <vector>
 
 #include "oracle.hpp"
@@ -773,6 +774,62 @@ int oracle_indicator(const cl_run* run, int64_t n, int32_t ns, double* x, double
                     ind_orbit<MATH_PORTABLE>(*run, i, ns, x, W, static_cast<uint8_t*>(states), code, hstep, grid,
                                              n_grid, R, fail, run->n0, steps);
             }
+        }
+    };
+    std::vector<std::thread> pool;
+    for (int t = 1; t < nt; ++t) pool.emplace_back(worker);
+    worker();
+    for (auto& th : pool) th.join();
+    return 0;
+}
+
+// advance_ensemble (src/Integrators/ensemble.jl:1-45) on the CPU: `steps` steps of size sys->dt from every state
+// of x0 (n x 4) into out, ok per orbit. A table method runs advance_n (stepper.jl:27-48: the kick weight held back
+// while no drift follows, across the step boundary too); Gauss(3) runs advance_checked per step and stops at a
+// failed step with the all-NaN state (gauss.jl:143-147, ensemble.jl:5-11).
+int oracle_advance(const cl_system* sys, int64_t n, const double* x0, double* out, uint8_t* ok, int64_t steps,
+                   int32_t threads) {
+    if (sys->kind != CL_SYS_HH_SPLIT && sys->kind != CL_SYS_HH_GAUSS) return CL_EUNSUPPORTED;
+    const int hw = static_cast<int>(std::max(1u, std::thread::hardware_concurrency()));
+    const int nt = static_cast<int>(std::min<int64_t>(threads > 0 ? threads : hw, std::max<int64_t>(n, 1)));
+    std::atomic<int64_t> next{0};
+    auto orbit = [&](int64_t i) {
+        double z[4];
+        std::memcpy(z, x0 + 4 * i, sizeof z);
+        uint8_t good = 1;
+        const double dt = sys->dt;
+        if (sys->kind == CL_SYS_HH_SPLIT) {
+            double pend = 0.0;
+            for (int64_t s = 0; s < steps; ++s)
+                for (int k = 0; k < sys->n_stages; ++k) {
+                    const double ck = sys->stage_c[k];
+                    if (ck != 0.0) {
+                        if (pend != 0.0) { hh_kick(z, pend * dt); pend = 0.0; }
+                        hh_drift(z, ck * dt);
+                    }
+                    pend = pend + sys->stage_d[k];
+                }
+            if (pend != 0.0) hh_kick(z, pend * dt);
+        } else {
+            const Gauss3 g(sys->gauss_maxiter, sys->gauss_tol);
+            for (int64_t s = 0; s < steps; ++s) {
+                double inc[4], Y[3][4];
+                if (!g.core(z, dt, inc, Y)) {
+                    for (double& v : z) v = std::numeric_limits<double>::quiet_NaN();
+                    good = 0;
+                    break;
+                }
+                for (int l = 0; l < 4; ++l) z[l] = z[l] + inc[l];
+            }
+        }
+        std::memcpy(out + 4 * i, z, sizeof z);
+        ok[i] = good;
+    };
+    auto worker = [&]() {
+        for (;;) {
+            const int64_t lo = next.fetch_add(16);
+            if (lo >= n) return;
+            for (int64_t i = lo; i < std::min<int64_t>(lo + 16, n); ++i) orbit(i);
         }
     };
     std::vector<std::thread> pool;
