@@ -7,20 +7,20 @@ reducers as parameter records, the argument checks, chunking, error and summary 
 """
 from .foundation import FALLBACK_REASONS, DeviceError, NumericalHealthError
 from .propagate import FrameSpec, PropagationResult, build_run, bytes_per_orbit, chunk_size, probe, propagate, propagate_frames
-from .reducers import (CGS, FLI, GALI, MEGNO, MGS, RGS, SALI, AugmentedQR, Benettin, GivensQR, HouseholderQR,
+from .reducers import (CGS, FLI, GALI, MEGNO, MGS, RGS, RLI, SALI, AugmentedQR, Benettin, GivensQR, HouseholderQR,
                        QRSpectrum)
 from .advance import advance_ensemble
-from .record import record, record_indicators, record_shadow
+from .record import pair_frame, pair_start, record, record_indicator_pairs, record_indicators, record_shadow
 from .shadow import propagate_shadow
 from .systems import (FroeschleMap, Gauss, HenonHeilesFlow, IntegratorMap, KahanLi, Leapfrog, LinearSymplecticMap,
                       SplittingMethod, StandardMap, StandardMapChain, WrappedStandardMap, energy_start, lift,
                       random_energy_starts, section_interval, torus_state)
 
 __all__ = [
-    "propagate", "propagate_frames", "propagate_shadow", "record", "record_indicators", "record_shadow", "advance_ensemble", "FrameSpec", "PropagationResult", "build_run", "bytes_per_orbit", "chunk_size",
+    "propagate", "propagate_frames", "propagate_shadow", "record", "record_indicators", "record_indicator_pairs", "pair_start", "pair_frame", "record_shadow", "advance_ensemble", "FrameSpec", "PropagationResult", "build_run", "bytes_per_orbit", "chunk_size",
     "probe", "NumericalHealthError", "DeviceError", "FALLBACK_REASONS",
     "QRSpectrum", "CGS", "MGS", "RGS", "HouseholderQR", "AugmentedQR", "GivensQR", "Benettin", "SALI", "GALI",
-    "MEGNO", "FLI",
+    "MEGNO", "FLI", "RLI",
     "StandardMap", "WrappedStandardMap", "FroeschleMap", "StandardMapChain", "LinearSymplecticMap", "IntegratorMap",
     "Gauss", "SplittingMethod", "KahanLi", "Leapfrog", "HenonHeilesFlow", "torus_state", "lift", "energy_start", "random_energy_starts", "section_interval",
 ]

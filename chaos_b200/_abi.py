@@ -18,7 +18,7 @@ NOALLOC_MAX_CLASSES = 64
 # enum cl_system_kind
 SYS_STANDARD, SYS_WRAPPED_STANDARD, SYS_FROESCHLE, SYS_CHAIN, SYS_LINEAR, SYS_HH_GAUSS, SYS_HH_SPLIT = 1, 2, 3, 4, 5, 6, 7
 # enum cl_reducer_kind
-RED_QR, RED_BENETTIN, RED_SALI, RED_GALI, RED_MEGNO, RED_FLI = 1, 2, 3, 4, 5, 6
+RED_QR, RED_BENETTIN, RED_SALI, RED_GALI, RED_MEGNO, RED_FLI, RED_RLI = 1, 2, 3, 4, 5, 6, 7
 # enum cl_qr_alg
 QR_CGS, QR_MGS, QR_RGS, QR_HOUSEHOLDER, QR_AUGMENTED, QR_GIVENS = 1, 2, 3, 4, 5, 6
 # enum cl_precision
@@ -143,7 +143,7 @@ class cl_ensemble_class(C.Structure):
 def state_bytes(kind: int, k: int) -> int:
     """Bytes of one reducer state in the Julia isbits layout (T = Float64)."""
     return {RED_QR: 16 * k + 72, RED_BENETTIN: 48, RED_SALI: 72, RED_GALI: 24 * k + 32,
-            RED_MEGNO: 200, RED_FLI: 96}[kind]
+            RED_MEGNO: 200, RED_FLI: 96, RED_RLI: 88}[kind]
 
 
 def frame_state_bytes(frame: cl_frame) -> int:
@@ -221,6 +221,12 @@ def declare(lib: C.CDLL) -> C.CDLL:
                                       C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p,
                                       P(cl_prov)]
     lib.cl_b200_indicator.restype = C.c_int
+    lib.cl_b200_indicator_pair_columns.argtypes = [P(cl_run), C.c_int32]
+    lib.cl_b200_indicator_pair_columns.restype = C.c_int32
+    lib.cl_b200_indicator_pair_device.argtypes = lib.cl_b200_indicator_device.argtypes
+    lib.cl_b200_indicator_pair_device.restype = C.c_int
+    lib.cl_b200_indicator_pair.argtypes = lib.cl_b200_indicator.argtypes
+    lib.cl_b200_indicator_pair.restype = C.c_int
     lib.cl_b200_ensemble_tune.restype = C.c_int
     lib.cl_b200_ensemble_graph_create.argtypes = [P(cl_ensemble_class), C.c_int32, P(C.c_void_p)]
     lib.cl_b200_ensemble_graph_create.restype = C.c_int
@@ -247,4 +253,5 @@ EXPORTS = ("cl_b200_propagate", "cl_b200_propagate_device", "cl_b200_check", "cl
            "cl_b200_record_state_bytes", "cl_b200_record_device", "cl_b200_record",
            "cl_b200_shadow_record_device", "cl_b200_shadow_record", "cl_b200_indicator_columns",
            "cl_b200_indicator_state_bytes", "cl_b200_indicator_device", "cl_b200_indicator",
-           "cl_b200_advance_ensemble_device", "cl_b200_advance_ensemble")
+           "cl_b200_advance_ensemble_device", "cl_b200_advance_ensemble", "cl_b200_indicator_pair_columns",
+           "cl_b200_indicator_pair_device", "cl_b200_indicator_pair")

@@ -50,6 +50,7 @@ const char* red_token(const cl_reducer& r, char* buf) {
         case CL_RED_GALI: return "GALI";
         case CL_RED_MEGNO: std::snprintf(buf, 16, "MEGNO%d", r.replace ? 1 : 0); return buf;
         case CL_RED_FLI: std::snprintf(buf, 16, "FLI%d", r.replace ? 1 : 0); return buf;
+        case CL_RED_RLI: std::snprintf(buf, 16, "RLI%d", r.replace ? 1 : 0); return buf;
     }
     return "?";
 }
@@ -75,6 +76,7 @@ int64_t state_bytes_of(const cl_reducer& r, int k) {
         case CL_RED_GALI: return 24 * k + 32;
         case CL_RED_MEGNO: return 200;
         case CL_RED_FLI: return 96;
+        case CL_RED_RLI: return 88;
     }
     return 0;
 }
@@ -149,6 +151,9 @@ int validate(const cl_run& r) {
                     break;
                 case CL_RED_FLI:
                     if (fr.k != 2) return fail(CL_EINVAL, "FLI needs k = 2");
+                    break;
+                case CL_RED_RLI:   // reducer_init (rli.jl:45-49); the pair stream doubles d, so it is even
+                    if (fr.k != 2) return fail(CL_EINVAL, "RLI needs k = 2");
                     break;
                 default: return fail(CL_EINVAL, "unknown reducer kind");
             }

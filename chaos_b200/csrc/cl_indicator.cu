@@ -5,6 +5,8 @@
 //   the members' columns (E24: SALI sali, L; FLI fli, fli1; MEGNO Y_1, Ybar_1, Ybar20_1, Y_2, Ybar_2, Ybar20_2),
 //   det_max, symp_max, M_max of the monitor, then the first ns coordinates of the orbit point.
 // A failure stores the 1-based grid index whose segment holds it and stops the orbit; everything is carried in place.
+// The pair kind runs the same body on PairMap(sys) (src/Systems/pair.jl:9-68) with the members RLI and MEGNO on the
+// block frame, the monitor reading orbit A (run_indicator_record.jl:6-10).
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -108,6 +110,51 @@ template <bool REP> struct Put<RMEGNO<REP>> {
     }
 };
 
+template <bool REP> struct Put<RRLI<REP>> {
+    static constexpr int cols = 2;
+    // reducer_final (rli.jl:98-101): DL at the last handoff and RLI = Q / K, zeros before the first handoff
+    static __device__ __forceinline__ void put(const RLIState& st, double* row) {
+        row[0] = st.K == 0 ? 0.0 : fabs((st.sB.s - st.sA.s) + (st.sB.c - st.sA.c)) / static_cast<double>(st.n);
+        row[1] = st.K == 0 ? 0.0 : cs_total(st.Q) / static_cast<double>(st.K);
+    }
+};
+
+// PairMap(sys) (pair.jl:9-68): the state (A; B), each half advanced by the base map alone; the tangent acts block by
+// block (PairTangent * W, pair.jl:37-41), the rows of each block multiplied by the base's own product, the zero
+// blocks never touched.
+template <class Base>
+struct SysPair {
+    static constexpr int Db = Base::D, Sb = Base::S, D = 2 * Db, S = 2 * Sb;
+    struct Jac { typename Base::Jac A, B; };
+    Base base;
+    __device__ __forceinline__ void jac(const double* x, Jac& J) const {
+        base.jac(x, J.A);
+        base.jac(x + Sb, J.B);
+    }
+    template <int KK>
+    __device__ __forceinline__ void apply(const Jac& J, double* W) const {
+        double Wa[Db * KK], Wb[Db * KK];
+#pragma unroll
+        for (int j = 0; j < KK; ++j)
+#pragma unroll
+            for (int l = 0; l < Db; ++l) { Wa[l + Db * j] = W[l + D * j]; Wb[l + Db * j] = W[Db + l + D * j]; }
+        base.template apply<KK>(J.A, Wa);
+        base.template apply<KK>(J.B, Wb);
+#pragma unroll
+        for (int j = 0; j < KK; ++j)
+#pragma unroll
+            for (int l = 0; l < Db; ++l) { W[l + D * j] = Wa[l + Db * j]; W[Db + l + D * j] = Wb[l + Db * j]; }
+    }
+    __device__ __forceinline__ void forward(double* x, const Jac& J) const {
+        base.forward(x, J.A);
+        base.forward(x + Sb, J.B);
+    }
+};
+
+// The map whose tangent the monitor reads at the orbit point: the system itself, or the base map at orbit A.
+template <class Sys> __device__ __forceinline__ const Sys& monitored(const Sys& s) { return s; }
+template <class Base> __device__ __forceinline__ const Base& monitored(const SysPair<Base>& s) { return s.base; }
+
 // _put_members! over the compile-time chain
 template <int D, int K>
 __device__ __forceinline__ int put_members(const Chain<D, K>&, double*) { return 0; }
@@ -138,7 +185,7 @@ struct IndOrbit {
             const int8_t cc = all_finite_x<D, S>(x) ? (all_finite<D * K>(W) ? STATUS_OK : STATUS_W) : STATUS_STATE;
             if (cc != STATUS_OK) return cc;
             ch.step(n, W, a.prm);
-            monitor_step(sys, x, mon);
+            monitor_step(monitored(sys), x, mon);
             if (ch.failed()) return STATUS_REDUCER;
         }
         return n == a.N ? (all_finite_x<D, S>(x) ? (all_finite<D * K>(W) ? STATUS_OK : STATUS_W) : STATUS_STATE)
@@ -208,9 +255,20 @@ __global__ void __launch_bounds__(128) ind_series_kernel(const IndArgs a, const 
 
 typedef cudaError_t (*IndFn)(const cl_run& run, const IndArgs& a, cudaStream_t st);
 
+template <class Sys> struct IndMaker {
+    static Sys make(const cl_run& run) { return SysMaker<Sys>::make(run, nullptr); }
+};
+template <class Base> struct IndMaker<SysPair<Base>> {
+    static SysPair<Base> make(const cl_run& run) {
+        SysPair<Base> s;
+        s.base = SysMaker<Base>::make(run, nullptr);
+        return s;
+    }
+};
+
 template <class Sys, class F>
 cudaError_t launch_ind(const cl_run& run, const IndArgs& a, cudaStream_t st) {
-    const Sys sys = SysMaker<Sys>::make(run, nullptr);
+    const Sys sys = IndMaker<Sys>::make(run);
     ind_series_kernel<Sys, F><<<static_cast<unsigned>((a.n + 127) / 128), 128, 0, st>>>(a, sys);
     return cudaGetLastError();
 }
@@ -239,15 +297,33 @@ const IndEntry kChains[] = {
     entry<Frame<2, RSALI, RFLI<true>>, 4>("SALI,FLI1"),
 };
 
+template <class F, int COLS>
+constexpr IndEntry pair_entry(const char* chain) {
+    return IndEntry{chain, launch_ind<SysPair<SysStandard>, F>, launch_ind<SysPair<SysWrapped>, F>,
+                    launch_ind<SysPair<SysLinear<2>>, F>, COLS};
+}
+
+// The pair chains of the reference's recorder specs (test/experiments/ex_d86_chains.jl:5).
+const IndEntry kPairChains[] = {
+    pair_entry<Frame<2, RRLI<true>>, 2>("RLI1"),
+    pair_entry<Frame<2, RRLI<false>, RMEGNO<true>>, 8>("RLI0,MEGNO1"),
+    pair_entry<Frame<2, RMEGNO<false>, RRLI<true>>, 8>("MEGNO0,RLI1"),
+};
+
 // "k2:MEGNO0,SALI|" of the run's key -> the member chain
-const IndEntry* find_chain(const cl_run& r) {
+const IndEntry* find_chain(const cl_run& r, bool pair) {
     const std::string key = run_key(r);
     const size_t a = key.find("|k2:");
     if (a == std::string::npos) return nullptr;
     const size_t b = key.find('|', a + 1);
     const std::string chain = key.substr(a + 4, b - a - 4);
-    for (const IndEntry& e : kChains)
-        if (chain == e.chain) return &e;
+    if (pair) {
+        for (const IndEntry& e : kPairChains)
+            if (chain == e.chain) return &e;
+    } else {
+        for (const IndEntry& e : kChains)
+            if (chain == e.chain) return &e;
+    }
     return nullptr;
 }
 
@@ -260,7 +336,13 @@ extern "C" {
 
 int32_t cl_b200_indicator_columns(const cl_run* run, int32_t ns) {
     if (!run) return -1;
-    const IndEntry* e = find_chain(*run);
+    const IndEntry* e = find_chain(*run, false);
+    return e ? e->cols + 3 + ns : -1;
+}
+
+int32_t cl_b200_indicator_pair_columns(const cl_run* run, int32_t ns) {
+    if (!run) return -1;
+    const IndEntry* e = find_chain(*run, true);
     return e ? e->cols + 3 + ns : -1;
 }
 
@@ -269,15 +351,18 @@ int64_t cl_b200_indicator_state_bytes(const cl_run* run) {
     return capi_frame_bytes(run->frames[0]) + static_cast<int64_t>(sizeof(MonState));
 }
 
-int cl_b200_indicator_device(const cl_run* run, int64_t n, int32_t ns, double* x, double* W, void* states,
-                             int8_t* code, int64_t* hstep, const int64_t* grid, int32_t n_grid, double* R,
-                             int64_t* fail, void* stream) {
+}  // extern "C"
+
+namespace {
+int indicator_device(const cl_run* run, bool pair, int64_t n, int32_t ns, double* x, double* W, void* states,
+                     int8_t* code, int64_t* hstep, const int64_t* grid, int32_t n_grid, double* R, int64_t* fail,
+                     void* stream) {
     if (!run || n <= 0 || !x || !W || !states || !code || !grid || n_grid < 1 || !R || !fail || ns < 0)
         return capi_fail(CL_EINVAL, "bad arguments");
     const int v = capi_validate(*run);
     if (v) return v;
-    if (ns > run->s) return capi_fail(CL_EINVAL, "ns exceeds the state length");
-    const IndEntry* e = find_chain(*run);
+    if (ns > (pair ? 2 : 1) * run->s) return capi_fail(CL_EINVAL, "ns exceeds the state length");
+    const IndEntry* e = find_chain(*run, pair);
     if (!e || run->n_frames != 1 || run->frames[0].k != 2 || run->precision != CL_PREC_FP64)
         return capi_fail(CL_EUNSUPPORTED, "indicator chain outside the compiled menu");
     IndFn fn = run->sys.kind == CL_SYS_STANDARD ? e->std : run->sys.kind == CL_SYS_WRAPPED_STANDARD ? e->wrapped
@@ -295,15 +380,18 @@ int cl_b200_indicator_device(const cl_run* run, int64_t n, int32_t ns, double* x
     return err == cudaSuccess ? 0 : capi_map_cuda(err, "indicator launch");
 }
 
-int cl_b200_indicator(const cl_run* run, int64_t n, int32_t ns, double* x, double* W, void* states, int8_t* code,
-                      int64_t* hstep, const int64_t* grid, int32_t n_grid, double* R, int64_t* fail, cl_prov* prov) {
+int indicator_host(const cl_run* run, bool pair, int64_t n, int32_t ns, double* x, double* W, void* states,
+                   int8_t* code, int64_t* hstep, const int64_t* grid, int32_t n_grid, double* R, int64_t* fail,
+                   cl_prov* prov) {
     if (!run || n <= 0 || !x || !W || !states || !code || !grid || n_grid < 1 || !R || !fail || ns < 0)
         return capi_fail(CL_EINVAL, "bad arguments");
     int rc = capi_validate(*run);
     if (rc) return rc;
-    const int ncol = cl_b200_indicator_columns(run, ns);
-    if (ncol < 0 || ns > run->s) return cl_b200_indicator_device(run, n, ns, x, W, states, code, hstep, grid, n_grid, R, fail, nullptr);
-    const int s = run->s, dk = run->d * run->frames[0].k;
+    const int ncol = pair ? cl_b200_indicator_pair_columns(run, ns) : cl_b200_indicator_columns(run, ns);
+    const int mult = pair ? 2 : 1;
+    if (ncol < 0 || ns > mult * run->s)
+        return indicator_device(run, pair, n, ns, x, W, states, code, hstep, grid, n_grid, R, fail, nullptr);
+    const int s = mult * run->s, dk = mult * run->d * run->frames[0].k;
     const size_t xb = sizeof(double) * s * n, wb = sizeof(double) * dk * n, sb = cl_b200_indicator_state_bytes(run) * n;
     const size_t gb = sizeof(int64_t) * n_grid, rb = sizeof(double) * ncol * n_grid * n, fb = sizeof(int64_t) * n;
     void *dx = nullptr, *dw = nullptr, *ds = nullptr, *dc = nullptr, *dh = nullptr, *dg = nullptr, *dr = nullptr, *df = nullptr;
@@ -335,10 +423,9 @@ int cl_b200_indicator(const cl_run* run, int64_t n, int32_t ns, double* x, doubl
         for (int64_t n0 = run->n0; n0 < run->N && rc == 0; n0 += L) {
             r.n0 = n0;
             r.steps = std::min<int64_t>(L, run->N - n0);
-            rc = cl_b200_indicator_device(&r, n, ns, static_cast<double*>(dx), static_cast<double*>(dw), ds,
-                                          static_cast<int8_t*>(dc), static_cast<int64_t*>(dh),
-                                          static_cast<int64_t*>(dg), n_grid, static_cast<double*>(dr),
-                                          static_cast<int64_t*>(df), st);
+            rc = indicator_device(&r, pair, n, ns, static_cast<double*>(dx), static_cast<double*>(dw), ds,
+                                  static_cast<int8_t*>(dc), static_cast<int64_t*>(dh), static_cast<int64_t*>(dg),
+                                  n_grid, static_cast<double*>(dr), static_cast<int64_t*>(df), st);
             ++launches;
         }
         cudaEventRecord(e1, st);
@@ -361,13 +448,40 @@ int cl_b200_indicator(const cl_run* run, int64_t n, int32_t ns, double* x, doubl
         prov->gpu_ms = ms;
         prov->launches = launches;
         prov->launch_steps = run->steps > 0 ? run->steps : run->N - run->n0;
-        std::snprintf(prov->variant, sizeof prov->variant, "indicator %d cols s%d", ncol, s);
+        std::snprintf(prov->variant, sizeof prov->variant, "indicator%s %d cols s%d", pair ? " pair" : "", ncol, s);
     }
     if (e0) cudaEventDestroy(e0);
     if (e1) cudaEventDestroy(e1);
     for (void* p : {dx, dw, ds, dc, dh, dg, dr, df}) cudaFree(p);
     if (st) cudaStreamDestroy(st);
     return rc;
+}
+
+}  // namespace
+
+extern "C" {
+
+int cl_b200_indicator_device(const cl_run* run, int64_t n, int32_t ns, double* x, double* W, void* states,
+                             int8_t* code, int64_t* hstep, const int64_t* grid, int32_t n_grid, double* R,
+                             int64_t* fail, void* stream) {
+    return indicator_device(run, false, n, ns, x, W, states, code, hstep, grid, n_grid, R, fail, stream);
+}
+
+int cl_b200_indicator(const cl_run* run, int64_t n, int32_t ns, double* x, double* W, void* states, int8_t* code,
+                      int64_t* hstep, const int64_t* grid, int32_t n_grid, double* R, int64_t* fail, cl_prov* prov) {
+    return indicator_host(run, false, n, ns, x, W, states, code, hstep, grid, n_grid, R, fail, prov);
+}
+
+int cl_b200_indicator_pair_device(const cl_run* run, int64_t n, int32_t ns, double* z, double* W, void* states,
+                                  int8_t* code, int64_t* hstep, const int64_t* grid, int32_t n_grid, double* R,
+                                  int64_t* fail, void* stream) {
+    return indicator_device(run, true, n, ns, z, W, states, code, hstep, grid, n_grid, R, fail, stream);
+}
+
+int cl_b200_indicator_pair(const cl_run* run, int64_t n, int32_t ns, double* z, double* W, void* states,
+                           int8_t* code, int64_t* hstep, const int64_t* grid, int32_t n_grid, double* R,
+                           int64_t* fail, cl_prov* prov) {
+    return indicator_host(run, true, n, ns, z, W, states, code, hstep, grid, n_grid, R, fail, prov);
 }
 
 }  // extern "C"

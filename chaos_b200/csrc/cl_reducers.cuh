@@ -1,5 +1,5 @@
 // cl_reducers.cuh -- the reducers fused into the orbit kernel: QRSpectrum (all six orthonormalisers), Benettin,
-// SALI, GALI, MEGNO and FLI. Each is a tag type with
+// SALI, GALI, MEGNO and FLI, and RLI for the pair streams of the indicator recorder. Each is a tag type with
 //   State<D, K>                the isbits layout of the reference's state struct with T = Float64
 //   step(st, n, W, prm)        `reducer_step` (src/Tangent/Tangent.jl:44-49): never throws, records failures
 //   failed(st)                 `reducer_failed`
@@ -273,6 +273,45 @@ struct RFLI {
         if (S1 > st.fB) { st.fB = S1; st.stepB = n; st.colB = 1; }
         if (S2 > st.fB) { st.fB = S2; st.stepB = n; st.colB = 2; }
         st.n = n;
+        if (REPLACE) {
+#pragma unroll
+            for (int i = 0; i < D; ++i) { W[i] = dv(W[i], a1); W[D + i] = dv(W[D + i], a2); }
+        }
+    }
+    template <int D, int K>
+    static __device__ __forceinline__ bool failed(const State<D, K>& st) { return st.code != 0; }
+};
+
+// ---- RLI (src/Indicators/rli.jl:24-114) -------------------------------------------------------------------------
+// On a pair stream (PairMap, d = 2h): the two arriving columns, (xi; 0) of orbit A and (0; xi) of orbit B, Benettin's
+// log sums per column, DL = |S_B - S_A| / n with the correction terms split out, and the compensated sum Q of the DL
+// series; the off-block entries must stay exactly 0 (code 2, "pairing").
+struct RLIState { CS sA, sB, Q; double value; i64 n, K, step; int8_t code, column; };
+static_assert(sizeof(RLIState) == 88, "RLIState layout");
+
+template <bool REPLACE>
+struct RRLI {
+    static constexpr int kind = CL_RED_RLI;
+    template <int D, int K> using State = RLIState;
+    template <int D, int K, typename T>
+    static __device__ __forceinline__ void step(State<D, K>& st, i64 n, T* W, const RedParams&) {
+        if (st.code != 0) return;
+        const T a1 = nrm<D>(W), a2 = nrm<D>(W + D);
+        if (!pair_norms(st, n, a1, a2)) return;
+        constexpr int h = D / 2;
+        T m1 = T(0), m2 = T(0);   // _offblock, rli.jl:58-65
+#pragma unroll
+        for (int i = 0; i < h; ++i) { m1 = jl_max(m1, fabs(W[h + i])); m2 = jl_max(m2, fabs(W[D + i])); }
+        if (!(m1 == T(0) && m2 == T(0))) {
+            const bool first_clean = m1 == T(0);
+            st.column = first_clean ? 2 : 1; st.value = static_cast<double>(first_clean ? m2 : m1); st.step = n; st.code = 2;
+            return;
+        }
+        cs_add(st.sA, lnr(a1));
+        cs_add(st.sB, lnr(a2));
+        cs_add(st.Q, fabs((st.sB.s - st.sA.s) + (st.sB.c - st.sA.c)) / static_cast<double>(n));   // rli_dl, rli.jl:53
+        st.n = n;
+        st.K = st.K + 1;
         if (REPLACE) {
 #pragma unroll
             for (int i = 0; i < D; ++i) { W[i] = dv(W[i], a1); W[D + i] = dv(W[D + i], a2); }

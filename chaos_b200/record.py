@@ -210,3 +210,123 @@ def record_indicators(sys, x0, N: int, tau: int, members, grid, *, ns: int = 2, 
         tuple(f"x{j + 1}" for j in range(ns))
     return IndicatorRecord(R=R, columns=cols, grid=grid, fail=fail, x=x, W=Wc.transpose(0, 2, 1), states=states,
                            code=code, hstep=hstep, gpu_ms=prov.gpu_ms)
+
+
+# ---- the pair kind ------------------------------------------------------------------------------------------------
+PAIR_MEMBER_COLUMNS = {"RLI": ("RLI.DL", "RLI.RLI"), "MEGNO": MEMBER_COLUMNS["MEGNO"]}
+
+
+def pair_chain(members) -> tuple:
+    """The reducers of a pair chain (RLI, MEGNO; run_indicator_chain.jl:26-28): the last member replacing."""
+    from .reducers import RLI
+    members = [str(m) for m in members]
+    if not members or any(m not in PAIR_MEMBER_COLUMNS for m in members):
+        raise ValueError(f"pair members must be a non-empty list of RLI, MEGNO, got {members}")
+    return tuple(RLI(replace=i == len(members) - 1) if m == "RLI" else MEGNO(replace=i == len(members) - 1)
+                 for i, m in enumerate(members))
+
+
+def _wrap_diff(u: float, tp: float) -> float:
+    """_wrap_diff (rli.jl:135): u - tp round(u / tp), round half to even as Julia's `round`."""
+    return u - tp * float(round(u / tp))
+
+
+def pair_distance(sys, z) -> float:
+    """pair_distance (rli.jl:150): safe_norm of the minimal-image separation of the halves of a pair state for the
+    standard maps (each coordinate difference reduced modulo 2 pi), the plain difference otherwise."""
+    from .shadow import _PI, _safe_norm
+    from .systems import StandardMap, WrappedStandardMap
+    z = [float(v) for v in z]
+    h = len(z) // 2
+    if isinstance(sys, (StandardMap, WrappedStandardMap)):
+        tp = 2 * _PI
+        return _safe_norm([_wrap_diff(z[h] - z[0], tp), _wrap_diff(z[h + 1] - z[1], tp)])
+    return _safe_norm([z[h + i] - z[i] for i in range(h)])
+
+
+def pair_start(sys, x0, u, Dx: float, *, orbit: int = 0):
+    """pair_start (rli.jl:182-193): (z, Dx, Dx_r, mode) with z = (A; B), A = x0 (torus_state(x0) for the wrapped map)
+    and B = A + Dx u (reduced with A's counts in wrapped mode); a Dx that is not finite and positive, or a realised
+    separation that is zero, not finite or outside [Dx / 2, 2 Dx], raises NumericalHealthError("separation") at
+    step 0 for `orbit`."""
+    import math
+    from .foundation import NumericalHealthError
+    from .shadow import _displaced
+    from .systems import WrappedStandardMap, torus_state
+    dx = float(Dx)
+    if not (math.isfinite(dx) and dx > 0):
+        raise NumericalHealthError("separation", dx, 0.0 if math.isfinite(dx) else math.inf, 0, orbit, "cpu")
+    zA = np.asarray(torus_state(x0) if isinstance(sys, WrappedStandardMap) else x0, dtype=np.float64)
+    zB = np.asarray(_displaced(sys, zA, [dx * float(v) for v in u]), dtype=np.float64)
+    z = np.concatenate([zA, zB])
+    dr = pair_distance(sys, z)
+    if not (math.isfinite(dr) and dr > 0):
+        raise NumericalHealthError("separation", dr, 0.0 if math.isfinite(dr) else math.inf, 0, orbit, "cpu")
+    if not (dr >= dx / 2 and dr <= 2 * dx):
+        raise NumericalHealthError("separation", dr, dx, 0, orbit, "cpu")
+    return z, dx, dr, "wrapped" if isinstance(sys, WrappedStandardMap) else "lifted"
+
+
+def pair_frame(xi) -> np.ndarray:
+    """The block frame of a pair, (xi; 0) and (0; xi) (run_indicator_record.jl:230-231), as a (2 d, 2) array."""
+    xi = np.asarray(xi, dtype=np.float64)
+    d = len(xi)
+    W = np.zeros((2 * d, 2))
+    W[:d, 0] = xi
+    W[d:, 1] = xi
+    return W
+
+
+def record_indicator_pairs(sys, z0, W0, N: int, tau: int, members, grid, *, ns: int = 2,
+                           launch_steps: int | None = None) -> IndicatorRecord:
+    """The indicator recorder's pair kind: the chain of `members` (RLI, MEGNO) and the monitor on PairMap(sys) from
+    the pair states z0 (n, 2 s; `pair_start`) and block frames W0 (n, 2 d, 2; `pair_frame`), rows at the step
+    counts `grid` as `record_indicators` writes them (RLI's columns DL, RLI; the monitor reads orbit A; the first
+    `ns` coordinates of the pair state)."""
+    from .systems import LinearSymplecticMap, StandardMap, WrappedStandardMap
+    if not isinstance(sys, (StandardMap, WrappedStandardMap, LinearSymplecticMap)):
+        raise TypeError("the pair kind covers the standard maps and 2 x 2 linear maps")
+    z0 = np.ascontiguousarray(np.asarray(z0, dtype=np.float64))
+    n, s2 = z0.shape
+    if s2 != 2 * sys.s:
+        raise ValueError(f"a pair state has {2 * sys.s} entries, got {s2}")
+    d = sys.d
+    W0 = np.asarray(W0, dtype=np.float64)
+    if W0.shape != (n, 2 * d, 2):
+        raise ValueError(f"W0 must be (orbits, {2 * d}, 2)")
+    chain = pair_chain(members)
+    grid = np.ascontiguousarray(np.asarray(grid, dtype=np.int64))
+    if grid.ndim != 1 or len(grid) < 1 or np.any(np.diff(grid) <= 0) or grid[0] < tau or grid[-1] > N or \
+            np.any(grid % tau):
+        raise ValueError("grid: increasing multiples of tau in tau..N")
+    if not 0 <= ns <= s2:
+        raise ValueError(f"ns must lie in 0..{s2}")
+    L = int(launch_steps) if launch_steps else int(N)
+    if L % tau:
+        raise ValueError("launch_steps must be a multiple of tau")
+    run = build_run(sys, N, tau, [FrameSpec(2, chain)], "fp64", 0, steps=L)
+    Lb = lib()
+    ncol = Lb.cl_b200_indicator_pair_columns(C.byref(run), ns)
+    if ncol < 0:
+        raise ValueError(f"pair chain {members} is outside the compiled menu")
+    sb = Lb.cl_b200_indicator_state_bytes(C.byref(run))
+    Wc = np.ascontiguousarray(W0.transpose(0, 2, 1))
+    x = z0.copy()
+    states = np.zeros((n, sb), np.uint8)
+    code = np.zeros(n, np.int8)
+    hstep = np.zeros(n, np.int64)
+    R = np.zeros((n, len(grid), ncol))
+    fail = np.zeros(n, np.int64)
+    prov = _abi.cl_prov()
+    rc = Lb.cl_b200_indicator_pair(C.byref(run), n, ns, x.ctypes.data, Wc.ctypes.data, states.ctypes.data,
+                                   code.ctypes.data, hstep.ctypes.data, grid.ctypes.data, len(grid), R.ctypes.data,
+                                   fail.ctypes.data, C.byref(prov))
+    if rc != 0:
+        msg = last_error()
+        if rc == _abi.EINVAL:
+            raise ValueError(msg)
+        raise DeviceError(rc, msg)
+    cols = tuple(c for m in members for c in PAIR_MEMBER_COLUMNS[m]) + ("det_max", "symp_max", "M_max") + \
+        tuple(f"z{j + 1}" for j in range(ns))
+    return IndicatorRecord(R=R, columns=cols, grid=grid, fail=fail, x=x, W=Wc.transpose(0, 2, 1), states=states,
+                           code=code, hstep=hstep, gpu_ms=prov.gpu_ms)

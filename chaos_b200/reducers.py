@@ -310,6 +310,52 @@ class FLI(Reducer):
         return dict(indicator="fli")
 
 
+class RLI(Reducer):
+    """RLI(; replace=True), src/Indicators/rli.jl:24-114 (k = 2, on a pair stream of even dimension)."""
+    kind = _abi.RED_RLI
+
+    def __init__(self, replace: bool = True):
+        self.replace = bool(replace)
+        self.replaces = self.replace
+
+    def __repr__(self):
+        return f"RLI(replace={self.replace})"
+
+    def to_cl(self):
+        return _abi.cl_reducer(kind=self.kind, replace=int(self.replace))
+
+    def check(self, d, k):
+        if k != 2:
+            raise ValueError(f"RLI needs k = 2, got k = {k}")
+        if d % 2:
+            raise ValueError(f"RLI needs an even dimension, got d = {d}")
+
+    def dtype(self, d, k):
+        return np.dtype(_cs("sA") + _cs("sB") + _cs("Q") + [("value", "<f8"), ("n", "<i8"), ("K", "<i8"),
+                                                            ("step", "<i8"), ("code", "i1"), ("column", "i1"),
+                                                            ("_p0", "V6")])
+
+    def final(self, st):   # rli.jl:98-101
+        n, K = int(st["n"]), int(st["K"])
+        f = np.float64
+        if K == 0:
+            dl = rli = 0.0
+        else:
+            dl = float(abs((f(st["sB_s"]) - f(st["sA_s"])) + (f(st["sB_c"]) - f(st["sA_c"]))) / f(n))
+            rli = float((f(st["Q_s"]) + f(st["Q_c"])) / f(K))
+        return dict(n=n, handoffs=K, DL=dl, RLI=rli, sum=np.array([st["sA_s"], st["sB_s"]], dtype=np.float64),
+                    comp=np.array([st["sA_c"], st["sB_c"]], dtype=np.float64), Q=_tot(st["Q_s"], st["Q_c"]))
+
+    def error(self, st, orbit, backend):   # rli.jl:92-96
+        v = float(st["value"])
+        what = "pairing" if int(st["code"]) == 2 else "deviation matrix"
+        return NumericalHealthError(what, v, 0.0 if math.isfinite(v) else math.inf, int(st["step"]), orbit, backend,
+                                    int(st["column"]))
+
+    def provenance(self):
+        return dict(indicator="rli", convention="same xi_0, shadow along xi_0, mean over the handoffs 1..K")
+
+
 def chain_dtype(reducers, d: int, k: int) -> np.dtype:
     """The isbits layout of the Julia tuple of the chain's states (each field 8-byte aligned, sizes multiples of 8)."""
     fields, off = [], 0

@@ -72,7 +72,8 @@ enum cl_reducer_kind {
     CL_RED_SALI = 3,     /* SALI()                              sali.jl:14-68        */
     CL_RED_GALI = 4,     /* GALI()                              gali.jl:17-201       */
     CL_RED_MEGNO = 5,    /* MEGNO(; replace)                    megno.jl:29-113      */
-    CL_RED_FLI = 6       /* FLI(; replace)                      fli.jl:26-96         */
+    CL_RED_FLI = 6,      /* FLI(; replace)                      fli.jl:26-96         */
+    CL_RED_RLI = 7       /* RLI(; replace), on a pair stream    rli.jl:24-114        */
 };
 
 /* Orthonormalizers of QRSpectrum (orthonormalize.jl:5-12, householder.jl:5-10). */
@@ -358,6 +359,18 @@ CL_API int cl_b200_indicator_device(const cl_run* run, int64_t n, int32_t ns, do
 CL_API int cl_b200_indicator(const cl_run* run, int64_t n, int32_t ns, double* x, double* W, void* states,
                              int8_t* code, int64_t* hstep, const int64_t* grid, int32_t n_grid, double* R,
                              int64_t* fail, cl_prov* prov);
+/* The pair kind: the same body on PairMap(run.sys) (src/Systems/pair.jl:9-68) -- run.sys, run.d and run.s describe
+ * the base map; z holds the pair state (state A; state B), 2 run.s doubles per orbit, and W the (2 run.d) x 2 block
+ * frame, column-major; the chain's members are RLI and MEGNO (RLI1; RLI0, MEGNO1; MEGNO0, RLI1: the reference's pair
+ * specs), RLI's columns DL, RLI (rli.jl:98-101); the monitor reads orbit A. ns <= 2 run.s. Replaces the pair kind's
+ * `_ind_series_kernel!` launches. */
+CL_API int32_t cl_b200_indicator_pair_columns(const cl_run* run, int32_t ns);
+CL_API int cl_b200_indicator_pair_device(const cl_run* run, int64_t n, int32_t ns, double* z, double* W,
+                                         void* states, int8_t* code, int64_t* hstep, const int64_t* grid,
+                                         int32_t n_grid, double* R, int64_t* fail, void* stream);
+CL_API int cl_b200_indicator_pair(const cl_run* run, int64_t n, int32_t ns, double* z, double* W, void* states,
+                                  int8_t* code, int64_t* hstep, const int64_t* grid, int32_t n_grid, double* R,
+                                  int64_t* fail, cl_prov* prov);
 
 /* ---- The learned screen's kernels (no reference counterpart: the reference has no learned component) ---------------
  * All enqueue on `stream` and take device pointers. BF16 matrices are row-major with 16-byte aligned rows. */

@@ -87,6 +87,10 @@ struct MEGNOStateJ {                    // src/Indicators/megno.jl:46-55
 struct FLIStateJ {                      // src/Indicators/fli.jl:33-46
     CS s1, s2; double f1, fB, value; int64_t n, step, step1, stepB; int8_t code, column, colB;
 };
+struct RLIStateJ {                      // src/Indicators/rli.jl:30-40
+    CS sA, sB, Q; double value; int64_t n, K, step; int8_t code, column;
+};
+static_assert(sizeof(RLIStateJ) == 88, "RLIState layout");
 static_assert(sizeof(QRStateJ<2>) == 16 * 2 + 72, "QRState layout");
 static_assert(sizeof(BenettinStateJ) == 48, "BenettinState layout");
 static_assert(sizeof(SALIStateJ) == 72, "SALIState layout");
@@ -102,6 +106,7 @@ inline int64_t state_bytes_of(const cl_reducer& r, int k) {
         case CL_RED_GALI: return 24 * k + 32;
         case CL_RED_MEGNO: return 200;
         case CL_RED_FLI: return 96;
+        case CL_RED_RLI: return 88;
     }
     return 0;
 }
@@ -875,6 +880,35 @@ struct Reducers {
         std::memcpy(b, &st, sizeof st);
     }
 
+    // RLI's reducer_step (rli.jl:67-84) on a pair stream, d = 2h rows: norms as Benettin's, then the off-block check,
+    // then the log sums, DL = |(sB.s - sA.s) + (sB.c - sA.c)| / n into Q, and the replacement when `replace`.
+    static void rli(const cl_reducer& rd, uint8_t* b, int64_t n, double* W, int d) {
+        RLIStateJ st; std::memcpy(&st, b, sizeof st);
+        if (st.code != 0) return;
+        const double a1 = safe_norm(W, d), a2 = safe_norm(W + d, d);
+        const bool ok1 = isfin(a1) && a1 > 0, ok2 = isfin(a2) && a2 > 0;
+        if (!(ok1 && ok2)) {
+            st.column = ok1 ? 2 : 1; st.value = ok1 ? a2 : a1; st.step = n; st.code = 1;
+            std::memcpy(b, &st, sizeof st);
+            return;
+        }
+        const int h = d / 2;
+        double m1 = 0.0, m2 = 0.0;
+        for (int i = 0; i < h; ++i) { m1 = jl_max(m1, std::fabs(W[h + i])); m2 = jl_max(m2, std::fabs(W[d + i])); }
+        if (!(m1 == 0 && m2 == 0)) {
+            st.column = m1 == 0 ? 2 : 1; st.value = m1 == 0 ? m2 : m1; st.step = n; st.code = 2;
+            std::memcpy(b, &st, sizeof st);
+            return;
+        }
+        st.sA = cs_add(st.sA, Mth::log(a1));
+        st.sB = cs_add(st.sB, Mth::log(a2));
+        st.Q = cs_add(st.Q, std::fabs((st.sB.s - st.sA.s) + (st.sB.c - st.sA.c)) / static_cast<double>(n));
+        st.n = n;
+        st.K = st.K + 1;
+        if (rd.replace) for (int i = 0; i < d; ++i) { W[i] = W[i] / a1; W[d + i] = W[d + i] / a2; }
+        std::memcpy(b, &st, sizeof st);
+    }
+
     static bool failed(const cl_reducer& rd, const uint8_t* b, int k) {
         switch (rd.kind) {
             case CL_RED_QR: return *reinterpret_cast<const int8_t*>(b + 16 * k + 32) != 0;
@@ -883,6 +917,7 @@ struct Reducers {
             case CL_RED_GALI: return *reinterpret_cast<const int8_t*>(b + 8 * (3 * k - 1) + 24) != 0;
             case CL_RED_MEGNO: return reinterpret_cast<const MEGNOStateJ*>(b)->code != 0;
             case CL_RED_FLI: return reinterpret_cast<const FLIStateJ*>(b)->code != 0;
+            case CL_RED_RLI: return reinterpret_cast<const RLIStateJ*>(b)->code != 0;
         }
         return false;
     }
@@ -895,6 +930,7 @@ struct Reducers {
             case CL_RED_GALI: gali(b, n, W, d, k); break;
             case CL_RED_MEGNO: megno(rd, b, n, W, d); break;
             case CL_RED_FLI: fli(rd, b, n, W, d); break;
+            case CL_RED_RLI: rli(rd, b, n, W, d); break;
         }
     }
 };

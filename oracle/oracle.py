@@ -57,9 +57,9 @@ def lib() -> C.CDLL:
                                      C.c_int32]
         L.oracle_state_bytes.argtypes = [P(_abi.cl_run), C.c_int32]
         L.oracle_state_bytes.restype = C.c_int64
-        L.oracle_indicator.argtypes = [P(_abi.cl_run), C.c_int64, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p,
-                                       C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p,
-                                       C.c_int32, C.c_int32]
+        L.oracle_indicator.argtypes = [P(_abi.cl_run), C.c_int32, C.c_int64, C.c_int32, C.c_void_p, C.c_void_p,
+                                       C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p,
+                                       C.c_void_p, C.c_int32, C.c_int32]
         L.oracle_shadow.argtypes = [P(_abi.cl_run), C.c_int64, dp, C.c_void_p, C.c_void_p, C.c_double, C.c_int32,
                                     C.c_int32, C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p]
         L.oracle_max_threads.restype = C.c_int32
@@ -205,7 +205,39 @@ def oracle_indicators(sys, x0, N, tau, members, grid, *, ns=2, W0=None, launch_s
     total, L, done = int(N), int(launch_steps) if launch_steps else int(N), 0
     while done < total:
         run.n0, run.steps = done, min(L, total - done)
-        rc = lib().oracle_indicator(C.byref(run), n, ns, x.ctypes.data, W.ctypes.data, states.ctypes.data,
+        rc = lib().oracle_indicator(C.byref(run), 0, n, ns, x.ctypes.data, W.ctypes.data, states.ctypes.data,
+                                    code.ctypes.data, hstep.ctypes.data, grid.ctypes.data, len(grid), R.ctypes.data,
+                                    fail.ctypes.data, MATH[math], threads)
+        if rc != 0:
+            raise ValueError(f"oracle_indicator returned {rc}")
+        done += run.steps
+    return dict(R=R, fail=fail, x=x, W=W.transpose(0, 2, 1), states=states, code=code, hstep=hstep)
+
+
+def oracle_indicator_pairs(sys, z0, W0, N, tau, members, grid, *, ns=2, launch_steps=None, math="portable",
+                           threads=0):
+    """The indicator recorder's pair kind on the oracle: the stream PairMap(sys) from the pair states z0 (n, 2 s) and
+    block frames W0 (n, 2 d, 2); dict R (n, n_grid, cols + 3 + ns), fail, x, W, states, code, hstep."""
+    from chaos_b200.record import pair_chain
+    x = np.ascontiguousarray(np.asarray(z0, dtype=np.float64)).copy()
+    n = len(x)
+    d = sys.d
+    chain = pair_chain(members)
+    run = build_run(sys, N, tau, [FrameSpec(2, chain)], "fp64", 0)
+    ncol = sum(6 if m == "MEGNO" else 2 for m in members) + 3 + ns
+    sb = lib().oracle_state_bytes(C.byref(run), 0) + 24
+    W = np.ascontiguousarray(np.asarray(W0, dtype=np.float64).transpose(0, 2, 1))
+    assert W.shape == (n, 2, 2 * d)
+    grid = np.ascontiguousarray(np.asarray(grid, dtype=np.int64))
+    states = np.zeros((n, sb), np.uint8)
+    code = np.zeros(n, np.int8)
+    hstep = np.zeros(n, np.int64)
+    R = np.zeros((n, len(grid), ncol))
+    fail = np.zeros(n, np.int64)
+    total, L, done = int(N), int(launch_steps) if launch_steps else int(N), 0
+    while done < total:
+        run.n0, run.steps = done, min(L, total - done)
+        rc = lib().oracle_indicator(C.byref(run), 1, n, ns, x.ctypes.data, W.ctypes.data, states.ctypes.data,
                                     code.ctypes.data, hstep.ctypes.data, grid.ctypes.data, len(grid), R.ctypes.data,
                                     fail.ctypes.data, MATH[math], threads)
         if rc != 0:

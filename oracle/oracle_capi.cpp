@@ -471,19 +471,29 @@ void rec_orbit(const cl_run& run, int64_t i, double* xs, double* Ws, uint8_t* st
     if (hstep) hstep[i] = h;
 }
 
-// ---- the indicator recorder, tangent kind (src/Experiments/run_indicator_device.jl:13-60) -----------------------
+// ---- the indicator recorder, tangent and pair kinds (src/Experiments/run_indicator_device.jl:13-60) -------------
 // _orbit_body (orbit.jl:44-60) with the chain (members..., RunMonitor): every member steps on the W the one before
-// returned, then the monitor; a failure of any member stops the segment
+// returned, then the monitor; a failure of any member stops the segment. `pair`: the stream is PairMap(sys)
+// (src/Systems/pair.jl:9-68): the state (A; B) of two base states each advanced alone, the tangent acting block by
+// block on the frame's rows (each block by the base's own product), the monitor reading orbit A
+// (run_indicator_record.jl:6-10).
 template <int MM>
-int8_t ind_body(const cl_run& run, double* x, double* W, uint8_t* st, double* mon, int64_t& n, int64_t steps) {
+int8_t ind_body(const cl_run& run, bool pair, double* x, double* W, uint8_t* st, double* mon, int64_t& n,
+                int64_t steps) {
     const cl_frame& fr = run.frames[0];
-    const int d = run.d, k = fr.k, s = run.s;
+    const int db = run.d, sb = run.s, k = fr.k;
+    const int d = pair ? 2 * db : db, s = pair ? 2 * sb : sb;
     for (int64_t h = 0; h < steps / run.tau; ++h) {
         for (int t = 0; t < run.tau; ++t) {
-            double M[4], Wn[4];
-            rec_map<MM>(run, x, M);
-            fused_product(M, W, Wn, d, d, k);
-            std::memcpy(W, Wn, sizeof(double) * d * k);
+            for (int half = 0; half < (pair ? 2 : 1); ++half) {
+                double M[4], Wb[4], Wn[4];
+                rec_map<MM>(run, x + half * sb, M);
+                for (int j = 0; j < k; ++j)
+                    for (int l = 0; l < db; ++l) Wb[l + db * j] = W[half * db + l + d * j];
+                fused_product(M, Wb, Wn, db, db, k);
+                for (int j = 0; j < k; ++j)
+                    for (int l = 0; l < db; ++l) W[half * db + l + d * j] = Wn[l + db * j];
+            }
         }
         n += run.tau;
         const int8_t c = status_of(x, s, W, d * k);
@@ -513,7 +523,8 @@ void ind_megno_series(const MegnoSumsJ& m, int64_t n, int64_t K, double* out) {
     out[2] = static_cast<double>(n / K) * (m.Q2.s + m.Q2.c) / (tn * tn * tn);
 }
 // _put! (run_indicator_record.jl:40-56) of one member from its state: SALI sali, L (sali.jl:62-66); FLI fli = fB,
-// fli1 = f1 (fli.jl:91-94); MEGNO Y, Ybar, Ybar20 of column 1 then of column 2. Returns the columns written.
+// fli1 = f1 (fli.jl:91-94); MEGNO Y, Ybar, Ybar20 of column 1 then of column 2; RLI DL, RLI. Returns the columns
+// written.
 int ind_put(const cl_reducer& rd, const uint8_t* b, double* row) {
     switch (rd.kind) {
         case CL_RED_SALI: {
@@ -534,6 +545,12 @@ int ind_put(const cl_reducer& rd, const uint8_t* b, double* row) {
             ind_megno_series(st.c2, st.n, st.K, row + 3);
             return 6;
         }
+        case CL_RED_RLI: {   // reducer_final (rli.jl:98-101): DL at the last handoff, RLI = Q / K; zeros before one
+            RLIStateJ st; std::memcpy(&st, b, sizeof st);
+            row[0] = st.K == 0 ? 0.0 : std::fabs((st.sB.s - st.sA.s) + (st.sB.c - st.sA.c)) / static_cast<double>(st.n);
+            row[1] = st.K == 0 ? 0.0 : (st.Q.s + st.Q.c) / static_cast<double>(st.K);
+            return 2;
+        }
     }
     return 0;
 }
@@ -544,11 +561,11 @@ int ind_cols(const cl_frame& fr) {
 }
 // _ind_series_kernel! (run_indicator_device.jl:31-60) for one orbit over one launch window
 template <int MM>
-void ind_orbit(const cl_run& run, int64_t i, int ns, double* xs, double* Ws, uint8_t* sts, int8_t* code, int64_t* hstep,
-               const int64_t* grid, int n_grid, double* R, int64_t* fail, int64_t n0, int64_t steps) {
+void ind_orbit(const cl_run& run, bool pair, int64_t i, int ns, double* xs, double* Ws, uint8_t* sts, int8_t* code,
+               int64_t* hstep, const int64_t* grid, int n_grid, double* R, int64_t* fail, int64_t n0, int64_t steps) {
     if (!(n0 == 0 || code[i] == STATUS_OK)) return;
     const cl_frame& fr = run.frames[0];
-    const int d = run.d, k = fr.k, s = run.s, ncol = ind_cols(fr) + 3 + ns;
+    const int d = pair ? 2 * run.d : run.d, k = fr.k, s = pair ? 2 * run.s : run.s, ncol = ind_cols(fr) + 3 + ns;
     const int64_t cb = frame_state_bytes(fr), sb = cb + 24;
     double* x = xs + i * s;
     double* W = Ws + i * d * k;
@@ -564,7 +581,7 @@ void ind_orbit(const cl_run& run, int64_t i, int ns, double* xs, double* Ws, uin
     while (ghi + 1 < n_grid && grid[ghi + 1] <= n0 + steps) ++ghi;
     double* Ri = R + i * static_cast<int64_t>(ncol) * n_grid;
     for (int g = glo; g <= ghi; ++g) {
-        c = ind_body<MM>(run, x, W, st, mon, n, grid[g] - n);
+        c = ind_body<MM>(run, pair, x, W, st, mon, n, grid[g] - n);
         h = n;
         if (c != STATUS_OK) { fail[i] = g + 1; break; }
         double* row = Ri + static_cast<int64_t>(g) * ncol;
@@ -580,7 +597,7 @@ void ind_orbit(const cl_run& run, int64_t i, int ns, double* xs, double* Ws, uin
         for (int j = 0; j < ns; ++j) row[off + 3 + j] = x[j];
     }
     if (c == STATUS_OK && n < n0 + steps) {
-        c = ind_body<MM>(run, x, W, st, mon, n, n0 + steps - n);
+        c = ind_body<MM>(run, pair, x, W, st, mon, n, n0 + steps - n);
         h = n;
         if (c != STATUS_OK) fail[i] = ghi + 2;
     }
@@ -752,12 +769,13 @@ int oracle_record(const cl_run* run, int64_t n, double* x, double* W, void* stat
 
 // The indicator recorder on the CPU: one window [run.n0, run.n0 + steps) of n orbits, buffers in place (see the
 // C ABI's cl_b200_indicator_device); R has ncols(chain) + 3 + ns columns per row.
-int oracle_indicator(const cl_run* run, int64_t n, int32_t ns, double* x, double* W, void* states, int8_t* code,
-                     int64_t* hstep, const int64_t* grid, int32_t n_grid, double* R, int64_t* fail, int32_t math_mode,
-                     int32_t threads) {
+// pair != 0: the stream is PairMap(run->sys), x holds 2 s and W (2 d) x 2 entries per orbit.
+int oracle_indicator(const cl_run* run, int32_t pair, int64_t n, int32_t ns, double* x, double* W, void* states,
+                     int8_t* code, int64_t* hstep, const int64_t* grid, int32_t n_grid, double* R, int64_t* fail,
+                     int32_t math_mode, int32_t threads) {
     const int64_t steps = run->steps > 0 ? run->steps : run->N - run->n0;
     if (run->tau <= 0 || steps % run->tau != 0 || run->n0 + steps > run->N || run->n_frames != 1 ||
-        run->frames[0].k != 2 || ns < 0 || ns > run->s)
+        run->frames[0].k != 2 || ns < 0 || ns > (pair ? 2 : 1) * run->s)
         return CL_EINVAL;
     const int hw = static_cast<int>(std::max(1u, std::thread::hardware_concurrency()));
     const int nt = static_cast<int>(std::min<int64_t>(threads > 0 ? threads : hw, std::max<int64_t>(n, 1)));
@@ -768,11 +786,11 @@ int oracle_indicator(const cl_run* run, int64_t n, int32_t ns, double* x, double
             if (lo >= n) return;
             for (int64_t i = lo; i < std::min<int64_t>(lo + 16, n); ++i) {
                 if (math_mode == MATH_LIBM)
-                    ind_orbit<MATH_LIBM>(*run, i, ns, x, W, static_cast<uint8_t*>(states), code, hstep, grid, n_grid,
-                                         R, fail, run->n0, steps);
+                    ind_orbit<MATH_LIBM>(*run, pair != 0, i, ns, x, W, static_cast<uint8_t*>(states), code, hstep,
+                                         grid, n_grid, R, fail, run->n0, steps);
                 else
-                    ind_orbit<MATH_PORTABLE>(*run, i, ns, x, W, static_cast<uint8_t*>(states), code, hstep, grid,
-                                             n_grid, R, fail, run->n0, steps);
+                    ind_orbit<MATH_PORTABLE>(*run, pair != 0, i, ns, x, W, static_cast<uint8_t*>(states), code,
+                                             hstep, grid, n_grid, R, fail, run->n0, steps);
             }
         }
     };

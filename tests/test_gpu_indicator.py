@@ -69,3 +69,45 @@ def test_indicator_failure(oracle):
     _same(dev, ref)
     assert dev.fail.tolist()[:3] == [0, 1, 0] and dev.fail[3] == 1
 
+
+
+# ---- the pair kind ------------------------------------------------------------------------------------------------
+PAIR_CHAINS = [["RLI"], ["RLI", "MEGNO"], ["MEGNO", "RLI"]]
+
+
+def _pairs(name, n=160):
+    from chaos_b200 import pair_frame, pair_start
+    sys, x0 = _system(name)
+    x0 = x0[:n]
+    if name == "wrapped":
+        x0 = x0[:, :2]
+    a = np.random.default_rng(41).uniform(0, 2 * np.pi, n)
+    xis = np.stack([np.cos(a), np.sin(a)], axis=1)
+    z0 = np.array([pair_start(sys, x, u, 1e-7 if name != "linear" else 1e-9)[0] for x, u in zip(x0, xis)])
+    return sys, z0, np.array([pair_frame(u) for u in xis])
+
+
+@pytest.mark.parametrize("members", PAIR_CHAINS, ids=",".join)
+@pytest.mark.parametrize("name", ["standard", "wrapped", "linear"])
+@pytest.mark.parametrize("tau", [1, 4])
+def test_pair_indicator_matches_oracle(oracle, members, name, tau):
+    from chaos_b200 import record_indicator_pairs
+    sys, z0, W0 = _pairs(name)
+    N = 200 if name != "linear" else 40
+    grid = sorted({g for g in (tau, 2 * tau, 10 * tau, 25 * tau, N) if g <= N})
+    ns = 2 * sys.s
+    dev = record_indicator_pairs(sys, z0, W0, N, tau, members, grid, ns=ns)
+    ref = oracle.oracle_indicator_pairs(sys, z0, W0, N, tau, members, grid, ns=ns)
+    _same(dev, ref)
+
+
+def test_pair_indicator_windows_and_failure(oracle):
+    from chaos_b200 import record_indicator_pairs
+    sys, z0, W0 = _pairs("standard", 64)
+    W0[5, 2, 0] = 1e-3                      # pairing failure at the first handoff
+    z0[9, 1] = np.inf                       # state failure
+    grid = [8, 16, 40, 96, 200]
+    dev = record_indicator_pairs(sys, z0, W0, 200, 4, ["RLI", "MEGNO"], grid, launch_steps=8)
+    ref = oracle.oracle_indicator_pairs(sys, z0, W0, 200, 4, ["RLI", "MEGNO"], grid)
+    _same(dev, ref)
+    assert dev.fail[5] == 1 and dev.fail[9] == 1 and (np.delete(dev.fail, [5, 9]) == 0).all()
