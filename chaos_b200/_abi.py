@@ -14,6 +14,8 @@ MAX_STAGES = 64
 MAX_DIM = 16
 MAX_K = 8
 NOALLOC_MAX_CLASSES = 64
+MAX_WINDOWS = 4
+MAX_OBSERVABLES = 8
 
 # enum cl_system_kind
 SYS_STANDARD, SYS_WRAPPED_STANDARD, SYS_FROESCHLE, SYS_CHAIN, SYS_LINEAR, SYS_HH_GAUSS, SYS_HH_SPLIT = 1, 2, 3, 4, 5, 6, 7
@@ -23,6 +25,9 @@ RED_QR, RED_BENETTIN, RED_SALI, RED_GALI, RED_MEGNO, RED_FLI, RED_RLI = 1, 2, 3,
 QR_CGS, QR_MGS, QR_RGS, QR_HOUSEHOLDER, QR_AUGMENTED, QR_GIVENS = 1, 2, 3, 4, 5, 6
 # enum cl_precision
 PREC_FP64, PREC_MIXED = 0, 1
+# enum cl_window_kind, enum cl_observable_kind
+WIN_PHASE_ADVANCE, WIN_BIRKHOFF = 1, 2
+OBS_PLANAR, OBS_LIFTED_ANGLE, OBS_COS, OBS_SIN, OBS_LIFTED, OBS_COORDINATE = 1, 2, 3, 4, 5, 6
 # enum cl_status
 OK, EINVAL, ENODEVICE, EUNSUPPORTED, ENOMEM, EDEVICE_LOST = 0, -1, -2, -3, -4, -9
 
@@ -94,6 +99,13 @@ class cl_buffers(C.Structure):
         ("code", C.c_void_p * MAX_FRAMES),
         ("hstep", C.c_void_p * MAX_FRAMES),
     ]
+
+
+class cl_window(C.Structure):
+    _fields_ = [("kind", C.c_int32), ("n_windows", C.c_int32), ("n_observables", C.c_int32),
+                ("birkhoff_order", C.c_int32), ("window", C.c_int64 * MAX_WINDOWS),
+                ("obs_kind", C.c_int32 * MAX_OBSERVABLES), ("obs_a", C.c_int32 * MAX_OBSERVABLES),
+                ("obs_b", C.c_int32 * MAX_OBSERVABLES)]
 
 
 class cl_prov(C.Structure):
@@ -227,6 +239,16 @@ def declare(lib: C.CDLL) -> C.CDLL:
     lib.cl_b200_indicator_pair_device.restype = C.c_int
     lib.cl_b200_indicator_pair.argtypes = lib.cl_b200_indicator.argtypes
     lib.cl_b200_indicator_pair.restype = C.c_int
+    lib.cl_b200_window_state_bytes.argtypes = [P(cl_window)]
+    lib.cl_b200_window_state_bytes.restype = C.c_int64
+    lib.cl_b200_indicator_window_device.argtypes = [P(cl_run), P(cl_window), C.c_int64, C.c_int32, C.c_void_p,
+                                                    C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32,
+                                                    C.c_void_p, C.c_void_p, C.c_void_p]
+    lib.cl_b200_indicator_window_device.restype = C.c_int
+    lib.cl_b200_indicator_window.argtypes = [P(cl_run), P(cl_window), C.c_int64, C.c_int32, C.c_void_p, C.c_void_p,
+                                             C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p,
+                                             P(cl_prov)]
+    lib.cl_b200_indicator_window.restype = C.c_int
     lib.cl_b200_ensemble_tune.restype = C.c_int
     lib.cl_b200_ensemble_graph_create.argtypes = [P(cl_ensemble_class), C.c_int32, P(C.c_void_p)]
     lib.cl_b200_ensemble_graph_create.restype = C.c_int
@@ -254,4 +276,5 @@ EXPORTS = ("cl_b200_propagate", "cl_b200_propagate_device", "cl_b200_check", "cl
            "cl_b200_shadow_record_device", "cl_b200_shadow_record", "cl_b200_indicator_columns",
            "cl_b200_indicator_state_bytes", "cl_b200_indicator_device", "cl_b200_indicator",
            "cl_b200_advance_ensemble_device", "cl_b200_advance_ensemble", "cl_b200_indicator_pair_columns",
-           "cl_b200_indicator_pair_device", "cl_b200_indicator_pair")
+           "cl_b200_indicator_pair_device", "cl_b200_indicator_pair", "cl_b200_window_state_bytes",
+           "cl_b200_indicator_window_device", "cl_b200_indicator_window")

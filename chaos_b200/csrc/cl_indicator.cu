@@ -16,6 +16,7 @@
 #include <type_traits>
 
 #include "../../include/chaoslab_b200.h"
+#include "cl_monitor.cuh"
 #include "cl_registry.cuh"
 
 namespace cl {
@@ -28,8 +29,6 @@ int64_t capi_frame_bytes(const cl_frame& f);          // cl_capi.cu
 std::string run_key(const cl_run& r);                 // cl_capi.cu
 
 namespace {
-
-struct MonState { double det_max, symp_max, M_max; };
 
 struct IndArgs {
     i64 n, n0, steps, N;
@@ -45,41 +44,6 @@ struct IndArgs {
     i64* fail;
     RedParams prm[CL_MAX_REDUCERS];
 };
-
-// The tangent at x, column-major 2 x 2, and the monitor's running maxima (run_record.jl:34-37).
-template <class Sys>
-__device__ __forceinline__ void monitor_step(const Sys& sys, const double* x, MonState& m) {
-    double M[4];
-    if constexpr (std::is_same<Sys, SysLinear<2>>::value) {
-#pragma unroll
-        for (int l = 0; l < 4; ++l) M[l] = sys.A[l];
-    } else {
-        StdJac J;
-        sys.jac(x, J);
-        const double o = 1.0;
-        M[0] = o + J.c; M[1] = J.c; M[2] = o; M[3] = o;
-    }
-    const double edet = fabs((M[0] * M[3] - M[2] * M[1]) - 1.0);
-    const double Om[4] = {0.0, -1.0, 1.0, 0.0};
-    double P[4], Q[4];
-#pragma unroll
-    for (int j = 0; j < 2; ++j)
-#pragma unroll
-        for (int i = 0; i < 2; ++i) P[i + 2 * j] = fma(M[1 + 2 * i], Om[1 + 2 * j], M[2 * i] * Om[2 * j]);
-#pragma unroll
-    for (int j = 0; j < 2; ++j)
-#pragma unroll
-        for (int i = 0; i < 2; ++i) Q[i + 2 * j] = fma(P[i + 2], M[1 + 2 * j], P[i] * M[2 * j]);
-    double es = fabs(Q[0] - Om[0]);
-#pragma unroll
-    for (int l = 1; l < 4; ++l) es = jl_max(es, fabs(Q[l] - Om[l]));
-    double mm = fabs(M[0]);
-#pragma unroll
-    for (int l = 1; l < 4; ++l) mm = jl_max(mm, fabs(M[l]));
-    m.det_max = jl_max(m.det_max, edet);
-    m.symp_max = jl_max(m.symp_max, es);
-    m.M_max = jl_max(m.M_max, mm);
-}
 
 // _put! (run_indicator_record.jl:40-56): a member's columns from its reducer_final
 template <class R> struct Put;

@@ -12,6 +12,7 @@
 //   cl_log:    x = m 2^e with m in [sqrt(1/2), sqrt(2)], f = m - 1, s = f / (2 + f), and the identity
 //              log(1 + f) = f - f^2/2 + s (f^2/2 + R(s^2)), R the atanh series 2z/3 + 2z^2/5 + ... to z^9, plus e ln 2
 //              with ln 2 split so that e LN2_HI is exact.
+//   cl_exp, cl_atan2: see their definitions below (Taylor polynomials after Cody-Waite / table reduction).
 // The constants come from chaos_b200/csrc/derive_constants.py (mathematical definitions, rounded once).
 #pragma once
 
@@ -163,6 +164,76 @@ __device__ __forceinline__ double cl_log_impl(double x) {
     return e * CL_LN2_HI - ((hfsq - (s * (hfsq + R) + e * CL_LN2_LO)) - f);
 }
 __device__ __forceinline__ double cl_log(double x) { return cl_log_impl(x); }
+
+// cl_exp: k = rint(x / ln 2), r = (x - k LN2_HI) - k LN2_LO (the first product exact), the Taylor polynomial of
+// exp(r) to r^13 in Horner form, then the scaling by 2^k in at most two products (the first exact). Bitwise the
+// oracle's p_exp.
+__device__ __forceinline__ double cl_pow2(int k) { return __longlong_as_double(static_cast<long long>(k + 1023) << 52); }
+__device__ __forceinline__ double cl_exp(double x) {
+    if (isnan(x)) return x;
+    if (x > 709.782712893384) return __longlong_as_double(0x7ff0000000000000LL);
+    if (x < -745.1332191019412) return 0.0;
+    const double k = rint(x * CL_INV_LN2);
+    const double r = (x - k * CL_LN2_HI) - k * CL_LN2_LO;
+    double p = CL_EXP_T13;
+    p = fma(p, r, CL_EXP_T12);
+    p = fma(p, r, CL_EXP_T11);
+    p = fma(p, r, CL_EXP_T10);
+    p = fma(p, r, CL_EXP_T9);
+    p = fma(p, r, CL_EXP_T8);
+    p = fma(p, r, CL_EXP_T7);
+    p = fma(p, r, CL_EXP_T6);
+    p = fma(p, r, CL_EXP_T5);
+    p = fma(p, r, CL_EXP_T4);
+    p = fma(p, r, CL_EXP_T3);
+    p = fma(p, r, CL_EXP_T2);
+    p = fma(p, r, 1.0);
+    p = fma(p, r, 1.0);
+    const int ki = static_cast<int>(k);
+    if (ki > 1023) return (p * cl_pow2(1023)) * cl_pow2(ki - 1023);
+    if (ki >= -1022) return p * cl_pow2(ki);
+    return (p * cl_pow2(ki + 1000)) * cl_pow2(-1000);
+}
+
+// cl_atan2: the octant reduction to z = min / max in [0, 1]; atan(z) = atan(c) + atan(u), c = k / 16 the nearest
+// table point, u = (z - c) / (1 + z c), |u| <= 1/32, atan(u) by its Taylor polynomial to u^13; then pi / 2 - a and
+// pi - a with split constants, and the C99 special cases for zeros and infinities. Bitwise the oracle's p_atan2.
+static __constant__ double c_atan_hi[17] = {CL_ATAN_HI_0, CL_ATAN_HI_1, CL_ATAN_HI_2, CL_ATAN_HI_3, CL_ATAN_HI_4,
+    CL_ATAN_HI_5, CL_ATAN_HI_6, CL_ATAN_HI_7, CL_ATAN_HI_8, CL_ATAN_HI_9, CL_ATAN_HI_10, CL_ATAN_HI_11, CL_ATAN_HI_12,
+    CL_ATAN_HI_13, CL_ATAN_HI_14, CL_ATAN_HI_15, CL_ATAN_HI_16};
+static __constant__ double c_atan_lo[17] = {CL_ATAN_LO_0, CL_ATAN_LO_1, CL_ATAN_LO_2, CL_ATAN_LO_3, CL_ATAN_LO_4,
+    CL_ATAN_LO_5, CL_ATAN_LO_6, CL_ATAN_LO_7, CL_ATAN_LO_8, CL_ATAN_LO_9, CL_ATAN_LO_10, CL_ATAN_LO_11, CL_ATAN_LO_12,
+    CL_ATAN_LO_13, CL_ATAN_LO_14, CL_ATAN_LO_15, CL_ATAN_LO_16};
+__device__ __forceinline__ double cl_atan01(double z) {
+    const int k = static_cast<int>(rint(z * 16.0));
+    const double c = k * 0.0625;
+    const double u = (z - c) / (1.0 + z * c);
+    const double u2 = u * u;
+    double q = CL_ATAN_T13;
+    q = fma(q, u2, CL_ATAN_T11);
+    q = fma(q, u2, CL_ATAN_T9);
+    q = fma(q, u2, CL_ATAN_T7);
+    q = fma(q, u2, CL_ATAN_T5);
+    q = fma(q, u2, CL_ATAN_T3);
+    const double at = fma(u * u2, q, u);
+    return c_atan_hi[k] + (at + c_atan_lo[k]);
+}
+__device__ __forceinline__ double cl_atan2(double y, double x) {
+    if (isnan(x) || isnan(y)) return x + y;
+    if (isinf(y)) {
+        const double a = isinf(x) ? (x > 0 ? CL_PIO2_1 * 0.5 : (CL_PI_HI - CL_PIO2_1 * 0.5) + CL_PI_LO) : CL_PIO2_1;
+        return copysign(a, y);
+    }
+    if (isinf(x)) return copysign(x > 0 ? 0.0 : CL_PI_HI, y);
+    if (y == 0.0) return signbit(x) ? copysign(CL_PI_HI, y) : y;
+    if (x == 0.0) return copysign(CL_PIO2_1, y);
+    const double ax = fabs(x), ay = fabs(y);
+    const bool swap = ay > ax;
+    double a = cl_atan01(swap ? ax / ay : ay / ax);
+    if (swap) a = (CL_PIO2_1 - a) + CL_PIO2_2;
+    if (x < 0.0) a = (CL_PI_HI - a) + CL_PI_LO;
+    return y < 0.0 ? -a : a;
+}
 
 // Neumaier compensated sum (src/Foundation/Foundation.jl:48-68); always Float64.
 struct CS { double s, c; };

@@ -9,6 +9,8 @@ Everything is computed in 100-digit decimal arithmetic and rounded once into bin
   rounded;
 * ln 2 split into a 42-bit head (so that e * LN2_HI is exact for every binary64 exponent e) and its rounded tail,
   for the logarithm;
+* 1 / ln 2 and the Taylor coefficients 1 / n! of exp; atan(k / 16) for k = 0..16 split head + tail, the Taylor
+  coefficients of atan, pi split head + tail, for this project's exp and atan2;
 * the 3-stage Gauss-Legendre coefficients A and b in closed form (nodes 1/2 -+ sqrt(15)/10, 1/2), each split into
   a correctly rounded head and the rounded remainder, as src/Integrators/gauss.jl:21-26 (`_split`) does with its
   320-bit values; the collocation conditions sum_j A_ij c_j^(k-1) = c_i^k / k are checked to 1e-90.
@@ -38,6 +40,26 @@ def _arctan_inv(n: int) -> Decimal:
         d = t / k
         if abs(d) < Decimal(10) ** -98:
             return s
+        s += d
+
+
+def _arctan_frac(k: int, m: int) -> Decimal:
+    """atan(k / m) for 0 <= k <= m by the series of atan(x) = sum (-1)^i x^(2i+1) / (2i+1) after two halvings of the
+    angle, atan(x) = 2 atan(x / (1 + sqrt(1 + x^2)))."""
+    if k == 0:
+        return Decimal(0)
+    x = Decimal(k) / m
+    for _ in range(2):
+        x = x / (1 + (1 + x * x).sqrt())
+    x2 = x * x
+    s = t = x
+    i = 1
+    while True:
+        t = -t * x2
+        i += 2
+        d = t / i
+        if abs(d) < Decimal(10) ** -98:
+            return 4 * s
         s += d
 
 
@@ -83,6 +105,22 @@ def derive() -> dict[str, float]:
     for i in range(1, 10):
         c[f"CL_LOG_T{i}"] = float(Decimal(2) / (2 * i + 1))
     c["CL_SQRT2"] = float(Decimal(2).sqrt())
+    # exp: 1 / ln 2 for k = rint(x / ln 2), the reduction x - k ln 2 by the split ln 2 above, and the Taylor
+    # coefficients 1 / n! of exp on |r| <= ln 2 / 2 (n = 2 .. 13; the terms 1 and r are exact)
+    c["CL_INV_LN2"] = float(1 / ln2)
+    for n in range(2, 14):
+        c[f"CL_EXP_T{n}"] = float(Decimal(1) / math.factorial(n))
+    # atan: atan(k / 16), k = 0 .. 16, as a correctly rounded head and the rounded remainder, for
+    # atan(z) = atan(c) + atan((z - c) / (1 + z c)) with c = k / 16 nearest to z in [0, 1]; the Taylor
+    # coefficients (-1)^n / (2 n + 1) of atan(u) (n = 1 .. 6) on |u| <= 1 / 32; pi and pi / 2 split in two
+    for k in range(17):
+        a = _arctan_frac(k, 16)
+        c[f"CL_ATAN_HI_{k}"] = float(a)
+        c[f"CL_ATAN_LO_{k}"] = float(a - Decimal(c[f"CL_ATAN_HI_{k}"]))
+    for n in range(1, 7):
+        c[f"CL_ATAN_T{2 * n + 1}"] = float(Decimal((-1) ** n) / (2 * n + 1))
+    c["CL_PI_HI"] = float(pi)
+    c["CL_PI_LO"] = float(pi - Decimal(c["CL_PI_HI"]))
     return c
 
 

@@ -50,6 +50,8 @@ extern "C" {
 #define CL_MAX_DIM 16
 #define CL_MAX_K 8
 #define CL_MAX_STAGES 64
+#define CL_MAX_WINDOWS 4
+#define CL_MAX_OBSERVABLES 8
 
 /* Systems (src/Systems): the fixed menu the compiled kernels cover. */
 enum cl_system_kind {
@@ -327,6 +329,42 @@ CL_API int cl_b200_record_device(const cl_run* run, int64_t n, double* x, double
 /* The same from run.n0 to run.N on host buffers, in windows of run.steps steps (synchronous). */
 CL_API int cl_b200_record(const cl_run* run, int64_t n, double* x, double* W, void* states, int8_t* code,
                           int64_t* hstep, const int64_t* grid, int32_t n_grid, double* R, int64_t* fail, cl_prov* prov);
+
+/* ---- The indicator recorder, window kinds (src/Experiments/run_indicator_device.jl:62-91) --------------------------
+ * The phase-advance and Birkhoff kinds: the orbit of the base map (run.sys, run.d = 2, frames[0].k = 1, no reducers)
+ * advanced one handoff at a time with the deviation column reset to (1, 0) at each handoff, the non-raising monitor
+ * and one reader reducer: WeightedPhaseAdvance (src/Indicators/naff_reducer.jl:122-243) or WeightedBirkhoff
+ * (wbirkhoff_reducer.jl:18-110), with the Birkhoff weight exp(-1 / (t^p (1 - t)^p)) at the mirrored index. At every
+ * grid step one row of R[col, g, orbit] of 3 + ns columns: det_max, symp_max, M_max, x[0 .. ns-1]. states per orbit:
+ * MonState{Float64} (24 bytes) then the reader's isbits state (cl_b200_window_state_bytes: WPAState{Float64, H},
+ * 64 H + 32 bytes; WBState{Float64, H, K}, 16 + H (16 + 40 K) bytes), carried in place; the tables are the
+ * reader's reducer_final on the host. fail: the 1-based grid index of the failing handoff's segment. */
+enum cl_window_kind { CL_WIN_PHASE_ADVANCE = 1, CL_WIN_BIRKHOFF = 2 };
+enum cl_observable_kind {
+    CL_OBS_PLANAR = 1,       /* PlanarObservable(a, b): z = x[a] + i x[b]                naff_reducer.jl:96-101   */
+    CL_OBS_LIFTED_ANGLE = 2, /* LiftedAngleObservable(a, b): (x[a], count x[b]; b = 0 none) naff_reducer.jl:103-117 */
+    CL_OBS_COS = 3,          /* CosObservable(a, b): cos(b x[a])                          wbirkhoff.jl:12-23      */
+    CL_OBS_SIN = 4,          /* SinObservable(a, b): sin(b x[a])                          wbirkhoff.jl:25-36      */
+    CL_OBS_LIFTED = 5,       /* LiftedObservable(a, b): x[a] + 2 pi x[b]                  wbirkhoff.jl:38-49      */
+    CL_OBS_COORDINATE = 6    /* IndCoordinate(a): x[a]                     src/Experiments/run_indicator_chain.jl:20-23 */
+};
+typedef struct cl_window {
+    int32_t kind;            /* enum cl_window_kind                                                       */
+    int32_t n_windows;       /* H, 1..CL_MAX_WINDOWS                                                      */
+    int32_t n_observables;   /* K: 1 for the phase advance, 1..CL_MAX_OBSERVABLES for Birkhoff            */
+    int32_t birkhoff_order;  /* p, 1..4                                                                   */
+    int64_t window[CL_MAX_WINDOWS];       /* the horizons N_h, each >= 16                                 */
+    int32_t obs_kind[CL_MAX_OBSERVABLES]; /* enum cl_observable_kind                                      */
+    int32_t obs_a[CL_MAX_OBSERVABLES];    /* 1-based coordinate index                                     */
+    int32_t obs_b[CL_MAX_OBSERVABLES];    /* second index (1-based, 0 = none) or the integer frequency    */
+} cl_window;
+CL_API int64_t cl_b200_window_state_bytes(const cl_window* win);
+CL_API int cl_b200_indicator_window_device(const cl_run* run, const cl_window* win, int64_t n, int32_t ns, double* x,
+                                           void* states, int8_t* code, int64_t* hstep, const int64_t* grid,
+                                           int32_t n_grid, double* R, int64_t* fail, void* stream);
+CL_API int cl_b200_indicator_window(const cl_run* run, const cl_window* win, int64_t n, int32_t ns, double* x,
+                                    void* states, int8_t* code, int64_t* hstep, const int64_t* grid, int32_t n_grid,
+                                    double* R, int64_t* fail, cl_prov* prov);
 
 /* ---- advance_ensemble (src/Integrators/ensemble.jl:13-45) ---------------------------------------------------------
  * `steps` steps of size sys->dt of the integrator of an IntegratorMap system (CL_SYS_HH_SPLIT: a table method,

@@ -39,6 +39,8 @@ def lib() -> C.CDLL:
         L.oracle_propagate.restype = C.c_int
         L.oracle_sincos.argtypes = [C.c_int32, dp, dp, dp, C.c_int64]
         L.oracle_log.argtypes = [C.c_int32, dp, dp, C.c_int64]
+        L.oracle_exp.argtypes = [C.c_int32, dp, dp, C.c_int64]
+        L.oracle_atan2.argtypes = [C.c_int32, dp, dp, dp, C.c_int64]
         L.oracle_fused_product.argtypes = [dp, dp, dp, C.c_int32, C.c_int32, C.c_int32]
         L.oracle_safe_norm.argtypes = [dp, C.c_int32]
         L.oracle_safe_norm.restype = C.c_double
@@ -55,6 +57,9 @@ def lib() -> C.CDLL:
                                     C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_int32, C.c_int32]
         L.oracle_advance.argtypes = [P(_abi.cl_system), C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64,
                                      C.c_int32]
+        L.oracle_indicator_window.argtypes = [P(_abi.cl_run), P(_abi.cl_window), C.c_int64, C.c_int32, C.c_void_p,
+                                              C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p,
+                                              C.c_void_p, C.c_int32, C.c_int32]
         L.oracle_state_bytes.argtypes = [P(_abi.cl_run), C.c_int32]
         L.oracle_state_bytes.restype = C.c_int64
         L.oracle_indicator.argtypes = [P(_abi.cl_run), C.c_int32, C.c_int64, C.c_int32, C.c_void_p, C.c_void_p,
@@ -244,6 +249,34 @@ def oracle_indicator_pairs(sys, z0, W0, N, tau, members, grid, *, ns=2, launch_s
             raise ValueError(f"oracle_indicator returned {rc}")
         done += run.steps
     return dict(R=R, fail=fail, x=x, W=W.transpose(0, 2, 1), states=states, code=code, hstep=hstep)
+
+
+def oracle_indicator_window(sys, x0, N, tau, reader, grid, *, ns=2, launch_steps=None, math="portable", threads=0):
+    """The indicator recorder's window kinds on the oracle: dict R (n, n_grid, 3 + ns), fail, x, states (MonState
+    then the reader's state), code, hstep, finals (the reader's reducer_final per orbit)."""
+    from chaos_b200.window import to_cl
+    x = np.ascontiguousarray(np.asarray(x0, dtype=np.float64)).copy()
+    n = len(x)
+    run = build_run(sys, N, tau, [FrameSpec(1, ())], "fp64", 0)
+    win = to_cl(reader)
+    sb = 24 + reader.state_bytes()
+    grid = np.ascontiguousarray(np.asarray(grid, dtype=np.int64))
+    states = np.zeros((n, sb), np.uint8)
+    code = np.zeros(n, np.int8)
+    hstep = np.zeros(n, np.int64)
+    R = np.zeros((n, len(grid), 3 + ns))
+    fail = np.zeros(n, np.int64)
+    total, L, done = int(N), int(launch_steps) if launch_steps else int(N), 0
+    while done < total:
+        run.n0, run.steps = done, min(L, total - done)
+        rc = lib().oracle_indicator_window(C.byref(run), C.byref(win), n, ns, x.ctypes.data, states.ctypes.data,
+                                           code.ctypes.data, hstep.ctypes.data, grid.ctypes.data, len(grid),
+                                           R.ctypes.data, fail.ctypes.data, MATH[math], threads)
+        if rc != 0:
+            raise ValueError(f"oracle_indicator_window returned {rc}")
+        done += run.steps
+    finals = [reader.final(states[i, 24:].tobytes()) for i in range(n)]
+    return dict(R=R, fail=fail, x=x, states=states, code=code, hstep=hstep, finals=finals)
 
 
 def oracle_shadow(sys, x0, N, *, d0, tau=1, seed=0, U0=None, math="portable", threads=0, launch_steps=None,

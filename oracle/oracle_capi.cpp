@@ -606,6 +606,208 @@ void ind_orbit(const cl_run& run, bool pair, int64_t i, int ns, double* xs, doub
     if (hstep) hstep[i] = h;
 }
 
+// ---- the indicator recorder, window kinds (src/Experiments/run_indicator_device.jl:62-91) ------------------------
+// Julia's x^n for n = 1..4 (Base.Math power by squaring with the error terms): x, x x, (x x) x, and for n = 4 the
+// square of the square with both product errors folded in.
+double jl_powi(double x, int n) {
+    if (n == 1) return x;
+    if (n == 2) return x * x;
+    if (n == 3) return x * x * x;
+    const double x2 = x * x, e2 = std::fma(x, x, -x2);
+    const double err = (x2 * 2) * e2;
+    const double x4 = x2 * x2, e4 = std::fma(x2, x2, -x4);
+    return x4 + (e4 + err);
+}
+// _wb (naff_reducer.jl:13-17): birkhoff_weight(min(j, N - j) / N, p) = exp(-1 / (t^p (1 - t)^p)), 0 at the ends
+template <int MM>
+double wb_weight(int64_t j, int64_t N, int p) {
+    const double t = static_cast<double>(std::min(j, N - j)) / static_cast<double>(N);
+    if (t <= 0.0 || t >= 1.0) return 0.0;
+    return Math<MM>::exp(-1.0 / (jl_powi(t, p) * jl_powi(1.0 - t, p)));
+}
+template <typename T> T fld(const uint8_t* b, int off) { T v; std::memcpy(&v, b + off, sizeof v); return v; }
+template <typename T> void fst(uint8_t* b, int off, T v) { std::memcpy(b + off, &v, sizeof v); }
+// _unit_scale (naff_reducer.jl:36-41)
+void unit_scale(double& re, double& im) {
+    const double m = jl_max(std::fabs(re), std::fabs(im));
+    int e = 0;
+    if (std::isfinite(m) && m > 0) {
+        e = static_cast<int>((bits_of(m) >> 52) & 0x7ff) - 1023;
+        e = std::min(1000, std::max(-1000, e));
+    }
+    const double sc = p_pow2(-e);
+    re = re * sc;
+    im = im * sc;
+}
+// _phase_inc (naff_reducer.jl:45-53): arg(z conj(zp)) by atan2, NaN if either sample is exactly 0
+template <int MM>
+double phase_inc(double pr, double pim, double zr, double zi) {
+    if ((pr == 0.0 && pim == 0.0) || (zr == 0.0 && zi == 0.0)) return std::numeric_limits<double>::quiet_NaN();
+    double wr = pr, wi = -pim;
+    double rr = zr * wr - zi * wi, ri = zr * wi + zi * wr;
+    const double sm = jl_max(std::fabs(rr), std::fabs(ri));
+    if (!(sm > 1e-280 && sm < 1e280)) {
+        unit_scale(zr, zi);
+        unit_scale(pr, pim);
+        wr = pr; wi = -pim;
+        rr = zr * wr - zi * wi;
+        ri = zr * wi + zi * wr;
+    }
+    return Math<MM>::atan2(ri, rr);
+}
+int64_t window_reader_bytes(const cl_window& w) {
+    return w.kind == CL_WIN_PHASE_ADVANCE ? 64 * static_cast<int64_t>(w.n_windows) + 32
+                                          : 16 + static_cast<int64_t>(w.n_windows) * (16 + 40 * w.n_observables);
+}
+// reducer_step of WeightedPhaseAdvance (naff_reducer.jl:194-207) on WPAState{Float64, H}
+template <int MM>
+void wpa_step(const cl_window& w, uint8_t* st, int64_t n, const double* x) {
+    const int H = w.n_windows, tail = 64 * H;
+    if (fld<int8_t>(st, tail + 30) != 0) return;
+    const int kind = w.obs_kind[0], ia = w.obs_a[0] - 1, ib = w.obs_b[0];
+    const double s1 = x[ia], s2 = kind == CL_OBS_PLANAR ? x[ib - 1] : (ib == 0 ? 0.0 : x[ib - 1]);
+    if (!(std::isfinite(s1) && std::isfinite(s2))) {
+        fst<int64_t>(st, tail + 16, n);
+        fst<int8_t>(st, tail + 30, 1);
+        return;
+    }
+    const int32_t s = fld<int32_t>(st, tail + 24);
+    const int32_t h1 = s < 2147483647 ? s + 1 : s;
+    if (s == 0) {
+        fst(st, tail, s1); fst(st, tail + 8, s2); fst<int64_t>(st, tail + 16, n); fst<int32_t>(st, tail + 24, h1);
+        return;
+    }
+    const double p1 = fld<double>(st, tail), p2 = fld<double>(st, tail + 8);
+    const double pi_ = 3.141592653589793;   // _pi(one(Float64))
+    const double d = kind == CL_OBS_PLANAR ? phase_inc<MM>(p1, p2, s1, s2) : (s1 - p1) + (2 * pi_) * (s2 - p2);
+    const int64_t j = s - 1;
+    int64_t maxwin = 0;
+    for (int h = 0; h < H; ++h) maxwin = std::max<int64_t>(maxwin, w.window[h]);
+    for (int h = 0; h < H; ++h) {   // _advance (:176-186), _accumulate (:66)
+        const int64_t N = w.window[h];
+        if (j >= 2 * N) continue;
+        const int off = 64 * h + (j < N ? 0 : 32);
+        const double wt = wb_weight<MM>(j < N ? j : j - N, N, w.birkhoff_order);
+        if (wt == 0.0) continue;
+        const CS A = cs_add(CS{fld<double>(st, off), fld<double>(st, off + 8)}, wt * d);
+        const CS B = cs_add(CS{fld<double>(st, off + 16), fld<double>(st, off + 24)}, wt);
+        fst(st, off, A.s); fst(st, off + 8, A.c); fst(st, off + 16, B.s); fst(st, off + 24, B.c);
+    }
+    const int16_t nw = fld<int16_t>(st, tail + 28);
+    const bool flagged = kind == CL_OBS_PLANAR && std::fabs(d) > (9.0 * pi_) / 10.0 && s <= 2 * maxwin && nw < 32767;
+    fst(st, tail, s1); fst(st, tail + 8, s2); fst<int64_t>(st, tail + 16, n); fst<int32_t>(st, tail + 24, h1);
+    if (flagged) fst<int16_t>(st, tail + 28, static_cast<int16_t>(nw + 1));
+}
+// the observables of a Birkhoff reader (wbirkhoff.jl:51-56; IndCoordinate, run_indicator_chain.jl:23)
+template <int MM>
+double wb_observable(const cl_window& w, int k, const double* x) {
+    const int ia = w.obs_a[k] - 1, ib = w.obs_b[k];
+    switch (w.obs_kind[k]) {
+        case CL_OBS_COS: return Math<MM>::cos(static_cast<double>(ib) * x[ia]);
+        case CL_OBS_SIN: return Math<MM>::sin(static_cast<double>(ib) * x[ia]);
+        case CL_OBS_LIFTED: return x[ia] + (2 * 3.141592653589793) * x[ib - 1];
+        default: return x[ia];
+    }
+}
+// reducer_step of WeightedBirkhoff (wbirkhoff_reducer.jl:72-84) on WBState{Float64, H, K}
+template <int MM>
+void wb_step(const cl_window& w, uint8_t* st, int64_t n, const double* x) {
+    const int H = w.n_windows, K = w.n_observables, hb = 16 + 40 * K, tail = H * hb;
+    if (fld<int16_t>(st, tail + 12) != 0) return;
+    int64_t maxwin = 0;
+    for (int h = 0; h < H; ++h) maxwin = std::max<int64_t>(maxwin, w.window[h]);
+    const int32_t hand = fld<int32_t>(st, tail + 8);
+    if (static_cast<int64_t>(hand) >= 2 * maxwin) {
+        fst<int64_t>(st, tail, n);
+        if (hand < 2147483647) fst<int32_t>(st, tail + 8, hand + 1);
+        return;
+    }
+    double v[CL_MAX_OBSERVABLES];
+    int bad = 0;
+    for (int k = 0; k < K; ++k) {
+        v[k] = wb_observable<MM>(w, k, x);
+        if (bad == 0 && !std::isfinite(v[k])) bad = k + 1;
+    }
+    if (bad) {
+        fst<int64_t>(st, tail, n);
+        fst<int16_t>(st, tail + 12, static_cast<int16_t>(bad));
+        return;
+    }
+    const int64_t j = hand;
+    for (int h = 0; h < H; ++h) {   // _wb_advance (:56-62), _wb_sample (wbirkhoff.jl:86-90)
+        const int64_t N = w.window[h];
+        if (j >= 2 * N) continue;
+        const int i = j >= N ? 1 : 0;
+        const double wt = wb_weight<MM>(j - i * N, N, w.birkhoff_order);
+        const int off = h * hb;
+        if (i == 0 && wt != 0.0) {
+            const CS B = cs_add(CS{fld<double>(st, off), fld<double>(st, off + 8)}, wt);
+            fst(st, off, B.s); fst(st, off + 8, B.c);
+        }
+        for (int k = 0; k < K; ++k) {
+            const int c = off + 16 + 40 * k;
+            fst(st, c + 32, jl_max(fld<double>(st, c + 32), std::fabs(v[k])));
+            if (wt == 0.0) continue;
+            const int ai = c + 16 * i;
+            const CS A = cs_add(CS{fld<double>(st, ai), fld<double>(st, ai + 8)}, wt * v[k]);
+            fst(st, ai, A.s); fst(st, ai + 8, A.c);
+        }
+    }
+    fst<int64_t>(st, tail, n);
+    fst<int32_t>(st, tail + 8, j < 2147483647 ? static_cast<int32_t>(j + 1) : hand);
+}
+// _ind_window_kernel! (run_indicator_device.jl:62-91) for one orbit over one launch window
+template <int MM>
+void win_orbit(const cl_run& run, const cl_window& w, int64_t i, int ns, double* xs, uint8_t* sts, int8_t* code,
+               int64_t* hstep, const int64_t* grid, int n_grid, double* R, int64_t* fail, int64_t n0, int64_t steps) {
+    if (!(n0 == 0 || code[i] == STATUS_OK)) return;
+    const int s = run.s, ncol = 3 + ns;
+    const int64_t rb = window_reader_bytes(w), sb = 24 + rb;
+    double* x = xs + i * s;
+    uint8_t* st = sts + i * sb;
+    double mon[3];
+    if (n0 == 0) { std::memset(st, 0, sb); mon[0] = mon[1] = mon[2] = 0.0; }
+    else std::memcpy(mon, st, 24);
+    uint8_t* rs = st + 24;
+    int g = 0;
+    while (g < n_grid && grid[g] <= n0) ++g;
+    int ghi = g - 1;
+    while (ghi + 1 < n_grid && grid[ghi + 1] <= n0 + steps) ++ghi;
+    double* Ri = R + i * static_cast<int64_t>(ncol) * n_grid;
+    int64_t n = n0, h = n0;
+    int8_t c = STATUS_OK;
+    for (int64_t hh = 0; hh < steps / run.tau; ++hh) {
+        double W[2] = {1.0, 0.0}, Wn[2], M[4];
+        for (int t = 0; t < run.tau; ++t) {
+            rec_map<MM>(run, x, M);
+            fused_product(M, W, Wn, 2, 2, 1);
+            W[0] = Wn[0]; W[1] = Wn[1];
+        }
+        const int64_t nn = n + run.tau;
+        c = status_of(x, s, W, 2);
+        if (c == STATUS_OK) {
+            rec_monitor<MM>(run, x, mon);
+            if (w.kind == CL_WIN_PHASE_ADVANCE) wpa_step<MM>(w, rs, nn, x);
+            else wb_step<MM>(w, rs, nn, x);
+            const bool failed = w.kind == CL_WIN_PHASE_ADVANCE ? fld<int8_t>(rs, 64 * w.n_windows + 30) != 0
+                                                               : fld<int16_t>(rs, static_cast<int>(rb) - 4) != 0;
+            if (failed) c = STATUS_REDUCER;
+        }
+        h = nn;
+        if (c != STATUS_OK) { fail[i] = (g <= ghi ? g : ghi + 1) + 1; break; }
+        n = nn;
+        if (g <= ghi && n == grid[g]) {
+            double* row = Ri + static_cast<int64_t>(g) * ncol;
+            row[0] = mon[0]; row[1] = mon[1]; row[2] = mon[2];
+            for (int j = 0; j < ns; ++j) row[3 + j] = x[j];
+            ++g;
+        }
+    }
+    std::memcpy(st, mon, 24);
+    code[i] = c;
+    if (hstep) hstep[i] = h;
+}
+
 }  // namespace
 
 extern "C" {
@@ -672,6 +874,14 @@ void oracle_sincos(int32_t mode, const double* x, double* s, double* c, int64_t 
 
 void oracle_log(int32_t mode, const double* x, double* y, int64_t n) {
     for (int64_t i = 0; i < n; ++i) y[i] = mode == MATH_LIBM ? std::log(x[i]) : p_log(x[i]);
+}
+
+void oracle_exp(int32_t mode, const double* x, double* y, int64_t n) {
+    for (int64_t i = 0; i < n; ++i) y[i] = mode == MATH_LIBM ? std::exp(x[i]) : p_exp(x[i]);
+}
+
+void oracle_atan2(int32_t mode, const double* y, const double* x, double* a, int64_t n) {
+    for (int64_t i = 0; i < n; ++i) a[i] = mode == MATH_LIBM ? std::atan2(y[i], x[i]) : p_atan2(y[i], x[i]);
 }
 
 void oracle_fused_product(const double* A, const double* B, double* C, int32_t m, int32_t p, int32_t nn) {
@@ -848,6 +1058,37 @@ int oracle_advance(const cl_system* sys, int64_t n, const double* x0, double* ou
             const int64_t lo = next.fetch_add(16);
             if (lo >= n) return;
             for (int64_t i = lo; i < std::min<int64_t>(lo + 16, n); ++i) orbit(i);
+        }
+    };
+    std::vector<std::thread> pool;
+    for (int t = 1; t < nt; ++t) pool.emplace_back(worker);
+    worker();
+    for (auto& th : pool) th.join();
+    return 0;
+}
+
+// The window kinds on the CPU: one window [run.n0, run.n0 + steps) of n orbits, buffers in place (see the C ABI's
+// cl_b200_indicator_window_device).
+int oracle_indicator_window(const cl_run* run, const cl_window* win, int64_t n, int32_t ns, double* x, void* states,
+                            int8_t* code, int64_t* hstep, const int64_t* grid, int32_t n_grid, double* R,
+                            int64_t* fail, int32_t math_mode, int32_t threads) {
+    const int64_t steps = run->steps > 0 ? run->steps : run->N - run->n0;
+    if (run->tau <= 0 || steps % run->tau != 0 || run->n0 + steps > run->N || ns < 0 || ns > run->s) return CL_EINVAL;
+    const int hw = static_cast<int>(std::max(1u, std::thread::hardware_concurrency()));
+    const int nt = static_cast<int>(std::min<int64_t>(threads > 0 ? threads : hw, std::max<int64_t>(n, 1)));
+    std::atomic<int64_t> next{0};
+    auto worker = [&]() {
+        for (;;) {
+            const int64_t lo = next.fetch_add(16);
+            if (lo >= n) return;
+            for (int64_t i = lo; i < std::min<int64_t>(lo + 16, n); ++i) {
+                if (math_mode == MATH_LIBM)
+                    win_orbit<MATH_LIBM>(*run, *win, i, ns, x, static_cast<uint8_t*>(states), code, hstep, grid, n_grid,
+                                         R, fail, run->n0, steps);
+                else
+                    win_orbit<MATH_PORTABLE>(*run, *win, i, ns, x, static_cast<uint8_t*>(states), code, hstep, grid,
+                                             n_grid, R, fail, run->n0, steps);
+            }
         }
     };
     std::vector<std::thread> pool;

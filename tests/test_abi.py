@@ -40,6 +40,7 @@ int main(void){
          sizeof(cl_buffers), sizeof(cl_prov), sizeof(cl_probe));
   printf("%zu %zu %zu %zu\n", offsetof(cl_run, sys), offsetof(cl_run, frames), offsetof(cl_run, orbit_base),
          offsetof(cl_system, A));
+  printf("%zu %zu %zu\n", sizeof(cl_window), offsetof(cl_window, window), offsetof(cl_window, obs_b));
   return 0; }
 '''
     import tempfile
@@ -55,6 +56,8 @@ int main(void){
     offs = [int(v) for v in lines[1].split()]
     assert offs == [_abi.cl_run.sys.offset, _abi.cl_run.frames.offset, _abi.cl_run.orbit_base.offset,
                     _abi.cl_system.A.offset]
+    assert [int(v) for v in lines[2].split()] == [C.sizeof(_abi.cl_window), _abi.cl_window.window.offset,
+                                                  _abi.cl_window.obs_b.offset]
 
 
 def _run_from_key(key: str) -> _abi.cl_run:
