@@ -34,8 +34,8 @@ Multi-GPU: orbits are independent, so N ranks run N shards of the same size with
   shadow    the two-trajectory estimator on the coupled-map workload's orbits (65536 x 1e5, tau = 10, d0 = 1e-8);
   record    the study recorder: the wrapped standard map K = 6, 4096 orbits x 1e5 steps, QRSpectrum(MGS), tau = 1,
             100 log-spaced grid rows;
-  advance   advance_ensemble(KahanLi(8), Henon-Heiles, tau = 0.05): 65536 starts on the E = 1/8 section x 2e4 steps,
-            states only;
+  advance   advance_ensemble(KahanLi(8), Henon-Heiles, tau = 0.05): 1048576 starts on the E = 1/8 section x 1250
+            steps, states only;
   indicators the indicator recorder's tangent kind: the chain FLI, MEGNO, SALI with the monitor on the wrapped
             standard map K = 6, 4096 orbits x 1e5 steps, tau = 1, 100 log-spaced grid rows.
 """
@@ -351,20 +351,7 @@ def main() -> None:
     h2d = x0_h.nbytes + 2 * W0h.nbytes
     d2h = res[0].x.nbytes + sum(r_.W.nbytes + r_.states.nbytes + r_.code.nbytes + r_.hstep.nbytes for r_ in res)
 
-    # FP64 peak: cuBLAS DGEMM (the library FP64 rate on this GPU), burst
-    a = torch.randn(8192, 8192, dtype=torch.float64, device=dev)
-    torch.matmul(a, a)
-    torch.cuda.synchronize(dev)
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    best = 1e30
-    for _ in range(3):
-        e0.record()
-        torch.matmul(a, a)
-        e1.record()
-        e1.synchronize()
-        best = min(best, e0.elapsed_time(e1))
-    fp64_peak = 2 * 8192 ** 3 / (best / 1e3) / 1e12
-    del a
+    fp64_peak = _dgemm_peak(torch, dev)
 
     fl = flops_per_orbit_step(TAU, mixed=True)
     fl64 = flops_per_orbit_step(TAU, mixed=False)
@@ -745,7 +732,24 @@ def workload_mlp(args):
           clocks=sampler.summary(), gpu_launches=int(n_fwd))
 
 
-def _host_call_workload(args, metric, unit, units_per_call, call, config, cpu, dtype="f64"):
+def _dgemm_peak(torch, dev) -> float:
+    """FP64 peak: cuBLAS DGEMM 8192^3 (the library FP64 rate on this GPU), best of three bursts, TFLOP/s."""
+    a = torch.randn(8192, 8192, dtype=torch.float64, device=dev)
+    torch.matmul(a, a)
+    torch.cuda.synchronize(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    best = 1e30
+    for _ in range(3):
+        e0.record()
+        torch.matmul(a, a)
+        e1.record()
+        e1.synchronize()
+        best = min(best, e0.elapsed_time(e1))
+    del a
+    return 2 * 8192 ** 3 / (best / 1e3) / 1e12
+
+
+def _host_call_workload(args, metric, unit, units_per_call, call, config, cpu, dtype="f64", roofline=None):
     """Steps of the public host entry point: `value` from the device events around its launches (inputs resident),
     `e2e` from the wall clock around the whole call (copies in and out included)."""
     torch, dev, L = _setup()
@@ -764,9 +768,10 @@ def _host_call_workload(args, metric, unit, units_per_call, call, config, cpu, d
     launches = L.cl_b200_launch_count() - l0
     value = units_per_call / (np.mean(gpu) / 1e3)
     e2e = units_per_call / np.mean(wall)
+    extra = {} if roofline is None else dict(roofline=roofline(value, torch, dev))
     _line(metric, value, unit, args, gpu, config, dtype=dtype,
           e2e=dict(value=e2e, unit=unit, h2d_bytes_per_step=int(h2d), d2h_bytes_per_step=int(d2h)),
-          cpu_baseline=None if args.no_cpu else cpu(), clocks=sampler.summary(), gpu_launches=int(launches))
+          cpu_baseline=None if args.no_cpu else cpu(), clocks=sampler.summary(), gpu_launches=int(launches), **extra)
 
 
 def workload_shadow(args):
@@ -903,7 +908,8 @@ def workload_advance(args):
     from chaos_b200.systems import IntegratorMap, random_energy_starts
     import ctypes as C_
     torch, dev, L = _setup()
-    n, N, tau = args.orbits or 65536, args.N if args.N != N_STEPS else 20_000, 0.05
+    n = args.orbits or 1_048_576
+    N, tau = args.N if args.N != N_STEPS else max(1, 1_310_720_000 // n), 0.05
     m, flow = KahanLi(8), HenonHeilesFlow()
     x0 = np.ascontiguousarray(random_energy_starts(0.125, n, SEED))
     cs = IntegratorMap(m, flow, tau).to_cl()
@@ -926,10 +932,31 @@ def workload_advance(args):
         O.oracle_advance(m, flow, x0[:4096], tau, 2000, threads=threads)
         return dict(value=4096 * 2000 / (time.perf_counter() - t), unit="orbit-steps/s", cores=threads, kind="port",
                     sample="4096 orbits x 2000 steps (oracle, all host threads)")
+    # FP64 operations per step of advance_n (no contraction: every multiply and add is its own operation): the
+    # pending-kick sum per stage, a drift (t = c dt, q += t p: 5), a kick (t = pend dt, the force 7, p -= t F: 12)
+    drifts = sum(1 for c in m.c if c != 0.0)
+    kicks, pend = 0, 0.0
+    for _ in range(2):                        # the second pass counts the steady state (the kick carried over)
+        kicks_pass = 0
+        for c, d in zip(m.c, m.d):
+            if c != 0.0:
+                if pend != 0.0:
+                    kicks_pass += 1
+                    pend = 0.0
+            pend += d
+        kicks = kicks_pass
+    ops = m.stages + 5 * drifts + 12 * kicks
+
+    def roofline(value, torch_, dev_):
+        peak = _dgemm_peak(torch_, dev_)
+        achieved = value * ops / 1e12
+        return dict(bound="fp64", achieved=achieved, peak=peak, unit="TFLOP/s", frac=achieved / peak, traffic=None,
+                    peak_source="cuBLAS DGEMM 8192^3 measured here (burst; an FMA counts 2, this kernel has none)",
+                    flops_per_orbit_step=ops, drifts=drifts, kicks=kicks)
     _host_call_workload(args, "orbit-steps/s (advance_ensemble, KahanLi(8) on the Henon-Heiles flow, states only)",
                         "orbit-steps/s", n * N, call,
                         dict(workload=f"advance-kahanli8-hh-{n}x{N:.0e}-dt0.05", orbits=n, N=N, tau=tau,
-                             stages=m.stages), cpu)
+                             stages=m.stages), cpu, roofline=roofline)
 
 
 def run_workload(args):
