@@ -13,7 +13,7 @@ using Chaoslab, StaticArrays
 using Chaoslab.Foundation: Foundation, NumericalHealthError
 using Chaoslab.Tangent: Tangent, STATUS_OK, STATUS_REDUCER
 using Chaoslab.Lyapunov: QRSpectrum, Benettin, CGS, MGS, RGS, HouseholderQR, AugmentedQR, GivensQR
-using Chaoslab.Indicators: SALI, GALI, MEGNO, FLI
+using Chaoslab.Indicators: SALI, GALI, MEGNO, FLI, RLI
 using Chaoslab.Systems: StandardMap, WrappedStandardMap, FroeschleMap, StandardMapChain, LinearSymplecticMap,
                         HenonHeilesFlow
 using Chaoslab.Integrators: IntegratorMap, Gauss
@@ -48,6 +48,15 @@ end
 struct ClProbe
     loadable::Int32; functional::Int32; compiles::Int32; sm::Int32
     free_bytes::Int64; total_bytes::Int64; sm_count::Int32; pad::Int32; device::NTuple{96, UInt8}
+end
+
+# The window kinds' reader (cl_window): kind 1 WeightedPhaseAdvance / 2 WeightedBirkhoff, the windows, the order,
+# the observables as (kind, a, b): 1 Planar(iq, ip), 2 LiftedAngle(iq, im), 3 Cos(i, k), 4 Sin(i, k),
+# 5 Lifted(iq, im), 6 IndCoordinate(i).
+struct ClWindow
+    kind::Int32; n_windows::Int32; n_observables::Int32; birkhoff_order::Int32
+    window::NTuple{4, Int64}
+    obs_kind::NTuple{8, Int32}; obs_a::NTuple{8, Int32}; obs_b::NTuple{8, Int32}
 end
 
 "A device call that failed; `code` is the library's return code (-2, -3, -4, -9)."
@@ -88,6 +97,7 @@ clred(::SALI) = ClReducer(3, 0, 0, 0, 0)
 clred(::GALI) = ClReducer(4, 0, 0, 0, 0)
 clred(r::MEGNO) = ClReducer(5, 0, r.replace, 0, 0)
 clred(r::FLI) = ClReducer(6, 0, r.replace, 0, 0)
+clred(r::RLI) = ClReducer(7, 0, r.replace, 0, 0)          # the pair kind of the indicator recorder only
 clred(r) = throw(ClB200Error(-3, "reducer $(typeof(r)) is not in the compiled menu"))
 
 const NOFRAME = ClFrame(0, 0, ntuple(_ -> ClReducer(0, 0, 0, 0, 0), 4))
