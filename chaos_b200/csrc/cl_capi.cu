@@ -207,7 +207,24 @@ void set_tuned_minb(const cl_run& r, int m) {
 }
 }  // namespace
 
+namespace {
+// The device's name, cached per device (cudaGetDeviceProperties costs milliseconds; the compute capability and SM
+// count come from cudaDeviceGetAttribute).
+std::mutex g_name_mu;
+std::string g_names[64];
+const char* device_name(int dev) {
+    std::lock_guard<std::mutex> g(g_name_mu);
+    if (dev < 0 || dev >= 64) return "";
+    if (g_names[dev].empty()) {
+        cudaDeviceProp p;
+        g_names[dev] = cudaGetDeviceProperties(&p, dev) == cudaSuccess ? std::string(p.name) : std::string("?");
+    }
+    return g_names[dev].c_str();
+}
+}  // namespace
+
 // Shared with the ensemble entry points (cl_ensemble_capi.cu).
+const char* capi_device_name(int dev) { return device_name(dev); }
 int capi_fail(int code, const std::string& msg) { return fail(code, msg); }
 int capi_map_cuda(cudaError_t e, const char* where) { return map_cuda(e, where); }
 int capi_validate(const cl_run& r) { return validate(r); }
@@ -299,6 +316,41 @@ int cl_b200_propagate_device(const cl_run* run, int64_t n_orbits, const cl_buffe
     return 0;
 }
 
+// The register budget of a run whose key the tuner has not seen: the compiled variants timed once on a sample of
+// the run's own start data (the first min(n, 65536) orbits, 20 handoffs), written into scratch outputs so the inputs
+// stay untouched, and the fastest kept for the key. Short runs (where the sample would cost more than ~2 % of the
+// run) and single-variant instances keep the first variant.
+static int auto_minb(const cl_run& run, const Instance* in, int64_t n, double* dx, double* const* dW0, cudaStream_t st) {
+    const int have = tuned_minb(run);
+    if (have) return have;
+    int variants = 0;
+    for (int m = 1; m <= 4; ++m) variants += (in->minb_mask >> (m - 1)) & 1u;
+    const int64_t ns = std::min<int64_t>(n, 65536);
+    const int64_t sample = 20 * static_cast<int64_t>(run.tau);
+    const double run_work = static_cast<double>(n) * static_cast<double>(run.N - run.n0);
+    const double tune_work = 2.0 * variants * static_cast<double>(ns) * static_cast<double>(sample);
+    if (variants < 2 || run.n0 != 0 || tune_work > 0.02 * run_work) return 0;
+    for (int f = 0; f < run.n_frames; ++f)
+        if (!dW0[f]) return 0;   // seeded frames: the tuner needs explicit start frames
+    DevBufs db;
+    cl_buffers dev;
+    std::memset(&dev, 0, sizeof dev);
+    dev.x0 = dx;
+    if (db.alloc(reinterpret_cast<void**>(&dev.x), sizeof(double) * ns * run.s) != cudaSuccess) return 0;
+    for (int f = 0; f < run.n_frames; ++f) {
+        const int64_t wb = sizeof(double) * ns * run.d * run.frames[f].k, sb = frame_bytes(run.frames[f]) * ns;
+        dev.W0[f] = dW0[f];
+        if (db.alloc(reinterpret_cast<void**>(&dev.W[f]), wb) != cudaSuccess ||
+            db.alloc(&dev.states[f], static_cast<size_t>(sb)) != cudaSuccess ||
+            db.alloc(reinterpret_cast<void**>(&dev.code[f]), ns) != cudaSuccess ||
+            db.alloc(reinterpret_cast<void**>(&dev.hstep[f]), sizeof(int64_t) * ns) != cudaSuccess)
+            return 0;
+    }
+    int32_t best = 0;
+    if (cl_b200_tune(&run, ns, &dev, 0, sample, st, &best) != 0) return 0;
+    return best;
+}
+
 int cl_b200_propagate(const cl_run* run, int64_t n, const cl_buffers* h, cl_prov* prov) {
     if (!run || !h) return fail(CL_EINVAL, "NULL argument");
     int v = validate(*run);
@@ -348,6 +400,7 @@ int cl_b200_propagate(const cl_run* run, int64_t n, const cl_buffers* h, cl_prov
     // start fresh, every later one carries the state in place.
     const int64_t total = run->N - run->n0;
     const int64_t L = run->steps > 0 ? run->steps : total;
+    const int minb = auto_minb(*run, in, n, dx, dW0, st);
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
@@ -372,7 +425,7 @@ int cl_b200_propagate(const cl_run* run, int64_t n, const cl_buffers* h, cl_prov
             a.code[f] = dcode[f];
             a.hstep[f] = dhs[f];
         }
-        e = in->fn(rr, a, nullptr, st, &info, tuned_minb(*run));
+        e = in->fn(rr, a, nullptr, st, &info, minb);
         g_launches.fetch_add(1);
         ++launches;
         if (e != cudaSuccess) { cudaEventDestroy(e0); cudaEventDestroy(e1); return map_cuda(e, "orbit kernel launch"); }
@@ -397,8 +450,7 @@ int cl_b200_propagate(const cl_run* run, int64_t n, const cl_buffers* h, cl_prov
         std::memset(prov, 0, sizeof *prov);
         int dev = 0;
         cudaGetDevice(&dev);
-        cudaDeviceProp p;
-        if (cudaGetDeviceProperties(&p, dev) == cudaSuccess) std::snprintf(prov->device, sizeof prov->device, "%s", p.name);
+        std::snprintf(prov->device, sizeof prov->device, "%s", device_name(dev));
         std::snprintf(prov->variant, sizeof prov->variant, "%s", in->key);
         prov->launch_steps = L;
         prov->launches = launches;
@@ -476,11 +528,14 @@ int cl_b200_probe(cl_probe* out) {
     if (e != cudaSuccess || count == 0) return fail(CL_ENODEVICE, "no CUDA device");
     int dev = 0;
     cudaGetDevice(&dev);
-    cudaDeviceProp p;
-    if ((e = cudaGetDeviceProperties(&p, dev)) != cudaSuccess) return map_cuda(e, "properties");
-    std::snprintf(out->device, sizeof out->device, "%s", p.name);
-    out->sm = p.major * 10 + p.minor;
-    out->sm_count = p.multiProcessorCount;
+    int major = 0, minor = 0, smc = 0;
+    if ((e = cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev)) != cudaSuccess ||
+        (e = cudaDeviceGetAttribute(&minor, cudaDevAttrComputeCapabilityMinor, dev)) != cudaSuccess ||
+        (e = cudaDeviceGetAttribute(&smc, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess)
+        return map_cuda(e, "properties");
+    std::snprintf(out->device, sizeof out->device, "%s", device_name(dev));
+    out->sm = major * 10 + minor;
+    out->sm_count = smc;
     size_t fr = 0, tot = 0;
     if (cudaMemGetInfo(&fr, &tot) == cudaSuccess) { out->free_bytes = fr; out->total_bytes = tot; }
     out->functional = 1;

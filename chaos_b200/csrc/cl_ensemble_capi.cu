@@ -16,6 +16,7 @@
 namespace cl {
 
 int capi_fail(int code, const std::string& msg);      // cl_capi.cu
+const char* capi_device_name(int dev);                // cl_capi.cu
 int capi_map_cuda(cudaError_t e, const char* where);  // cl_capi.cu
 int capi_validate(const cl_run& r);                   // cl_capi.cu
 int64_t capi_frame_bytes(const cl_frame& f);          // cl_capi.cu
@@ -274,8 +275,7 @@ int cl_b200_ensemble(const cl_ensemble_class* classes, int32_t n_classes, cl_pro
         prov->launches = n_classes;
         int dev = 0;
         cudaGetDevice(&dev);
-        cudaDeviceProp p;
-        if (cudaGetDeviceProperties(&p, dev) == cudaSuccess) std::snprintf(prov->device, sizeof prov->device, "%s", p.name);
+        std::snprintf(prov->device, sizeof prov->device, "%s", capi_device_name(dev));
         std::snprintf(prov->variant, sizeof prov->variant, "ensemble x%d", n_classes);
     }
     cudaEventDestroy(e0);
