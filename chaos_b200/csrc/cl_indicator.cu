@@ -14,8 +14,10 @@
 #include <cstring>
 #include <string>
 #include <type_traits>
+#include <vector>
 
 #include "../../include/chaoslab_b200.h"
+#include "cl_hostcall.cuh"
 #include "cl_monitor.cuh"
 #include "cl_registry.cuh"
 
@@ -356,69 +358,24 @@ int indicator_host(const cl_run* run, bool pair, int64_t n, int32_t ns, double* 
     if (ncol < 0 || ns > mult * run->s)
         return indicator_device(run, pair, n, ns, x, W, states, code, hstep, grid, n_grid, R, fail, nullptr);
     const int s = mult * run->s, dk = mult * run->d * run->frames[0].k;
-    const size_t xb = sizeof(double) * s * n, wb = sizeof(double) * dk * n, sb = cl_b200_indicator_state_bytes(run) * n;
-    const size_t gb = sizeof(int64_t) * n_grid, rb = sizeof(double) * ncol * n_grid * n, fb = sizeof(int64_t) * n;
-    void *dx = nullptr, *dw = nullptr, *ds = nullptr, *dc = nullptr, *dh = nullptr, *dg = nullptr, *dr = nullptr, *df = nullptr;
-    cudaStream_t st = nullptr;
-    cudaEvent_t e0 = nullptr, e1 = nullptr;
-    cudaError_t e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
-    if (e == cudaSuccess) e = cudaMalloc(&dx, xb);
-    if (e == cudaSuccess) e = cudaMalloc(&dw, wb);
-    if (e == cudaSuccess) e = cudaMalloc(&ds, sb);
-    if (e == cudaSuccess) e = cudaMalloc(&dc, n);
-    if (e == cudaSuccess) e = cudaMalloc(&dh, sizeof(int64_t) * n);
-    if (e == cudaSuccess) e = cudaMalloc(&dg, gb);
-    if (e == cudaSuccess) e = cudaMalloc(&dr, rb);
-    if (e == cudaSuccess) e = cudaMalloc(&df, fb);
-    if (e == cudaSuccess) e = cudaEventCreate(&e0);
-    if (e == cudaSuccess) e = cudaEventCreate(&e1);
-    int launches = 0;
-    if (e == cudaSuccess) {
-        cudaMemcpyAsync(dx, x, xb, cudaMemcpyHostToDevice, st);
-        cudaMemcpyAsync(dw, W, wb, cudaMemcpyHostToDevice, st);
-        cudaMemcpyAsync(ds, states, sb, cudaMemcpyHostToDevice, st);
-        cudaMemcpyAsync(dc, code, n, cudaMemcpyHostToDevice, st);
-        cudaMemcpyAsync(dg, grid, gb, cudaMemcpyHostToDevice, st);
-        cudaMemcpyAsync(dr, R, rb, cudaMemcpyHostToDevice, st);
-        cudaMemcpyAsync(df, fail, fb, cudaMemcpyHostToDevice, st);
-        cudaEventRecord(e0, st);
-        const int64_t L = run->steps > 0 ? run->steps : run->N - run->n0;
-        cl_run r = *run;
-        for (int64_t n0 = run->n0; n0 < run->N && rc == 0; n0 += L) {
-            r.n0 = n0;
-            r.steps = std::min<int64_t>(L, run->N - n0);
-            rc = indicator_device(&r, pair, n, ns, static_cast<double*>(dx), static_cast<double*>(dw), ds,
-                                  static_cast<int8_t*>(dc), static_cast<int64_t*>(dh), static_cast<int64_t*>(dg),
-                                  n_grid, static_cast<double*>(dr), static_cast<int64_t*>(df), st);
-            ++launches;
-        }
-        cudaEventRecord(e1, st);
-        if (rc == 0) {
-            cudaMemcpyAsync(x, dx, xb, cudaMemcpyDeviceToHost, st);
-            cudaMemcpyAsync(W, dw, wb, cudaMemcpyDeviceToHost, st);
-            cudaMemcpyAsync(states, ds, sb, cudaMemcpyDeviceToHost, st);
-            cudaMemcpyAsync(code, dc, n, cudaMemcpyDeviceToHost, st);
-            if (hstep) cudaMemcpyAsync(hstep, dh, sizeof(int64_t) * n, cudaMemcpyDeviceToHost, st);
-            cudaMemcpyAsync(R, dr, rb, cudaMemcpyDeviceToHost, st);
-            cudaMemcpyAsync(fail, df, fb, cudaMemcpyDeviceToHost, st);
-        }
-        e = cudaStreamSynchronize(st);
-    }
-    if (rc == 0 && e != cudaSuccess) rc = capi_map_cuda(e, "indicator");
-    if (rc == 0 && prov) {
-        std::memset(prov, 0, sizeof *prov);
-        float ms = 0.f;
-        cudaEventElapsedTime(&ms, e0, e1);
-        prov->gpu_ms = ms;
-        prov->launches = launches;
-        prov->launch_steps = run->steps > 0 ? run->steps : run->N - run->n0;
+    std::vector<HostArray> arr = {
+        {x, sizeof(double) * s * n, true, nullptr},
+        {W, sizeof(double) * dk * n, true, nullptr},
+        {states, static_cast<size_t>(cl_b200_indicator_state_bytes(run) * n), true, nullptr},
+        {code, static_cast<size_t>(n), true, nullptr},
+        {hstep, sizeof(int64_t) * n, true, nullptr},
+        {const_cast<int64_t*>(grid), sizeof(int64_t) * n_grid, false, nullptr},
+        {R, sizeof(double) * ncol * n_grid * n, true, nullptr},
+        {fail, sizeof(int64_t) * n, true, nullptr}};
+    const int r = host_windows(*run, arr, [&](const cl_run& w, cudaStream_t st) {
+        return indicator_device(&w, pair, n, ns, static_cast<double*>(arr[0].dev), static_cast<double*>(arr[1].dev),
+                                arr[2].dev, static_cast<int8_t*>(arr[3].dev), static_cast<int64_t*>(arr[4].dev),
+                                static_cast<int64_t*>(arr[5].dev), n_grid, static_cast<double*>(arr[6].dev),
+                                static_cast<int64_t*>(arr[7].dev), st);
+    }, prov, "indicator");
+    if (r == 0 && prov)
         std::snprintf(prov->variant, sizeof prov->variant, "indicator%s %d cols s%d", pair ? " pair" : "", ncol, s);
-    }
-    if (e0) cudaEventDestroy(e0);
-    if (e1) cudaEventDestroy(e1);
-    for (void* p : {dx, dw, ds, dc, dh, dg, dr, df}) cudaFree(p);
-    if (st) cudaStreamDestroy(st);
-    return rc;
+    return r;
 }
 
 }  // namespace

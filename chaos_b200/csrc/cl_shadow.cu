@@ -15,9 +15,11 @@
 #include <cstring>
 #include <string>
 #include <type_traits>
+#include <vector>
 
 #include "../../include/chaoslab_b200.h"
 #include "cl_gauss.cuh"
+#include "cl_hostcall.cuh"
 #include "cl_split.cuh"
 
 namespace cl {
@@ -358,67 +360,23 @@ static int shadow_host(const cl_run* run, int64_t n, const double* x0, const dou
     int rc = check_shadow(*run, d0, &fn);
     if (rc) return rc;
     const int S = run->s, D = run->d, ncol = 1 + 7 + S;
-    const size_t xb = sizeof(double) * S * n, ub = sizeof(double) * D * n, eb = static_cast<size_t>(cl_b200_shadow_bytes(S)) * n;
-    const size_t gb = grid ? sizeof(int64_t) * n_grid : 0, rb = grid ? sizeof(double) * ncol * n_grid * n : 0,
-                 fb = grid ? sizeof(int64_t) * n : 0;
-    double *dx = nullptr, *du = nullptr, *dr = nullptr;
-    int64_t *dg = nullptr, *df = nullptr;
-    void* de = nullptr;
-    cudaStream_t st = nullptr;
-    cudaError_t e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
-    if (e == cudaSuccess) e = cudaMalloc(reinterpret_cast<void**>(&dx), xb);
-    if (e == cudaSuccess && u0) e = cudaMalloc(reinterpret_cast<void**>(&du), ub);
-    if (e == cudaSuccess) e = cudaMalloc(&de, eb);
-    if (e == cudaSuccess && grid) e = cudaMalloc(reinterpret_cast<void**>(&dg), gb);
-    if (e == cudaSuccess && grid) e = cudaMalloc(reinterpret_cast<void**>(&dr), rb);
-    if (e == cudaSuccess && grid) e = cudaMalloc(reinterpret_cast<void**>(&df), fb);
-    cudaEvent_t e0 = nullptr, e1 = nullptr;
-    int launches = 0;
-    if (e == cudaSuccess) {
-        cudaMemcpyAsync(dx, x0, xb, cudaMemcpyHostToDevice, st);
-        if (u0) cudaMemcpyAsync(du, u0, ub, cudaMemcpyHostToDevice, st);
-        if (run->n0 > 0) cudaMemcpyAsync(de, ends, eb, cudaMemcpyHostToDevice, st);
-        if (grid) {
-            cudaMemcpyAsync(dg, grid, gb, cudaMemcpyHostToDevice, st);
-            cudaMemcpyAsync(dr, R, rb, cudaMemcpyHostToDevice, st);
-            cudaMemcpyAsync(df, fail, fb, cudaMemcpyHostToDevice, st);
-        }
-        cudaEventCreate(&e0);
-        cudaEventCreate(&e1);
-        cudaEventRecord(e0, st);
-        const int64_t L = run->steps > 0 ? run->steps : run->N - run->n0;
-        for (int64_t n0 = run->n0; n0 < run->N && e == cudaSuccess; n0 += L) {
-            const int64_t steps = std::min<int64_t>(L, run->N - n0);
-            e = fn(*run, shargs(*run, n, dx, du, de, d0, n0, steps),
-                   RecOut{reinterpret_cast<const i64*>(dg), n_grid, dr, reinterpret_cast<i64*>(df)}, st);
-            capi_count_launch();
-            ++launches;
-        }
-        cudaEventRecord(e1, st);
-        if (e == cudaSuccess) e = cudaMemcpyAsync(ends, de, eb, cudaMemcpyDeviceToHost, st);
-        if (e == cudaSuccess && grid) e = cudaMemcpyAsync(R, dr, rb, cudaMemcpyDeviceToHost, st);
-        if (e == cudaSuccess && grid) e = cudaMemcpyAsync(fail, df, fb, cudaMemcpyDeviceToHost, st);
-        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-    }
-    if (e != cudaSuccess) rc = capi_map_cuda(e, "two-trajectory");
-    if (rc == 0 && prov) {
-        std::memset(prov, 0, sizeof *prov);
-        float ms = 0.f;
-        cudaEventElapsedTime(&ms, e0, e1);
-        prov->gpu_ms = ms;
-        prov->launches = launches;
-        prov->launch_steps = run->steps > 0 ? run->steps : run->N - run->n0;
+    std::vector<HostArray> arr = {
+        {const_cast<double*>(x0), sizeof(double) * S * n, false, nullptr},
+        {const_cast<double*>(u0), sizeof(double) * D * n, false, nullptr},
+        {ends, static_cast<size_t>(cl_b200_shadow_bytes(S)) * n, true, nullptr},
+        {const_cast<int64_t*>(grid), grid ? sizeof(int64_t) * n_grid : 0, false, nullptr},
+        {grid ? R : nullptr, grid ? sizeof(double) * ncol * n_grid * n : 0, true, nullptr},
+        {grid ? fail : nullptr, grid ? sizeof(int64_t) * n : 0, true, nullptr}};
+    rc = host_windows(*run, arr, [&](const cl_run& w, cudaStream_t st) {
+        const cudaError_t e = fn(w, shargs(w, n, static_cast<double*>(arr[0].dev), static_cast<double*>(arr[1].dev),
+                                           arr[2].dev, d0, w.n0, w.steps),
+                                 RecOut{static_cast<const i64*>(arr[3].dev), n_grid, static_cast<double*>(arr[4].dev),
+                                        static_cast<i64*>(arr[5].dev)}, st);
+        capi_count_launch();
+        return e == cudaSuccess ? 0 : capi_map_cuda(e, "two-trajectory launch");
+    }, prov, "two-trajectory");
+    if (rc == 0 && prov)
         std::snprintf(prov->variant, sizeof prov->variant, "two-trajectory s%d d%d%s", S, D, grid ? " records" : "");
-    }
-    if (e0) cudaEventDestroy(e0);
-    if (e1) cudaEventDestroy(e1);
-    cudaFree(dx);
-    cudaFree(du);
-    cudaFree(de);
-    cudaFree(dg);
-    cudaFree(dr);
-    cudaFree(df);
-    if (st) cudaStreamDestroy(st);
     return rc;
 }
 

@@ -14,8 +14,10 @@
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <vector>
 
 #include "../../include/chaoslab_b200.h"
+#include "cl_hostcall.cuh"
 #include "cl_monitor.cuh"
 #include "cl_registry.cuh"
 
@@ -380,68 +382,25 @@ int cl_b200_indicator_window(const cl_run* run, const cl_window* win, int64_t n,
     rc = check_window(*run, win);
     if (rc) return rc;
     const int s = run->s, ncol = 3 + ns;
-    const size_t xb = sizeof(double) * s * n, sb = (24 + reader_bytes(*win)) * n;
-    const size_t gb = sizeof(int64_t) * n_grid, rb = sizeof(double) * ncol * n_grid * n, fb = sizeof(int64_t) * n;
-    void *dx = nullptr, *ds = nullptr, *dc = nullptr, *dh = nullptr, *dg = nullptr, *dr = nullptr, *df = nullptr;
-    cudaStream_t st = nullptr;
-    cudaEvent_t e0 = nullptr, e1 = nullptr;
-    cudaError_t e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
-    if (e == cudaSuccess) e = cudaMalloc(&dx, xb);
-    if (e == cudaSuccess) e = cudaMalloc(&ds, sb);
-    if (e == cudaSuccess) e = cudaMalloc(&dc, n);
-    if (e == cudaSuccess) e = cudaMalloc(&dh, sizeof(int64_t) * n);
-    if (e == cudaSuccess) e = cudaMalloc(&dg, gb);
-    if (e == cudaSuccess) e = cudaMalloc(&dr, rb);
-    if (e == cudaSuccess) e = cudaMalloc(&df, fb);
-    if (e == cudaSuccess) e = cudaEventCreate(&e0);
-    if (e == cudaSuccess) e = cudaEventCreate(&e1);
-    int launches = 0;
-    if (e == cudaSuccess) {
-        cudaMemcpyAsync(dx, x, xb, cudaMemcpyHostToDevice, st);
-        cudaMemcpyAsync(ds, states, sb, cudaMemcpyHostToDevice, st);
-        cudaMemcpyAsync(dc, code, n, cudaMemcpyHostToDevice, st);
-        cudaMemcpyAsync(dg, grid, gb, cudaMemcpyHostToDevice, st);
-        cudaMemcpyAsync(dr, R, rb, cudaMemcpyHostToDevice, st);
-        cudaMemcpyAsync(df, fail, fb, cudaMemcpyHostToDevice, st);
-        cudaEventRecord(e0, st);
-        const int64_t L = run->steps > 0 ? run->steps : run->N - run->n0;
-        cl_run r = *run;
-        for (int64_t n0 = run->n0; n0 < run->N && rc == 0; n0 += L) {
-            r.n0 = n0;
-            r.steps = std::min<int64_t>(L, run->N - n0);
-            rc = window_device(&r, win, n, ns, static_cast<double*>(dx), ds, static_cast<int8_t*>(dc),
-                               static_cast<int64_t*>(dh), static_cast<int64_t*>(dg), n_grid, static_cast<double*>(dr),
-                               static_cast<int64_t*>(df), st);
-            ++launches;
-        }
-        cudaEventRecord(e1, st);
-        if (rc == 0) {
-            cudaMemcpyAsync(x, dx, xb, cudaMemcpyDeviceToHost, st);
-            cudaMemcpyAsync(states, ds, sb, cudaMemcpyDeviceToHost, st);
-            cudaMemcpyAsync(code, dc, n, cudaMemcpyDeviceToHost, st);
-            if (hstep) cudaMemcpyAsync(hstep, dh, sizeof(int64_t) * n, cudaMemcpyDeviceToHost, st);
-            cudaMemcpyAsync(R, dr, rb, cudaMemcpyDeviceToHost, st);
-            cudaMemcpyAsync(fail, df, fb, cudaMemcpyDeviceToHost, st);
-        }
-        e = cudaStreamSynchronize(st);
-    }
-    if (rc == 0 && e != cudaSuccess) rc = capi_map_cuda(e, "window");
-    if (rc == 0 && prov) {
-        std::memset(prov, 0, sizeof *prov);
-        float ms = 0.f;
-        cudaEventElapsedTime(&ms, e0, e1);
-        prov->gpu_ms = ms;
-        prov->launches = launches;
-        prov->launch_steps = run->steps > 0 ? run->steps : run->N - run->n0;
+    std::vector<HostArray> arr = {
+        {x, sizeof(double) * s * n, true, nullptr},
+        {states, static_cast<size_t>((24 + reader_bytes(*win)) * n), true, nullptr},
+        {code, static_cast<size_t>(n), true, nullptr},
+        {hstep, sizeof(int64_t) * n, true, nullptr},
+        {const_cast<int64_t*>(grid), sizeof(int64_t) * n_grid, false, nullptr},
+        {R, sizeof(double) * ncol * n_grid * n, true, nullptr},
+        {fail, sizeof(int64_t) * n, true, nullptr}};
+    const int r = host_windows(*run, arr, [&](const cl_run& w, cudaStream_t st) {
+        return window_device(&w, win, n, ns, static_cast<double*>(arr[0].dev), arr[1].dev,
+                             static_cast<int8_t*>(arr[2].dev), static_cast<int64_t*>(arr[3].dev),
+                             static_cast<int64_t*>(arr[4].dev), n_grid, static_cast<double*>(arr[5].dev),
+                             static_cast<int64_t*>(arr[6].dev), st);
+    }, prov, "window");
+    if (r == 0 && prov)
         std::snprintf(prov->variant, sizeof prov->variant, "indicator window %s H%d K%d",
                       win->kind == CL_WIN_PHASE_ADVANCE ? "phase-advance" : "birkhoff", win->n_windows,
                       win->n_observables);
-    }
-    if (e0) cudaEventDestroy(e0);
-    if (e1) cudaEventDestroy(e1);
-    for (void* p : {dx, ds, dc, dh, dg, dr, df}) cudaFree(p);
-    if (st) cudaStreamDestroy(st);
-    return rc;
+    return r;
 }
 
 }  // extern "C"
