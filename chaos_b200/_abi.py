@@ -221,6 +221,10 @@ def declare(lib: C.CDLL) -> C.CDLL:
     lib.cl_b200_advance_ensemble.argtypes = [P(cl_system), C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64,
                                              C.c_int64, P(cl_prov)]
     lib.cl_b200_advance_ensemble.restype = C.c_int
+    lib.cl_b200_variants.argtypes = [P(cl_run)]
+    lib.cl_b200_variants.restype = C.c_int32
+    lib.cl_b200_set_variant.argtypes = [P(cl_run), C.c_int32]
+    lib.cl_b200_set_variant.restype = C.c_int
     lib.cl_b200_indicator_columns.argtypes = [P(cl_run), C.c_int32]
     lib.cl_b200_indicator_columns.restype = C.c_int32
     lib.cl_b200_indicator_state_bytes.argtypes = [P(cl_run)]
@@ -277,4 +281,5 @@ EXPORTS = ("cl_b200_propagate", "cl_b200_propagate_device", "cl_b200_check", "cl
            "cl_b200_indicator_state_bytes", "cl_b200_indicator_device", "cl_b200_indicator",
            "cl_b200_advance_ensemble_device", "cl_b200_advance_ensemble", "cl_b200_indicator_pair_columns",
            "cl_b200_indicator_pair_device", "cl_b200_indicator_pair", "cl_b200_window_state_bytes",
-           "cl_b200_indicator_window_device", "cl_b200_indicator_window")
+           "cl_b200_indicator_window_device", "cl_b200_indicator_window", "cl_b200_variants",
+           "cl_b200_set_variant")

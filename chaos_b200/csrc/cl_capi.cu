@@ -519,6 +519,24 @@ int cl_b200_tune(const cl_run* run, int64_t n_orbits, const cl_buffers* dev, int
     return 0;
 }
 
+int32_t cl_b200_variants(const cl_run* run) {
+    if (!run || validate(*run) != 0) return 0;
+    const Instance* in = find_instance(run_key(*run));
+    return in ? static_cast<int32_t>(in->minb_mask) : 0;
+}
+
+int cl_b200_set_variant(const cl_run* run, int32_t variant) {
+    if (!run) return fail(CL_EINVAL, "run is NULL");
+    const int v = validate(*run);
+    if (v) return v;
+    const Instance* in = lookup(*run);
+    if (!in) return CL_EUNSUPPORTED;
+    if (variant != 0 && !(variant >= 1 && variant <= 4 && (in->minb_mask >> (variant - 1)) & 1u))
+        return fail(CL_EINVAL, "variant not compiled for this instance");
+    set_tuned_minb(*run, variant);
+    return 0;
+}
+
 int cl_b200_probe(cl_probe* out) {
     if (!out) return fail(CL_EINVAL, "NULL argument");
     std::memset(out, 0, sizeof *out);

@@ -12,9 +12,7 @@
 //     (Julia runs OpenBLAS there); the CPU oracle restates the same order.
 //   `forward` reruns the same core on the same point (advance_n, :149-158): it gives the same bits, so the step
 //     computes it once.
-// The mixed kernels keep the fixed point in Float64 and solve the tangent system in Float32 through its block
-// structure: with dY_i = [P_i; Q_i] and J_i = [[0, I], [-H_i, 0]], Q eliminates to a 6 x 6 system
-// (I + h^2 (A^2)_il H_l) P = I_top + h (A 1) I_bot.
+// The mixed kernels run the same Float64 step (fixed point and tangent solve) and keep only the frames in Float32.
 #pragma once
 
 #include "cl_math.cuh"

@@ -247,7 +247,7 @@ __device__ __forceinline__ T window_Gw(const T* R0) {
     for (int l = 1; l < K * K; ++l) m = mx(m, static_cast<T>(fabs(R0[l])));
     // T(1e100) is Inf and T(1e-100) is 0 in Float32, so the rescale never fires there (as in the reference).
     bool rescale = false;
-    if (sizeof(T) == 8) rescale = (m > T(1e100) || m < T(1e-100)) && isfin(m) && m > T(0);
+    if constexpr (sizeof(T) == 8) rescale = (m > T(1e100) || m < T(1e-100)) && isfin(m) && m > T(0);
 #pragma unroll
     for (int l = 0; l < K * K; ++l) R[l] = rescale ? dv(R0[l], m) : R0[l];
     T Ri[K * K];

@@ -202,11 +202,17 @@ CL_API int cl_b200_propagate(const cl_run* run, int64_t n_orbits, const cl_buffe
 CL_API int cl_b200_propagate_device(const cl_run* run, int64_t n_orbits, const cl_buffers* dev, int32_t soa, void* stream);
 
 /* Autotune the register budget of the instance that covers `run`: times each compiled variant (1, 2, 3 or 4
- * resident blocks of 128 threads per SM) over `sample_steps` steps of the n_orbits orbits on the device buffers
- * (whose contents are overwritten), remembers the fastest for this run's instance and tau in the process, and
- * writes it to *minb_out. Later propagate calls of the same instance use it. No reference counterpart. */
+ * resident blocks of 128 threads per SM) over `sample_steps` steps of the n_orbits
+ * orbits on the device buffers (whose contents are overwritten), remembers the fastest for this run's instance and
+ * tau in the process, and writes it to *minb_out. Later propagate calls of the same instance use it. No reference
+ * counterpart. */
 CL_API int cl_b200_tune(const cl_run* run, int64_t n_orbits, const cl_buffers* dev, int32_t soa, int64_t sample_steps,
                         void* stream, int32_t* minb_out);
+/* The compiled variants of the instance that covers `run` as a bit set (bit v - 1: variant v), 0 if none covers it;
+ * and pinning one of them for this run's instance and tau, as cl_b200_tune would (variant 0 clears the pin, the next
+ * public call then tunes again). CL_EINVAL for a variant the instance does not have. No reference counterpart. */
+CL_API int32_t cl_b200_variants(const cl_run* run);
+CL_API int cl_b200_set_variant(const cl_run* run, int32_t variant);
 
 /* 0 when a compiled kernel instance covers `run`, else CL_EINVAL (ill-formed run, message in cl_b200_last_error)
  * or CL_EUNSUPPORTED (well-formed, but not in the compiled menu: the caller falls back with reason 3). */

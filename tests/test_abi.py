@@ -137,3 +137,18 @@ def test_unsupported_is_reason_3():
     with pytest.raises(DeviceError) as e:   # mixed-precision RGS on Froeschle k = 3 is not in the compiled menu
         propagate(FroeschleMap(1, 1, 0), np.zeros((2, 4)), 10, k=3, reducers=(QRSpectrum(RGS()),), precision="mixed")
     assert e.value.reason == 3
+
+
+def test_variant_pinning_on_the_host():
+    from chaos_b200 import FrameSpec as FS, Gauss, HenonHeilesFlow, IntegratorMap, MGS, QRSpectrum, StandardMap
+    from chaos_b200.propagate import build_run
+    lb = lib()
+    g = build_run(IntegratorMap(Gauss(3), HenonHeilesFlow(), 0.01), 10, 1, [FS(2, (QRSpectrum(MGS()),))], "fp64", 0)
+    assert lb.cl_b200_variants(C.byref(g)) == 0b1              # one register budget compiled for the Gauss step
+    assert lb.cl_b200_set_variant(C.byref(g), 1) == 0 and lb.cl_b200_set_variant(C.byref(g), 0) == 0
+    assert lb.cl_b200_set_variant(C.byref(g), 3) == _abi.EINVAL
+    assert lb.cl_b200_set_variant(C.byref(g), 7) == _abi.EINVAL
+    s = build_run(StandardMap(1.0), 10, 1, [FS(2, (QRSpectrum(MGS()),))], "fp64", 0)
+    mask = lb.cl_b200_variants(C.byref(s))
+    assert mask != 0 and lb.cl_b200_set_variant(C.byref(s), 1 + int(np.log2(mask & -mask))) == 0
+    lb.cl_b200_set_variant(C.byref(s), 0)
