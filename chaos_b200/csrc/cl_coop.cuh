@@ -53,7 +53,7 @@ __device__ __forceinline__ T window_Gw_sm(const T* R0, T* ri) {
 #pragma unroll 1
     for (int l = 1; l < K * K; ++l) m = mx(m, static_cast<T>(fabs(R0[l])));
     bool rescale = false;
-    if (sizeof(T) == 8) rescale = (m > T(1e100) || m < T(1e-100)) && isfin(m) && m > T(0);
+    if constexpr (sizeof(T) == 8) rescale = (m > T(1e100) || m < T(1e-100)) && isfin(m) && m > T(0);
     T a = rv(R0, 0, rescale, m) * rv(R0, 0, rescale, m);
 #pragma unroll 1
     for (int l = 1; l < K * K; ++l) a = a + rv(R0, l, rescale, m) * rv(R0, l, rescale, m);
