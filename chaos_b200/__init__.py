@@ -12,9 +12,13 @@ from .reducers import (CGS, FLI, GALI, MEGNO, MGS, RGS, RLI, SALI, AugmentedQR, 
 from .advance import advance_ensemble
 from .record import pair_frame, pair_start, record, record_indicator_pairs, record_indicators, record_shadow
 from .shadow import propagate_shadow
-from .systems import (FroeschleMap, Gauss, HenonHeilesFlow, IntegratorMap, KahanLi, Leapfrog, LinearSymplecticMap,
-                      SplittingMethod, StandardMap, StandardMapChain, WrappedStandardMap, energy_start, lift,
-                      random_energy_starts, section_interval, torus_state)
+from .systems import (ABA864, ABAH864, PEFRL, SABA, SABAC, SBAB, SBABC, CalvoSanzSerna4, CorrectedMethod, ForestRuth,
+                      FroeschleMap, Gauss, HenonHeilesFlow, IntegratorMap, KahanLi, Leapfrog, LinearSymplecticMap,
+                      McLachlan2, Ruth3, SofroniouSpaletta10, SplittingMethod, StandardMap, StandardMapChain,
+                      SymplecticEuler, WrappedStandardMap, Yoshida, adjoint_method, coefficients, energy_start,
+                      force_evaluations, is_palindromic, isolated_force_evaluations, lift, method_name, method_source,
+                      nominal_order, random_energy_starts, section_interval, stage_count, suzuki_jump, table_digits,
+                      torus_state, triple_jump)
 
 __all__ = [
     "propagate", "propagate_frames", "propagate_shadow", "record", "record_indicators", "record_indicator_pairs", "pair_start", "pair_frame", "record_shadow", "advance_ensemble", "FrameSpec", "PropagationResult", "build_run", "bytes_per_orbit", "chunk_size",
@@ -22,5 +26,9 @@ __all__ = [
     "QRSpectrum", "CGS", "MGS", "RGS", "HouseholderQR", "AugmentedQR", "GivensQR", "Benettin", "SALI", "GALI",
     "MEGNO", "FLI", "RLI",
     "StandardMap", "WrappedStandardMap", "FroeschleMap", "StandardMapChain", "LinearSymplecticMap", "IntegratorMap",
-    "Gauss", "SplittingMethod", "KahanLi", "Leapfrog", "HenonHeilesFlow", "torus_state", "lift", "energy_start", "random_energy_starts", "section_interval",
+    "Gauss", "SplittingMethod", "CorrectedMethod", "SymplecticEuler", "Leapfrog", "McLachlan2", "Ruth3", "ForestRuth",
+    "triple_jump", "suzuki_jump", "PEFRL", "CalvoSanzSerna4", "Yoshida", "KahanLi", "SofroniouSpaletta10", "SABA",
+    "SBAB", "SABAC", "SBABC", "ABA864", "ABAH864", "adjoint_method", "coefficients", "stage_count", "nominal_order",
+    "is_palindromic", "table_digits", "force_evaluations", "isolated_force_evaluations", "method_name",
+    "method_source", "HenonHeilesFlow", "torus_state", "lift", "energy_start", "random_energy_starts", "section_interval",
 ]

@@ -10,7 +10,7 @@ import ctypes as C
 ABI_VERSION = 2
 MAX_FRAMES = 3
 MAX_REDUCERS = 4
-MAX_STAGES = 64
+MAX_STAGES = 128
 MAX_DIM = 16
 MAX_K = 8
 NOALLOC_MAX_CLASSES = 64

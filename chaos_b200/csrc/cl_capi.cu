@@ -114,7 +114,7 @@ int validate(const cl_run& r) {
     }
     if (r.sys.kind == CL_SYS_HH_SPLIT) {
         if (!(r.sys.n_stages >= 1 && r.sys.n_stages <= CL_MAX_STAGES))
-            return fail(CL_EUNSUPPORTED, "a splitting table needs 1..64 stages");
+            return fail(CL_EUNSUPPORTED, "a splitting table needs 1..CL_MAX_STAGES (128) stages");
         if (!(std::isfinite(r.sys.dt) && r.sys.dt != 0.0)) return fail(CL_EINVAL, "the step dt must be finite and nonzero");
         for (int i = 0; i < r.sys.n_stages; ++i)
             if (!(std::isfinite(r.sys.stage_c[i]) && std::isfinite(r.sys.stage_d[i])))

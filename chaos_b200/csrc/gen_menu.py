@@ -116,7 +116,7 @@ def menu():
     add("hh", SYS_HH, 4, 0, [(1, ["BEN"])])
     add("hh_mixed", SYS_HH, 4, 1, [(2, ["MEGNO0", "FLI0", "QR6"])])
     add("hh_mixed", SYS_HH, 4, 1, [(2, ["QR2"])])
-    # IntegratorMap(SplittingMethod(c, d), HenonHeilesFlow(), dt): any table of at most 64 stages
+    # IntegratorMap(SplittingMethod(c, d), HenonHeilesFlow(), dt): any table of at most CL_MAX_STAGES (128) stages
     for ch in (["MEGNO0", "FLI0", "QR6"], ["QR2"], ["QR6"], ["MEGNO1"], ["FLI1"], ["SALI"], ["GALI"]):
         add("split", SYS_SPLIT, 4, 0, [(2, ch)])
     for ch in (["QR2"], ["QR4"], ["GALI"]):

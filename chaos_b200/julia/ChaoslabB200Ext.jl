@@ -80,9 +80,9 @@ function clsys(m::LinearSymplecticMap{Float64, D}) where {D}
 end
 clsys(m::IntegratorMap{<:Gauss{Float64, 3}, HenonHeilesFlow, Float64}) =
     ClSystem(6, 0, 0, m.method.maxiter, 0, 0, 0, 0, 0, m.method.tol, m.tau, ZA, 0, 0, ZS, ZS)
-# a table method's weights travel as they are (Integrators/splitting.jl:16-21), at most 64 stages
+# a table method's weights travel as they are (Integrators/splitting.jl:16-21), at most 128 stages
 function clsys(m::IntegratorMap{<:SplittingMethod{Float64, K}, HenonHeilesFlow, Float64}) where {K}
-    K <= 64 || throw(ClB200Error(-3, "a splitting table of $K stages is above the compiled limit (64)"))
+    K <= 128 || throw(ClB200Error(-3, "a splitting table of $K stages is above the compiled limit (128)"))
     c, d = coefficients(m.method)
     return ClSystem(7, 0, 0, 0, 0, 0, 0, 0, 0, NaN, m.tau, ZA, K, 0, ntuple(i -> i <= K ? c[i] : 0.0, 64),
                     ntuple(i -> i <= K ? d[i] : 0.0, 64))

@@ -49,7 +49,7 @@ extern "C" {
 #define CL_MAX_REDUCERS 4
 #define CL_MAX_DIM 16
 #define CL_MAX_K 8
-#define CL_MAX_STAGES 64
+#define CL_MAX_STAGES 128
 #define CL_MAX_WINDOWS 4
 #define CL_MAX_OBSERVABLES 8
 
