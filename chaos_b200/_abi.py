@@ -184,6 +184,8 @@ def declare(lib: C.CDLL) -> C.CDLL:
     lib.cl_b200_version.restype = C.c_char_p
     lib.cl_b200_launch_count.argtypes = []
     lib.cl_b200_launch_count.restype = C.c_int64
+    lib.cl_b200_release_cache.argtypes = []
+    lib.cl_b200_release_cache.restype = C.c_int
     lib.cl_b200_ensemble_device.argtypes = [P(cl_ensemble_class), C.c_int32, C.c_void_p]
     lib.cl_b200_ensemble_device.restype = C.c_int
     lib.cl_b200_ensemble_device_noalloc.argtypes = [P(cl_ensemble_class), C.c_int32, C.c_void_p]
@@ -269,7 +271,7 @@ def declare(lib: C.CDLL) -> C.CDLL:
 
 # Every symbol include/chaoslab_b200.h declares (checked by the CPU tests against the built library).
 EXPORTS = ("cl_b200_propagate", "cl_b200_propagate_device", "cl_b200_check", "cl_b200_state_bytes",
-           "cl_b200_probe", "cl_b200_last_error", "cl_b200_version", "cl_b200_launch_count",
+           "cl_b200_probe", "cl_b200_last_error", "cl_b200_version", "cl_b200_launch_count", "cl_b200_release_cache",
            "cl_b200_menu_size", "cl_b200_menu_key", "cl_b200_ensemble_device", "cl_b200_ensemble",
            "cl_b200_ensemble_tune", "cl_b200_ensemble_graph_create", "cl_b200_ensemble_graph_launch",
            "cl_b200_ensemble_graph_destroy", "cl_b200_ensemble_device_noalloc", "cl_b200_tune",

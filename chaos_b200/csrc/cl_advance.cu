@@ -19,12 +19,12 @@
 
 #include "../../include/chaoslab_b200.h"
 #include "cl_gauss.cuh"
+#include "cl_hostcall.cuh"
 #include "cl_split.cuh"
 
 namespace cl {
 
 int capi_fail(int code, const std::string& msg);      // cl_capi.cu
-int capi_map_cuda(cudaError_t e, const char* where);  // cl_capi.cu
 void capi_count_launch();                             // cl_capi.cu
 
 namespace {
@@ -146,9 +146,9 @@ int cl_b200_advance_ensemble(const cl_system* sys, int64_t n, const double* x0, 
     cudaStream_t st = nullptr;
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     cudaError_t e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
-    if (e == cudaSuccess) e = cudaMalloc(&dx, sizeof(double) * 4 * csz);
-    if (e == cudaSuccess) e = cudaMalloc(&dout, sizeof(double) * 4 * csz);
-    if (e == cudaSuccess) e = cudaMalloc(&dok, csz);
+    if (e == cudaSuccess) e = pool_alloc(&dx, sizeof(double) * 4 * csz, st);
+    if (e == cudaSuccess) e = pool_alloc(&dout, sizeof(double) * 4 * csz, st);
+    if (e == cudaSuccess) e = pool_alloc(&dok, csz, st);
     if (e == cudaSuccess) e = cudaEventCreate(&e0);
     if (e == cudaSuccess) e = cudaEventCreate(&e1);
     float total_ms = 0.f;
@@ -162,6 +162,8 @@ int cl_b200_advance_ensemble(const cl_system* sys, int64_t n, const double* x0, 
         cudaEventRecord(e1, st);
         ++launches;
         if (rc) break;
+        touch_pages(out + 4 * lo, sizeof(double) * 4 * len);
+        touch_pages(ok + lo, static_cast<size_t>(len));
         cudaMemcpyAsync(out + 4 * lo, dout, sizeof(double) * 4 * len, cudaMemcpyDeviceToHost, st);
         cudaMemcpyAsync(ok + lo, dok, len, cudaMemcpyDeviceToHost, st);
         e = cudaStreamSynchronize(st);
@@ -183,7 +185,7 @@ int cl_b200_advance_ensemble(const cl_system* sys, int64_t n, const double* x0, 
     }
     if (e0) cudaEventDestroy(e0);
     if (e1) cudaEventDestroy(e1);
-    for (void* p : {dx, dout, dok}) cudaFree(p);
+    for (void* p : {dx, dout, dok}) pool_free(p, st);
     if (st) cudaStreamDestroy(st);
     return rc;
 }

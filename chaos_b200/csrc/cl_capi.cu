@@ -12,6 +12,7 @@
 #include <vector>
 
 #include "../../include/chaoslab_b200.h"
+#include "cl_hostcall.cuh"
 #include "cl_registry.cuh"
 
 namespace cl {
@@ -175,18 +176,94 @@ const Instance* lookup(const cl_run& r) {
     return in;
 }
 
+// The per-call device buffers of the host-buffer entry points, from the library's pool on the call's stream,
+// returned to it (in stream order) when the call ends.
 struct DevBufs {
+    cudaStream_t st;
     std::vector<void*> ptrs;
-    ~DevBufs() { for (void* p : ptrs) cudaFree(p); }
+    explicit DevBufs(cudaStream_t s) : st(s) {}
+    ~DevBufs() { for (void* p : ptrs) pool_free(p, st); }
     cudaError_t alloc(void** p, size_t bytes) {
-        if (bytes == 0) { *p = nullptr; return cudaSuccess; }
-        cudaError_t e = cudaMalloc(p, bytes);
-        if (e == cudaSuccess) ptrs.push_back(*p);
+        cudaError_t e = pool_alloc(p, bytes, st);
+        if (e == cudaSuccess && *p) ptrs.push_back(*p);
         return e;
     }
 };
 
+// One stream-ordered memory pool per device, owned by the library: a host-buffer call takes its device buffers
+// from it and gives them back when it ends, and the pool keeps the memory (release threshold: never) so the next
+// call of the same size allocates nothing from the driver -- a cudaMalloc / cudaFree pair per buffer cost more
+// than the copies of the 65536-orbit workload. cl_b200_release_cache returns the kept memory to the driver.
+std::mutex g_pool_mu;
+constexpr int kMaxDevices = 64;
+cudaMemPool_t g_pools[kMaxDevices] = {};
+int8_t g_pool_state[kMaxDevices] = {};   // 0 unset, 1 pool, -1 no pool support (plain cudaMalloc)
+
+int device_pool(int dev, cudaMemPool_t* out) {
+    *out = nullptr;
+    if (dev < 0 || dev >= kMaxDevices) return -1;
+    std::lock_guard<std::mutex> g(g_pool_mu);
+    if (g_pool_state[dev] == 0) {
+        int supported = 0;
+        cudaDeviceGetAttribute(&supported, cudaDevAttrMemoryPoolsSupported, dev);
+        g_pool_state[dev] = -1;
+        if (supported) {
+            cudaMemPoolProps props;
+            std::memset(&props, 0, sizeof props);
+            props.allocType = cudaMemAllocationTypePinned;
+            props.handleTypes = cudaMemHandleTypeNone;
+            props.location.type = cudaMemLocationTypeDevice;
+            props.location.id = dev;
+            cudaMemPool_t pool = nullptr;
+            if (cudaMemPoolCreate(&pool, &props) == cudaSuccess) {
+                uint64_t keep = ~uint64_t(0);
+                cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+                g_pools[dev] = pool;
+                g_pool_state[dev] = 1;
+            } else {
+                cudaGetLastError();
+            }
+        }
+    }
+    *out = g_pools[dev];
+    return g_pool_state[dev];
+}
+
+// Memory the device's pool keeps but no call uses: free for the library's next call, so the probe counts it free.
+size_t pool_idle_bytes(int dev) {
+    std::lock_guard<std::mutex> g(g_pool_mu);
+    if (dev < 0 || dev >= kMaxDevices || g_pool_state[dev] != 1) return 0;
+    uint64_t reserved = 0, used = 0;
+    if (cudaMemPoolGetAttribute(g_pools[dev], cudaMemPoolAttrReservedMemCurrent, &reserved) != cudaSuccess ||
+        cudaMemPoolGetAttribute(g_pools[dev], cudaMemPoolAttrUsedMemCurrent, &used) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return reserved > used ? static_cast<size_t>(reserved - used) : 0;
+}
+
 }  // namespace
+
+cudaError_t pool_alloc(void** p, size_t bytes, cudaStream_t st) {
+    *p = nullptr;
+    if (bytes == 0) return cudaSuccess;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    cudaMemPool_t pool;
+    if (device_pool(dev, &pool) == 1) return cudaMallocFromPoolAsync(p, bytes, pool, st);
+    return cudaMalloc(p, bytes);
+}
+
+void pool_free(void* p, cudaStream_t st) {
+    if (!p) return;
+    cudaPointerAttributes at;
+    int dev = 0;
+    if (cudaPointerGetAttributes(&at, p) == cudaSuccess) dev = at.device;
+    cudaMemPool_t pool;
+    if (device_pool(dev, &pool) == 1) cudaFreeAsync(p, st);
+    else cudaFree(p);
+}
 
 void register_instance(const char* key, LaunchFn fn, unsigned mask) { registry_list().push_back(Instance{key, fn, mask}); }
 
@@ -332,7 +409,7 @@ static int auto_minb(const cl_run& run, const Instance* in, int64_t n, double* d
     if (variants < 2 || run.n0 != 0 || tune_work > 0.02 * run_work) return 0;
     for (int f = 0; f < run.n_frames; ++f)
         if (!dW0[f]) return 0;   // seeded frames: the tuner needs explicit start frames
-    DevBufs db;
+    DevBufs db(st);
     cl_buffers dev;
     std::memset(&dev, 0, sizeof dev);
     dev.x0 = dx;
@@ -351,6 +428,17 @@ static int auto_minb(const cl_run& run, const Instance* in, int64_t n, double* d
     return best;
 }
 
+int cl_b200_release_cache(void) {
+    std::lock_guard<std::mutex> g(g_pool_mu);
+    for (int dev = 0; dev < kMaxDevices; ++dev) {
+        if (g_pool_state[dev] != 1) continue;
+        // every host-buffer call has synchronised its stream before returning, so no buffer is in flight
+        const cudaError_t e = cudaMemPoolTrimTo(g_pools[dev], 0);
+        if (e != cudaSuccess) return map_cuda(e, "release cache");
+    }
+    return 0;
+}
+
 int cl_b200_propagate(const cl_run* run, int64_t n, const cl_buffers* h, cl_prov* prov) {
     if (!run || !h) return fail(CL_EINVAL, "NULL argument");
     int v = validate(*run);
@@ -366,7 +454,7 @@ int cl_b200_propagate(const cl_run* run, int64_t n, const cl_buffers* h, cl_prov
     cudaError_t e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
     if (e != cudaSuccess) return map_cuda(e, "stream");
     struct StreamGuard { cudaStream_t s; ~StreamGuard() { cudaStreamDestroy(s); } } sg{st};
-    DevBufs db;
+    DevBufs db(st);
     double* dx = nullptr;
     double* dW[CL_MAX_FRAMES] = {};
     double* dW0[CL_MAX_FRAMES] = {};
@@ -431,6 +519,14 @@ int cl_b200_propagate(const cl_run* run, int64_t n, const cl_buffers* h, cl_prov
         if (e != cudaSuccess) { cudaEventDestroy(e0); cudaEventDestroy(e1); return map_cuda(e, "orbit kernel launch"); }
     }
     cudaEventRecord(e1, st);
+    // the inputs are staged (pageable copies return once the source is read), so the outputs' pages can be touched
+    touch_pages(h->x, sizeof(double) * n * s);
+    for (int f = 0; f < nf; ++f) {
+        touch_pages(h->W[f], sizeof(double) * n * d * run->frames[f].k);
+        touch_pages(h->states[f], static_cast<size_t>(frame_bytes(run->frames[f]) * n));
+        touch_pages(h->code[f], static_cast<size_t>(n));
+        if (h->hstep[f]) touch_pages(h->hstep[f], sizeof(int64_t) * n);
+    }
     if ((e = cudaMemcpyAsync(h->x, dx, sizeof(double) * n * s, cudaMemcpyDeviceToHost, st)) != cudaSuccess) return map_cuda(e, "D2H");
     for (int f = 0; f < nf; ++f) {
         const int k = run->frames[f].k;
@@ -555,7 +651,7 @@ int cl_b200_probe(cl_probe* out) {
     out->sm = major * 10 + minor;
     out->sm_count = smc;
     size_t fr = 0, tot = 0;
-    if (cudaMemGetInfo(&fr, &tot) == cudaSuccess) { out->free_bytes = fr; out->total_bytes = tot; }
+    if (cudaMemGetInfo(&fr, &tot) == cudaSuccess) { out->free_bytes = fr + pool_idle_bytes(dev); out->total_bytes = tot; }
     out->functional = 1;
     out->compiles = out->sm == 100 ? 1 : 0;   // the cubins are sm_100a only
     return out->compiles ? 0 : fail(CL_EUNSUPPORTED, "device is not sm_100 (B200)");

@@ -12,6 +12,7 @@
 
 #include "../../include/chaoslab_b200.h"
 #include "cl_coop.cuh"
+#include "cl_hostcall.cuh"
 
 namespace cl {
 
@@ -210,15 +211,14 @@ int cl_b200_ensemble(const cl_ensemble_class* classes, int32_t n_classes, cl_pro
     if (!classes || n_classes < 1) return capi_fail(CL_EINVAL, "no classes");
     std::vector<cl_ensemble_class> dc(classes, classes + n_classes);
     std::vector<void*> allocs;
-    auto alloc = [&](void** p, size_t b) -> cudaError_t {
-        if (!b) { *p = nullptr; return cudaSuccess; }
-        cudaError_t e = cudaMalloc(p, b);
-        if (e == cudaSuccess) allocs.push_back(*p);
-        return e;
-    };
-    auto cleanup = [&]() { for (void* p : allocs) cudaFree(p); };
     cudaStream_t st;
     cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+    auto alloc = [&](void** p, size_t b) -> cudaError_t {
+        cudaError_t e = pool_alloc(p, b, st);
+        if (e == cudaSuccess && *p) allocs.push_back(*p);
+        return e;
+    };
+    auto cleanup = [&]() { for (void* p : allocs) pool_free(p, st); };
     int rc = 0;
     for (int c = 0; c < n_classes && rc == 0; ++c) {
         ELaunchFn fn;
@@ -254,6 +254,15 @@ int cl_b200_ensemble(const cl_ensemble_class* classes, int32_t n_classes, cl_pro
         rc = cl_b200_ensemble_device(dc.data(), n_classes, st);
         cudaEventRecord(e1, st);
     }
+    for (int c = 0; c < n_classes && rc == 0; ++c) {   // outputs' first touch overlaps the kernels
+        const cl_ensemble_class& h = classes[c];
+        const int64_t n = h.n_orbits, dk = int64_t(h.run.d) * h.run.frames[0].k;
+        touch_pages(h.buf.x, static_cast<size_t>(8 * n * h.run.s));
+        touch_pages(h.buf.W[0], static_cast<size_t>(8 * n * dk));
+        touch_pages(h.buf.states[0], static_cast<size_t>(capi_frame_bytes(h.run.frames[0]) * n));
+        touch_pages(h.buf.code[0], static_cast<size_t>(n));
+        if (h.buf.hstep[0]) touch_pages(h.buf.hstep[0], static_cast<size_t>(8 * n));
+    }
     for (int c = 0; c < n_classes && rc == 0; ++c) {
         const cl_ensemble_class& h = classes[c];
         const cl_ensemble_class& d = dc[c];
@@ -280,8 +289,8 @@ int cl_b200_ensemble(const cl_ensemble_class* classes, int32_t n_classes, cl_pro
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
-    cudaStreamDestroy(st);
     cleanup();
+    cudaStreamDestroy(st);
     return rc;
 }
 

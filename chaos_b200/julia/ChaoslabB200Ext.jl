@@ -132,6 +132,12 @@ function Foundation.free_memory(::B200Device)
     ccall((:cl_b200_probe, libcl), Cint, (Ref{ClProbe},), p)
     return Int(p[].free_bytes)
 end
+# the device memory the library's pools keep between calls, back to the driver (as CUDA.reclaim() does for CUDA.jl)
+function reclaim()
+    rc = ccall((:cl_b200_release_cache, libcl), Cint, ())
+    rc == 0 || throw(ClB200Error(rc, last_error()))
+    return nothing
+end
 function Foundation.probe(::B200Device, ::Type{T}) where {T}
     p = Ref{ClProbe}()
     rc = ccall((:cl_b200_probe, libcl), Cint, (Ref{ClProbe},), p)

@@ -137,6 +137,14 @@ def probe() -> dict:
                 total_bytes=p.total_bytes)
 
 
+def release_cache() -> None:
+    """Return the device memory the library's pools keep between host-buffer calls to the driver
+    (`cl_b200_release_cache`, the counterpart of CUDA.jl's `CUDA.reclaim()`)."""
+    rc = lib().cl_b200_release_cache()
+    if rc != 0:
+        raise DeviceError(rc, last_error())
+
+
 def _ptr(a):
     return None if a is None else a.ctypes.data
 

@@ -233,6 +233,12 @@ CL_API const char* cl_b200_version(void);
 /* Number of orbit-kernel launches since the library was loaded (a device-launch counter for audits). */
 CL_API int64_t cl_b200_launch_count(void);
 
+/* The host-buffer entry points take their device buffers from a stream-ordered pool per device that the library
+ * owns and that keeps its memory between calls (a call of the same sizes as an earlier one allocates nothing from
+ * the driver). This returns the memory the pools keep to the driver; a later call grows them again. The
+ * counterpart of CUDA.jl's `CUDA.reclaim()` for the memory pool the reference's device runs allocate from. */
+CL_API int cl_b200_release_cache(void);
+
 /* ---- Batched uneven ensembles ------------------------------------------------------------------------------------
  * One class = orbits of one system kind and dimension with one frame and chain; every orbit may carry its own map
  * parameter K (K[i]), its own length N[i] (a multiple of tau) and an escape stop: at the first handoff where
