@@ -16,7 +16,7 @@ from .shadow import propagate_shadow
 from .systems import (ABA864, ABAH864, PEFRL, SABA, SABAC, SBAB, SBABC, CalvoSanzSerna4, CorrectedMethod, ForestRuth,
                       FroeschleMap, Gauss, HenonHeilesFlow, IntegratorMap, KahanLi, Leapfrog, LinearSymplecticMap,
                       McLachlan2, Ruth3, SofroniouSpaletta10, SplittingMethod, StandardMap, StandardMapChain,
-                      SymplecticEuler, WrappedStandardMap, Yoshida, adjoint_method, coefficients, energy_start,
+                      SymplecticEuler, WrappedFroeschleMap, WrappedStandardMap, WrappedStandardMapChain, Yoshida, adjoint_method, coefficients, energy_start,
                       force_evaluations, is_palindromic, isolated_force_evaluations, lift, method_name, method_source,
                       nominal_order, random_energy_starts, section_interval, stage_count, suzuki_jump, table_digits,
                       torus_state, triple_jump)
@@ -26,7 +26,8 @@ __all__ = [
     "probe", "release_cache", "NumericalHealthError", "DeviceError", "FALLBACK_REASONS",
     "QRSpectrum", "CGS", "MGS", "RGS", "HouseholderQR", "AugmentedQR", "GivensQR", "Benettin", "SALI", "GALI",
     "MEGNO", "FLI", "RLI",
-    "StandardMap", "WrappedStandardMap", "FroeschleMap", "StandardMapChain", "LinearSymplecticMap", "IntegratorMap",
+    "StandardMap", "WrappedStandardMap", "FroeschleMap", "WrappedFroeschleMap", "StandardMapChain",
+    "WrappedStandardMapChain", "LinearSymplecticMap", "IntegratorMap",
     "Gauss", "SplittingMethod", "CorrectedMethod", "SymplecticEuler", "Leapfrog", "McLachlan2", "Ruth3", "ForestRuth",
     "triple_jump", "suzuki_jump", "PEFRL", "CalvoSanzSerna4", "Yoshida", "KahanLi", "SofroniouSpaletta10", "SABA",
     "SBAB", "SABAC", "SBABC", "ABA864", "ABAH864", "adjoint_method", "coefficients", "stage_count", "nominal_order",

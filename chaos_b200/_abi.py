@@ -19,6 +19,7 @@ MAX_OBSERVABLES = 8
 
 # enum cl_system_kind
 SYS_STANDARD, SYS_WRAPPED_STANDARD, SYS_FROESCHLE, SYS_CHAIN, SYS_LINEAR, SYS_HH_GAUSS, SYS_HH_SPLIT = 1, 2, 3, 4, 5, 6, 7
+SYS_WRAPPED_FROESCHLE, SYS_WRAPPED_CHAIN = 8, 9
 # enum cl_reducer_kind
 RED_QR, RED_BENETTIN, RED_SALI, RED_GALI, RED_MEGNO, RED_FLI, RED_RLI = 1, 2, 3, 4, 5, 6, 7
 # enum cl_qr_alg

@@ -59,14 +59,17 @@ const char* red_token(const cl_reducer& r, char* buf) {
 int sys_dim(const cl_system& s, int d) {
     switch (s.kind) {
         case CL_SYS_STANDARD: case CL_SYS_WRAPPED_STANDARD: return 2;
-        case CL_SYS_FROESCHLE: case CL_SYS_HH_GAUSS: case CL_SYS_HH_SPLIT: return 4;
-        case CL_SYS_CHAIN: return 2 * s.n_sites;
+        case CL_SYS_FROESCHLE: case CL_SYS_HH_GAUSS: case CL_SYS_HH_SPLIT: case CL_SYS_WRAPPED_FROESCHLE: return 4;
+        case CL_SYS_CHAIN: case CL_SYS_WRAPPED_CHAIN: return 2 * s.n_sites;
         case CL_SYS_LINEAR: return d;
     }
     return -1;
 }
+// the wrapped maps carry one winding count per coordinate after the coordinates
 int sys_state_len(const cl_system& s, int d) {
-    return s.kind == CL_SYS_WRAPPED_STANDARD ? 4 : sys_dim(s, d);
+    const bool wrapped = s.kind == CL_SYS_WRAPPED_STANDARD || s.kind == CL_SYS_WRAPPED_FROESCHLE ||
+                         s.kind == CL_SYS_WRAPPED_CHAIN;
+    return wrapped ? 2 * sys_dim(s, d) : sys_dim(s, d);
 }
 
 int64_t state_bytes_of(const cl_reducer& r, int k) {
@@ -96,9 +99,10 @@ int validate(const cl_run& r) {
         return fail(CL_EINVAL, "launch window must be multiples of tau inside 0..N");
     const int d = sys_dim(r.sys, r.d);
     if (d < 0) return fail(CL_EINVAL, "unknown system kind");
-    if (r.sys.kind == CL_SYS_CHAIN && !(r.sys.n_sites >= 2 && r.sys.n_sites <= CL_MAX_DIM / 2))
+    const bool chain = r.sys.kind == CL_SYS_CHAIN || r.sys.kind == CL_SYS_WRAPPED_CHAIN;
+    if (chain && !(r.sys.n_sites >= 2 && r.sys.n_sites <= CL_MAX_DIM / 2))
         return fail(CL_EUNSUPPORTED, "StandardMapChain sites outside the compiled menu (2..8)");
-    if (r.sys.kind == CL_SYS_CHAIN && r.sys.ring && r.sys.n_sites < 3) return fail(CL_EINVAL, "a ring needs N >= 3");
+    if (chain && r.sys.ring && r.sys.n_sites < 3) return fail(CL_EINVAL, "a ring needs N >= 3");
     if (r.d != d) {
         std::snprintf(msg, sizeof msg, "d = %d does not match the system dimension %d", r.d, d);
         return fail(CL_EINVAL, msg);

@@ -1,0 +1,28 @@
+// Generated by chaos_b200/csrc/gen_menu.py (do not edit): compiled orbit-kernel instances, group "wfro_mixed".
+#include "cl_registry.cuh"
+
+namespace cl {
+namespace {
+
+cudaError_t L0(const cl_run& r, const KArgs& a, const double* A, cudaStream_t s, LaunchInfo* i, int m) {
+    return launch_instance<SysWrappedFroeschle, float, Frame<4, RQR<4>>, Frame<4, RGALI<true>>, NoFrame, 2, 1, 2, 3, 4>(r, a, A, s, i, m);
+}
+const Registrar R0("s8d4p1|k4:QR4|k4:GALI,SALI|", L0, minb_mask<1, 2, 3, 4>());
+
+cudaError_t L1(const cl_run& r, const KArgs& a, const double* A, cudaStream_t s, LaunchInfo* i, int m) {
+    return launch_instance<SysWrappedFroeschle, float, Frame<4, RQR<4>>, NoFrame, NoFrame, 1, 1>(r, a, A, s, i, m);
+}
+const Registrar R1("s8d4p1|k4:QR4|", L1, minb_mask<1>());
+
+cudaError_t L2(const cl_run& r, const KArgs& a, const double* A, cudaStream_t s, LaunchInfo* i, int m) {
+    return launch_instance<SysWrappedFroeschle, float, Frame<4, RGALI<true>>, NoFrame, NoFrame, 1, 1>(r, a, A, s, i, m);
+}
+const Registrar R2("s8d4p1|k4:GALI,SALI|", L2, minb_mask<1>());
+
+cudaError_t L3(const cl_run& r, const KArgs& a, const double* A, cudaStream_t s, LaunchInfo* i, int m) {
+    return launch_instance<SysWrappedFroeschle, float, Frame<2, RQR<2>>, NoFrame, NoFrame, 1, 1>(r, a, A, s, i, m);
+}
+const Registrar R3("s8d4p1|k2:QR2|", L3, minb_mask<1>());
+
+}  // namespace
+}  // namespace cl

@@ -36,6 +36,9 @@ template <> inline SysWrapped make_sys<SysWrapped>(const cl_run& r, const double
 template <> inline SysFroeschle make_sys<SysFroeschle>(const cl_run& r, const double*) {
     SysFroeschle s; s.nu = r.sys.nu; s.kappa = r.sys.kappa; s.mu = r.sys.mu; return s;
 }
+template <> inline SysWrappedFroeschle make_sys<SysWrappedFroeschle>(const cl_run& r, const double*) {
+    SysWrappedFroeschle s; s.nu = r.sys.nu; s.kappa = r.sys.kappa; s.mu = r.sys.mu; return s;
+}
 template <class Sys> struct SysMaker;
 template <int DD> struct SysMaker<SysLinear<DD>> {
     static SysLinear<DD> make(const cl_run& r, const double*) {
@@ -47,6 +50,11 @@ template <int DD> struct SysMaker<SysLinear<DD>> {
 template <int NS> struct SysMaker<SysChain<NS>> {
     static SysChain<NS> make(const cl_run& r, const double*) {
         SysChain<NS> s; s.K = r.sys.K; s.eps = r.sys.eps; s.ring = r.sys.ring; return s;
+    }
+};
+template <int NS> struct SysMaker<SysWrappedChain<NS>> {
+    static SysWrappedChain<NS> make(const cl_run& r, const double*) {
+        SysWrappedChain<NS> s; s.K = r.sys.K; s.eps = r.sys.eps; s.ring = r.sys.ring; return s;
     }
 };
 template <class Sys> struct SysMaker {

@@ -204,6 +204,85 @@ struct SysFroeschle {
     }
 };
 
+// ---- WrappedFroeschleMap (froeschle_map.jl:60-126) -----------------------------------------------------------------
+// State (x1, x2, p1, p2, c1, c2, c3, c4). The tangent is _f3_tangent at the UNREDUCED sums u = x + p (:108), the
+// forward map's sines at the reduced new positions (:84-92): six trigonometric arguments per step, not three.
+struct WFroJac { double x1, x2, b1, b2, s1, s2, c12, a, b, c; };
+struct WFroJacF { double x1, x2, b1, b2, s1, s2, c12; float a, b, c; };   // mixed: Float32 A
+
+struct SysWrappedFroeschle {
+    static constexpr int D = 4, S = 8;
+    using Jac = WFroJac;
+    template <typename R> using JacR = typename std::conditional<sizeof(R) == 8, WFroJac, WFroJacF>::type;
+    double nu, kappa, mu;
+    // positions reduced with their counts, then the forward map's Float64 sines (split evaluation, bit-identical
+    // to cl_sincos)
+    template <class JJ>
+    __device__ __forceinline__ void positions(double u1, double u2, JJ& J) const {
+        const double tp = 2 * jl_pi();
+        wrap_reduce(u1, tp, J.x1, J.b1);
+        wrap_reduce(u2, tp, J.x2, J.b2);
+        J.s1 = cl_sin_split(cl_reduce(J.x1));
+        J.s2 = cl_sin_split(cl_reduce(J.x2));
+        J.c12 = cl_cos_split(cl_reduce(J.x1 + J.x2));
+    }
+    __device__ __forceinline__ void jac(const double* z, WFroJac& J) const {
+        const double u1 = z[0] + z[2], u2 = z[1] + z[3];
+        const double t = mu * cl_sin_split(cl_reduce(u1 + u2));   // _abc (:35-39) at the unreduced sums
+        J.a = -nu * cl_cos_split(cl_reduce(u1)) - t;
+        J.b = -t;
+        J.c = -kappa * cl_cos_split(cl_reduce(u2)) - t;
+        positions(u1, u2, J);
+    }
+    __device__ __forceinline__ void jac(const double* z, WFroJacF& J) const {
+        const double u1 = z[0] + z[2], u2 = z[1] + z[3];
+        float s1f, c1f, s2f, c2f, s12f, c12f;
+        cl_sincos32(cl_reduce(u1), &s1f, &c1f);
+        cl_sincos32(cl_reduce(u2), &s2f, &c2f);
+        cl_sincos32(cl_reduce(u1 + u2), &s12f, &c12f);
+        const float t = static_cast<float>(mu) * s12f;
+        J.a = -static_cast<float>(nu) * c1f - t;
+        J.b = -t;
+        J.c = -static_cast<float>(kappa) * c2f - t;
+        positions(u1, u2, J);
+    }
+    template <int KK>
+    __device__ __forceinline__ void apply(const WFroJac& J, double* W) const {   // the dense fused product
+        const double o = 1.0, Z = 0.0;
+        const double M[16] = {o, Z, J.a, J.b, Z, o, J.b, J.c, o, Z, o + J.a, J.b, Z, o, J.b, o + J.c};
+        fused_dense<4, KK>(M, W);
+    }
+    template <int KK>
+    __device__ __forceinline__ void apply(const WFroJacF& J, float* W) const {   // [[I, I], [A, I + A]] by blocks
+#pragma unroll
+        for (int j = 0; j < KK; ++j) {
+            float* w = W + 4 * j;
+            const float t1 = w[0] + w[2], t2 = w[1] + w[3];
+            const float b1 = __fmaf_rn(J.a, t1, __fmaf_rn(J.b, t2, w[2]));
+            const float b2 = __fmaf_rn(J.b, t1, __fmaf_rn(J.c, t2, w[3]));
+            w[0] = t1; w[1] = t2; w[2] = b1; w[3] = b2;
+        }
+    }
+    // forward (:84-92) with _checked8 (:69-73): momenta reduced with their counts, m' = m + n + b, n' = n + a
+    template <class JJ>
+    __device__ __forceinline__ void forward(double* z, const JJ& J) const {
+        const double tp = 2 * jl_pi();
+        const double f = mu * (1.0 - J.c12);
+        double p1, a1, p2, a2;
+        wrap_reduce(z[2] - nu * J.s1 - f, tp, p1, a1);
+        wrap_reduce(z[3] - kappa * J.s2 - f, tp, p2, a2);
+        const double m1 = z[4] + z[6] + J.b1, m2 = z[5] + z[7] + J.b2, n1 = z[6] + a1, n2 = z[7] + a2;
+        const double lim = 0x1p53;
+        if (fabs(m1) < lim && fabs(m2) < lim && fabs(n1) < lim && fabs(n2) < lim) {
+            z[0] = J.x1; z[1] = J.x2; z[2] = p1; z[3] = p2; z[4] = m1; z[5] = m2; z[6] = n1; z[7] = n2;
+        } else {
+            const double nan = __longlong_as_double(0x7ff8000000000000LL);
+#pragma unroll
+            for (int i = 0; i < 8; ++i) z[i] = nan;
+        }
+    }
+};
+
 // ---- LinearSymplecticMap (linear_symplectic.jl): z' = A z (fused StaticArrays product), tangent A ----------------
 template <int DD>
 struct SysLinear {
@@ -351,6 +430,49 @@ struct SysChain {
     template <class JJ>
     __device__ __forceinline__ void forward(double* z, const JJ& J) const {
         if (ring) forward_impl<true>(z, J); else forward_impl<false>(z, J);
+    }
+};
+
+// ---- WrappedStandardMapChain (wrapped_standard_map_chain.jl): the chain on the torus with winding counts, state
+// (q_1..q_N, p_1..p_N, counts of q, counts of p). The band and the forces are those of the chain at the reduced
+// positions (W-E3, :63-67), so `jac` and `apply` are the chain's; only the forward step differs.
+template <int NS>
+struct SysWrappedChain : SysChain<NS> {
+    static constexpr int S = 4 * NS;
+    // forward (:117-124, W-E2): p~_j = p_j + F_j(q) reduced with count a_j, n_j' = n_j + a_j; q~_j = q_j + p_j'
+    // reduced with count b_j, m_j' = m_j + n_j' + b_j; _guard_counts (:101-107)
+    template <bool RING, class JJ>
+    __device__ __forceinline__ void forward_w(double* z, const JJ& J) const {
+        using B = SysChain<NS>;
+        const double tp = 2 * jl_pi();
+        double p[NS], nn[NS];
+#pragma unroll
+        for (int j = 0; j < NS; ++j) {
+            double s = 0.0;
+            if (B::template L<RING>(j) >= 0) s = s + J.sl[j];
+            if (B::template R<RING>(j) >= 0) s = s + J.sr[j];
+            double a;
+            wrap_reduce(z[NS + j] + (this->K * J.sq[j] + this->eps * s), tp, p[j], a);
+            nn[j] = z[3 * NS + j] + a;
+        }
+        bool ok = true;
+#pragma unroll
+        for (int j = 0; j < NS; ++j) {
+            double q, b;
+            wrap_reduce(z[j] + p[j], tp, q, b);
+            const double m = z[2 * NS + j] + nn[j] + b;
+            z[j] = q; z[NS + j] = p[j]; z[2 * NS + j] = m; z[3 * NS + j] = nn[j];
+            ok = ok && fabs(m) < 0x1p53 && fabs(nn[j]) < 0x1p53;
+        }
+        if (!ok) {
+            const double nan = __longlong_as_double(0x7ff8000000000000LL);
+#pragma unroll
+            for (int i = 0; i < S; ++i) z[i] = nan;
+        }
+    }
+    template <class JJ>
+    __device__ __forceinline__ void forward(double* z, const JJ& J) const {
+        if (this->ring) forward_w<true>(z, J); else forward_w<false>(z, J);
     }
 };
 

@@ -11,6 +11,7 @@ import os
 HERE = os.path.dirname(os.path.abspath(__file__))
 
 SYS_STANDARD, SYS_WRAPPED, SYS_FROESCHLE, SYS_CHAIN, SYS_LINEAR, SYS_HH, SYS_SPLIT = 1, 2, 3, 4, 5, 6, 7
+SYS_WRAPPED_FRO, SYS_WRAPPED_CHAIN = 8, 9
 QR = [f"QR{a}" for a in range(1, 7)]   # CGS, MGS, RGS, Householder, augmented, Givens
 
 
@@ -44,7 +45,8 @@ def red_type(tokens):
 def sys_type(kind, d):
     return {SYS_STANDARD: "SysStandard", SYS_WRAPPED: "SysWrapped", SYS_FROESCHLE: "SysFroeschle",
             SYS_CHAIN: f"SysChain<{d // 2}>", SYS_LINEAR: f"SysLinear<{d}>", SYS_HH: "SysGauss3HH",
-            SYS_SPLIT: "SysSplitHH"}[kind]
+            SYS_SPLIT: "SysSplitHH", SYS_WRAPPED_FRO: "SysWrappedFroeschle",
+            SYS_WRAPPED_CHAIN: f"SysWrappedChain<{d // 2}>"}[kind]
 
 
 def key(kind, d, prec, frames):
@@ -97,6 +99,19 @@ def menu():
         add("fro_mixed", SYS_FROESCHLE, 4, 1, [(4, ch)])
     for ch in (["QR2"], ["SALI"], ["MEGNO1"], ["MEGNO0", "SALI"]):
         add("fro_mixed", SYS_FROESCHLE, 4, 1, [(2, ch)])
+    # the same map on the torus with winding counts (the C2 ensemble's coordinates in [0, 2 pi)^4)
+    for ch in k1_chains[:3]:
+        add("wfro", SYS_WRAPPED_FRO, 4, 0, [(1, ch)])
+    for ch in (["QR2"], ["QR6"], ["SALI"], ["MEGNO1"], ["FLI1"], ["MEGNO0", "FLI0", "QR6"], ["MEGNO0", "SALI"]):
+        add("wfro", SYS_WRAPPED_FRO, 4, 0, [(2, ch)])
+    for ch in (["QR4"], ["QR2"], ["GALI"], ["GALI", "SALI"]):
+        add("wfro", SYS_WRAPPED_FRO, 4, 0, [(4, ch)])
+    for prec in (0, 1):
+        add("wfro" if prec == 0 else "wfro_mixed", SYS_WRAPPED_FRO, 4, prec, [(4, ["QR4"]), (4, ["GALI", "SALI"])],
+            minbs=(1, 2, 3) if prec == 0 else (1, 2, 3, 4))
+    for ch in (["QR4"], ["GALI", "SALI"]):
+        add("wfro_mixed", SYS_WRAPPED_FRO, 4, 1, [(4, ch)])
+    add("wfro_mixed", SYS_WRAPPED_FRO, 4, 1, [(2, ["QR2"])])
     # coupled standard-map lattices, N = 2..8 sites
     for N in range(2, 9):
         d = 2 * N
@@ -108,6 +123,13 @@ def menu():
             for ch in (["QR2"], ["SALI"], ["MEGNO1"]):
                 add(g, SYS_CHAIN, d, prec, [(2, ch)])
         add(g, SYS_CHAIN, d, 0, [(1, ["BEN"])])
+        # the lattice on the torus with winding counts
+        for prec in (0, 1):
+            for ch in (["QR2"], ["QR4"], ["GALI"]):
+                add("w" + g, SYS_WRAPPED_CHAIN, d, prec, [(kk, ch)])
+        for ch in (["QR2"], ["SALI"], ["MEGNO1"]):
+            add("w" + g, SYS_WRAPPED_CHAIN, d, 0, [(2, ch)])
+        add("w" + g, SYS_WRAPPED_CHAIN, d, 0, [(1, ["BEN"])])
     # IntegratorMap(Gauss(Float64, 3), HenonHeilesFlow(), dt)
     for ch in (["MEGNO0", "FLI0", "QR6"], ["QR2"], ["QR6"], ["MEGNO1"], ["FLI1"], ["SALI"], ["GALI"]):
         add("hh", SYS_HH, 4, 0, [(2, ch)])

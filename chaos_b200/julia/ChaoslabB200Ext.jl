@@ -15,7 +15,7 @@ using Chaoslab.Tangent: Tangent, STATUS_OK, STATUS_REDUCER
 using Chaoslab.Lyapunov: QRSpectrum, Benettin, CGS, MGS, RGS, HouseholderQR, AugmentedQR, GivensQR
 using Chaoslab.Indicators: SALI, GALI, MEGNO, FLI, RLI
 using Chaoslab.Systems: StandardMap, WrappedStandardMap, FroeschleMap, StandardMapChain, LinearSymplecticMap,
-                        HenonHeilesFlow
+                        HenonHeilesFlow, WrappedFroeschleMap, WrappedStandardMapChain
 using Chaoslab.Integrators: IntegratorMap, Gauss
 
 const libcl = get(ENV, "CHAOSLAB_B200_LIB", joinpath(@__DIR__, "libchaoslab_b200.so"))
@@ -26,7 +26,7 @@ struct ClSystem
     K::Float64; eps::Float64; nu::Float64; kappa::Float64; mu::Float64; gauss_tol::Float64; dt::Float64
     A::NTuple{256, Float64}
     n_stages::Int32; reserved::Int32
-    stage_c::NTuple{64, Float64}; stage_d::NTuple{64, Float64}
+    stage_c::NTuple{128, Float64}; stage_d::NTuple{128, Float64}
 end
 struct ClReducer
     kind::Int32; alg::Int32; replace::Int32; pad::Int32; orthogonality_tol::Float64
@@ -70,11 +70,14 @@ Foundation.is_device_lost(e::ClB200Error) = e.code == -9
 
 # ---- the menu: system and reducer records ----------------------------------------------------------------------
 const ZA = ntuple(_ -> 0.0, 256)
-const ZS = ntuple(_ -> 0.0, 64)
+const ZS = ntuple(_ -> 0.0, 128)
 clsys(m::StandardMap{Float64}) = ClSystem(1, 0, 0, 0, m.K, 0, 0, 0, 0, NaN, 0, ZA, 0, 0, ZS, ZS)
 clsys(m::WrappedStandardMap{Float64}) = ClSystem(2, 0, 0, 0, m.K, 0, 0, 0, 0, NaN, 0, ZA, 0, 0, ZS, ZS)
 clsys(m::FroeschleMap{Float64}) = ClSystem(3, 0, 0, 0, 0, 0, m.nu, m.kappa, m.mu, NaN, 0, ZA, 0, 0, ZS, ZS)
 clsys(m::StandardMapChain{Float64}) = ClSystem(4, m.N, m.ring, 0, m.K, m.eps, 0, 0, 0, NaN, 0, ZA, 0, 0, ZS, ZS)
+clsys(m::WrappedFroeschleMap{Float64}) = ClSystem(8, 0, 0, 0, 0, 0, m.nu, m.kappa, m.mu, NaN, 0, ZA, 0, 0, ZS, ZS)
+clsys(m::WrappedStandardMapChain{Float64}) =
+    ClSystem(9, m.chain.N, m.chain.ring, 0, m.chain.K, m.chain.eps, 0, 0, 0, NaN, 0, ZA, 0, 0, ZS, ZS)
 function clsys(m::LinearSymplecticMap{Float64, D}) where {D}
     return ClSystem(5, 0, 0, 0, 0, 0, 0, 0, 0, NaN, 0, ntuple(l -> l <= D * D ? m.A[l] : 0.0, 256), 0, 0, ZS, ZS)
 end
@@ -84,8 +87,8 @@ clsys(m::IntegratorMap{<:Gauss{Float64, 3}, HenonHeilesFlow, Float64}) =
 function clsys(m::IntegratorMap{<:SplittingMethod{Float64, K}, HenonHeilesFlow, Float64}) where {K}
     K <= 128 || throw(ClB200Error(-3, "a splitting table of $K stages is above the compiled limit (128)"))
     c, d = coefficients(m.method)
-    return ClSystem(7, 0, 0, 0, 0, 0, 0, 0, 0, NaN, m.tau, ZA, K, 0, ntuple(i -> i <= K ? c[i] : 0.0, 64),
-                    ntuple(i -> i <= K ? d[i] : 0.0, 64))
+    return ClSystem(7, 0, 0, 0, 0, 0, 0, 0, 0, NaN, m.tau, ZA, K, 0, ntuple(i -> i <= K ? c[i] : 0.0, 128),
+                    ntuple(i -> i <= K ? d[i] : 0.0, 128))
 end
 clsys(m) = throw(ClB200Error(-3, "system $(typeof(m)) is not in the compiled menu"))
 

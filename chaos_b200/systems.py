@@ -68,6 +68,31 @@ class FroeschleMap(System):
         return _abi.cl_system(kind=_abi.SYS_FROESCHLE, nu=float(self.nu), kappa=float(self.kappa), mu=float(self.mu))
 
 
+@dataclass(frozen=True)
+class WrappedFroeschleMap(System):
+    """WrappedFroeschleMap(nu, kappa, mu), src/Systems/froeschle_map.jl:60-126: the Froeschle map on the torus with
+    winding counts, state (x1, x2, p1, p2, c1, c2, c3, c4), coordinates in [0, 2 pi) and exact integer counts; the
+    tangent is evaluated at the unreduced sums x + p."""
+    nu: float
+    kappa: float
+    mu: float
+    d: int = field(default=4, init=False)
+    s: int = field(default=8, init=False)
+    name: str = field(default="WrappedFroeschleMap", init=False)
+
+    def to_cl(self):
+        return _abi.cl_system(kind=_abi.SYS_WRAPPED_FROESCHLE, nu=float(self.nu), kappa=float(self.kappa),
+                              mu=float(self.mu))
+
+    def torus_state(self, z) -> np.ndarray:
+        """torus_state(sys, z) (:110-114): each coordinate of the lifted z reduced into [0, 2 pi) with its count."""
+        return _torus(z, 4)
+
+    def lift(self, s) -> np.ndarray:
+        """lift(sys, s) (:121-124): z_j + 2 pi c_j."""
+        return _lift(s, 4)
+
+
 class StandardMapChain(System):
     """StandardMapChain(N, K, eps; boundary=:open), src/Systems/standard_map_chain.jl:11-31, state
     (q_1..q_N, p_1..p_N), banded tangent (chain_tangent.jl). The compiled menu covers N in 2..8."""
@@ -88,6 +113,35 @@ class StandardMapChain(System):
 
     def __repr__(self):
         return f"StandardMapChain({self.N}, {self.K}, {self.eps}, boundary={'ring' if self.ring else 'open'})"
+
+
+class WrappedStandardMapChain(StandardMapChain):
+    """WrappedStandardMapChain(N, K, eps; boundary=:open), src/Systems/wrapped_standard_map_chain.jl: the chain on
+    the torus with winding counts, state (q_1..q_N, p_1..p_N, counts of q, counts of p), d = 2N, s = 4N."""
+
+    def __init__(self, N: int, K: float, eps: float, boundary: str = "open"):
+        super().__init__(N, K, eps, boundary)
+        self.s = 4 * self.N
+        self.name = "WrappedStandardMapChain"
+
+    def to_cl(self):
+        return _abi.cl_system(kind=_abi.SYS_WRAPPED_CHAIN, n_sites=self.N, ring=int(self.ring), K=self.K,
+                              eps=self.eps)
+
+    def torus_state(self, z) -> np.ndarray:
+        """torus_state(sys, z) (:75-83): (reduced coordinates, counts)."""
+        if len(z) != self.d:
+            raise ValueError("lifted state length is not 2N for this chain")
+        return _torus(z, self.d)
+
+    def lift(self, s) -> np.ndarray:
+        """lift(sys, s) (:90-94)."""
+        if len(s) != self.s:
+            raise ValueError("wrapped state length is not 4N for this chain")
+        return _lift(s, self.d)
+
+    def __repr__(self):
+        return f"WrappedStandardMapChain({self.N}, {self.K}, {self.eps}, boundary={'ring' if self.ring else 'open'})"
 
 
 class LinearSymplecticMap(System):
@@ -684,18 +738,32 @@ def _reduce(u: float, tp: float):
     return float(r), float(a)
 
 
-def torus_state(z) -> np.ndarray:
-    """torus_state((X, P)) -> (x, p, m, n), src/Systems/wrapped_standard_map.jl:63-69."""
+def _torus(z, d: int) -> np.ndarray:
+    """The d coordinates of z each reduced into [0, 2 pi) (_reduce), followed by their d counts."""
     tp = 2 * _PI
-    x, m = _reduce(float(z[0]), tp)
-    p, n = _reduce(float(z[1]), tp)
-    return np.array([x, p, m, n])
+    r = [_reduce(float(v), tp) for v in z[:d]]
+    return np.array([v for v, _ in r] + [c for _, c in r])
 
 
-def lift(s) -> np.ndarray:
-    """lift((x, p, m, n)) -> (x + 2 pi m, p + 2 pi n), src/Systems/wrapped_standard_map.jl:77-80."""
+def _lift(s, d: int) -> np.ndarray:
     tp = 2 * _PI
-    return np.array([s[0] + tp * s[2], s[1] + tp * s[3]])
+    return np.array([s[j] + tp * s[d + j] for j in range(d)])
+
+
+def torus_state(*args) -> np.ndarray:
+    """torus_state((X, P)) -> (x, p, m, n), src/Systems/wrapped_standard_map.jl:63-69; torus_state(sys, z) for the
+    wrapped Froeschle map and the wrapped chain."""
+    if len(args) == 2:
+        return args[0].torus_state(args[1])
+    return _torus(args[0], 2)
+
+
+def lift(*args) -> np.ndarray:
+    """lift((x, p, m, n)) -> (x + 2 pi m, p + 2 pi n), src/Systems/wrapped_standard_map.jl:77-80; lift(sys, s) for
+    the wrapped Froeschle map and the wrapped chain."""
+    if len(args) == 2:
+        return args[0].lift(args[1])
+    return _lift(args[0], 2)
 
 
 def _hh_u(q2: float) -> float:  # Equation 7: V(0, q2), src/Systems/henon_heiles.jl:4

@@ -62,9 +62,13 @@ enum cl_system_kind {
     CL_SYS_LINEAR = 5,           /* LinearSymplecticMap(A), d = s                    linear_symplectic.jl:1-40   */
     CL_SYS_HH_GAUSS = 6,         /* IntegratorMap(Gauss(Float64, 3; tol), HenonHeilesFlow(), dt), d = s = 4
                                     integrator_map.jl:12-23, gauss.jl:49-192, flow_models.jl:101-103        */
-    CL_SYS_HH_SPLIT = 7          /* IntegratorMap(SplittingMethod(c, d), HenonHeilesFlow(), dt), d = s = 4: a table
+    CL_SYS_HH_SPLIT = 7,         /* IntegratorMap(SplittingMethod(c, d), HenonHeilesFlow(), dt), d = s = 4: a table
                                     method (drift c_i dt, then kick d_i dt), forward with merged kicks, tangent the
                                     product of the stage Jacobians; stepper.jl:27-48,108-118, flow_core.jl:59-72  */
+    CL_SYS_WRAPPED_FROESCHLE = 8, /* WrappedFroeschleMap(nu, kappa, mu), d = 4, s = 8: (x1, x2, p1, p2) in [0, 2pi)
+                                    and four exact winding counts; froeschle_map.jl:60-126                     */
+    CL_SYS_WRAPPED_CHAIN = 9     /* WrappedStandardMapChain(N, K, eps), d = 2N, s = 4N: (q, p) in [0, 2pi) and 2N
+                                    exact winding counts; wrapped_standard_map_chain.jl:1-154                  */
 };
 
 /* Reducers (src/Lyapunov, src/Indicators). */
@@ -105,8 +109,8 @@ enum cl_status {
 
 typedef struct cl_system {
     int32_t kind;          /* enum cl_system_kind                                                       */
-    int32_t n_sites;       /* CL_SYS_CHAIN: N in 2..8                                                   */
-    int32_t ring;          /* CL_SYS_CHAIN: 1 for boundary = :ring (N >= 3), 0 for :open                */
+    int32_t n_sites;       /* CL_SYS_CHAIN, CL_SYS_WRAPPED_CHAIN: N in 2..8                             */
+    int32_t ring;          /* the chains: 1 for boundary = :ring (N >= 3), 0 for :open                  */
     int32_t gauss_maxiter; /* CL_SYS_HH_GAUSS: fixed-point iteration cap (reference default 50)         */
     double K;              /* standard maps and chain                                                   */
     double eps;            /* chain coupling                                                            */

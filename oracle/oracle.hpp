@@ -165,6 +165,31 @@ struct Systems {
         const double p2 = z[3] - kappa * Mth::sin(x2) - f;
         z[0] = x1; z[1] = x2; z[2] = p1; z[3] = p2;
     }
+    // WrappedFroeschleMap, froeschle_map.jl:60-126, state (x1, x2, p1, p2, c1..c4): tangent _f3_tangent at the
+    // unreduced sums u = x + p (:108); forward (:84-92) reduces the new positions (counts b), evaluates the force at
+    // them, reduces the new momenta (counts a); m' = m + n + b, n' = n + a; _checked8 (:69-73).
+    static void wrapped_froeschle(double nu, double kappa, double mu, double* z, double* M) {
+        const double u1 = z[0] + z[2], u2 = z[1] + z[3];
+        const double t = mu * Mth::sin(u1 + u2);
+        const double a = -nu * Mth::cos(u1) - t, b = -t, c = -kappa * Mth::cos(u2) - t;
+        const double o = 1.0, Z = 0.0;
+        const double Mv[16] = {o, Z, a, b, Z, o, b, c, o, Z, o + a, b, Z, o, b, o + c};
+        std::memcpy(M, Mv, sizeof Mv);
+        const double tp = 2 * jl_pi();
+        double x1, b1, x2, b2, p1, a1, p2, a2;
+        wrap_reduce(u1, tp, &x1, &b1);
+        wrap_reduce(u2, tp, &x2, &b2);
+        const double f = mu * (1.0 - Mth::cos(x1 + x2));
+        wrap_reduce(z[2] - nu * Mth::sin(x1) - f, tp, &p1, &a1);
+        wrap_reduce(z[3] - kappa * Mth::sin(x2) - f, tp, &p2, &a2);
+        const double m1 = z[4] + z[6] + b1, m2 = z[5] + z[7] + b2, n1 = z[6] + a1, n2 = z[7] + a2;
+        const double lim = 0x1p53;
+        if (std::fabs(m1) < lim && std::fabs(m2) < lim && std::fabs(n1) < lim && std::fabs(n2) < lim) {
+            z[0] = x1; z[1] = x2; z[2] = p1; z[3] = p2; z[4] = m1; z[5] = m2; z[6] = n1; z[7] = n2;
+        } else {
+            for (int i = 0; i < 8; ++i) z[i] = NaN;
+        }
+    }
     // LinearSymplecticMap, linear_symplectic.jl: forward A z (StaticArrays product, fused), tangent A.
     static void linear(const double* A, int d, double* z, double* M) {
         double zn[CL_MAX_DIM];
@@ -229,6 +254,27 @@ struct Chain {
         double p[CL_MAX_DIM / 2];
         for (int j = 0; j < N; ++j) p[j] = z[N + j] + force(z, j);
         for (int j = 0; j < N; ++j) { z[j] = z[j] + p[j]; z[N + j] = p[j]; }
+    }
+    // WrappedStandardMapChain forward (wrapped_standard_map_chain.jl:117-124), state (q, p, counts of q, counts
+    // of p): p~ = p + F(q) reduced (counts a), n' = n + a; q~ = q + p' reduced (counts b), m' = m + n' + b;
+    // _guard_counts (:101-107). The band is the chain's at the reduced positions (:135-137).
+    void forward_wrapped(double* z) const {
+        const double tp = 2 * jl_pi();
+        double p[CL_MAX_DIM / 2], nn[CL_MAX_DIM / 2];
+        for (int j = 0; j < N; ++j) {
+            double a;
+            wrap_reduce(z[N + j] + force(z, j), tp, &p[j], &a);
+            nn[j] = z[3 * N + j] + a;
+        }
+        bool ok = true;
+        for (int j = 0; j < N; ++j) {
+            double q, b;
+            wrap_reduce(z[j] + p[j], tp, &q, &b);
+            const double m = z[2 * N + j] + nn[j] + b;
+            z[j] = q; z[N + j] = p[j]; z[2 * N + j] = m; z[3 * N + j] = nn[j];
+            ok = ok && std::fabs(m) < 0x1p53 && std::fabs(nn[j]) < 0x1p53;
+        }
+        if (!ok) for (int i = 0; i < 4 * N; ++i) z[i] = NaN;
     }
 };
 

@@ -55,7 +55,7 @@ void run_orbit(const cl_run& run0, int64_t i, const cl_buffers& b, const double*
     const int d = run.d, s = run.s, nf = run.n_frames;
     const int64_t n0 = run.n0;
     const int64_t steps = run.steps > 0 ? run.steps : run.N - n0;
-    double x[CL_MAX_DIM];
+    double x[2 * CL_MAX_DIM];   // the wrapped maps carry a winding count per coordinate
     double W[CL_MAX_FRAMES][CL_MAX_DIM * CL_MAX_K];
     std::vector<uint8_t> st[CL_MAX_FRAMES];
     bool alive[CL_MAX_FRAMES];
@@ -106,7 +106,7 @@ void run_orbit(const cl_run& run0, int64_t i, const cl_buffers& b, const double*
     const int64_t handoffs = steps / tau;
     for (int64_t h = 0; h < handoffs; ++h) {
         for (int t = 0; t < tau; ++t) {
-            if (run.sys.kind == CL_SYS_CHAIN) {
+            if (run.sys.kind == CL_SYS_CHAIN || run.sys.kind == CL_SYS_WRAPPED_CHAIN) {
                 double g[CL_MAX_DIM / 2], gl[CL_MAX_DIM / 2], gr[CL_MAX_DIM / 2];
                 chain.band(x, g, gl, gr);
                 for (int f = 0; f < nf; ++f) {
@@ -114,13 +114,17 @@ void run_orbit(const cl_run& run0, int64_t i, const cl_buffers& b, const double*
                     chain.apply(g, gl, gr, W[f], run.frames[f].k);
                     if (sali_slot[f] >= 0) chain.apply(g, gl, gr, Ws[f], 2);
                 }
-                chain.forward(x);
+                if (run.sys.kind == CL_SYS_WRAPPED_CHAIN) chain.forward_wrapped(x);
+                else chain.forward(x);
             } else {
                 double M[CL_MAX_DIM * CL_MAX_DIM];
                 switch (run.sys.kind) {
                     case CL_SYS_STANDARD: Systems<MM>::standard(run.sys.K, x, M); break;
                     case CL_SYS_WRAPPED_STANDARD: Systems<MM>::wrapped(run.sys.K, x, M); break;
                     case CL_SYS_FROESCHLE: Systems<MM>::froeschle(run.sys.nu, run.sys.kappa, run.sys.mu, x, M); break;
+                    case CL_SYS_WRAPPED_FROESCHLE:
+                        Systems<MM>::wrapped_froeschle(run.sys.nu, run.sys.kappa, run.sys.mu, x, M);
+                        break;
                     case CL_SYS_LINEAR: Systems<MM>::linear(run.sys.A, d, x, M); break;
                     case CL_SYS_HH_GAUSS: gauss.step(x, run.sys.dt, M); break;
                     case CL_SYS_HH_SPLIT: split.step(x, run.sys.dt, M); break;

@@ -63,8 +63,9 @@ int main(void){
 def _run_from_key(key: str) -> _abi.cl_run:
     m = re.match(r"s(\d+)d(\d+)p(\d+)\|(.*)", key)
     kind, d, p, rest = int(m[1]), int(m[2]), int(m[3]), m[4]
-    r = _abi.cl_run(abi_version=_abi.ABI_VERSION, d=d, s=4 if kind == _abi.SYS_WRAPPED_STANDARD else d, tau=1, N=10,
-                    n_frames=0, precision=p)
+    wrapped = kind in (_abi.SYS_WRAPPED_STANDARD, _abi.SYS_WRAPPED_FROESCHLE, _abi.SYS_WRAPPED_CHAIN)
+    r = _abi.cl_run(abi_version=_abi.ABI_VERSION, d=d, s=2 * d if wrapped else d, tau=1, N=10, n_frames=0,
+                    precision=p)
     r.sys.kind = kind
     r.sys.n_sites = d // 2
     r.sys.gauss_maxiter = 50
