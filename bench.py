@@ -176,7 +176,7 @@ def main() -> None:
     ap.add_argument("--only", choices=["fp64", "mixed"], default=None,
                     help="time one kernel of the default workload and print a short line (a small case for ncu)")
     ap.add_argument("--workload", default="coupled", choices=["coupled", "standard", "gauss", "lattice", "screen", "mlp", "split", "shadow",
-                                                             "record", "indicators", "advance"])
+                                                             "record", "indicators", "advance", "torus"])
     args = ap.parse_args()
     if args.workload != "coupled":
         run_workload(args)
@@ -959,10 +959,34 @@ def workload_advance(args):
                              stages=m.stages), cpu, roofline=roofline)
 
 
+def workload_torus(args):
+    """The coupled-maps ensemble on the torus: WrappedFroeschleMap(1.5, 1.5, 0.05), coordinates in [0, 2 pi)^4
+    with zero winding counts, the same two frames as the default workload (QRSpectrum(Householder) k = 4 and
+    GALI_4 + SALI k = 4), 65536 orbits x 1e5 steps, tau = 10."""
+    from chaos_b200 import GALI, SALI, HouseholderQR, QRSpectrum, WrappedFroeschleMap, torus_state
+    from chaos_b200.propagate import FrameSpec
+    n, N = args.orbits or N_ORBITS, args.N
+    sysm = WrappedFroeschleMap(NU, KAPPA, MU)
+    z = np.random.default_rng(SEED).uniform(0, 2 * np.pi, (n, 4))
+    x0 = np.array([torus_state(sysm, v) for v in z])
+    frames = [FrameSpec(4, (QRSpectrum(HouseholderQR()),)), FrameSpec(4, (GALI(), SALI()))]
+
+    def cpu():
+        W0 = np.broadcast_to(np.eye(4), (512, 4, 4)).copy()
+        fr = [FrameSpec(4, (QRSpectrum(HouseholderQR()),), W0), FrameSpec(4, (GALI(), SALI()), W0)]
+        return _cpu_port(sysm, x0[:512], 4000, TAU, fr, "orbit-steps/s",
+                         "512 orbits x 4000 steps of the workload (oracle, all host threads)")
+    _propagate_workload(args, "WrappedFroeschleMap(1.5, 1.5, 0.05) on the torus, QRSpectrum(Householder) k=4 | "
+                        "GALI_4+SALI k=4, tau=10", sysm, x0, N, TAU, frames, "orbit-steps", cpu,
+                        dict(workload=f"froeschle-torus-{n}x{N:.0e}-tau10-qr-householder+gali4+sali", orbits=n, N=N,
+                             tau=TAU, W0="I"))
+
+
 def run_workload(args):
     {"standard": workload_standard, "gauss": workload_gauss, "lattice": workload_lattice,
      "screen": workload_screen, "mlp": workload_mlp, "split": workload_split, "shadow": workload_shadow,
-     "record": workload_record, "indicators": workload_indicators, "advance": workload_advance}[args.workload](args)
+     "record": workload_record, "indicators": workload_indicators, "advance": workload_advance,
+     "torus": workload_torus}[args.workload](args)
 
 
 
