@@ -19,7 +19,7 @@ from .systems import (ABA864, ABAH864, PEFRL, SABA, SABAC, SBAB, SBABC, CalvoSan
                       SymplecticEuler, WrappedFroeschleMap, WrappedStandardMap, WrappedStandardMapChain, Yoshida, adjoint_method, coefficients, energy_start,
                       force_evaluations, is_palindromic, isolated_force_evaluations, lift, method_name, method_source,
                       nominal_order, random_energy_starts, section_interval, stage_count, suzuki_jump, table_digits,
-                      torus_state, triple_jump)
+                      torus_state, triple_jump, rotation_block, hyperbolic_block, block_diagonal, conjugated)
 
 __all__ = [
     "propagate", "propagate_frames", "propagate_shadow", "record", "record_indicators", "record_indicator_pairs", "pair_start", "pair_frame", "record_shadow", "advance_ensemble", "FrameSpec", "PropagationResult", "build_run", "bytes_per_orbit", "chunk_size",
@@ -27,7 +27,7 @@ __all__ = [
     "QRSpectrum", "CGS", "MGS", "RGS", "HouseholderQR", "AugmentedQR", "GivensQR", "Benettin", "SALI", "GALI",
     "MEGNO", "FLI", "RLI",
     "StandardMap", "WrappedStandardMap", "FroeschleMap", "WrappedFroeschleMap", "StandardMapChain",
-    "WrappedStandardMapChain", "LinearSymplecticMap", "IntegratorMap",
+    "WrappedStandardMapChain", "rotation_block", "hyperbolic_block", "block_diagonal", "conjugated", "LinearSymplecticMap", "IntegratorMap",
     "Gauss", "SplittingMethod", "CorrectedMethod", "SymplecticEuler", "Leapfrog", "McLachlan2", "Ruth3", "ForestRuth",
     "triple_jump", "suzuki_jump", "PEFRL", "CalvoSanzSerna4", "Yoshida", "KahanLi", "SofroniouSpaletta10", "SABA",
     "SBAB", "SABAC", "SBABC", "ABA864", "ABAH864", "adjoint_method", "coefficients", "stage_count", "nominal_order",

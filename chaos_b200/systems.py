@@ -165,6 +165,81 @@ class LinearSymplecticMap(System):
         return c
 
 
+def _fma(a: float, b: float, c: float) -> float:
+    """fma(a, b, c) rounded once (the exact value of a b + c in rational arithmetic, correctly rounded), with the
+    IEEE sign of a zero result; finite arguments."""
+    from fractions import Fraction
+    p = Fraction(a) * Fraction(b)
+    t = p + Fraction(c)
+    if t != 0:
+        return float(t)
+    if p == 0 and c == 0:
+        neg_p = (math.copysign(1.0, a) * math.copysign(1.0, b)) < 0
+        return -0.0 if (neg_p and math.copysign(1.0, c) < 0) else 0.0
+    return 0.0
+
+
+def _smatmul(A, B):
+    """StaticArrays' unrolled SMatrix product: C[i, j] = A[i, 1] B[1, j], then muladd(A[i, q], B[q, j], C[i, j]) for
+    q = 2..n, the muladd fused (the chain `fused_product` restates, src/Foundation/product.jl:9-20)."""
+    A, B = np.asarray(A, dtype=np.float64), np.asarray(B, dtype=np.float64)
+    n, m, p = A.shape[0], A.shape[1], B.shape[1]
+    C = np.empty((n, p))
+    for i in range(n):
+        for j in range(p):
+            acc = float(A[i, 0]) * float(B[0, j])
+            for q in range(1, m):
+                acc = _fma(float(A[i, q]), float(B[q, j]), acc)
+            C[i, j] = acc
+    return C
+
+
+def rotation_block(theta: float) -> np.ndarray:
+    """rotation_block(Float64, theta), src/Systems/linear_symplectic.jl:43-46: [[cos, sin], [-sin, cos]]; the
+    sine and cosine are the host libm's (Julia's own libm may differ in the last bit)."""
+    s, c = math.sin(float(theta)), math.cos(float(theta))
+    return np.array([[c, s], [-s, c]])
+
+
+def hyperbolic_block(mu: float) -> np.ndarray:
+    """hyperbolic_block(Float64, mu), linear_symplectic.jl:53-56: [[cosh, sinh], [sinh, cosh]], eigenvalues
+    exp(+-mu)."""
+    m = float(mu)
+    ch, sh = math.cosh(m), math.sinh(m)
+    return np.array([[ch, sh], [sh, ch]])
+
+
+def block_diagonal(*blocks) -> np.ndarray:
+    """block_diagonal(blocks...), linear_symplectic.jl:58-77: the direct sum of 2 x 2 blocks on the pairs
+    (q_j, p_j), reordered to (q_1..q_N, p_1..p_N)."""
+    N = len(blocks)
+    D = 2 * N
+    A = np.zeros((D, D))
+    for j, b in enumerate(blocks):
+        b = np.asarray(b, dtype=np.float64)
+        for r in range(2):
+            for c in range(2):
+                A[j + r * N, j + c * N] = b[r, c]
+    return A
+
+
+def conjugated(A, B) -> np.ndarray:
+    """conjugated(A, B), linear_symplectic.jl:79-91: the non-normal S^-1 A S with S = [I B; 0 I], B symmetric
+    N x N, evaluated as (S(-1) A) S(1) with the SMatrix product."""
+    A, B = np.asarray(A, dtype=np.float64), np.asarray(B, dtype=np.float64)
+    D, N = A.shape[0], B.shape[0]
+    if D != 2 * N:
+        raise ValueError(f"A is {D} x {D} but B is {N} x {N}")
+    if not np.array_equal(B, B.T):
+        raise ValueError("B must be symmetric")
+
+    def S(sgn):
+        M = np.eye(D)
+        M[:N, N:] = sgn * B
+        return M
+    return _smatmul(_smatmul(S(-1.0), A), S(1.0))
+
+
 @dataclass(frozen=True)
 class HenonHeilesFlow:
     """HenonHeilesFlow(), src/Systems/flow_models.jl:30,101-103: H = |p|^2/2 + |q|^2/2 + q1^2 q2 - q2^3/3."""
