@@ -7,7 +7,7 @@ reducers as parameter records, the argument checks, chunking, error and summary 
 """
 from .foundation import FALLBACK_REASONS, DeviceError, NumericalHealthError
 from .propagate import (FrameSpec, PropagationResult, build_run, bytes_per_orbit, chunk_size, probe, propagate,
-                        propagate_frames, release_cache)
+                        propagate_frames, propagate_orbit, release_cache)
 from .reducers import (CGS, FLI, GALI, MEGNO, MGS, RGS, RLI, SALI, AugmentedQR, Benettin, GivensQR, HouseholderQR,
                        QRSpectrum)
 from .advance import advance_ensemble
@@ -22,7 +22,7 @@ from .systems import (ABA864, ABAH864, PEFRL, SABA, SABAC, SBAB, SBABC, CalvoSan
                       torus_state, triple_jump, rotation_block, hyperbolic_block, block_diagonal, conjugated)
 
 __all__ = [
-    "propagate", "propagate_frames", "propagate_shadow", "record", "record_indicators", "record_indicator_pairs", "pair_start", "pair_frame", "record_shadow", "advance_ensemble", "FrameSpec", "PropagationResult", "build_run", "bytes_per_orbit", "chunk_size",
+    "propagate", "propagate_frames", "propagate_orbit", "propagate_shadow", "record", "record_indicators", "record_indicator_pairs", "pair_start", "pair_frame", "record_shadow", "advance_ensemble", "FrameSpec", "PropagationResult", "build_run", "bytes_per_orbit", "chunk_size",
     "probe", "release_cache", "NumericalHealthError", "DeviceError", "FALLBACK_REASONS",
     "QRSpectrum", "CGS", "MGS", "RGS", "HouseholderQR", "AugmentedQR", "GivensQR", "Benettin", "SALI", "GALI",
     "MEGNO", "FLI", "RLI",

@@ -272,3 +272,23 @@ def propagate(sys: System, x0, N: int, *, k: int, tau: int = 1, seed: int = 0, r
         raise ValueError("backend must be :gpu or :auto here; the CPU path is the reference's own")
     return propagate_frames(sys, x0, N, [FrameSpec(int(k), tuple(reducers), W0)], tau=tau, seed=seed,
                             precision=precision, chunk=chunk, launch_steps=launch_steps, finals=finals)[0]
+
+
+def propagate_orbit(sys: System, x0, W0, N: int, tau: int, reducers, *, orbit: int = 1, precision: str = "fp64"):
+    """propagate_orbit(sys, x0, W0, N, tau, reducers; orbit = 1) -> (x, W, states), src/Tangent/orbit.jl:77-99: one
+    orbit from `x0` (length s) with the deviation matrix `W0` (d x k) through the same kernel, the reducer states in
+    the Julia layout; a reducer failure raises that reducer's NumericalHealthError and a non-finite state or frame
+    at a handoff the health error, each naming `orbit`."""
+    x0 = np.asarray(x0, dtype=np.float64).reshape(1, -1)
+    W0 = np.asarray(W0, dtype=np.float64)
+    if W0.ndim != 2:
+        raise ValueError("W0 must be a d x k matrix")
+    _check_steps(int(N), int(tau))
+    fr = FrameSpec(W0.shape[1], tuple(reducers), W0[None])
+    r = propagate_frames(sys, x0, N, [fr], tau=tau, precision=precision, finals=False, throw=False)[0]
+    code = int(r.code[0])
+    if code == STATUS_REDUCER:
+        raise _reducer_error(tuple(reducers), r.states[0], int(orbit), "gpu")
+    if code != STATUS_OK:
+        raise _health_error(code, r.x[0], r.W[0], int(r.hstep[0]), int(orbit), "gpu")
+    return r.x[0], r.W[0], (r.states[0] if r.states is not None else None)

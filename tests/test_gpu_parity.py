@@ -179,3 +179,22 @@ def test_henon_heiles_splitting(oracle, k, chain, method):
     x0 = random_energy_starts(1 / 8, n, seed=12)
     sysm = IntegratorMap(m, HenonHeilesFlow(), 0.05)
     _compare(sysm, x0, 800, [FrameSpec(k, chain, haar_frames(n, 4, k, 13))], 10, oracle)
+
+
+def test_propagate_orbit(oracle):
+    """propagate_orbit (src/Tangent/orbit.jl:77-99): one orbit through the kernel, the oracle's bits, and the
+    errors of a failing orbit naming the orbit id the caller gives."""
+    from chaos_b200 import NumericalHealthError, propagate_orbit
+    x0 = np.array([0.3, 1.1, 2.0, 0.7])
+    W0 = haar_frames(1, 4, 4, 3)[0]
+    sysm = FroeschleMap(1.5, 1.5, 0.05)
+    x, W, st = propagate_orbit(sysm, x0, W0, 1000, 10, (QRSpectrum(HouseholderQR()),))
+    ref = oracle.oracle_frames(sysm, x0[None], 1000, [FrameSpec(4, (QRSpectrum(HouseholderQR()),), W0[None])], tau=10,
+                               math="portable")[0]
+    assert same_bits(x, ref["x"][0]) and same_bits(W, ref["W"][0]) and states_equal(st[None], ref["states"])
+    with pytest.raises(NumericalHealthError) as e:
+        propagate_orbit(sysm, np.array([np.nan, 0.0, 0.0, 0.0]), W0, 100, 10, (QRSpectrum(MGS()),), orbit=7)
+    assert e.value.orbit == 7 and e.value.what == "state" and e.value.step == 10
+    with pytest.raises(NumericalHealthError) as e:
+        propagate_orbit(StandardMap(6.0), np.array([0.1, 0.2]), np.zeros((2, 2)), 50, 5, (QRSpectrum(MGS()),), orbit=3)
+    assert e.value.orbit == 3
