@@ -173,7 +173,7 @@ def propagate_frames(sys: System, x0, N: int, frames: list[FrameSpec], *, tau: i
     if launch_steps is not None and (launch_steps < 1 or launch_steps % tau):
         raise ValueError(f"forced steps per launch must be a positive multiple of tau, got L = {launch_steps}, tau = {tau}")
     W0s = []
-    for fr in frames:
+    for f, fr in enumerate(frames):
         _check_frame(sys, fr)
         if fr.W0 is not None:
             W0 = np.asarray(fr.W0, dtype=np.float64)
@@ -181,7 +181,8 @@ def propagate_frames(sys: System, x0, N: int, frames: list[FrameSpec], *, tau: i
                 raise ValueError("W0 needs one matrix per orbit")
             if W0.shape[1:] != (d, fr.k):
                 raise ValueError(f"W0 matrices must be {d} x {fr.k}")
-            W0s.append(np.ascontiguousarray(W0.transpose(0, 2, 1)))   # column-major per orbit
+            same = [g for g in range(f) if frames[g].W0 is fr.W0]   # one frame's W0 given again: one copy
+            W0s.append(W0s[same[0]] if same else np.ascontiguousarray(W0.transpose(0, 2, 1)))   # column-major per orbit
         else:
             W0s.append(None)
     run = build_run(sys, N, tau, frames, precision, seed, steps=launch_steps or 0)
