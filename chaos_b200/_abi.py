@@ -48,7 +48,7 @@ class cl_system(C.Structure):
         ("dt", C.c_double),
         ("A", C.c_double * (MAX_DIM * MAX_DIM)),
         ("n_stages", C.c_int32),
-        ("reserved", C.c_int32),
+        ("corrector", C.c_int32),
         ("stage_c", C.c_double * MAX_STAGES),
         ("stage_d", C.c_double * MAX_STAGES),
     ]

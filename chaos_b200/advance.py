@@ -11,7 +11,7 @@ import numpy as np
 from . import _abi
 from ._lib import last_error, lib
 from .foundation import DeviceError
-from .systems import Gauss, HenonHeilesFlow, IntegratorMap, SplittingMethod
+from .systems import CorrectedMethod, Gauss, HenonHeilesFlow, IntegratorMap, SplittingMethod
 
 
 def advance_ensemble(m, flow, x0, tau: float, n: int, *, chunk: int | None = None):
@@ -19,8 +19,8 @@ def advance_ensemble(m, flow, x0, tau: float, n: int, *, chunk: int | None = Non
     with kicks merged across the step boundary, or Gauss(3), advanced by advance_checked per step) on `flow`
     (HenonHeilesFlow) from every row of `x0`. `ok[j]` is False when an implicit step of orbit j failed; its state is
     then all NaN. The result of an orbit does not depend on `chunk`."""
-    if not isinstance(m, (SplittingMethod, Gauss)):
-        raise TypeError("the compiled menu advances a SplittingMethod table or Gauss(3)")
+    if not isinstance(m, (SplittingMethod, CorrectedMethod, Gauss)):
+        raise TypeError("the compiled menu advances a SplittingMethod table, a CorrectedMethod or Gauss(3)")
     if not isinstance(flow, HenonHeilesFlow):
         raise TypeError("the compiled menu integrates HenonHeilesFlow")
     x0 = np.ascontiguousarray(np.asarray(x0, dtype=np.float64))

@@ -59,6 +59,20 @@ __global__ void __launch_bounds__(128) advance_split_kernel(const double* __rest
     ok[i] = 1;
 }
 
+// advance_n(::CorrectedMethod, n) (stepper.jl:142-152): every step the corrector kick, the base table's step with
+// its pending kick flushed at the step's end, the corrector kick
+__global__ void __launch_bounds__(128) advance_corrected_kernel(const double* __restrict__ x0,
+                                                                double* __restrict__ out, uint8_t* __restrict__ ok,
+                                                                int64_t n, int64_t steps, const SysSplitHH m) {
+    const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double4 v = reinterpret_cast<const double4*>(x0)[i];
+    double z[4] = {v.x, v.y, v.z, v.w};
+    for (int64_t s = 0; s < steps; ++s) m.step(z);
+    reinterpret_cast<double4*>(out)[i] = make_double4(z[0], z[1], z[2], z[3]);
+    ok[i] = 1;
+}
+
 __global__ void __launch_bounds__(128) advance_gauss_kernel(const double* __restrict__ x0, double* __restrict__ out,
                                                             uint8_t* __restrict__ ok, int64_t n, int64_t steps,
                                                             const SysGauss3HH g) {
@@ -91,6 +105,8 @@ int check_sys(const cl_system* sys) {
         for (int k = 0; k < sys->n_stages; ++k)
             if (!std::isfinite(sys->stage_c[k]) || !std::isfinite(sys->stage_d[k]))
                 return capi_fail(CL_EINVAL, "the table's weights must be finite");
+        if (!(sys->corrector == 0 || (sys->corrector == 1 && std::isfinite(sys->eps))))
+            return capi_fail(CL_EINVAL, "corrector must be 0, or 1 with a finite coefficient in eps");
     } else if (sys->kind == CL_SYS_HH_GAUSS) {
         if (sys->gauss_maxiter < 2) return capi_fail(CL_EINVAL, "maxiter must be at least 2");
     } else {
@@ -117,7 +133,12 @@ int cl_b200_advance_ensemble_device(const cl_system* sys, int64_t n, const doubl
     if (n == 0) return 0;
     const unsigned blocks = static_cast<unsigned>((n + 127) / 128);
     cudaStream_t st = static_cast<cudaStream_t>(stream);
-    if (sys->kind == CL_SYS_HH_SPLIT) {
+    if (sys->kind == CL_SYS_HH_SPLIT && sys->corrector) {
+        cl_run r;
+        std::memset(&r, 0, sizeof r);
+        r.sys = *sys;
+        advance_corrected_kernel<<<blocks, 128, 0, st>>>(x0, out, ok, n, steps, SysMaker<SysSplitHH>::make(r, nullptr));
+    } else if (sys->kind == CL_SYS_HH_SPLIT) {
         Table m;
         std::memset(&m, 0, sizeof m);
         m.dt = sys->dt;

@@ -124,6 +124,8 @@ int validate(const cl_run& r) {
         for (int i = 0; i < r.sys.n_stages; ++i)
             if (!(std::isfinite(r.sys.stage_c[i]) && std::isfinite(r.sys.stage_d[i])))
                 return fail(CL_EINVAL, "the splitting table has a non-finite weight");
+        if (!(r.sys.corrector == 0 || (r.sys.corrector == 1 && std::isfinite(r.sys.eps))))
+            return fail(CL_EINVAL, "corrector must be 0, or 1 with a finite coefficient in eps");
     }
     if (r.n_frames < 1 || r.n_frames > CL_MAX_FRAMES) return fail(CL_EINVAL, "n_frames must be in 1..3");
     if (r.precision != CL_PREC_FP64 && r.precision != CL_PREC_MIXED) return fail(CL_EINVAL, "unknown precision");

@@ -22,6 +22,8 @@ struct SysSplitHH {
     template <typename R> using JacR = SplitJac;
     double dt;
     int n;
+    int corr;       // CorrectedMethod: the corrector kick before and after every step
+    double kap;     // its kappa = dt^3 eps^2 c / 2 (stepper.jl:131-134), eps = perturbation_scale = 1 here
     double c[CL_MAX_STAGES], d[CL_MAX_STAGES];
 
     // force (flow_models.jl:102): (q1 + 2 q1 q2, q2 + q1^2 - q2^2), left to right as Julia evaluates it
@@ -36,6 +38,41 @@ struct SysSplitHH {
         force(z[0], z[1], F1, F2);
         z[2] = z[2] - t * F1;
         z[3] = z[3] - t * F2;
+    }
+    // corrector_force (flow_models.jl:106): 2 (Hs g), Hs the force Jacobian, g the force, the SMatrix-vector
+    // product fused as StaticArrays unrolls it
+    static __device__ __forceinline__ void corrector_force(double q1, double q2, double& C1, double& C2) {
+        double F1, F2;
+        force(q1, q2, F1, F2);
+        const double h11 = 1 + 2 * q2, h21 = 2 * q1, h12 = 2 * q1, h22 = 1 - 2 * q2;
+        C1 = 2 * fma(h12, F2, h11 * F1);
+        C2 = 2 * fma(h22, F2, h21 * F1);
+    }
+    // _corrector_kick (stepper.jl:136): p + kappa * corrector_force
+    __device__ __forceinline__ void corrector_kick(double* z) const {
+        double C1, C2;
+        corrector_force(z[0], z[1], C1, C2);
+        z[2] = z[2] + kap * C1;
+        z[3] = z[3] + kap * C2;
+    }
+    // _corrector_jacobian (stepper.jl:137-140): [[I, 0], [kappa Hc, I]], Hc = corrector_hessian
+    // (flow_models.jl:107-112) = 2 (Hs Hs + g1 T1 + g2 T2), T1 = [0 2; 2 0], T2 = [2 0; 0 -2]
+    __device__ __forceinline__ void corrector_jacobian(const double* z, double* J) const {
+        double F1, F2;
+        force(z[0], z[1], F1, F2);
+        const double h[4] = {1 + 2 * z[1], 2 * z[0], 2 * z[0], 1 - 2 * z[1]};   // column-major Hs
+        const double t1[4] = {0, 2, 2, 0}, t2[4] = {2, 0, 0, -2};
+        double hc[4];
+#pragma unroll
+        for (int j = 0; j < 2; ++j)
+#pragma unroll
+            for (int i = 0; i < 2; ++i) {
+                const double hh = fma(h[i + 2], h[1 + 2 * j], h[i] * h[2 * j]);
+                hc[i + 2 * j] = 2 * ((hh + F1 * t1[i + 2 * j]) + F2 * t2[i + 2 * j]);
+            }
+        const double Jv[16] = {1, 0, kap * hc[0], kap * hc[1], 0, 1, kap * hc[2], kap * hc[3], 0, 0, 1, 0, 0, 0, 0, 1};
+#pragma unroll
+        for (int l = 0; l < 16; ++l) J[l] = Jv[l];
     }
     // W <- J W for a 4 x 4 frame, both column-major, entry (i, j): J[i,0] W[0,j], then fma over q = 1..3
     static __device__ __forceinline__ void mul4(const double* J, double* W) {
@@ -58,6 +95,12 @@ struct SysSplitHH {
         double* W = Jc.T;
 #pragma unroll
         for (int l = 0; l < 16; ++l) W[l] = (l % 5 == 0) ? 1.0 : 0.0;
+        if (corr) {   // tangent_advance(::CorrectedMethod) (stepper.jl:154-160): the corrector's Jacobian, its kick
+            double J[16];
+            corrector_jacobian(z, J);
+            mul4(J, W);
+            corrector_kick(z);
+        }
 #pragma unroll 1
         for (int i = 0; i < n; ++i) {
             const double ci = c[i], di = d[i];
@@ -78,10 +121,19 @@ struct SysSplitHH {
                 kick(z, t);
             }
         }
+        if (corr) {
+            double J[16];
+            corrector_jacobian(z, J);
+            mul4(J, W);
+        }
     }
     template <int KK, typename T>
     __device__ __forceinline__ void apply(const SplitJac& Jc, T* W) const { fused_dense<4, KK>(Jc.T, W); }
-    __device__ __forceinline__ void forward(double* x, const SplitJac&) const {
+    __device__ __forceinline__ void forward(double* x, const SplitJac&) const { step(x); }
+    // one step of advance_n; a corrected method (stepper.jl:142-152): kick, the base step with its own merged
+    // kicks, kick (no merging across the corrector)
+    __device__ __forceinline__ void step(double* x) const {
+        if (corr) corrector_kick(x);
         double pend = 0.0;
 #pragma unroll 1
         for (int i = 0; i < n; ++i) {
@@ -93,6 +145,7 @@ struct SysSplitHH {
             pend = pend + d[i];
         }
         if (pend != 0.0) kick(x, pend * dt);
+        if (corr) corrector_kick(x);
     }
 };
 
@@ -101,6 +154,9 @@ template <> struct SysMaker<SysSplitHH> {
         SysSplitHH s;
         s.dt = r.sys.dt;
         s.n = r.sys.n_stages;
+        s.corr = r.sys.corrector;
+        // kappa = tau * tau * tau * (eps * eps) * c / 2 left to right, eps * eps the integer 1
+        s.kap = r.sys.corrector ? (((r.sys.dt * r.sys.dt) * r.sys.dt) * r.sys.eps) / 2 : 0.0;
         for (int i = 0; i < CL_MAX_STAGES; ++i) {
             s.c[i] = i < s.n ? r.sys.stage_c[i] : 0.0;
             s.d[i] = i < s.n ? r.sys.stage_d[i] : 0.0;

@@ -16,7 +16,7 @@ using Chaoslab.Lyapunov: QRSpectrum, Benettin, CGS, MGS, RGS, HouseholderQR, Aug
 using Chaoslab.Indicators: SALI, GALI, MEGNO, FLI, RLI
 using Chaoslab.Systems: StandardMap, WrappedStandardMap, FroeschleMap, StandardMapChain, LinearSymplecticMap,
                         HenonHeilesFlow, WrappedFroeschleMap, WrappedStandardMapChain
-using Chaoslab.Integrators: IntegratorMap, Gauss
+using Chaoslab.Integrators: IntegratorMap, Gauss, SplittingMethod, CorrectedMethod, coefficients
 
 const libcl = get(ENV, "CHAOSLAB_B200_LIB", joinpath(@__DIR__, "libchaoslab_b200.so"))
 
@@ -25,7 +25,7 @@ struct ClSystem
     kind::Int32; n_sites::Int32; ring::Int32; gauss_maxiter::Int32
     K::Float64; eps::Float64; nu::Float64; kappa::Float64; mu::Float64; gauss_tol::Float64; dt::Float64
     A::NTuple{256, Float64}
-    n_stages::Int32; reserved::Int32
+    n_stages::Int32; corrector::Int32
     stage_c::NTuple{128, Float64}; stage_d::NTuple{128, Float64}
 end
 struct ClReducer
@@ -88,6 +88,13 @@ function clsys(m::IntegratorMap{<:SplittingMethod{Float64, K}, HenonHeilesFlow, 
     K <= 128 || throw(ClB200Error(-3, "a splitting table of $K stages is above the compiled limit (128)"))
     c, d = coefficients(m.method)
     return ClSystem(7, 0, 0, 0, 0, 0, 0, 0, 0, NaN, m.tau, ZA, K, 0, ntuple(i -> i <= K ? c[i] : 0.0, 128),
+                    ntuple(i -> i <= K ? d[i] : 0.0, 128))
+end
+# a corrected method (tables_near.jl:113-128): the base table, the corrector flag and its coefficient c in `eps`
+function clsys(m::IntegratorMap{<:CorrectedMethod{Float64, <:SplittingMethod{Float64, K}}, HenonHeilesFlow, Float64}) where {K}
+    K <= 128 || throw(ClB200Error(-3, "a splitting table of $K stages is above the compiled limit (128)"))
+    c, d = coefficients(m.method.base)
+    return ClSystem(7, 0, 0, 0, 0, m.method.c, 0, 0, 0, NaN, m.tau, ZA, K, 1, ntuple(i -> i <= K ? c[i] : 0.0, 128),
                     ntuple(i -> i <= K ? d[i] : 0.0, 128))
 end
 clsys(m) = throw(ClB200Error(-3, "system $(typeof(m)) is not in the compiled menu"))

@@ -693,9 +693,8 @@ def _corrector_c(n: int, sbab: bool) -> float:
 @dataclass(frozen=True)
 class CorrectedMethod:
     """CorrectedMethod(base, c), tables_near.jl:113-123 and stepper.jl:131-173: the corrector kick
-    exp(-kappa L_F), F = |grad V|^2, kappa = tau^3 eps^2 c / 2, before and after the symmetric table `base`. The
-    corrector needs `corrector_force` of the flow, which the reference defines for the harmonic oscillator, the
-    pendulum and Kepler; the Henon-Heiles flow has none, so an IntegratorMap of it rejects a corrected method."""
+    exp(-kappa L_F), F = |grad V|^2, kappa = tau^3 eps^2 c / 2, before and after the symmetric table `base`
+    (for the Henon-Heiles flow eps = perturbation_scale = 1 and grad F = 2 Hs grad V, flow_models.jl:106-112)."""
     base: SplittingMethod
     c: float
     order: int
@@ -775,25 +774,25 @@ class IntegratorMap(System):
     def __init__(self, method, flow: HenonHeilesFlow, tau: float):
         if not isinstance(flow, HenonHeilesFlow):
             raise TypeError("the compiled menu integrates HenonHeilesFlow")
-        if isinstance(method, CorrectedMethod):
-            raise TypeError("HenonHeilesFlow has no corrector_force (a corrected method needs |grad V|^2 of the "
-                            "perturbation: the harmonic oscillator, the pendulum or Kepler)")
-        if not isinstance(method, (Gauss, SplittingMethod)):
+        if not isinstance(method, (Gauss, SplittingMethod, CorrectedMethod)):
             raise TypeError("the compiled menu integrates with Gauss(3) or a SplittingMethod table")
-        if isinstance(method, SplittingMethod) and method.stages > _abi.MAX_STAGES:
+        if isinstance(method, (SplittingMethod, CorrectedMethod)) and method.stages > _abi.MAX_STAGES:
             raise ValueError(f"a table of {method.stages} stages is above the compiled limit ({_abi.MAX_STAGES})")
         self.method, self.flow, self.tau = method, flow, float(tau)
         self.d = self.s = 4
-        kind = "Gauss3" if isinstance(method, Gauss) else "SplittingMethod"
+        kind = "Gauss3" if isinstance(method, Gauss) else type(method).__name__
         self.name = f"IntegratorMap{{{kind},HenonHeilesFlow}}"
 
     def to_cl(self):
-        if isinstance(self.method, SplittingMethod):
-            k = self.method.stages
-            cs = _abi.cl_system(kind=_abi.SYS_HH_SPLIT, dt=self.tau, n_stages=k, gauss_tol=math.nan)
+        if isinstance(self.method, (SplittingMethod, CorrectedMethod)):
+            corrected = isinstance(self.method, CorrectedMethod)
+            table = self.method.base if corrected else self.method
+            k = table.stages
+            cs = _abi.cl_system(kind=_abi.SYS_HH_SPLIT, dt=self.tau, n_stages=k, gauss_tol=math.nan,
+                                corrector=int(corrected), eps=float(self.method.c) if corrected else 0.0)
             for i in range(k):
-                cs.stage_c[i] = self.method.c[i]
-                cs.stage_d[i] = self.method.d[i]
+                cs.stage_c[i] = table.c[i]
+                cs.stage_d[i] = table.d[i]
             return cs
         tol = math.nan if self.method.tol is None else float(self.method.tol)
         return _abi.cl_system(kind=_abi.SYS_HH_GAUSS, gauss_maxiter=self.method.maxiter, gauss_tol=tol, dt=self.tau)

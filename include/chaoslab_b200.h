@@ -119,7 +119,9 @@ typedef struct cl_system {
     double dt;             /* IntegratorMap step tau of the flow                                        */
     double A[CL_MAX_DIM * CL_MAX_DIM]; /* CL_SYS_LINEAR: d x d matrix, column-major                     */
     int32_t n_stages;      /* CL_SYS_HH_SPLIT: stages k of the table, 1..CL_MAX_STAGES                          */
-    int32_t reserved;      /* 0                                                                          */
+    int32_t corrector;     /* CL_SYS_HH_SPLIT: 1 for CorrectedMethod(table, c) (SABAC / SBABC): the corrector
+                              kick p += kappa grad|grad V|^2 before and after every step, kappa = dt^3 c / 2 with
+                              c in `eps` (stepper.jl:131-160, tables_near.jl:113-128); else 0                   */
     double stage_c[CL_MAX_STAGES]; /* CL_SYS_HH_SPLIT: drift weights c_1..c_k (splitting.jl:16-21)      */
     double stage_d[CL_MAX_STAGES]; /* CL_SYS_HH_SPLIT: kick weights d_1..d_k                            */
 } cl_system;

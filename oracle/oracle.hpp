@@ -491,12 +491,57 @@ struct SplitHH {
     int n;
     const double* c;
     const double* d;
+    int corr = 0;       // CorrectedMethod (stepper.jl:131-173): the corrector kick before and after each step
+    double kap = 0.0;   // kappa = tau^3 eps^2 c / 2, eps = perturbation_scale(HenonHeilesFlow()) = 1
+    static SplitHH of(const cl_system& s) {
+        SplitHH m{s.n_stages, s.stage_c, s.stage_d};
+        m.corr = s.corrector;
+        m.kap = s.corrector ? (((s.dt * s.dt) * s.dt) * s.eps) / 2 : 0.0;
+        return m;
+    }
+    // corrector_force (flow_models.jl:106): 2 (Hs g), the SMatrix-vector product a fused chain
+    static void corrector_force(const double* z, double* C) {
+        double f[4];
+        hh_vf(z, f);   // (p, -F(q))
+        const double F1 = -f[2], F2 = -f[3];
+        const double h11 = 1 + 2 * z[1], h21 = 2 * z[0], h12 = 2 * z[0], h22 = 1 - 2 * z[1];
+        C[0] = 2 * std::fma(h12, F2, h11 * F1);
+        C[1] = 2 * std::fma(h22, F2, h21 * F1);
+    }
+    void corrector_kick(double* z) const {   // stepper.jl:136
+        double C[2];
+        corrector_force(z, C);
+        z[2] = z[2] + kap * C[0];
+        z[3] = z[3] + kap * C[1];
+    }
+    // _corrector_jacobian (stepper.jl:137-140) with corrector_hessian (flow_models.jl:107-112)
+    void corrector_jacobian(const double* z, double* J) const {
+        double f[4];
+        hh_vf(z, f);
+        const double F1 = -f[2], F2 = -f[3];
+        const double h[4] = {1 + 2 * z[1], 2 * z[0], 2 * z[0], 1 - 2 * z[1]};
+        const double t1[4] = {0, 2, 2, 0}, t2[4] = {2, 0, 0, -2};
+        double hc[4];
+        for (int j = 0; j < 2; ++j)
+            for (int i = 0; i < 2; ++i) {
+                const double hh = std::fma(h[i + 2], h[1 + 2 * j], h[i] * h[2 * j]);
+                hc[i + 2 * j] = 2 * ((hh + F1 * t1[i + 2 * j]) + F2 * t2[i + 2 * j]);
+            }
+        const double Jv[16] = {1, 0, kap * hc[0], kap * hc[1], 0, 1, kap * hc[2], kap * hc[3], 0, 0, 1, 0, 0, 0, 0, 1};
+        std::memcpy(J, Jv, sizeof Jv);
+    }
     // tangent_advance with the identity frame (stepper.jl:108-118): per stage, drift then kick where the weight is
     // nonzero, each Jacobian (at the point before the sub-step) multiplied onto the frame by the StaticArrays
     // product (the fused chain of fused_product); the state advanced without merging kicks.
     void tangent(const double* x, double dt, double* T) const {
         double z[4] = {x[0], x[1], x[2], x[3]};
         double W[16] = {1, 0, 0, 0, 0, 1, 0, 0, 0, 0, 1, 0, 0, 0, 0, 1}, J[16], Wn[16];
+        if (corr) {
+            corrector_jacobian(z, J);
+            fused_product(J, W, Wn, 4, 4, 4);
+            std::memcpy(W, Wn, sizeof W);
+            corrector_kick(z);
+        }
         for (int i = 0; i < n; ++i) {
             if (c[i] != 0.0) {
                 const double t = c[i] * dt;
@@ -513,10 +558,16 @@ struct SplitHH {
                 hh_kick(z, t);
             }
         }
+        if (corr) {
+            corrector_jacobian(z, J);
+            fused_product(J, W, Wn, 4, 4, 4);
+            std::memcpy(W, Wn, sizeof W);
+        }
         std::memcpy(T, W, sizeof W);
     }
     // advance_n(m, flow, z, dt, 1) (stepper.jl:27-48): kicks with no drift between them merged into one.
     void forward(double* z, double dt) const {
+        if (corr) corrector_kick(z);
         double pend = 0.0;
         for (int i = 0; i < n; ++i) {
             const double ci = c[i];
@@ -527,6 +578,7 @@ struct SplitHH {
             pend = pend + d[i];
         }
         if (pend != 0.0) hh_kick(z, pend * dt);
+        if (corr) corrector_kick(z);
     }
     // the orbit body's map step: the tangent at the old point, then forward (orbit.jl:44-50)
     void step(double* x, double dt, double* T) const {

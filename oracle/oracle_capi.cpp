@@ -99,7 +99,7 @@ void run_orbit(const cl_run& run0, int64_t i, const cl_buffers& b, const double*
     (void)sysf;
     Chain<MM> chain{run.sys.n_sites, run.sys.K, run.sys.eps, run.sys.ring != 0};
     Gauss3 gauss(run.sys.gauss_maxiter, run.sys.gauss_tol);
-    const SplitHH split{run.sys.n_stages, run.sys.stage_c, run.sys.stage_d};
+    const SplitHH split = SplitHH::of(run.sys);
     int64_t n = n0;
     bool escaped = false;
     const int tau = run.tau;
@@ -284,7 +284,7 @@ struct ShOrb {
         const int s = run.s, d = run.d;
         const Chain<MM> chain{run.sys.n_sites, run.sys.K, run.sys.eps, run.sys.ring != 0};
         Gauss3 gauss(run.sys.gauss_maxiter, run.sys.gauss_tol);
-        const SplitHH split{run.sys.n_stages, run.sys.stage_c, run.sys.stage_d};
+        const SplitHH split = SplitHH::of(run.sys);
         double delta[CL_MAX_DIM] = {};
         for (int64_t h = 0; h < steps / run.tau; ++h) {
             for (int t = 0; t < run.tau; ++t) {
@@ -1030,7 +1030,10 @@ int oracle_advance(const cl_system* sys, int64_t n, const double* x0, double* ou
         std::memcpy(z, x0 + 4 * i, sizeof z);
         uint8_t good = 1;
         const double dt = sys->dt;
-        if (sys->kind == CL_SYS_HH_SPLIT) {
+        if (sys->kind == CL_SYS_HH_SPLIT && sys->corrector) {   // advance_n(::CorrectedMethod), stepper.jl:142-152
+            const SplitHH m = SplitHH::of(*sys);
+            for (int64_t s = 0; s < steps; ++s) m.forward(z, dt);
+        } else if (sys->kind == CL_SYS_HH_SPLIT) {
             double pend = 0.0;
             for (int64_t s = 0; s < steps; ++s)
                 for (int k = 0; k < sys->n_stages; ++k) {

@@ -327,7 +327,7 @@ def test_adjoint(oracle):
 
 def test_corrected_methods():
     """SABAC / SBABC (tables_near.jl:100-128): the corrector coefficients of Table II (closed forms in binary64 for
-    the small n), the names and orders; the Henon-Heiles flow has no corrector force, so IntegratorMap refuses."""
+    the small n), the names and orders, and the record an IntegratorMap of the Henon-Heiles flow hands the kernel."""
     with mpmath.workprec(200):
         exact = {("SABA", 1): mpmath.mpf(1) / 12, ("SABA", 2): (2 - mpmath.sqrt(3)) / 24,
                  ("SABA", 3): (54 - 13 * mpmath.sqrt(15)) / 648, ("SBAB", 1): -mpmath.mpf(1) / 24,
@@ -343,8 +343,8 @@ def test_corrected_methods():
     assert cb.force_evaluations(cb.SABAC(2)) == cb.isolated_force_evaluations(cb.SABA(2)) + 2
     with pytest.raises(ValueError):
         cb.SABAC(11)
-    with pytest.raises(TypeError):
-        IntegratorMap(cb.SABAC(2), HenonHeilesFlow(), 0.1)
+    cs = IntegratorMap(cb.SABAC(2), HenonHeilesFlow(), 0.1).to_cl()
+    assert cs.corrector == 1 and cs.eps == cb.SABAC(2).c and cs.n_stages == cb.SABA(2).stages
 
 
 def test_pow_is_not_near_a_tie():
@@ -362,3 +362,35 @@ def test_pow_is_not_near_a_tie():
             frac = abs((v - mpmath.mpf(r)) / ulp)
         assert frac <= 0.5 and 0.5 - frac >= 1e-3
         assert r == x ** y          # the platform's pow agrees
+
+
+@pytest.mark.parametrize("make", [lambda: cb.SABAC(2), lambda: cb.SBABC(3), lambda: cb.SABAC(5)], ids=["SABAC2", "SBABC3", "SABAC5"])
+def test_corrected_method_on_the_oracle(oracle, make):
+    """The corrected step on the Henon-Heiles flow (stepper.jl:142-160): symmetric, S(-tau) S(tau) = id to
+    round-off; its tangent (the corrector Jacobians around the base table's) equals central differences of the
+    forward step; and it differs from the base table's step by the corrector's O(tau^3) kicks."""
+    m = make()
+    flow = HenonHeilesFlow()
+    rng = np.random.default_rng(8)
+    z0 = rng.uniform(-0.3, 0.3, (12, 4))
+    z1, ok1 = oracle.oracle_advance(m, flow, z0, 0.1, 1)
+    z2, ok2 = oracle.oracle_advance(m, flow, z1, -0.1, 1)
+    assert ok1.all() and ok2.all() and np.max(np.abs(z2 - z0)) <= 64 * EPS
+    zb, _ = oracle.oracle_advance(m.base, flow, z0, 0.1, 1)
+    diff = np.max(np.abs(zb - z1))
+    assert 1e-9 < diff < 1e-2
+    from chaos_b200.propagate import FrameSpec
+    sysm = IntegratorMap(m, flow, 0.1)
+    h = 1e-6
+    for z in z0[:4]:
+        # the one-step Jacobian: W after one step from W0 = I with a non-replacing chain (Benettin would normalise)
+        r = oracle.oracle_frames(sysm, z[None], 1, [FrameSpec(4, (), np.eye(4)[None])], tau=1, math="portable")[0]
+        T = r["W"][0]
+        fd = np.empty((4, 4))
+        for j in range(4):
+            e = np.zeros(4)
+            e[j] = h
+            zp, _ = oracle.oracle_advance(m, flow, (z + e)[None], 0.1, 1)
+            zm, _ = oracle.oracle_advance(m, flow, (z - e)[None], 0.1, 1)
+            fd[:, j] = (zp[0] - zm[0]) / (2 * h)
+        assert np.max(np.abs(T - fd)) <= 1e-8

@@ -6,7 +6,7 @@ from __future__ import annotations
 import numpy as np
 import pytest
 
-from chaos_b200 import (SABA, SBAB, CalvoSanzSerna4, Gauss, HenonHeilesFlow, KahanLi, Leapfrog, Ruth3, SplittingMethod,
+from chaos_b200 import (SABA, SABAC, SBAB, SBABC, CalvoSanzSerna4, Gauss, HenonHeilesFlow, KahanLi, Leapfrog, Ruth3, SplittingMethod,
                         SymplecticEuler, advance_ensemble, suzuki_jump)
 from chaos_b200.systems import random_energy_starts
 from helpers import same_bits
@@ -17,7 +17,7 @@ FLOW = HenonHeilesFlow()
 METHODS = {"DKD": Leapfrog("DKD"), "KDK": Leapfrog("KDK"), "KL6": KahanLi(6), "KL8": KahanLi(8),
            "KL7": KahanLi("s7odr6"), "SABA5": SABA(5), "SBAB4": SBAB(4), "Ruth3": Ruth3(),
            "CSS4": CalvoSanzSerna4(), "Suzuki8": suzuki_jump(Leapfrog(), 8), "SEKD": SymplecticEuler("KD"),
-           "Gauss3": Gauss()}
+           "SABAC2": SABAC(2), "SBABC4": SBABC(4), "Gauss3": Gauss()}
 
 
 def _starts(n=3000, seed=11):

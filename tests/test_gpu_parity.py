@@ -165,7 +165,8 @@ def test_henon_heiles_gauss3(oracle, k, chain, tol):
                                      (2, (QRSpectrum(MGS()),)), (2, (SALI(),)), (4, (QRSpectrum(HouseholderQR()),)),
                                      (4, (GALI(),)), (1, (Benettin(),))], ids=repr)
 @pytest.mark.parametrize("method", ["KahanLi8", "KahanLi6", "LeapfrogKDK", "SABA4", "SBAB3", "Ruth3", "CalvoSanzSerna4",
-                                    "SymplecticEulerKD", "SofroniouSpaletta10", "Suzuki8", "ABAH864"])
+                                    "SymplecticEulerKD", "SofroniouSpaletta10", "Suzuki8", "ABAH864", "SABAC2",
+                                    "SBABC3"])
 def test_henon_heiles_splitting(oracle, k, chain, method):
     """IntegratorMap(SplittingMethod, HenonHeilesFlow(), 0.05): merged-kick forward, the stage-Jacobian tangent and the
     reducers, bit for bit against the oracle on E = 1/8 energy-shell starts."""
@@ -174,7 +175,8 @@ def test_henon_heiles_splitting(oracle, k, chain, method):
     m = {"KahanLi8": lambda: cb.KahanLi(8), "KahanLi6": lambda: cb.KahanLi(6), "LeapfrogKDK": lambda: cb.Leapfrog("KDK"),
          "SABA4": lambda: cb.SABA(4), "SBAB3": lambda: cb.SBAB(3), "Ruth3": cb.Ruth3, "CalvoSanzSerna4": cb.CalvoSanzSerna4,
          "SymplecticEulerKD": lambda: cb.SymplecticEuler("KD"), "SofroniouSpaletta10": cb.SofroniouSpaletta10,
-         "Suzuki8": lambda: cb.suzuki_jump(cb.Leapfrog(), 8), "ABAH864": cb.ABAH864}[method]()
+         "Suzuki8": lambda: cb.suzuki_jump(cb.Leapfrog(), 8), "ABAH864": cb.ABAH864, "SABAC2": lambda: cb.SABAC(2),
+         "SBABC3": lambda: cb.SBABC(3)}[method]()
     n = 160
     x0 = random_energy_starts(1 / 8, n, seed=12)
     sysm = IntegratorMap(m, HenonHeilesFlow(), 0.05)
