@@ -15,11 +15,12 @@
 namespace cl {
 
 struct SplitJac { double T[16]; };
+struct SplitJacF { float T[16]; };   // mixed kernels: the step's tangent in Float32
 
 struct SysSplitHH {
     static constexpr int D = 4, S = 4;
     using Jac = SplitJac;
-    template <typename R> using JacR = SplitJac;
+    template <typename R> using JacR = typename std::conditional<sizeof(R) == 8, SplitJac, SplitJacF>::type;
     double dt;
     int n;
     int corr;       // CorrectedMethod: the corrector kick before and after every step
@@ -129,7 +130,61 @@ struct SysSplitHH {
     }
     template <int KK, typename T>
     __device__ __forceinline__ void apply(const SplitJac& Jc, T* W) const { fused_dense<4, KK>(Jc.T, W); }
-    __device__ __forceinline__ void forward(double* x, const SplitJac&) const { step(x); }
+
+    // the p rows of the Float32 product += [a c; b dd] times its q rows
+    static __device__ __forceinline__ void lower(float* T, float a, float b, float c, float dd) {
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const float q1 = T[4 * j], q2 = T[4 * j + 1];
+            T[4 * j + 2] = __fmaf_rn(a, q1, __fmaf_rn(c, q2, T[4 * j + 2]));
+            T[4 * j + 3] = __fmaf_rn(b, q1, __fmaf_rn(dd, q2, T[4 * j + 3]));
+        }
+    }
+    // Mixed kernels: the same stage sequence with the stage states in Float64 (the points where the reference
+    // evaluates each Jacobian), the product built in Float32 from the blocks of the stage Jacobians -- a drift adds
+    // t * (p rows) to the q rows, a kick subtracts t * Hs (q rows) from the p rows, the corrector adds kappa * Hc
+    // (q rows) -- instead of the dense 4 x 4 Float64 products of the plain kernel.
+    __device__ __forceinline__ void jac(const double* x, SplitJacF& Jc) const {
+        double z[4] = {x[0], x[1], x[2], x[3]};
+        float* T = Jc.T;
+#pragma unroll
+        for (int l = 0; l < 16; ++l) T[l] = (l % 5 == 0) ? 1.0f : 0.0f;
+        if (corr) {
+            double J[16];
+            corrector_jacobian(z, J);
+            lower(T, static_cast<float>(J[2]), static_cast<float>(J[3]), static_cast<float>(J[6]), static_cast<float>(J[7]));
+            corrector_kick(z);
+        }
+#pragma unroll 1
+        for (int i = 0; i < n; ++i) {
+            const double ci = c[i], di = d[i];
+            if (ci != 0.0) {
+                const float t = static_cast<float>(ci * dt);
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    T[4 * j] = __fmaf_rn(t, T[4 * j + 2], T[4 * j]);
+                    T[4 * j + 1] = __fmaf_rn(t, T[4 * j + 3], T[4 * j + 1]);
+                }
+                drift(z, ci * dt);
+            }
+            if (di != 0.0) {
+                const float mt = static_cast<float>(-(di * dt));
+                const float h11 = static_cast<float>(1 + 2 * z[1]), h12 = static_cast<float>(2 * z[0]);
+                const float h22 = static_cast<float>(1 - 2 * z[1]);
+                lower(T, mt * h11, mt * h12, mt * h12, mt * h22);
+                kick(z, di * dt);
+            }
+        }
+        if (corr) {
+            double J[16];
+            corrector_jacobian(z, J);
+            lower(T, static_cast<float>(J[2]), static_cast<float>(J[3]), static_cast<float>(J[6]), static_cast<float>(J[7]));
+        }
+    }
+    template <int KK>
+    __device__ __forceinline__ void apply(const SplitJacF& Jc, float* W) const { fused_dense<4, KK>(Jc.T, W); }
+    template <class JJ>
+    __device__ __forceinline__ void forward(double* x, const JJ&) const { step(x); }
     // one step of advance_n; a corrected method (stepper.jl:142-152): kick, the base step with its own merged
     // kicks, kick (no merging across the corrector)
     __device__ __forceinline__ void step(double* x) const {

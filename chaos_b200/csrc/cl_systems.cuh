@@ -56,6 +56,22 @@ __device__ __forceinline__ void fused_dense(const double* M, float* W) {   // mi
     for (int l = 0; l < D * K; ++l) W[l] = Wn[l];
 }
 
+template <int D, int K>
+__device__ __forceinline__ void fused_dense(const float* M, float* W) {    // mixed kernels: a Float32 tangent
+    float Wn[D * K];
+#pragma unroll
+    for (int j = 0; j < K; ++j)
+#pragma unroll
+        for (int i = 0; i < D; ++i) {
+            float acc = M[i] * W[j * D];
+#pragma unroll
+            for (int q = 1; q < D; ++q) acc = __fmaf_rn(M[i + q * D], W[q + j * D], acc);
+            Wn[i + j * D] = acc;
+        }
+#pragma unroll
+    for (int l = 0; l < D * K; ++l) W[l] = Wn[l];
+}
+
 // ---- StandardMap (standard_map.jl:8-44) and WrappedStandardMap (wrapped_standard_map.jl:12-57) -----------------
 struct StdJac { double s, c; };   // sin x, K cos x at the old x
 struct StdJacF { double s; float c; };   // mixed kernels: sin x in Float64 (orbit), K cos x in Float32 (tangent)

@@ -138,6 +138,9 @@ def menu():
     add("hh", SYS_HH, 4, 0, [(1, ["BEN"])])
     add("hh_mixed", SYS_HH, 4, 1, [(2, ["MEGNO0", "FLI0", "QR6"])])
     add("hh_mixed", SYS_HH, 4, 1, [(2, ["QR2"])])
+    # the same in the mixed kernels (Float64 orbit and stage states, Float32 tangent)
+    for ch, k in ((["MEGNO0", "FLI0", "QR6"], 2), (["QR2"], 2), (["QR4"], 4), (["GALI"], 4)):
+        add("split_mixed", SYS_SPLIT, 4, 1, [(k, ch)], minbs=(1, 2, 3, 4))
     # IntegratorMap(SplittingMethod(c, d), HenonHeilesFlow(), dt): any table of at most CL_MAX_STAGES (128) stages
     for ch in (["MEGNO0", "FLI0", "QR6"], ["QR2"], ["QR6"], ["MEGNO1"], ["FLI1"], ["SALI"], ["GALI"]):
         add("split", SYS_SPLIT, 4, 0, [(2, ch)])

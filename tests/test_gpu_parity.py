@@ -200,3 +200,26 @@ def test_propagate_orbit(oracle):
     with pytest.raises(NumericalHealthError) as e:
         propagate_orbit(StandardMap(6.0), np.array([0.1, 0.2]), np.zeros((2, 2)), 50, 5, (QRSpectrum(MGS()),), orbit=3)
     assert e.value.orbit == 3
+
+
+@pytest.mark.parametrize("method", ["KahanLi8", "SABAC2"])
+def test_henon_heiles_splitting_mixed(method):
+    """The mixed splitting kernel (Float64 orbit and stage states, Float32 tangent from the stage Jacobians'
+    blocks): the orbit bit for bit the plain kernel's, lambda_1 within 1e-3 of the plain kernel's."""
+    import chaos_b200 as cb
+    from chaos_b200 import HenonHeilesFlow, IntegratorMap, random_energy_starts
+    m = {"KahanLi8": lambda: cb.KahanLi(8), "SABAC2": lambda: cb.SABAC(2)}[method]()
+    n, N = 512, 20000
+    x0 = random_energy_starts(1 / 8, n, seed=21)
+    sysm = IntegratorMap(m, HenonHeilesFlow(), 0.05)
+    for k, chain in ((2, (MEGNO(replace=False), FLI(replace=False), QRSpectrum(GivensQR()))),
+                     (4, (QRSpectrum(HouseholderQR()),))):
+        fr = [FrameSpec(k, chain, identity_frames(n, 4, k))]
+        a = propagate_frames(sysm, x0, N, fr, tau=10, finals=False, throw=False)[0]
+        b = propagate_frames(sysm, x0, N, fr, tau=10, precision="mixed", finals=False, throw=False)[0]
+        assert same_bits(a.x, b.x)
+        key = "r2" if k == 2 else "r0"
+        la = (a.states[key]["sums"][:, 0, 0] + a.states[key]["sums"][:, 0, 1]) / N
+        lb = (b.states[key]["sums"][:, 0, 0] + b.states[key]["sums"][:, 0, 1]) / N
+        ok = (a.code == 0) & (b.code == 0)
+        assert ok.mean() > 0.99 and np.max(np.abs(la[ok] - lb[ok])) <= 1e-3
