@@ -223,3 +223,22 @@ def test_henon_heiles_splitting_mixed(method):
         lb = (b.states[key]["sums"][:, 0, 0] + b.states[key]["sums"][:, 0, 1]) / N
         ok = (a.code == 0) & (b.code == 0)
         assert ok.mean() > 0.99 and np.max(np.abs(la[ok] - lb[ok])) <= 1e-3
+
+
+@pytest.mark.parametrize("dt", [0.01, 0.05])
+def test_henon_heiles_gauss3_mixed(dt):
+    """The mixed Gauss kernel (the Float64 step, the tangent's linear system in Float32 by its fixed-point form):
+    the orbit bit for bit the plain kernel's, lambda_1 and the MEGNO average within 1e-3 of the plain kernel's."""
+    from chaos_b200 import Gauss, HenonHeilesFlow, IntegratorMap, random_energy_starts
+    n, N = 512, 20000
+    x0 = random_energy_starts(1 / 8, n, seed=23)
+    sysm = IntegratorMap(Gauss(3, tol=1e-14), HenonHeilesFlow(), dt)
+    chain = (MEGNO(replace=False), FLI(replace=False), QRSpectrum(GivensQR()))
+    fr = [FrameSpec(2, chain, identity_frames(n, 4, 2))]
+    a = propagate_frames(sysm, x0, N, fr, tau=10, finals=False, throw=False)[0]
+    b = propagate_frames(sysm, x0, N, fr, tau=10, precision="mixed", finals=False, throw=False)[0]
+    assert same_bits(a.x, b.x)
+    la = (a.states["r2"]["sums"][:, 0, 0] + a.states["r2"]["sums"][:, 0, 1]) / N
+    lb = (b.states["r2"]["sums"][:, 0, 0] + b.states["r2"]["sums"][:, 0, 1]) / N
+    ok = (a.code == 0) & (b.code == 0)
+    assert ok.mean() > 0.99 and np.max(np.abs(la[ok] - lb[ok])) <= 1e-3
