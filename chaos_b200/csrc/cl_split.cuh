@@ -15,7 +15,7 @@
 namespace cl {
 
 struct SplitJac { double T[16]; };
-struct SplitJacF { float T[16]; };   // mixed kernels: the step's tangent in Float32
+struct SplitJacF { float T[16]; double xn[4]; };   // mixed kernels: the step's tangent in Float32 and the new point
 
 struct SysSplitHH {
     static constexpr int D = 4, S = 4;
@@ -140,10 +140,11 @@ struct SysSplitHH {
             T[4 * j + 3] = __fmaf_rn(b, q1, __fmaf_rn(dd, q2, T[4 * j + 3]));
         }
     }
-    // Mixed kernels: the same stage sequence with the stage states in Float64 (the points where the reference
-    // evaluates each Jacobian), the product built in Float32 from the blocks of the stage Jacobians -- a drift adds
-    // t * (p rows) to the q rows, a kick subtracts t * Hs (q rows) from the p rows, the corrector adds kappa * Hc
-    // (q rows) -- instead of the dense 4 x 4 Float64 products of the plain kernel.
+    // Mixed kernels: one pass along the forward step (advance_n's merged kicks, Float64 points) that also builds
+    // the step's tangent in Float32 from the blocks of the Jacobians of the sub-steps it takes -- a drift adds
+    // t * (p rows) to the q rows, a kick subtracts t * Hs (q rows) from the p rows (a merged kick's Jacobian is the
+    // product of its parts' at the same q), the corrector adds kappa * Hc (q rows) -- instead of the plain kernel's
+    // separate unmerged tangent pass with dense 4 x 4 Float64 products.
     __device__ __forceinline__ void jac(const double* x, SplitJacF& Jc) const {
         double z[4] = {x[0], x[1], x[2], x[3]};
         float* T = Jc.T;
@@ -155,10 +156,12 @@ struct SysSplitHH {
             lower(T, static_cast<float>(J[2]), static_cast<float>(J[3]), static_cast<float>(J[6]), static_cast<float>(J[7]));
             corrector_kick(z);
         }
+        double pend = 0.0;
 #pragma unroll 1
         for (int i = 0; i < n; ++i) {
-            const double ci = c[i], di = d[i];
+            const double ci = c[i];
             if (ci != 0.0) {
+                if (pend != 0.0) { kick_t(z, T, pend * dt); pend = 0.0; }
                 const float t = static_cast<float>(ci * dt);
 #pragma unroll
                 for (int j = 0; j < 4; ++j) {
@@ -167,24 +170,33 @@ struct SysSplitHH {
                 }
                 drift(z, ci * dt);
             }
-            if (di != 0.0) {
-                const float mt = static_cast<float>(-(di * dt));
-                const float h11 = static_cast<float>(1 + 2 * z[1]), h12 = static_cast<float>(2 * z[0]);
-                const float h22 = static_cast<float>(1 - 2 * z[1]);
-                lower(T, mt * h11, mt * h12, mt * h12, mt * h22);
-                kick(z, di * dt);
-            }
+            pend = pend + d[i];
         }
+        if (pend != 0.0) kick_t(z, T, pend * dt);
         if (corr) {
             double J[16];
             corrector_jacobian(z, J);
             lower(T, static_cast<float>(J[2]), static_cast<float>(J[3]), static_cast<float>(J[6]), static_cast<float>(J[7]));
+            corrector_kick(z);
         }
+#pragma unroll
+        for (int l = 0; l < 4; ++l) Jc.xn[l] = z[l];
+    }
+    // a kick of time t on the Float64 point and its Jacobian [[I, 0], [-t Hs, I]] on the Float32 tangent
+    static __device__ __forceinline__ void kick_t(double* z, float* T, double t) {
+        const float mt = static_cast<float>(-t);
+        const float h11 = static_cast<float>(1 + 2 * z[1]), h12 = static_cast<float>(2 * z[0]);
+        const float h22 = static_cast<float>(1 - 2 * z[1]);
+        lower(T, mt * h11, mt * h12, mt * h12, mt * h22);
+        kick(z, t);
     }
     template <int KK>
     __device__ __forceinline__ void apply(const SplitJacF& Jc, float* W) const { fused_dense<4, KK>(Jc.T, W); }
-    template <class JJ>
-    __device__ __forceinline__ void forward(double* x, const JJ&) const { step(x); }
+    __device__ __forceinline__ void forward(double* x, const SplitJac&) const { step(x); }
+    __device__ __forceinline__ void forward(double* x, const SplitJacF& J) const {   // the point jac took the step to
+#pragma unroll
+        for (int l = 0; l < 4; ++l) x[l] = J.xn[l];
+    }
     // one step of advance_n; a corrected method (stepper.jl:142-152): kick, the base step with its own merged
     // kicks, kick (no merging across the corrector)
     __device__ __forceinline__ void step(double* x) const {
