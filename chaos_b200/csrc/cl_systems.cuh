@@ -127,9 +127,17 @@ struct SysStandard {
     }
 };
 
-// _reduce (wrapped_standard_map.jl:15-28)
+// _reduce (wrapped_standard_map.jl:15-28). The count a = floor(u / tp) of the IEEE quotient is taken from
+// q = u * RN(1 / tp) where that is provably the same: |q - u / tp| <= 2^-52 |q| and RN(u / tp) lies within half an
+// ulp of u / tp, so when the fraction of q is more than 2^-50 |q| + 2^-52 away from 0 and 1 (the 2^-52 covers the
+// rounding of the fraction itself), floor(q) = floor(RN(u / tp)). Otherwise -- near an integer, 0, |q| >= 2^51,
+// NaN or Inf -- the division decides, as in the reference. The remainder and the guards are the reference's.
 __device__ __forceinline__ void wrap_reduce(double u, double tp, double& r, double& a) {
-    a = floor(u / tp);
+    const double q = u * (1.0 / tp);
+    const double k = floor(q);
+    const double f = q - k;
+    const double margin = fabs(q) * 0x1p-50 + 0x1p-52;
+    a = (f > margin && f < 1.0 - margin) ? k : floor(u / tp);
     r = u - tp * a;
     if (r < 0) { r += tp; a -= 1; }
     if (r >= tp) { r -= tp; a += 1; }
