@@ -7,7 +7,7 @@ from __future__ import annotations
 
 import ctypes as C
 
-ABI_VERSION = 2
+ABI_VERSION = 3
 MAX_FRAMES = 3
 MAX_REDUCERS = 4
 MAX_STAGES = 128

@@ -115,7 +115,7 @@ function clrun(sys, d, s, k, tau, N, n0, steps, reducers, seed, base)
     rs = map(clred, reducers)
     length(rs) <= 4 || throw(ClB200Error(-3, "more than four reducers"))
     fr = ClFrame(k, length(rs), ntuple(i -> i <= length(rs) ? rs[i] : ClReducer(0, 0, 0, 0, 0), 4))
-    return ClRun(2, d, s, tau, N, n0, steps, 1, 0, seed % UInt64, base, clsys(sys), (fr, NOFRAME, NOFRAME))
+    return ClRun(3, d, s, tau, N, n0, steps, 1, 0, seed % UInt64, base, clsys(sys), (fr, NOFRAME, NOFRAME))
 end
 
 function last_error()

@@ -44,7 +44,7 @@ extern "C" {
 #define CL_API
 #endif
 
-#define CL_B200_ABI_VERSION 2
+#define CL_B200_ABI_VERSION 3
 #define CL_MAX_FRAMES 3
 #define CL_MAX_REDUCERS 4
 #define CL_MAX_DIM 16
