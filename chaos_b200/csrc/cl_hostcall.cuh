@@ -25,9 +25,17 @@ void pool_free(void* p, cudaStream_t st);
 // Write one byte in every page of a caller's output array while the device computes: a fresh array's pages are
 // mapped and zeroed by the operating system on first touch, and when that happens inside the copy back from the
 // device it costs about as much as the copy itself (38 MB: 9.4 ms into fresh pages, 2.3 ms into touched ones); here
-// it overlaps the kernels. The array's contents are overwritten by the copy that follows.
+// it overlaps the kernels. The array's contents are overwritten by the copy that follows. Only pageable memory is
+// touched: a copy from it to the device has read it before cudaMemcpyAsync returns, while a pinned (or managed)
+// array is resident already and may still be in flight as an input.
 inline void touch_pages(void* p, size_t bytes) {
     if (!p || !bytes) return;
+    cudaPointerAttributes at;
+    if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+        cudaGetLastError();
+        return;
+    }
+    if (at.type != cudaMemoryTypeUnregistered) return;
     volatile char* c = static_cast<volatile char*>(p);
     for (size_t o = 0; o < bytes; o += 4096) c[o] = 0;
     c[bytes - 1] = 0;
