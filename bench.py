@@ -176,7 +176,7 @@ def main() -> None:
     ap.add_argument("--only", choices=["fp64", "mixed"], default=None,
                     help="time one kernel of the default workload and print a short line (a small case for ncu)")
     ap.add_argument("--workload", default="coupled", choices=["coupled", "standard", "gauss", "lattice", "screen", "mlp", "split", "shadow",
-                                                             "record", "indicators", "advance", "torus"])
+                                                             "record", "indicators", "advance", "torus", "record_mixed"])
     args = ap.parse_args()
     if args.workload != "coupled":
         run_workload(args)
@@ -809,7 +809,7 @@ def workload_shadow(args):
                         cpu)
 
 
-def workload_record(args):
+def workload_record(args, precision="fp64"):
     from chaos_b200 import MGS, QRSpectrum, WrappedStandardMap, torus_state
     from chaos_b200.propagate import build_run, FrameSpec
     import ctypes as C_
@@ -820,7 +820,7 @@ def workload_record(args):
     xp = np.random.default_rng(SEED).uniform(0, 2 * np.pi, (n, 2))
     x0 = np.array([torus_state(z) for z in xp])
     grid = np.unique(np.round(np.logspace(0, np.log10(N), 100)).astype(np.int64))
-    run = build_run(sysm, N, tau, [FrameSpec(2, (QRSpectrum(MGS()),))], "fp64", SEED)
+    run = build_run(sysm, N, tau, [FrameSpec(2, (QRSpectrum(MGS()),))], precision, SEED)
     ncol = L.cl_b200_record_columns(C_.byref(run))
     sb = L.cl_b200_record_state_bytes(C_.byref(run))
 
@@ -849,10 +849,11 @@ def workload_record(args):
         O.oracle_record(sysm, x0[:512], 20000, tau, QRSpectrum(MGS()), g, threads=threads)
         return dict(value=512 * 20000 / (time.perf_counter() - t), unit="orbit-steps/s", cores=threads, kind="port",
                     sample="512 orbits x 20000 steps with the grid rows up to 20000 (oracle, all host threads)")
-    _host_call_workload(args, "orbit-steps/s (study recorder, wrapped standard map K=6, QRSpectrum(MGS), 100 grid "
-                        "rows)", "orbit-steps/s", n * N, call,
+    _host_call_workload(args, f"orbit-steps/s (study recorder, wrapped standard map K=6, QRSpectrum(MGS), 100 grid "
+                        f"rows, {precision})", "orbit-steps/s", n * N, call,
                         dict(workload=f"record-wrapped-k6-{n}x{N:.0e}-tau1-mgs-{len(grid)}rows", orbits=n, N=N, tau=tau,
-                             grid_rows=int(len(grid))), cpu)
+                             grid_rows=int(len(grid)), precision=precision), cpu,
+                        dtype="f64" if precision == "fp64" else "f64 orbit + f32 frame")
 
 
 def workload_indicators(args):
@@ -986,7 +987,7 @@ def run_workload(args):
     {"standard": workload_standard, "gauss": workload_gauss, "lattice": workload_lattice,
      "screen": workload_screen, "mlp": workload_mlp, "split": workload_split, "shadow": workload_shadow,
      "record": workload_record, "indicators": workload_indicators, "advance": workload_advance,
-     "torus": workload_torus}[args.workload](args)
+     "torus": workload_torus, "record_mixed": lambda a: workload_record(a, "mixed")}[args.workload](args)
 
 
 

@@ -45,12 +45,14 @@ struct RecArgs {
     RedParams prm;
 };
 
-template <class Sys, class Est, int K>
+// Real = double: the reference's arithmetic; Real = float: the mixed recorder (Float64 orbit, monitor and log sums,
+// Float32 frame and QR), as the mixed orbit kernels.
+template <class Sys, class Est, int K, typename Real = double>
 struct RecOrbit {
     static constexpr int D = Sys::D, S = Sys::S;
     using EstState = typename Est::template State<D, K>;
     double x[S];
-    double W[D * K];
+    Real W[D * K];
     EstState est;
     MonState mon;
 
@@ -58,7 +60,7 @@ struct RecOrbit {
     __device__ __forceinline__ int8_t body(const Sys& sys, i64& n, i64 steps, i64 N, int tau, const RedParams& prm) {
         for (i64 h = 0; h < steps / tau; ++h) {
             for (int t = 0; t < tau; ++t) {
-                typename Sys::Jac J;
+                typename Sys::template JacR<Real> J;
                 sys.jac(x, J);
                 sys.template apply<K>(J, W);
                 sys.forward(x, J);
@@ -92,9 +94,9 @@ template <int ALG> struct EstFinal<RQR<ALG>> {
     }
 };
 
-template <class Sys, class Est, int K>
+template <class Sys, class Est, int K, typename Real>
 __global__ void __launch_bounds__(128) record_kernel(const RecArgs a, const Sys sys) {
-    using O = RecOrbit<Sys, Est, K>;
+    using O = RecOrbit<Sys, Est, K, Real>;
     constexpr int S = O::S, D = O::D, NCOL = K + 7 + S;
     constexpr int EW = sizeof(typename O::EstState) / 8, MW = sizeof(MonState) / 8;
     const i64 i = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x;
@@ -104,7 +106,7 @@ __global__ void __launch_bounds__(128) record_kernel(const RecArgs a, const Sys 
 #pragma unroll
     for (int c = 0; c < S; ++c) o.x[c] = a.x[i * S + c];
 #pragma unroll
-    for (int l = 0; l < D * K; ++l) o.W[l] = a.W[i * D * K + l];
+    for (int l = 0; l < D * K; ++l) o.W[l] = static_cast<Real>(a.W[i * D * K + l]);
     uint64_t* st = a.states + i * (EW + MW);
     uint64_t* ew = reinterpret_cast<uint64_t*>(&o.est);
     uint64_t* mw = reinterpret_cast<uint64_t*>(&o.mon);
@@ -152,7 +154,7 @@ __global__ void __launch_bounds__(128) record_kernel(const RecArgs a, const Sys 
 #pragma unroll
     for (int k2 = 0; k2 < S; ++k2) a.x[i * S + k2] = o.x[k2];
 #pragma unroll
-    for (int l = 0; l < D * K; ++l) a.W[i * D * K + l] = o.W[l];
+    for (int l = 0; l < D * K; ++l) a.W[i * D * K + l] = static_cast<double>(o.W[l]);
 #pragma unroll
     for (int w = 0; w < EW; ++w) st[w] = ew[w];
 #pragma unroll
@@ -163,35 +165,42 @@ __global__ void __launch_bounds__(128) record_kernel(const RecArgs a, const Sys 
 
 typedef cudaError_t (*RecordFn)(const cl_run& run, const RecArgs& a, cudaStream_t st);
 
-template <class Sys, class Est, int K>
+template <class Sys, class Est, int K, typename Real>
 cudaError_t launch_record(const cl_run& run, const RecArgs& a, cudaStream_t st) {
     const Sys sys = SysMaker<Sys>::make(run, nullptr);
-    record_kernel<Sys, Est, K><<<static_cast<unsigned>((a.n + 127) / 128), 128, 0, st>>>(a, sys);
+    record_kernel<Sys, Est, K, Real><<<static_cast<unsigned>((a.n + 127) / 128), 128, 0, st>>>(a, sys);
     return cudaGetLastError();
 }
 
-template <class Sys>
+template <class Sys, typename Real>
 RecordFn record_fn_for(const cl_frame& f) {
     const cl_reducer& r = f.reducers[0];
-    if (f.k == 1 && r.kind == CL_RED_BENETTIN) return launch_record<Sys, RBenettin, 1>;
+    if (f.k == 1 && r.kind == CL_RED_BENETTIN) return launch_record<Sys, RBenettin, 1, Real>;
     if (f.k != 2 || r.kind != CL_RED_QR) return nullptr;
     switch (r.alg) {
-        case CL_QR_CGS: return launch_record<Sys, RQR<CL_QR_CGS>, 2>;
-        case CL_QR_MGS: return launch_record<Sys, RQR<CL_QR_MGS>, 2>;
-        case CL_QR_RGS: return launch_record<Sys, RQR<CL_QR_RGS>, 2>;
-        case CL_QR_HOUSEHOLDER: return launch_record<Sys, RQR<CL_QR_HOUSEHOLDER>, 2>;
-        case CL_QR_AUGMENTED: return launch_record<Sys, RQR<CL_QR_AUGMENTED>, 2>;
+        case CL_QR_CGS: return launch_record<Sys, RQR<CL_QR_CGS>, 2, Real>;
+        case CL_QR_MGS: return launch_record<Sys, RQR<CL_QR_MGS>, 2, Real>;
+        case CL_QR_RGS: return launch_record<Sys, RQR<CL_QR_RGS>, 2, Real>;
+        case CL_QR_HOUSEHOLDER: return launch_record<Sys, RQR<CL_QR_HOUSEHOLDER>, 2, Real>;
+        case CL_QR_AUGMENTED: return launch_record<Sys, RQR<CL_QR_AUGMENTED>, 2, Real>;
+    }
+    return nullptr;
+}
+
+template <typename Real>
+RecordFn record_fn_prec(const cl_run& r) {
+    switch (r.sys.kind) {
+        case CL_SYS_STANDARD: return record_fn_for<SysStandard, Real>(r.frames[0]);
+        case CL_SYS_WRAPPED_STANDARD: return record_fn_for<SysWrapped, Real>(r.frames[0]);
+        case CL_SYS_LINEAR: return r.d == 2 ? record_fn_for<SysLinear<2>, Real>(r.frames[0]) : nullptr;
     }
     return nullptr;
 }
 
 RecordFn record_fn(const cl_run& r) {
-    if (r.n_frames != 1 || r.frames[0].n_reducers != 1 || r.precision != CL_PREC_FP64) return nullptr;
-    switch (r.sys.kind) {
-        case CL_SYS_STANDARD: return record_fn_for<SysStandard>(r.frames[0]);
-        case CL_SYS_WRAPPED_STANDARD: return record_fn_for<SysWrapped>(r.frames[0]);
-        case CL_SYS_LINEAR: return r.d == 2 ? record_fn_for<SysLinear<2>>(r.frames[0]) : nullptr;
-    }
+    if (r.n_frames != 1 || r.frames[0].n_reducers != 1) return nullptr;
+    if (r.precision == CL_PREC_FP64) return record_fn_prec<double>(r);
+    if (r.precision == CL_PREC_MIXED) return record_fn_prec<float>(r);
     return nullptr;
 }
 

@@ -49,11 +49,13 @@ class RecordResult:
         return self.R[:, :, k + COLUMNS.index(name) - 1]
 
 
-def record(sys, x0, N: int, tau: int, estimator, grid, *, W0=None, launch_steps: int | None = None) -> RecordResult:
+def record(sys, x0, N: int, tau: int, estimator, grid, *, W0=None, launch_steps: int | None = None,
+           precision: str = "fp64") -> RecordResult:
     """Record n orbits of `sys` (StandardMap, WrappedStandardMap or a 2 x 2 LinearSymplecticMap) with `estimator`
     (Benettin() with k = 1, or QRSpectrum(CGS / MGS / RGS / HouseholderQR / AugmentedQR) with k = 2) at the step
     counts `grid` (increasing multiples of tau, at most N). W0 defaults to I[:, 1:k]; `launch_steps` splits the run
-    into launches that carry everything (the grid rows of a launch are written by it)."""
+    into launches that carry everything (the grid rows of a launch are written by it). `precision` "mixed" keeps the
+    orbit, the monitor and the log sums in Float64 and the frame and its QR in Float32."""
     x0 = np.ascontiguousarray(np.asarray(x0, dtype=np.float64))
     n, s = x0.shape
     d = sys.d
@@ -67,7 +69,7 @@ def record(sys, x0, N: int, tau: int, estimator, grid, *, W0=None, launch_steps:
     L = int(launch_steps) if launch_steps else int(N)
     if L % tau:
         raise ValueError("launch_steps must be a multiple of tau")
-    run = build_run(sys, N, tau, [FrameSpec(k, (estimator,))], "fp64", 0, steps=L)
+    run = build_run(sys, N, tau, [FrameSpec(k, (estimator,))], precision, 0, steps=L)
     Lb = lib()
     ncol = Lb.cl_b200_record_columns(C.byref(run))
     sb = Lb.cl_b200_record_state_bytes(C.byref(run))

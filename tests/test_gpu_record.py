@@ -93,3 +93,17 @@ def test_shadow_record_matches_oracle(oracle, name, L):
     assert same_bits(R, rR) and np.array_equal(fail, rfail)
     assert np.array_equal(_words(ends), _words(rends))
     assert fail[5] == 1
+
+
+@pytest.mark.parametrize("name", ["wrapped", "standard"])
+def test_record_mixed(name):
+    """The mixed recorder (Float64 orbit, monitor and log sums, Float32 frame and QR): the orbit bit for bit the
+    plain recorder's and every exponent row within 1e-3 of it."""
+    sysm, x0 = _system(name)
+    grid = np.array([10, 100, 1000, 5000])
+    a = record(sysm, x0, 5000, 1, QRSpectrum(MGS()), grid)
+    b = record(sysm, x0, 5000, 1, QRSpectrum(MGS()), grid, precision="mixed")
+    assert same_bits(a.x, b.x)
+    ok = (a.code == 0) & (b.code == 0)
+    assert ok.mean() > 0.99
+    assert np.max(np.abs(a.R[ok][:, :, :2] - b.R[ok][:, :, :2])) <= 1e-3
