@@ -183,7 +183,7 @@ int cl_b200_advance_ensemble(const cl_system* sys, int64_t n, const double* x0, 
         cudaEventRecord(e1, st);
         ++launches;
         if (rc) break;
-        touch_pages(out + 4 * lo, sizeof(double) * 4 * len);
+        if (out != x0) touch_pages(out + 4 * lo, sizeof(double) * 4 * len);   // an in-place call keeps its input
         touch_pages(ok + lo, static_cast<size_t>(len));
         cudaMemcpyAsync(out + 4 * lo, dout, sizeof(double) * 4 * len, cudaMemcpyDeviceToHost, st);
         cudaMemcpyAsync(ok + lo, dok, len, cudaMemcpyDeviceToHost, st);

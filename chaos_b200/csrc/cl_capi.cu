@@ -525,13 +525,17 @@ int cl_b200_propagate(const cl_run* run, int64_t n, const cl_buffers* h, cl_prov
         if (e != cudaSuccess) { cudaEventDestroy(e0); cudaEventDestroy(e1); return map_cuda(e, "orbit kernel launch"); }
     }
     cudaEventRecord(e1, st);
-    // the inputs are staged (pageable copies return once the source is read), so the outputs' pages can be touched
-    touch_pages(h->x, sizeof(double) * n * s);
-    for (int f = 0; f < nf; ++f) {
-        touch_pages(h->W[f], sizeof(double) * n * d * run->frames[f].k);
-        touch_pages(h->states[f], static_cast<size_t>(frame_bytes(run->frames[f]) * n));
-        touch_pages(h->code[f], static_cast<size_t>(n));
-        if (h->hstep[f]) touch_pages(h->hstep[f], sizeof(int64_t) * n);
+    // The inputs are staged (pageable copies return once the source is read), so the outputs' pages can be touched.
+    // Only arrays that are outputs alone: an array that was also copied in (a carried launch window, or x given as
+    // x0) keeps the caller's values if a kernel or a copy back fails.
+    if (!carry) {
+        if (h->x != h->x0) touch_pages(h->x, sizeof(double) * n * s);
+        for (int f = 0; f < nf; ++f) {
+            if (h->W[f] != h->W0[f]) touch_pages(h->W[f], sizeof(double) * n * d * run->frames[f].k);
+            touch_pages(h->states[f], static_cast<size_t>(frame_bytes(run->frames[f]) * n));
+            touch_pages(h->code[f], static_cast<size_t>(n));
+            if (h->hstep[f]) touch_pages(h->hstep[f], sizeof(int64_t) * n);
+        }
     }
     if ((e = cudaMemcpyAsync(h->x, dx, sizeof(double) * n * s, cudaMemcpyDeviceToHost, st)) != cudaSuccess) return map_cuda(e, "D2H");
     for (int f = 0; f < nf; ++f) {

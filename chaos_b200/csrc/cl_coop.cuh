@@ -430,14 +430,11 @@ cudaError_t launch_coop_v(const cl_run& run, const EArgs& a, int grid, cudaStrea
     const SysChain<NS> sys = SysMaker<SysChain<NS>>::make(run, nullptr);
     auto k = coop_kernel<NS, Real, K, U, MINB>;
     const size_t smem = static_cast<size_t>(128 / NS) * CoopSmem<2 * NS, K>::words * sizeof(Real);
-    // the workspace of one block can exceed the 48 KB default (d = 16 in Float64: 57 KB); one attribute call per
-    // instantiation (idempotent, so two threads racing on the flag is harmless)
-    static bool attr = false;
-    if (!attr) {
-        const cudaError_t ea = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
-        if (ea != cudaSuccess) return ea;
-        attr = true;
-    }
+    // the workspace of one block can exceed the 48 KB default (d = 16 in Float64: 57 KB). The attribute belongs to
+    // the current device's context, so it is set before every launch (a cheap, idempotent host call) rather than
+    // cached once per process.
+    const cudaError_t ea = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+    if (ea != cudaSuccess) return ea;
     k<<<grid, 128, smem, st>>>(a, sys);
     cudaError_t e = cudaGetLastError();
     if (info) {

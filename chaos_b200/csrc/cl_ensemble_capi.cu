@@ -170,6 +170,16 @@ void register_ensemble(const char* key, ELaunchFn fn) { ereg().emplace_back(key,
 
 // The classes one after another on `st`, each class's queue head at heads[c] (already zeroed by the caller). Creates
 // no stream, event or buffer: the entry point without allocations (cl_noalloc.cu) runs through here.
+// Every class checked (menu, sizes, buffers) before anything is enqueued: 0 or the first error.
+int validate_classes(const cl_ensemble_class* cs, int nc) {
+    for (int c = 0; c < nc; ++c) {
+        ELaunchFn fn = nullptr;
+        const int v = check_class(cs[c], &fn);
+        if (v) return v;
+    }
+    return 0;
+}
+
 int enqueue_classes_in_order(const cl_ensemble_class* cs, int nc, unsigned long long* heads, cudaStream_t st) {
     std::vector<ELaunchFn> fns(nc);
     for (int c = 0; c < nc; ++c) {
@@ -257,8 +267,9 @@ int cl_b200_ensemble(const cl_ensemble_class* classes, int32_t n_classes, cl_pro
     for (int c = 0; c < n_classes && rc == 0; ++c) {   // outputs' first touch overlaps the kernels
         const cl_ensemble_class& h = classes[c];
         const int64_t n = h.n_orbits, dk = int64_t(h.run.d) * h.run.frames[0].k;
-        touch_pages(h.buf.x, static_cast<size_t>(8 * n * h.run.s));
-        touch_pages(h.buf.W[0], static_cast<size_t>(8 * n * dk));
+        // outputs alone: an array that is also the class's input keeps the caller's values if the run fails
+        if (h.buf.x != h.buf.x0) touch_pages(h.buf.x, static_cast<size_t>(8 * n * h.run.s));
+        if (h.buf.W[0] != h.buf.W0[0]) touch_pages(h.buf.W[0], static_cast<size_t>(8 * n * dk));
         touch_pages(h.buf.states[0], static_cast<size_t>(capi_frame_bytes(h.run.frames[0]) * n));
         touch_pages(h.buf.code[0], static_cast<size_t>(n));
         if (h.buf.hstep[0]) touch_pages(h.buf.hstep[0], static_cast<size_t>(8 * n));

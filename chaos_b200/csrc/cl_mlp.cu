@@ -160,6 +160,7 @@ __global__ void __launch_bounds__(128, 1) gemm_bf16_tc(const __nv_bfloat16* __re
         }
         cp_async_commit();
     }
+    int issued = -1;   // the last block whose MMAs were committed (thread 0 commits; the count is uniform)
     for (int i = 0; i < nkb && ok; ++i) {
         const int s = i % STAGES;
         cp_async_wait<STAGES - 2>();          // this thread's copies of block i have landed
@@ -181,13 +182,18 @@ __global__ void __launch_bounds__(128, 1) gemm_bf16_tc(const __nv_bfloat16* __re
             asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n"
                          :: "r"(smem_u32(&mbar[s])) : "memory");
         }
-        // refill the stage of block i - 1 with block i + STAGES - 1, once block i - 1's MMAs are done with it
+        issued = i;
+        // refill the stage of block i - 1 with block i + STAGES - 1, once block i - 1's MMAs are done with it. Every
+        // thread waits (bounded) and the CTA then agrees: one thread that gives up makes all of them leave the loop
+        // at this same iteration, so every later barrier is reached by all threads.
         const int nx = i + STAGES - 1;
-        if (nx < nkb) {
+        if (nx < nkb) {   // uniform: i and nkb are the same in every thread
+            bool w = true;
             if (i >= 1) {
                 const int ps = (i - 1) % STAGES;
-                ok = mbar_wait(smem_u32(&mbar[ps]), static_cast<uint32_t>(((i - 1) / STAGES) & 1));
+                w = mbar_wait(smem_u32(&mbar[ps]), static_cast<uint32_t>(((i - 1) / STAGES) & 1));
             }
+            ok = __syncthreads_and(w) != 0;
             if (ok) {
                 const uint32_t st = sbase + (nx % STAGES) * STAGE_BYTES;
                 stage_tile<BM>(st, A, lda, m0, M, (kb0 + nx) * BK, K, tid);
@@ -197,8 +203,14 @@ __global__ void __launch_bounds__(128, 1) gemm_bf16_tc(const __nv_bfloat16* __re
         cp_async_commit();
     }
     cp_async_wait<0>();
-    // the last block's commit completes after every earlier MMA
-    if (ok && nkb > 0) ok = mbar_wait(smem_u32(&mbar[(nkb - 1) % STAGES]), static_cast<uint32_t>(((nkb - 1) / STAGES) & 1));
+    // The last committed block's barrier completes after every earlier MMA (they run in issue order). It is awaited
+    // whether or not an earlier wait gave up, so the accumulator is neither read nor deallocated while an MMA that
+    // was issued may still write it; a second give-up leaves the error flag set and the tile unwritten.
+    {
+        bool w = true;
+        if (issued >= 0) w = mbar_wait(smem_u32(&mbar[issued % STAGES]), static_cast<uint32_t>((issued / STAGES) & 1));
+        ok = __syncthreads_and(w && ok) != 0;
+    }
     asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
 
     if (ok && nkb > 0) {
@@ -421,12 +433,9 @@ cudaError_t launch_gemm(const void* A, int lda, const void* B, int ldb, int M, i
     constexpr int STAGES = NT >= 256 ? 2 : 3;
     constexpr int smem = STAGES * (BM + NT) * BK * 2;
     auto k = gemm_bf16_tc<NT, STAGES>;
-    static bool attr = false;   // one attribute call per instantiation (idempotent)
-    if (!attr) {
-        const cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-        if (e != cudaSuccess) return e;
-        attr = true;
-    }
+    // the attribute belongs to the current device's context: set before every launch (cheap and idempotent)
+    const cudaError_t ea = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (ea != cudaSuccess) return ea;
     dim3 grid((M + BM - 1) / BM, (N + NT - 1) / NT, splits);
     k<<<grid, 128, smem, st>>>(static_cast<const __nv_bfloat16*>(A), lda, static_cast<const __nv_bfloat16*>(B), ldb,
                                M, N, K, bias, epi, C32, static_cast<__nv_bfloat16*>(Cb), ldc, pre, acc);

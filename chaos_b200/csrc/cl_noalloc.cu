@@ -12,7 +12,9 @@
 // symbol itself: once per device, with that device current, the first call asks the runtime for the array's device
 // address (cudaGetSymbolAddress) and keeps it; every call passes that address to the kernels. That first call on
 // a device should come before any stream capture. Every call shares the array and clears the heads it uses
-// (cudaMemsetAsync, on the caller's stream) before its launches; calls that overlap on the GPU race on it.
+// (cudaMemsetAsync, on the caller's stream) before its launches; calls that overlap on the GPU race on it. A call
+// whose classes are rejected enqueues nothing. The address is kept for the life of the process, so the device must
+// not be reset (cudaDeviceReset, or a reset of its primary context) between calls.
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -25,6 +27,7 @@ namespace cl {
 
 int capi_fail(int code, const std::string& msg);
 int capi_map_cuda(cudaError_t e, const char* where);
+int validate_classes(const cl_ensemble_class* cs, int nc);
 int enqueue_classes_in_order(const cl_ensemble_class* cs, int nc, unsigned long long* heads, cudaStream_t st);
 
 namespace {
@@ -62,8 +65,11 @@ extern "C" int cl_b200_ensemble_device_noalloc(const cl_ensemble_class* classes,
     if (n_classes > CL_NOALLOC_MAX_CLASSES)
         return capi_fail(CL_EINVAL, "at most " + std::to_string(CL_NOALLOC_MAX_CLASSES) +
                                         " classes per call without allocation (the fixed queue-head array)");
+    // a rejected call enqueues nothing, not even the clearing of the shared heads
+    int rc = validate_classes(classes, n_classes);
+    if (rc) return rc;
     unsigned long long* heads = nullptr;
-    int rc = heads_on_current_device(&heads);
+    rc = heads_on_current_device(&heads);
     if (rc) return rc;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     const cudaError_t e = cudaMemsetAsync(heads, 0, sizeof(unsigned long long) * n_classes, st);

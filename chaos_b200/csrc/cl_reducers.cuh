@@ -190,7 +190,7 @@ struct RGALI {
                 S.s.n = n;
             }
         }
-        T g = T(1);   // _gram_core!, gali.jl:214-234
+        T g = T(1);   // _gram_core!, gali.jl:81-100
 #pragma unroll
         for (int j = 0; j < K; ++j) {
 #pragma unroll
@@ -268,7 +268,7 @@ struct RFLI {
         if (!pair_norms(st, n, a1, a2)) return;
         cs_add(st.s1, lnr(a1));
         cs_add(st.s2, lnr(a2));
-        const double S1 = cs_total(st.s1), S2 = cs_total(st.s2);   // fli_maxima, fli.jl:187-193
+        const double S1 = cs_total(st.s1), S2 = cs_total(st.s2);   // fli_maxima, fli.jl:54-60
         if (S1 > st.f1) { st.f1 = S1; st.step1 = n; }
         if (S1 > st.fB) { st.fB = S1; st.stepB = n; st.colB = 1; }
         if (S2 > st.fB) { st.fB = S2; st.stepB = n; st.colB = 2; }

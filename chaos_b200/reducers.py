@@ -188,7 +188,7 @@ class GALI(Reducer):
         return np.dtype([("s", "<f8", (k,)), ("c", "<f8", (k,)), ("gali", "<f8", (k - 1,)), ("value", "<f8"),
                          ("n", "<i8"), ("step", "<i8"), ("code", "i1"), ("_p0", "V7"), ("column", "<i8")])
 
-    def final(self, st, d=None):   # gali.jl:319-332
+    def final(self, st, d=None):   # gali.jl:186-199
         k = st["s"].shape[0]
         n = int(st["n"])
         L = None
@@ -295,7 +295,7 @@ class FLI(Reducer):
                                                  ("step", "<i8"), ("step1", "<i8"), ("stepB", "<i8"), ("code", "i1"),
                                                  ("column", "i1"), ("colB", "i1"), ("_p0", "V5")])
 
-    def final(self, st):   # fli.jl:224-227
+    def final(self, st):   # fli.jl:91-94
         return dict(n=int(st["n"]), fli=float(st["fB"]), fli1=float(st["f1"]),
                     sum=np.array([st["s1_s"], st["s2_s"]], dtype=np.float64),
                     comp=np.array([st["s1_c"], st["s2_c"]], dtype=np.float64),

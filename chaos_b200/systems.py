@@ -440,7 +440,7 @@ def adjoint_method(m):
 
 
 def _palindromic_leapfrog(half, order, name, source, digits) -> SplittingMethod:
-    """The leapfrog (DKD) composed with the step fractions half + reversed(half[:-1]) (splitting.jl:180-182)."""
+    """The leapfrog (DKD) composed with the step fractions half + reversed(half[:-1]) (splitting.jl:176-178)."""
     half = list(half)
     return _compose(Leapfrog("DKD"), half + half[-2::-1], order, name, source=source, digits=digits)
 
@@ -692,7 +692,7 @@ def _corrector_c(n: int, sbab: bool) -> float:
 
 @dataclass(frozen=True)
 class CorrectedMethod:
-    """CorrectedMethod(base, c), tables_near.jl:113-123 and stepper.jl:131-173: the corrector kick
+    """CorrectedMethod(base, c), tables_near.jl:113-123 and stepper.jl:131-172: the corrector kick
     exp(-kappa L_F), F = |grad V|^2, kappa = tau^3 eps^2 c / 2, before and after the symmetric table `base`
     (for the Henon-Heiles flow eps = perturbation_scale = 1 and grad F = 2 Hs grad V, flow_models.jl:106-112)."""
     base: SplittingMethod

@@ -5,8 +5,8 @@
  * The reference reaches its device through Julia hooks, not a C ABI: `Tangent._run_chunk!` launches the
  * KernelAbstractions kernel `_orbit_kernel!` (src/Tangent/propagate.jl:32-50, launch at :105, synchronize :106),
  * and ext/ChaoslabCUDAExt.jl:16-93 fills the device hooks of src/Foundation/Foundation.jl:84-104. A Julia
- * package extension binds the entry points below with `ccall` in place of that launch (the binding is shown in
- * INTEGRATION.md). The ABI carries only plain pointers, sizes and POD structs.
+ * package extension binds the entry points below with `ccall` in place of that launch. The ABI carries only plain
+ * pointers, sizes and POD structs.
  *
  * Layouts (all host buffers are owned by the caller; no pointer is kept after a call returns):
  *  - x0, x   : n_orbits x s doubles, orbit-major (Julia `Vector{SVector{s,Float64}}`).
@@ -279,8 +279,9 @@ CL_API int cl_b200_ensemble_device(const cl_ensemble_class* classes, int32_t n_c
  * No counterpart in the reference. The classes run one after another on `stream`; their queue heads live in a
  * fixed array inside the library, CL_NOALLOC_MAX_CLASSES heads (512 bytes) held on every GPU that loads the
  * library until exit, and more classes than that are rejected with CL_EINVAL. The first call on a device looks
- * the array's device address up (make it before any stream capture); each call clears the heads it uses on
- * `stream`; calls that overlap on the GPU race on the shared array. */
+ * the array's device address up (make it before any stream capture) and keeps it for the life of the process, so
+ * the device must not be reset between calls; each call clears the heads it uses on `stream`, and a call whose
+ * classes are rejected enqueues nothing; calls that overlap on the GPU race on the shared array. */
 #define CL_NOALLOC_MAX_CLASSES 64
 CL_API int cl_b200_ensemble_device_noalloc(const cl_ensemble_class* classes, int32_t n_classes, void* stream);
 

@@ -203,7 +203,7 @@ struct Systems {
     }
 };
 
-// StandardMapChain with the banded ChainTangent (src/Systems/standard_map_chain.jl:159-179, chain_tangent.jl:
+// StandardMapChain with the banded ChainTangent (src/Systems/standard_map_chain.jl:141-171, chain_tangent.jl:
 // 38-61 / :62-97): the product `ChainTangent * W` is not a fused_product (the band has its own method).
 template <int MM>
 struct Chain {
@@ -491,7 +491,7 @@ struct SplitHH {
     int n;
     const double* c;
     const double* d;
-    int corr = 0;       // CorrectedMethod (stepper.jl:131-173): the corrector kick before and after each step
+    int corr = 0;       // CorrectedMethod (stepper.jl:131-172): the corrector kick before and after each step
     double kap = 0.0;   // kappa = tau^3 eps^2 c / 2, eps = perturbation_scale(HenonHeilesFlow()) = 1
     static SplitHH of(const cl_system& s) {
         SplitHH m{s.n_stages, s.stage_c, s.stage_d};
@@ -879,10 +879,10 @@ struct Reducers {
         std::memcpy(b, &st, sizeof st);
     }
 
-    // _norm_col (gali.jl:180-191): the loop form of safe_norm over column j.
+    // _norm_col (gali.jl:47-58): the loop form of safe_norm over column j.
     static double norm_col(const double* c, int d) { return safe_norm(c, d); }
 
-    // GALI, gali.jl:289-301 with _gram_core! (:214-234). GALIState{Float64, d, K, K-1} at runtime K.
+    // GALI, gali.jl:156-169 with _gram_core! (:81-100). GALIState{Float64, d, K, K-1} at runtime K.
     static void gali(uint8_t* b, int64_t n, double* W, int d, int K) {
         double* s = reinterpret_cast<double*>(b);
         double* c = s + K;
@@ -955,7 +955,7 @@ struct Reducers {
         std::memcpy(b, &st, sizeof st);
     }
 
-    // FLI, fli.jl:187-208.
+    // FLI, fli.jl:54-76.
     static void fli(const cl_reducer& rd, uint8_t* b, int64_t n, double* W, int d) {
         FLIStateJ st; std::memcpy(&st, b, sizeof st);
         if (st.code != 0) return;

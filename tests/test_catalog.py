@@ -237,7 +237,7 @@ def _hh_force(q):
 
 
 def test_calvo_sanz_serna_rkn_form(oracle):
-    """AC3b5 (ic_ac01_03.jl:158-190): the table (kick first, gamma_1 = 0, sum b = 1, gamma_5 = 1) and one step of the
+    """AC3b5 (ic_ac01_03.jl:154-185): the table (kick first, gamma_1 = 0, sum b = 1, gamma_5 = 1) and one step of the
     splitting on the oracle against the RKN formulas Q_i = q + h gamma_i p + h^2 sum_(j<i) b_j (gamma_i - gamma_j)
     f(Q_j), here on the Henon-Heiles flow, within 16 eps max(1, |z|)."""
     m = cb.CalvoSanzSerna4()
