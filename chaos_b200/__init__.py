@@ -6,6 +6,7 @@ include/chaoslab_b200.h. This Python package is the host side of that boundary: 
 reducers as parameter records, the argument checks, chunking, error and summary records.
 """
 from .foundation import FALLBACK_REASONS, DeviceError, NumericalHealthError
+from .diagnostics import eps_pair, eps_sum, spectrum_residuals, sum_threshold
 from .propagate import (FrameSpec, PropagationResult, build_run, bytes_per_orbit, chunk_size, probe, propagate,
                         propagate_frames, propagate_orbit, release_cache)
 from .reducers import (CGS, FLI, GALI, MEGNO, MGS, RGS, RLI, SALI, AugmentedQR, Benettin, GivensQR, HouseholderQR,
@@ -23,7 +24,7 @@ from .systems import (ABA864, ABAH864, PEFRL, SABA, SABAC, SBAB, SBABC, CalvoSan
 
 __all__ = [
     "propagate", "propagate_frames", "propagate_orbit", "propagate_shadow", "record", "record_indicators", "record_indicator_pairs", "pair_start", "pair_frame", "record_shadow", "advance_ensemble", "FrameSpec", "PropagationResult", "build_run", "bytes_per_orbit", "chunk_size",
-    "probe", "release_cache", "NumericalHealthError", "DeviceError", "FALLBACK_REASONS",
+    "probe", "release_cache", "eps_sum", "eps_pair", "sum_threshold", "spectrum_residuals", "NumericalHealthError", "DeviceError", "FALLBACK_REASONS",
     "QRSpectrum", "CGS", "MGS", "RGS", "HouseholderQR", "AugmentedQR", "GivensQR", "Benettin", "SALI", "GALI",
     "MEGNO", "FLI", "RLI",
     "StandardMap", "WrappedStandardMap", "FroeschleMap", "WrappedFroeschleMap", "StandardMapChain",

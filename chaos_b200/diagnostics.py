@@ -1,7 +1,18 @@
-"""Residual records of a spectrum (src/Diagnostics/residuals.jl), evaluated on the host from the reducers' finals.
+"""Residual records of a Lyapunov spectrum (src/Diagnostics/residuals.jl), evaluated on the host from the QRSpectrum
+finals a propagation returns.
 
-`eps_sum` (:26) and `eps_pair` (:29-32) are the residual record the reference keeps with every QR spectrum;
-`sum_threshold` (:55) is its bound. Float64 arithmetic in the reference's order.
+* `eps_sum(lambda)` (residuals.jl:13): |sum_i lambda_i| (spec D5);
+* `eps_pair(lambda)` (residuals.jl:16-18): max_i |lambda_i + lambda_{M+1-i}| over i = 1..M/2, estimator order, no
+  sorting (spec D1);
+* `sum_threshold(tol, T, G_max, tau, M_max)` (residuals.jl:32): tol eps(T) (G_max / tau + M_max), the bound of both
+  residuals that `monitor_exponents` (src/Diagnostics/monitor.jl:79-88) and the study recorder's thresholds
+  (src/Experiments/run_record.jl:189-197) apply, with the default multiplier `pairing_residual_tol = 16`
+  (_config/numerics-defaults.toml:10).
+
+`spectrum_residuals(result, tau=...)` gives the three per orbit for a QRSpectrum result (k = d: the whole spectrum),
+with G_max from the QR state itself and M_max, the largest entry of a one-step tangent, from the system's bound
+`tangent_bound()` unless the caller passes the observed maximum (the reference's caller passes its monitor's
+running maximum, which the bound dominates).
 """
 from __future__ import annotations
 
@@ -9,28 +20,78 @@ import numpy as np
 
 from .foundation import EPS
 
+PAIRING_RESIDUAL_TOL = 16.0
+EPS32 = float(np.finfo(np.float32).eps)
+
+
+def effective_eps(T: str = "Float64") -> float:
+    """effective_eps(T) (src/Foundation/Foundation.jl:44): eps of the element type."""
+    if T in ("Float64", np.float64, "f64"):
+        return EPS
+    if T in ("Float32", np.float32, "f32"):
+        return EPS32
+    raise ValueError(f"unknown element type {T!r}")
+
 
 def eps_sum(lam) -> float:
-    """|sum_i lambda_i| (spec D5), the sum a left fold."""
-    s = np.float64(0.0)
-    for i, v in enumerate(np.asarray(lam, dtype=np.float64)):
-        s = np.float64(v) if i == 0 else s + np.float64(v)
+    """|sum_i lambda_i| (spec D5); the sum is the left fold of StaticArrays' `sum`."""
+    lam = np.asarray(lam, dtype=np.float64).ravel()
+    s = lam[0]
+    for v in lam[1:]:
+        s = s + v
     return float(abs(s))
 
 
 def eps_pair(lam) -> float:
-    """max_i |lambda_i + lambda_{2N+1-i}| over i = 1..M/2, estimator order, no sorting (spec D1)."""
-    lam = np.asarray(lam, dtype=np.float64)
+    """max_i |lambda_i + lambda_{M+1-i}| over i = 1..M/2, estimator order, no sorting (spec D1)."""
+    lam = np.asarray(lam, dtype=np.float64).ravel()
     M = lam.size
+    if M < 2:
+        raise ValueError("pairing needs at least two exponents")
     return float(max(abs(lam[i] + lam[M - 1 - i]) for i in range(M // 2)))
 
 
-def sum_threshold(tol: float, G_max: float, tau: int, M_max: float) -> float:
-    """tol eps (G_max / tau + M_max), independent of the run length (residuals.jl:55)."""
-    return float(np.float64(tol) * EPS * (np.float64(G_max) / tau + np.float64(M_max)))
+def sum_threshold(tol: float, T, G_max, tau, M_max):
+    """T(tol) effective_eps(T) (T(G_max) / tau + T(M_max)), independent of the run length (residuals.jl:32).
+    Arrays of G_max broadcast."""
+    return np.float64(tol) * effective_eps(T) * (np.asarray(G_max, dtype=np.float64) / tau + np.float64(M_max))
+
+
+def _lambdas(states) -> np.ndarray:
+    """lambda_i = (s_i + c_i) / n per orbit from QRState records (qr_spectrum.jl:85-91); 0 before any handoff."""
+    sums = states["sums"]
+    n = states["n"].astype(np.float64)
+    tot = sums[..., 0] + sums[..., 1]
+    with np.errstate(invalid="ignore", divide="ignore"):
+        return np.where(n[:, None] > 0, tot / n[:, None], 0.0)
+
+
+def spectrum_residuals(result, *, tau: int, tol: float = PAIRING_RESIDUAL_TOL, M_max=None, T="Float64",
+                       system=None) -> dict:
+    """Per-orbit residual records of a QRSpectrum result with k = d: `eps_sum`, `eps_pair`, their common
+    `threshold` = sum_threshold(tol, T, G_max, tau, M_max) and `sum_ok` = eps_sum <= threshold (the check
+    `monitor_exponents` raises on). `result` is a PropagationResult whose chain's first reducer is QRSpectrum;
+    `T` is the element type of the frame ("Float32" for the mixed kernels' frames). M_max defaults to
+    `system.tangent_bound()`."""
+    from .reducers import QRSpectrum
+
+    if not result.reducers or not isinstance(result.reducers[0], QRSpectrum):
+        raise ValueError("the residual records need a QRSpectrum frame")
+    st = result.states["r0"]
+    lam = _lambdas(st)
+    n, k = lam.shape
+    if M_max is None:
+        if system is None or getattr(system, "tangent_bound", lambda: None)() is None:
+            raise ValueError("M_max is needed (no tangent bound for this system)")
+        M_max = system.tangent_bound()
+    # eps_sum as the left fold (cumsum adds left to right)
+    es = np.abs(np.cumsum(lam, axis=1)[:, -1]) if k else np.zeros(n)
+    ep = np.max(np.abs(lam[:, : k // 2] + lam[:, ::-1][:, : k // 2]), axis=1) if k >= 2 else np.zeros(n)
+    thr = sum_threshold(tol, T, st["G_max"], tau, M_max)
+    return dict(lam=lam, eps_sum=es, eps_pair=ep, threshold=thr, sum_ok=es <= thr)
 
 
 def orth_loss(Q) -> float:
-    """eps_orth: max |Q'Q - I| (spec D4)."""
+    """eps_orth: max |Q'Q - I| (spec D4, residuals.jl:10)."""
     Q = np.asarray(Q, dtype=np.float64)
     return float(np.max(np.abs(Q.T @ Q - np.eye(Q.shape[1]))))

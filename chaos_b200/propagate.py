@@ -20,7 +20,7 @@ import numpy as np
 from . import _abi
 from ._lib import last_error, lib
 from .foundation import DeviceError, NumericalHealthError
-from .reducers import GALI, SALI, Reducer, chain_dtype
+from .reducers import GALI, SALI, Finals, Reducer, chain_dtype
 from .systems import System
 
 STATUS_OK, STATUS_STATE, STATUS_W, STATUS_REDUCER = 0, 1, 2, 3
@@ -47,6 +47,14 @@ class PropagationResult:
     code: np.ndarray | None = None
     hstep: np.ndarray | None = None
     reducers: tuple = field(default=())
+
+    def spectrum_residuals(self, system=None, *, tol: float = 16.0, M_max=None) -> dict:
+        """The residual records of a QRSpectrum frame with k = d (src/Diagnostics/residuals.jl:13-32): per orbit
+        eps_sum, eps_pair and their threshold sum_threshold(tol, T, G_max, tau, M_max), T the frame's element type
+        (Float32 for a mixed-precision frame), M_max from `system.tangent_bound()` unless given."""
+        from .diagnostics import spectrum_residuals
+        T = "Float32" if self.provenance.get("precision", "Float64") != "Float64" else "Float64"
+        return spectrum_residuals(self, tau=int(self.provenance["tau"]), tol=tol, M_max=M_max, T=T, system=system)
 
 
 def bytes_per_orbit(d: int, k: int, s: int | None = None) -> int:
@@ -118,14 +126,6 @@ def _reducer_error(reducers, st, orbit, backend):   # orbit.jl:34-37: the first 
         if r.failed(sub):
             return r.error(sub, orbit, backend)
     raise AssertionError("STATUS_REDUCER without a failed reducer")
-
-
-def _finals(reducers, st_row, d):
-    out = []
-    for i, r in enumerate(reducers):
-        sub = st_row[f"r{i}"]
-        out.append(r.final(sub, d) if isinstance(r, GALI) else r.final(sub))
-    return tuple(out)
 
 
 def probe() -> dict:
@@ -255,7 +255,7 @@ def propagate_frames(sys: System, x0, N: int, frames: list[FrameSpec], *, tau: i
         W = Wout[f].transpose(0, 2, 1)
         fin = None
         if finals and states[f] is not None:
-            fin = [_finals(tuple(fr.reducers), states[f][i], d) for i in range(n)]
+            fin = Finals(tuple(fr.reducers), states[f], d)
         elif finals:
             fin = [() for _ in range(n)]
         results.append(PropagationResult(x=x, W=W, finals=fin, provenance=prov, states=states[f], code=codes[f],

@@ -79,6 +79,11 @@ class Reducer:
     def failed(self, st) -> bool:
         return int(st["code"]) != 0
 
+    def finals(self, st, d=None) -> dict | None:
+        """Columns of `final` over every orbit at once (arrays with the orbit as the first axis), the same values as
+        `final` per orbit; None where only the per-orbit form exists."""
+        return None
+
     def provenance(self) -> dict:
         return {}
 
@@ -113,6 +118,15 @@ class QRSpectrum(Reducer):
         return dict(n=n, sum=s.copy(), comp=c.copy(), **{"lambda": lam}, G_max=float(st["G_max"]),
                     orth_max=float(st["orth_max"]), count_max=int(st["count_max"]))
 
+    def finals(self, st, d=None):
+        n = st["n"].astype(np.int64)
+        s = st["sums"][:, :, 0].astype(np.float64)
+        c = st["sums"][:, :, 1].astype(np.float64)
+        with np.errstate(invalid="ignore", divide="ignore"):
+            lam = np.where(n[:, None] == 0, 0.0, (s + c) / n[:, None].astype(np.float64))
+        return dict(n=n, sum=s, comp=c, **{"lambda": lam}, G_max=st["G_max"].astype(np.float64),
+                    orth_max=st["orth_max"].astype(np.float64), count_max=st["count_max"].astype(np.int64))
+
     def error(self, st, orbit, backend):   # qr_spectrum.jl:80-83
         kind = "orthogonality" if int(st["code"]) == 4 else "orthonormalisation breakdown"
         return NumericalHealthError(kind, float(st["value"]), float(st["threshold"]), int(st["step"]), orbit,
@@ -138,6 +152,13 @@ class Benettin(Reducer):
         n = int(st["n"])
         lam = 0.0 if n == 0 else _tot(st["sum_s"], st["sum_c"]) / n
         return dict(n=n, sum=np.array([st["sum_s"]]), comp=np.array([st["sum_c"]]), **{"lambda": np.array([lam])})
+
+    def finals(self, st, d=None):
+        n = st["n"].astype(np.int64)
+        s, c = st["sum_s"].astype(np.float64), st["sum_c"].astype(np.float64)
+        with np.errstate(invalid="ignore", divide="ignore"):
+            lam = np.where(n == 0, 0.0, (s + c) / n.astype(np.float64))
+        return dict(n=n, sum=s[:, None], comp=c[:, None], **{"lambda": lam[:, None]})
 
     def error(self, st, orbit, backend):
         v = float(st["value"])
@@ -166,6 +187,13 @@ class SALI(Reducer):
         n = int(st["n"])
         L = 0.0 if n == 0 else -((s[0] + s[1]) + (c[0] + c[1]))
         return dict(n=n, sali=float(st["sali"]), L=float(L), sum=s, comp=c, floor=4 * EPS)
+
+    def finals(self, st, d=None):
+        n = st["n"].astype(np.int64)
+        s = np.stack([st["s1_s"], st["s2_s"]], axis=1).astype(np.float64)
+        c = np.stack([st["s1_c"], st["s2_c"]], axis=1).astype(np.float64)
+        L = np.where(n == 0, 0.0, -((s[:, 0] + s[:, 1]) + (c[:, 0] + c[:, 1])))
+        return dict(n=n, sali=st["sali"].astype(np.float64), L=L, sum=s, comp=c, floor=np.full(len(n), 4 * EPS))
 
     def error(self, st, orbit, backend):
         v = float(st["value"])
@@ -204,6 +232,21 @@ class GALI(Reducer):
         floors = np.array([2 * (i + 1) * EPS for i in range(1, k)])
         return dict(n=n, gali=st["gali"].astype(np.float64).copy(), L=L, sum=st["s"].astype(np.float64).copy(),
                     comp=st["c"].astype(np.float64).copy(), floor=floors)
+
+    def finals(self, st, d=None):
+        k = st["s"].shape[1]
+        n = st["n"].astype(np.int64)
+        S = st["s"].astype(np.float64)
+        Cc = st["c"].astype(np.float64)
+        L = None
+        if d is not None and k == d:
+            s, c = S[:, 0].copy(), Cc[:, 0].copy()
+            for i in range(1, k):   # left folds, as _log_form (gali.jl:186-193)
+                s = s + S[:, i]
+                c = c + Cc[:, i]
+            L = np.where(n == 0, 0.0, -(s + c))
+        floors = np.broadcast_to(np.array([2 * (i + 1) * EPS for i in range(1, k)]), (len(n), k - 1))
+        return dict(n=n, gali=st["gali"].astype(np.float64), L=L, sum=S, comp=Cc, floor=floors)
 
     def error(self, st, orbit, backend):
         v = float(st["value"])
@@ -263,6 +306,26 @@ class MEGNO(Reducer):
         return dict(n=n, handoffs=K, Y=np.array([y1, y2]), Ybar=np.array([b1, b2]), Ybar20=np.array([e1, e2]),
                     sum=pair("s", "s"), comp=pair("s", "c"), R1=tot("R1"), R2=tot("R2"), Q=tot("Q"), Q2=tot("Q2"))
 
+    def finals(self, st, d=None):
+        n, K = st["n"].astype(np.int64), st["K"].astype(np.int64)
+        f = np.float64
+        tn = n.astype(f)
+        cols = {nm: np.zeros((len(n), 2)) for nm in ("Y", "Ybar", "Ybar20")}
+        with np.errstate(invalid="ignore", divide="ignore"):
+            nk = np.where(K == 0, 0, n // np.where(K == 0, 1, K)).astype(f)
+            for j, col in enumerate(("c1", "c2")):
+                R1 = st[f"{col}_R1_s"].astype(f) + st[f"{col}_R1_c"].astype(f)
+                Q = st[f"{col}_Q_s"].astype(f) + st[f"{col}_Q_c"].astype(f)
+                Q2 = st[f"{col}_Q2_s"].astype(f) + st[f"{col}_Q2_c"].astype(f)
+                cols["Y"][:, j] = np.where(K == 0, 0.0, 2 * R1 / tn)
+                cols["Ybar"][:, j] = np.where(K == 0, 0.0, Q / K.astype(f))
+                cols["Ybar20"][:, j] = np.where(K == 0, 0.0, nk * Q2 / (tn * tn * tn))
+        pair = lambda nm, comp: np.stack([st[f"c1_{nm}_{comp}"], st[f"c2_{nm}_{comp}"]], axis=1).astype(f)  # noqa
+        tot = lambda nm: np.stack([st[f"c1_{nm}_s"].astype(f) + st[f"c1_{nm}_c"].astype(f),  # noqa
+                                   st[f"c2_{nm}_s"].astype(f) + st[f"c2_{nm}_c"].astype(f)], axis=1)
+        return dict(n=n, handoffs=K, Y=cols["Y"], Ybar=cols["Ybar"], Ybar20=cols["Ybar20"], sum=pair("s", "s"),
+                    comp=pair("s", "c"), R1=tot("R1"), R2=tot("R2"), Q=tot("Q"), Q2=tot("Q2"))
+
     def error(self, st, orbit, backend):
         v = float(st["value"])
         return NumericalHealthError("deviation matrix", v, 0.0 if math.isfinite(v) else math.inf, int(st["step"]),
@@ -300,6 +363,13 @@ class FLI(Reducer):
                     sum=np.array([st["s1_s"], st["s2_s"]], dtype=np.float64),
                     comp=np.array([st["s1_c"], st["s2_c"]], dtype=np.float64),
                     stepB=int(st["stepB"]), colB=int(st["colB"]), step1=int(st["step1"]))
+
+    def finals(self, st, d=None):
+        return dict(n=st["n"].astype(np.int64), fli=st["fB"].astype(np.float64), fli1=st["f1"].astype(np.float64),
+                    sum=np.stack([st["s1_s"], st["s2_s"]], axis=1).astype(np.float64),
+                    comp=np.stack([st["s1_c"], st["s2_c"]], axis=1).astype(np.float64),
+                    stepB=st["stepB"].astype(np.int64), colB=st["colB"].astype(np.int64),
+                    step1=st["step1"].astype(np.int64))
 
     def error(self, st, orbit, backend):
         v = float(st["value"])
@@ -371,3 +441,48 @@ def chain_dtype(reducers, d: int, k: int) -> np.dtype:
     if not reducers:
         return np.dtype([])
     return np.dtype({"names": names, "formats": formats, "offsets": offsets, "itemsize": off})
+
+
+class Finals:
+    """`finals` of a result: one tuple of `reducer_final` records per orbit (src/Tangent/propagate.jl:116-118),
+    computed for every orbit at once from the state columns (the same Float64 arithmetic as `final`, vectorised) and
+    handed out per orbit on access: `finals[i]` is the tuple of dicts `final` gives for orbit i."""
+
+    def __init__(self, reducers, states, d: int):
+        self.reducers = tuple(reducers)
+        self.n = 0 if states is None else len(states)
+        self.d = d
+        self._states = states
+        self.columns = [r.finals(states[f"r{i}"], d) if isinstance(r, GALI) else r.finals(states[f"r{i}"])
+                        for i, r in enumerate(self.reducers)]
+
+    def __len__(self):
+        return self.n
+
+    def __getitem__(self, i):
+        if isinstance(i, slice):
+            return [self[j] for j in range(*i.indices(self.n))]
+        if i < 0:
+            i += self.n
+        if not 0 <= i < self.n:
+            raise IndexError(i)
+        out = []
+        for j, (r, cols) in enumerate(zip(self.reducers, self.columns)):
+            if cols is None:
+                st = self._states[f"r{j}"][i]
+                out.append(r.final(st, self.d) if isinstance(r, GALI) else r.final(st))
+                continue
+            rec = {}
+            for key, v in cols.items():
+                if v is None:
+                    rec[key] = None
+                elif v.ndim == 1:
+                    rec[key] = int(v[i]) if v.dtype.kind in "iu" else float(v[i])
+                else:
+                    rec[key] = np.array(v[i])
+            out.append(rec)
+        return tuple(out)
+
+    def __iter__(self):
+        for i in range(self.n):
+            yield self[i]

@@ -40,6 +40,10 @@ class StandardMap(System):
         c = _abi.cl_system(kind=_abi.SYS_STANDARD, K=float(self.K))
         return c
 
+    def tangent_bound(self) -> float:
+        """Largest |entry| a one-step tangent [[1 + c, 1], [c, 1]], c = K cos x, can have: 1 + |K|."""
+        return 1.0 + abs(self.K)
+
 
 @dataclass(frozen=True)
 class WrappedStandardMap(System):
@@ -52,6 +56,14 @@ class WrappedStandardMap(System):
 
     def to_cl(self):
         return _abi.cl_system(kind=_abi.SYS_WRAPPED_STANDARD, K=float(self.K))
+
+    def tangent_bound(self) -> float:
+        """Largest |entry| of a one-step tangent (the standard map's): 1 + |K|."""
+        return 1.0 + abs(self.K)
+
+    def torus_state(self, z) -> np.ndarray:
+        """torus_state((X, P)) (wrapped_standard_map.jl:63-69) of the lifted point z = (X, P)."""
+        return _torus(z, 2)
 
 
 @dataclass(frozen=True)
@@ -66,6 +78,10 @@ class FroeschleMap(System):
 
     def to_cl(self):
         return _abi.cl_system(kind=_abi.SYS_FROESCHLE, nu=float(self.nu), kappa=float(self.kappa), mu=float(self.mu))
+
+    def tangent_bound(self) -> float:
+        """Largest |entry| a tangent [[I, I], [A, I + A]] can have (|a| <= |nu| + |mu|, |c| <= |kappa| + |mu|)."""
+        return 1.0 + max(abs(self.nu), abs(self.kappa)) + abs(self.mu)
 
 
 @dataclass(frozen=True)
@@ -83,6 +99,10 @@ class WrappedFroeschleMap(System):
     def to_cl(self):
         return _abi.cl_system(kind=_abi.SYS_WRAPPED_FROESCHLE, nu=float(self.nu), kappa=float(self.kappa),
                               mu=float(self.mu))
+
+    def tangent_bound(self) -> float:
+        """Largest |entry| of a one-step tangent (the lifted map's bound)."""
+        return 1.0 + max(abs(self.nu), abs(self.kappa)) + abs(self.mu)
 
     def torus_state(self, z) -> np.ndarray:
         """torus_state(sys, z) (:110-114): each coordinate of the lifted z reduced into [0, 2 pi) with its count."""
@@ -110,6 +130,10 @@ class StandardMapChain(System):
 
     def to_cl(self):
         return _abi.cl_system(kind=_abi.SYS_CHAIN, n_sites=self.N, ring=int(self.ring), K=self.K, eps=self.eps)
+
+    def tangent_bound(self) -> float:
+        """Largest |entry| of a one-step tangent: the band's diagonal 1 + K cos q_j + eps (two neighbours' cos)."""
+        return 1.0 + abs(self.K) + 2.0 * abs(self.eps)
 
     def __repr__(self):
         return f"StandardMapChain({self.N}, {self.K}, {self.eps}, boundary={'ring' if self.ring else 'open'})"
@@ -156,6 +180,10 @@ class LinearSymplecticMap(System):
         self.A = A
         self.d = self.s = A.shape[0]
         self.name = "LinearSymplecticMap"
+
+    def tangent_bound(self) -> float:
+        """The tangent is A: max |A_ij|."""
+        return float(np.max(np.abs(self.A)))
 
     def to_cl(self):
         c = _abi.cl_system(kind=_abi.SYS_LINEAR)

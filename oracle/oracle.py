@@ -36,6 +36,8 @@ def lib() -> C.CDLL:
         P = C.POINTER
         dp = P(C.c_double)
         L.oracle_propagate.argtypes = [P(_abi.cl_run), C.c_int64, P(_abi.cl_buffers), C.c_int32, C.c_int32]
+        L.oracle_static_supported.argtypes = [P(_abi.cl_run)]
+        L.oracle_static_propagate.argtypes = [P(_abi.cl_run), C.c_int64, P(_abi.cl_buffers), C.c_int32]
         L.oracle_propagate.restype = C.c_int
         L.oracle_sincos.argtypes = [C.c_int32, dp, dp, dp, C.c_int64]
         L.oracle_log.argtypes = [C.c_int32, dp, dp, C.c_int64]
@@ -306,8 +308,10 @@ def oracle_shadow(sys, x0, N, *, d0, tau=1, seed=0, U0=None, math="portable", th
 
 
 def oracle_frames(sys, x0, N, frames: list[FrameSpec], *, tau=1, seed=0, math="portable", threads=0,
-                  launch_steps=None, orbit_base=0):
-    """Run the oracle; returns a list (per frame) of dicts x (n, s), W (n, d, k), states, code, hstep."""
+                  launch_steps=None, orbit_base=0, engine="runtime"):
+    """Run the oracle; returns a list (per frame) of dicts x (n, s), W (n, d, k), states, code, hstep.
+    engine "static": the statically sized drivers of static_leg.cpp (map systems, one K for every frame, portable
+    math), bit for bit the runtime-sized oracle's records at the reference CPU algorithm's own speed."""
     x0 = np.ascontiguousarray(np.asarray(x0, dtype=np.float64))
     n, s = x0.shape
     d = sys.d
@@ -336,7 +340,12 @@ def oracle_frames(sys, x0, N, frames: list[FrameSpec], *, tau=1, seed=0, math="p
             b.states[f] = None if sts[f] is None else sts[f].ctypes.data
             b.code[f] = codes[f].ctypes.data
             b.hstep[f] = hs[f].ctypes.data
-        rc = lib().oracle_propagate(C.byref(run), n, C.byref(b), MATH[math], threads)
+        if engine == "static":
+            if math != "portable" or lib().oracle_static_supported(C.byref(run)) != 0:
+                raise ValueError("the static oracle covers map systems with one K per run and portable math")
+            rc = lib().oracle_static_propagate(C.byref(run), n, C.byref(b), threads)
+        else:
+            rc = lib().oracle_propagate(C.byref(run), n, C.byref(b), MATH[math], threads)
         if rc != 0:
             raise ValueError(f"oracle_propagate returned {rc}")
         done += run.steps
