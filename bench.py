@@ -68,32 +68,29 @@ METRIC = "orbit-steps/s (4D coupled standard maps, QRSpectrum(Householder) + GAL
 
 
 # ---- algorithmic operation counts ---------------------------------------------------------------------------------
-# Counting convention: add, sub, mul = 1, fma = 2, div and sqrt = 1, compare/select = 0. The transcendentals are this
-# library's own polynomials, counted by the arithmetic they execute: one FP64 sincos = 3 fma (reduction) + 1 mul
-# + 2 x 8 fma + 1 mul/fma (assembly) + 2 mul/sub (quadrant) = 44 flops; one FP64 log = 1 div + 2 add + 9 fma +
-# ~10 add/mul = 31 flops. Per orbit-step of the workload above:
+# The counting convention of the hot path's roofline: add, sub, mul = 1, fma = 2, div and sqrt = 1, compares and
+# selects 0; the transcendentals (sin, cos, log) are counted apart, by kind and precision. The counts are the
+# ALGORITHM's, the same for both kernels (the dense tangent product 2 d^2 k even where a kernel exploits the
+# tangent's zeros), split by the precision each kernel computes them in. Per orbit-step of the workload above
+# (d = k = 4, tau = 10, two frames: QR and GALI with SALI read off GALI's columns 1-2):
+#   map: x' = x + p (2), x1' + x2' (1), _abc (5), forward (8) and the force sums (4): 20 flops + 3 sin + 3 cos
+#   tangent products: 2 d^2 k = 128 per frame
+#   per handoff: Householder QR 4 d k^2 = 256; window_Gw 2 k^3 / 3 + 2 k^2 = 74; orth_loss (the k (k + 1) / 2
+#   distinct dots of Q'Q) 2 d k (k + 1) / 2 = 80; GALI: column norms 2 d k, unit columns d k, the twice-orthogonalised
+#   Gram-Schmidt 2 sum_j j 4 d = 192, the nested norms 2 d k and scaling d k, the k - 1 products: 307; SALI 3 d 2 = 24;
+#   k + k logs with a Neumaier add (4 flops) each: 32 (Float64 in both kernels)
 def flops_per_orbit_step(tau: int = TAU, mixed: bool = False) -> dict:
     d, k = 4, 4
-    log64, sincos64 = 31, 44
-    if mixed:
-        # the orbit's three values by the split evaluation (reduction 10 + one polynomial 18 = 28 FP64 flops each);
-        # the tangent's three complementary values in Float32 (two degree-5 polynomials, 24 flops each)
-        map64 = 3 * 28 + 16
-        map32 = 3 * 24 + 8
-        tangent32 = 2 * k * (2 + 2 * 4)          # per frame: 2 adds + 2 x (2 fma) per column, structured
-    else:
-        map64 = 3 * sincos64 + 16                # x' (2), x1'+x2' (1), _abc (5), forward (8)
-        tangent64 = 2 * d * k * (1 + 2 * (d - 1))  # per frame fused_product: 1 mul + (d-1) fma per entry
-    # per handoff: Householder QR d = k = 4 (3 reflectors + Q formation + sign fix), window_Gw, orth_loss
-    hh = 3 * (2 * d + 3 + 2 * d + 2 + d + 4 * (2 * d + d)) + 3 * 4 * (2 * d + 2 * d) + 2 * d * k
-    gw = 60 + 2 * k * k * 2
-    orth = k * k * (2 * d)
-    gali = k * (3 * d + 2) + d * k + 2 * sum(j * 4 * d for j in range(k)) + k * (3 * d + 2) + 2 * (3 * d + 2)
-    handoff = hh + gw + orth + gali
-    nlogs = 2 * k
-    if mixed:   # frames, norms, QR and GALI in Float32; logs as hardware log2 times ln 2, sums Float64
-        return dict(fp64=map64 + nlogs * (1 + 4) / tau, fp32=map32 + tangent32 + handoff / tau)
-    return dict(fp64=map64 + tangent64 + (handoff + nlogs * (log64 + 4)) / tau, fp32=0.0)
+    map_flops, trig = 20, 6
+    products = 2 * (2 * d * d * k)
+    handoff = 4 * d * k * k + (2 * k ** 3 // 3 + 2 * k * k) + d * k * (k + 1) + \
+        (2 * d * k + d * k + 2 * sum(j * 4 * d for j in range(k)) + 2 * d * k + d * k + (k - 1)) + 6 * d
+    logsum = 2 * k * 4
+    if mixed:   # the orbit, its three sines / cosines and the log sums Float64; frames, QR, GALI, SALI Float32
+        return dict(fp64=map_flops + logsum / tau, fp32=products + handoff / tau, trig_fp64=trig / 2,
+                    trig_fp32=trig / 2, log=2 * k / tau, handoff_flops=handoff + logsum)
+    return dict(fp64=map_flops + products + (handoff + logsum) / tau, fp32=0.0, trig_fp64=trig, trig_fp32=0.0,
+                log=2 * k / tau, handoff_flops=handoff + logsum)
 
 
 class ClockSampler:
@@ -159,9 +156,17 @@ def cpu_reference(sample_orbits: int, sample_steps: int, threads: int) -> dict:
     W0 = np.broadcast_to(np.eye(4), (sample_orbits, 4, 4)).copy()
     frames = [FrameSpec(4, (QRSpectrum(HouseholderQR()),), W0), FrameSpec(4, (GALI(), SALI()), W0)]
     t = time.perf_counter()
-    O.oracle_frames(FroeschleMap(NU, KAPPA, MU), x0, sample_steps, frames, tau=TAU, math="portable", threads=threads)
+    O.oracle_frames(FroeschleMap(NU, KAPPA, MU), x0, sample_steps, frames, tau=TAU, math="portable", threads=threads,
+                    engine="static")
     dt = time.perf_counter() - t
     return dict(value=sample_orbits * sample_steps / dt, seconds=dt, threads=threads)
+
+
+# The CPU sample of the workload: its first CPU_ORBITS orbits for CPU_STEPS steps (same map, frames, tau and W0), on
+# the statically sized oracle (the reference's algorithm specialised on d = k = 4 as StaticArrays specialises it).
+CPU_ORBITS, CPU_STEPS = 2048, 20000
+CPU_SAMPLE = (f"{CPU_ORBITS} orbits x {CPU_STEPS} steps of the workload (the statically sized oracle, d = k = 4 "
+              "compile-time, all host threads; Julia, the reference's runtime, is absent)")
 
 
 def main() -> None:
@@ -190,8 +195,8 @@ def main() -> None:
         if rank != 0:
             return
         threads = os.cpu_count() or 1
-        # a bounded sample of the same workload per step: 1024 orbits x 4000 steps
-        so, ss = 1024, 4000
+        # a bounded sample of the same workload per step
+        so, ss = CPU_ORBITS, CPU_STEPS
         vals = []
         for i in range(args.warmup + args.steps):
             r = cpu_reference(so, ss, threads)
@@ -203,8 +208,7 @@ def main() -> None:
                     vs_baseline=None, dtype="f64", data="synthetic", impl="reference",
                     config=dict(workload="froeschle-4d-65536x1e5-tau10-qr-householder+gali4+sali", orbits=args.orbits or N_ORBITS,
                                 N=args.N, tau=TAU),
-                    cpu_baseline=dict(value=v, unit="orbit-steps/s", cores=threads, kind="port",
-                                      sample=f"{so} orbits x {ss} steps of the workload per step (oracle, all host threads; Julia absent)"),
+                    cpu_baseline=dict(value=v, unit="orbit-steps/s", cores=threads, kind="port", sample=CPU_SAMPLE),
                     e2e=dict(value=v, unit="orbit-steps/s", h2d_bytes_per_step=0, d2h_bytes_per_step=0))
         print(json.dumps(line), flush=True)
         return
@@ -335,7 +339,7 @@ def main() -> None:
     from chaos_b200.propagate import propagate_frames
     W0h = np.broadcast_to(np.eye(4), (n, 4, 4)).copy()
     fr_h = [FrameSpec(4, (QRSpectrum(HouseholderQR()),), W0h), FrameSpec(4, (GALI(), SALI()), W0h)]
-    propagate_frames(sysm, x0_h, N, fr_h, tau=TAU, seed=SEED, precision="mixed", finals=False, throw=False)
+    propagate_frames(sysm, x0_h, N, fr_h, tau=TAU, seed=SEED, precision="mixed", finals=True, throw=False)
     torch.cuda.synchronize(dev)
     if world > 1:
         dist.barrier()
@@ -344,7 +348,7 @@ def main() -> None:
     te = []
     for _ in range(max(args.steps, 5)):
         t0 = time.perf_counter()
-        res = propagate_frames(sysm, x0_h, N, fr_h, tau=TAU, seed=SEED, precision="mixed", finals=False, throw=False)
+        res = propagate_frames(sysm, x0_h, N, fr_h, tau=TAU, seed=SEED, precision="mixed", finals=True, throw=False)
         te.append(time.perf_counter() - t0)
     tt = torch.tensor([float(np.median(te)), float(np.mean(te))], dtype=torch.float64, device=dev)
     if world > 1:
@@ -366,9 +370,8 @@ def main() -> None:
     cpu = None
     if rank == 0 and not args.no_cpu:
         threads = os.cpu_count() or 1
-        cb_ = cpu_reference(512, 4000, threads)
-        cpu = dict(value=cb_["value"], unit="orbit-steps/s", cores=threads, kind="port",
-                   sample="512 orbits x 4000 steps of the workload (oracle, all host threads)")
+        cb_ = cpu_reference(CPU_ORBITS, CPU_STEPS, threads)
+        cpu = dict(value=cb_["value"], unit="orbit-steps/s", cores=threads, kind="port", sample=CPU_SAMPLE)
 
     if rank == 0:
         clocks = sampler.summary()

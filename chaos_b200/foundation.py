@@ -49,6 +49,11 @@ def total(s: float, c: float) -> float:
     return float(np.float64(s) + np.float64(c))
 
 
+class DimensionMismatch(ValueError):
+    """Julia's `DimensionMismatch`: two arrays of different sizes met in an elementwise operation (StaticArrays
+    throws it for `SVector{m} + SVector{n}`, m != n)."""
+
+
 class DeviceError(RuntimeError):
     """A device call failed; `reason` is the 1-based FALLBACK_REASONS index it maps to (3, 4 or 9), as
     `_fallback_reason` classifies device exceptions (src/Tangent/propagate.jl:121-129)."""

@@ -16,7 +16,7 @@ import numpy as np
 
 from . import _abi
 from ._lib import last_error, lib
-from .foundation import DeviceError, NumericalHealthError
+from .foundation import DeviceError, DimensionMismatch, NumericalHealthError
 from .propagate import FrameSpec, PropagationResult, build_run
 from .systems import WrappedStandardMap, _reduce
 
@@ -96,6 +96,12 @@ def propagate_shadow(sys, x0, N: int, *, d0: float, tau: int = 1, seed: int = 0,
     d0 = float(d0)
     if not (math.isfinite(d0) and d0 > 0):
         raise ValueError(f"d0 must be finite and positive, got {d0}")
+    if s != d and not isinstance(sys, WrappedStandardMap) and n:
+        # Algorithm 1's start check runs on the host for every orbit before any launch (_check_starts,
+        # two_trajectory.jl:158-162, called at :190): `displaced(sys, x, d0 u0)` falls back to `x + d0 u0`
+        # (separation.jl:17) for every system but WrappedStandardMap, an SVector{s} plus an SVector{d}, which
+        # StaticArrays rejects when s != d (the wrapped Froeschle map, s = 8, and the wrapped chain, s = 4N).
+        raise DimensionMismatch(f"Sizes ({s},) and ({d},) of input arrays do not match")
     u = None
     if U0 is not None:
         U0 = np.asarray(U0, dtype=np.float64)

@@ -104,3 +104,21 @@ def test_argument_errors():
     with pytest.raises(NumericalHealthError) as ei:
         propagate_shadow(WrappedStandardMap(0.5), x, 10, d0=5.0, seed=1, U0=[[1.0, 0.0]])
     assert ei.value.what == "separation" and ei.value.step == 0 and ei.value.threshold == 5.0
+
+
+@pytest.mark.parametrize("mk", [lambda: __import__("chaos_b200").WrappedFroeschleMap(1.5, 1.5, 0.05),
+                                lambda: __import__("chaos_b200").WrappedStandardMapChain(3, 1.0, 0.05)],
+                         ids=["wrapped-froeschle", "wrapped-chain"])
+def test_wrapped_coupled_maps_dimension_mismatch(mk):
+    """On the wrapped coupled maps the reference's start check (two_trajectory.jl:158-162) evaluates the generic
+    `displaced(sys, x, d0 u0) = x + d0 u0` (separation.jl:17) with an s-vector state and a d-vector direction
+    (s = 8 against d = 4; s = 4N against d = 2N) and StaticArrays throws DimensionMismatch before any launch: the
+    host side raises the same error, seeded directions or given ones."""
+    from chaos_b200 import propagate_shadow
+    from chaos_b200.foundation import DimensionMismatch
+    sysm = mk()
+    x0 = np.array([sysm.torus_state(z) for z in np.random.default_rng(1).uniform(0, 6, (3, sysm.d))])
+    with pytest.raises(DimensionMismatch):
+        propagate_shadow(sysm, x0, 100, d0=1e-8, tau=10, seed=1)
+    with pytest.raises(DimensionMismatch):
+        propagate_shadow(sysm, x0, 100, d0=1e-8, tau=10, U0=np.ones((3, sysm.d)))
