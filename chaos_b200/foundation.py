@@ -60,5 +60,5 @@ class DeviceError(RuntimeError):
 
     def __init__(self, code: int, message: str):
         self.code = code
-        self.reason = {-2: 2, -3: 3, -4: 4, -9: 9}.get(code, 0)
+        self.reason = {-2: 2, -3: 3, -4: 4, -8: 8, -9: 9}.get(code, 0)
         super().__init__(f"libchaoslab_b200 error {code}: {message}")

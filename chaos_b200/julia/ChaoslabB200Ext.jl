@@ -9,7 +9,7 @@ Drop-in next to ext/ChaoslabCUDAExt.jl (same hooks: src/Foundation/Foundation.jl
 """
 module ChaoslabB200Ext
 
-using Chaoslab, StaticArrays
+using Chaoslab, StaticArrays, TOML
 using Chaoslab.Foundation: Foundation, NumericalHealthError
 using Chaoslab.Tangent: Tangent, STATUS_OK, STATUS_REDUCER
 using Chaoslab.Lyapunov: QRSpectrum, Benettin, CGS, MGS, RGS, HouseholderQR, AugmentedQR, GivensQR
@@ -162,8 +162,27 @@ function Tangent._alloc_bufs(::B200Backend, ::Type{SVector{s, T}}, ::Val{d}, ::V
             Vector{Int8}(undef, m), Vector{Int}(undef, m), zeros(UInt32, max(mws, 1), m))
 end
 
-# `_run_chunk!` (propagate.jl:92-119) with the launches replaced by one cl_b200_propagate call; the host-side
-# error and summary handling is the reference's, unchanged.
+# The one-wave record of the launch plan (propagate.jl:183-190): the same per-machine file and table layout as the
+# CUDA extension's record (ext/ChaoslabCUDAExt.jl:42-62), written next to the library by the Python host's first
+# measurement (chaos_b200/launch_plan.py); no record gives `nothing`, so the plan uses DEFAULT_GPU_NS.
+const RECORD = joinpath(dirname(libcl), "data", "gpu-benchmark.toml")
+function Foundation.gpu_step_ns(::B200Device, ::Type{T}) where {T}
+    T === Float64 || return nothing
+    try
+        isfile(RECORD) || return nothing
+        p = Ref{ClProbe}()
+        ccall((:cl_b200_probe, libcl), Cint, (Ref{ClProbe},), p)
+        name = String(filter(!iszero, collect(p[].device)))
+        v = get(TOML.parsefile(RECORD)[name]["Float64"], "gpu_ns_per_step_wave", nothing)
+        return v isa Real && isfinite(v) && v > 0 ? Float64(v) : nothing
+    catch
+        return nothing
+    end
+end
+
+# `_run_chunk!` (propagate.jl:92-119) with each launch of `args.L` steps one cl_b200_propagate call on the carried
+# host buffers (the first from x0 / W0, every later one continuing from x, W, states, code, hstep), the
+# `_before_launch` hook before each; the host-side error and summary handling is the reference's, unchanged.
 function Tangent._run_chunk!(out, bufs, Wh, r, args, who::Symbol, backend::B200Backend, ci::Int = 0)
     x, W, so, code, hstep, wsb = bufs
     len = length(r)
@@ -172,18 +191,26 @@ function Tangent._run_chunk!(out, bufs, Wh, r, args, who::Symbol, backend::B200B
     copyto!(W, 1, Wh, 1, len)
     d, k = size(eltype(W))
     s = length(eltype(x))
-    run = clrun(args.sys, d, s, k, args.tau, args.N, 0, args.L, args.reducers, args.seed, first(r) - 1)
     nul = Ptr{Float64}(0)
-    GC.@preserve x W so code hstep begin
-        bufsC = ClBuffers(pointer(x) |> Ptr{Float64}, pointer(x) |> Ptr{Float64},
-                          (pointer(W) |> Ptr{Float64}, nul, nul), (pointer(W) |> Ptr{Float64}, nul, nul),
-                          (sizeof(eltype(so)) == 0 ? Ptr{Cvoid}(0) : Ptr{Cvoid}(pointer(so)), Ptr{Cvoid}(0), Ptr{Cvoid}(0)),
-                          (pointer(code), Ptr{Int8}(0), Ptr{Int8}(0)), (pointer(hstep), Ptr{Int64}(0), Ptr{Int64}(0)))
-        rc = ccall((:cl_b200_propagate, libcl), Cint, (Ref{ClRun}, Int64, Ref{ClBuffers}, Ptr{Cvoid}),
-                   run, len, bufsC, C_NULL)
+    n0, launch = 0, 0
+    args.done[] = 0
+    while n0 < args.N
+        steps = min(args.L, args.N - n0)
+        launch += 1
+        Tangent._before_launch(Foundation.DEVICE[], ci, launch, (x = x, W = W, states = so, workspace = wsb))
+        run = clrun(args.sys, d, s, k, args.tau, args.N, n0, steps, args.reducers, args.seed, first(r) - 1)
+        GC.@preserve x W so code hstep begin
+            bufsC = ClBuffers(pointer(x) |> Ptr{Float64}, pointer(x) |> Ptr{Float64},
+                              (pointer(W) |> Ptr{Float64}, nul, nul), (pointer(W) |> Ptr{Float64}, nul, nul),
+                              (sizeof(eltype(so)) == 0 ? Ptr{Cvoid}(0) : Ptr{Cvoid}(pointer(so)), Ptr{Cvoid}(0), Ptr{Cvoid}(0)),
+                              (pointer(code), Ptr{Int8}(0), Ptr{Int8}(0)), (pointer(hstep), Ptr{Int64}(0), Ptr{Int64}(0)))
+            rc = ccall((:cl_b200_propagate, libcl), Cint, (Ref{ClRun}, Int64, Ref{ClBuffers}, Ptr{Cvoid}),
+                       run, len, bufsC, C_NULL)
+        end
+        rc == 0 || throw(ClB200Error(rc, last_error()))
+        args.done[] = launch
+        n0 += steps
     end
-    rc == 0 || throw(ClB200Error(rc, last_error()))
-    args.done[] = cld(args.N, args.L)
     i = findfirst(!=(STATUS_OK), view(code, 1:len))
     i === nothing || code[i] != STATUS_REDUCER || throw(Tangent._reducer_error(args.reducers, so[i], first(r) + i - 1, who))
     i === nothing || throw(Tangent._health_error(code[i], x[i], W[i], hstep[i], first(r) + i - 1, who))

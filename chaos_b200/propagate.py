@@ -17,7 +17,7 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
-from . import _abi
+from . import _abi, launch_plan
 from ._lib import last_error, lib
 from .foundation import DeviceError, NumericalHealthError
 from .reducers import GALI, SALI, Finals, Reducer, chain_dtype
@@ -185,7 +185,7 @@ def propagate_frames(sys: System, x0, N: int, frames: list[FrameSpec], *, tau: i
             W0s.append(W0s[same[0]] if same else np.ascontiguousarray(W0.transpose(0, 2, 1)))   # column-major per orbit
         else:
             W0s.append(None)
-    run = build_run(sys, N, tau, frames, precision, seed, steps=launch_steps or 0)
+    run = build_run(sys, N, tau, frames, precision, seed)
     L = lib()
     rc = L.cl_b200_check(C.byref(run))
     if rc != 0:
@@ -193,6 +193,13 @@ def propagate_frames(sys: System, x0, N: int, frames: list[FrameSpec], *, tau: i
         if rc == _abi.EINVAL:
             raise ValueError(msg)
         raise DeviceError(rc, msg)
+    # the launch plan (propagate.jl:183-190): steps per launch within the budget for one wave, and the orbit cap
+    forced = launch_steps if launch_steps is not None else launch_plan.forced_launch(tau)
+    ns = launch_plan.gpu_step_ns(precision)
+    Lsteps, cap = launch_plan.device_plan(forced, N, tau, ns)
+    if Lsteps == 0:
+        raise DeviceError(-8, f"a launch of tau = {tau} steps exceeds the launch budget for one wave")
+    run.steps = Lsteps
     dtypes = [chain_dtype(fr.reducers, d, fr.k) for fr in frames]
     rbytes = sum(dt.itemsize for dt in dtypes)
     if chunk is None:
@@ -201,7 +208,7 @@ def propagate_frames(sys: System, x0, N: int, frames: list[FrameSpec], *, tau: i
         csize = chunk_size(pr["free_bytes"], d, kk, reducer_bytes=rbytes, s=s) if pr["free_bytes"] else n
     else:
         csize = chunk
-    csize = min(csize, n) if n else 1
+    csize = min(csize, cap, n) if n else 1
     x = np.empty((n, s))
     Wout = [np.empty((n, fr.k, d)) for fr in frames]
     states = [np.zeros(n, dtype=dt) if dt.itemsize else None for dt in dtypes]
@@ -222,10 +229,28 @@ def propagate_frames(sys: System, x0, N: int, frames: list[FrameSpec], *, tau: i
             bufs.states[f] = None if states[f] is None else states[f][lo:hi].ctypes.data
             bufs.code[f] = codes[f][lo:hi].ctypes.data
             bufs.hstep[f] = hsteps[f][lo:hi].ctypes.data
-        rc = L.cl_b200_propagate(C.byref(run), hi - lo, C.byref(bufs), C.byref(prov_dev))
-        if rc != 0:
-            raise DeviceError(rc, last_error())
-        gpu_ms += prov_dev.gpu_ms
+        hook = launch_plan.BEFORE_LAUNCH
+        if hook is None:   # every launch of the chunk inside one library call
+            rc = L.cl_b200_propagate(C.byref(run), hi - lo, C.byref(bufs), C.byref(prov_dev))
+            if rc != 0:
+                raise DeviceError(rc, last_error())
+            gpu_ms += prov_dev.gpu_ms
+        else:   # launch by launch, the hook before each with the live carried buffers (propagate.jl:101-104)
+            launch, n0, w = 0, 0, 0.0
+            while n0 < N:
+                launch += 1
+                hook(prov_dev.device.decode() or "B200", chunks + 1, launch,
+                     dict(x=x[lo:hi], W=[Wo[lo:hi] for Wo in Wout],
+                          states=[None if st is None else st[lo:hi] for st in states], workspace=None))
+                run.n0, run.steps = n0, min(Lsteps, N - n0)
+                rc = L.cl_b200_propagate(C.byref(run), hi - lo, C.byref(bufs), C.byref(prov_dev))
+                if rc != 0:
+                    raise DeviceError(rc, last_error())
+                w += prov_dev.gpu_ms
+                n0 += run.steps
+            run.n0, run.steps = 0, Lsteps
+            prov_dev.launch_steps, prov_dev.launches = Lsteps, launch
+            gpu_ms += w
         chunks += 1
         for f, fr in enumerate(frames):   # lowest failing orbit id first (propagate.jl:111-113)
             if errors[f] is not None:
