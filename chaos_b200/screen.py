@@ -3,7 +3,10 @@ the orbits the network is unsure about (plus a random audit). No reference count
 by full integration only (its screening loop, src/Experiments/screening.jl:26-52, runs every orbit to the end).
 
 The map is the 4D coupled standard map (FroeschleMap), one k = 2 frame with the chain (MEGNO(replace = false),
-SALI()) and tau = 10, on the mixed-precision kernels. Features: every 100 steps up to 2000, the column-1 log-stretch
+SALI()) and tau = 10, on the Float64 kernels by default (`precision="fp64"`: the training labels, the full
+integrations of the unsure and audited orbits and the plain full run that the screen is judged against all come
+from the reference's Float64 arithmetic; `precision="mixed"` runs the same pipeline on the mixed kernels). The
+training set is the coupled-maps ensemble: coordinates uniform in [0, 2 pi)^4. Features: every 100 steps up to 2000, the column-1 log-stretch
 rate, log10 SALI and the running MEGNO Y (cl_b200_screen_features reads them off the reducer states between
 relaunch windows, which carry the state bit for bit). Label: the final mean MEGNO Ybar of column 1 > 2.2 at
 N = 1e5; regression target: the final lambda_1 estimate. The orbits kept for full integration continue from their
@@ -52,7 +55,7 @@ class Carried:
 
 
 class Screen:
-    def __init__(self, torch, device, sysm=None, precision: str = "mixed", seed: int = 1):
+    def __init__(self, torch, device, sysm=None, precision: str = "fp64", seed: int = 1):
         self.t, self.dev = torch, device
         self.sys = sysm or FroeschleMap(1.5, 1.5, 0.05)
         self.precision = precision
@@ -113,11 +116,11 @@ class Screen:
                        code=b.code.index_select(0, ii), hstep=b.hstep.index_select(0, ii), n=len(idx))
 
     # ---- the pipeline -----------------------------------------------------------------------------------------------
-    def training_set(self, n: int, N: int = N_FULL, seed: int = 11, plane: bool = True):
-        """n labelled orbits: (x1, p1) uniform on [0, 2 pi)^2 with x2 = p2 = 0.1 (the plane the grid screens; on this
-        map ~85 % of it is chaotic), or, with plane = False, all four coordinates uniform (~97 % chaotic: the
-        coupling's mu (1 - cos) term leaves few regular orbits in the full torus). Returns the BF16 features of
-        the orbits that finished without a failure, their labels and their final lambda_1."""
+    def training_set(self, n: int, N: int = N_FULL, seed: int = 11, plane: bool = False):
+        """n labelled orbits of the coupled-maps ensemble: all four coordinates uniform in [0, 2 pi) (~97 % chaotic:
+        the coupling's mu (1 - cos) term leaves few regular orbits in the full torus), or, with plane = True,
+        (x1, p1) uniform on [0, 2 pi)^2 with x2 = p2 = 0.1 (the plane the grid screens; ~85 % chaotic). Returns the
+        BF16 features of the orbits that finished without a failure, their labels and their final lambda_1."""
         rng = np.random.default_rng(seed)
         if plane:
             x0 = np.stack([rng.uniform(0, 2 * math.pi, n), np.full(n, 0.1), rng.uniform(0, 2 * math.pi, n),
