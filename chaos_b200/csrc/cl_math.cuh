@@ -86,7 +86,9 @@ __device__ __forceinline__ Reduced cl_reduce(double x) {
     r = fma(-k, CL_PIO2_3, r);
     w.r = r;
     w.z = r * r;
-    w.q = static_cast<int>(k - 4.0 * floor(k * 0.25));
+    // k - 4 floor(k / 4) of cl_sincos, from the integer: k is integral, so its two's-complement low bits are that
+    // remainder for every |k| < 2^63 (a non-finite x gives a NaN r and the quadrant does not matter)
+    w.q = static_cast<int>(static_cast<long long>(k) & 3);
     return w;
 }
 // cos-form (cosf = true) or sin-form polynomial of the reduced argument, exactly as cl_sincos evaluates it.
@@ -102,33 +104,29 @@ __device__ __forceinline__ double cl_poly(const Reduced& w, bool cosf) {
     p = fma(p, z, cosf ? CL_COS_T2 : CL_SIN_T3);
     return cosf ? fma(z, p, 1.0) : fma(w.r * z, p, w.r);
 }
-// sin(x) bit-identical to cl_sincos's: quadrant 0 s, 1 c, 2 -s, 3 -c
+// sin(x) bit-identical to cl_sincos's: quadrant 0 s, 1 c, 2 -s, 3 -c. Branch-free: a non-finite x reduces to a NaN
+// r and gives NaN as cl_sincos does; x = +-0 reduces to r = +0, so the signed zero is selected.
 __device__ __forceinline__ double cl_sin_split(const Reduced& w) {
-    if (!isfin(w.x)) return w.x - w.x;
-    if (w.x == 0.0) return w.x;
     const double v = cl_poly(w, (w.q & 1) != 0);
-    return w.q >= 2 ? -v : v;
+    const double s = (w.q & 2) ? -v : v;
+    return w.x == 0.0 ? w.x : s;
 }
-// cos(x) bit-identical to cl_sincos's: quadrant 0 c, 1 -s, 2 -c, 3 s
+// cos(x) bit-identical to cl_sincos's: quadrant 0 c, 1 -s, 2 -c, 3 s (cos(+-0): r = +0, q = 0, exactly 1)
 __device__ __forceinline__ double cl_cos_split(const Reduced& w) {
-    if (!isfin(w.x)) return w.x - w.x;
-    if (w.x == 0.0) return 1.0;
-    const double v = cl_poly(w, (w.q & 1) != 0 ? false : true);
-    return (w.q == 1 || w.q == 2) ? -v : v;
+    const double v = cl_poly(w, (w.q & 1) == 0);
+    return ((w.q + 1) & 2) ? -v : v;
 }
 // Float32 sin / cos from the same reduction: the hardware sine and cosine (special-function unit, absolute error
 // below 2^-21.4 on [-pi, pi]) of the reduced argument |r| <= pi/4, then the quadrant. Two issue slots instead of
 // two polynomials: the tangent's trigonometry is Float32 in the mixed kernels, and the orbit's stays Float64.
+// Branch-free: quadrant 0 (s, c), 1 (c, -s), 2 (-s, -c), 3 (-c, s); a non-finite x has a NaN r, so NaN comes out.
 __device__ __forceinline__ void cl_sincos32(const Reduced& w, float* sn, float* cs) {
-    if (!isfin(w.x)) { const float nan = __int_as_float(0x7fc00000); *sn = nan; *cs = nan; return; }
     float s, c;
     __sincosf(static_cast<float>(w.r), &s, &c);
-    switch (w.q) {
-        case 0: *sn = s; *cs = c; break;
-        case 1: *sn = c; *cs = -s; break;
-        case 2: *sn = -s; *cs = -c; break;
-        default: *sn = -c; *cs = s; break;
-    }
+    const bool odd = (w.q & 1) != 0;
+    const float a = odd ? c : s, b = odd ? s : c;
+    *sn = (w.q & 2) ? -a : a;
+    *cs = ((w.q + 1) & 2) ? -b : b;
 }
 
 __device__ __forceinline__ double cl_sin(double x) { double s, c; cl_sincos(x, &s, &c); return s; }
