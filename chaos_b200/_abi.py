@@ -25,7 +25,7 @@ RED_QR, RED_BENETTIN, RED_SALI, RED_GALI, RED_MEGNO, RED_FLI, RED_RLI = 1, 2, 3,
 # enum cl_qr_alg
 QR_CGS, QR_MGS, QR_RGS, QR_HOUSEHOLDER, QR_AUGMENTED, QR_GIVENS = 1, 2, 3, 4, 5, 6
 # enum cl_precision
-PREC_FP64, PREC_MIXED = 0, 1
+PREC_FP64, PREC_MIXED, PREC_MIXED_IND64 = 0, 1, 2
 # enum cl_window_kind, enum cl_observable_kind
 WIN_PHASE_ADVANCE, WIN_BIRKHOFF = 1, 2
 OBS_PLANAR, OBS_LIFTED_ANGLE, OBS_COS, OBS_SIN, OBS_LIFTED, OBS_COORDINATE = 1, 2, 3, 4, 5, 6

@@ -128,7 +128,8 @@ int validate(const cl_run& r) {
             return fail(CL_EINVAL, "corrector must be 0, or 1 with a finite coefficient in eps");
     }
     if (r.n_frames < 1 || r.n_frames > CL_MAX_FRAMES) return fail(CL_EINVAL, "n_frames must be in 1..3");
-    if (r.precision != CL_PREC_FP64 && r.precision != CL_PREC_MIXED) return fail(CL_EINVAL, "unknown precision");
+    if (r.precision != CL_PREC_FP64 && r.precision != CL_PREC_MIXED && r.precision != CL_PREC_MIXED_IND64)
+        return fail(CL_EINVAL, "unknown precision");
     for (int f = 0; f < r.n_frames; ++f) {
         const cl_frame& fr = r.frames[f];
         if (!(fr.k >= 1 && fr.k <= d)) {

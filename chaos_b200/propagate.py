@@ -25,7 +25,9 @@ from .systems import System
 
 STATUS_OK, STATUS_STATE, STATUS_W, STATUS_REDUCER = 0, 1, 2, 3
 CHUNK_HEADROOM = 0.5
-PRECISIONS = {"fp64": _abi.PREC_FP64, "mixed": _abi.PREC_MIXED}
+PRECISIONS = {"fp64": _abi.PREC_FP64, "mixed": _abi.PREC_MIXED, "mixed-ind64": _abi.PREC_MIXED_IND64}
+PRECISION_LABELS = {"fp64": "Float64", "mixed": "Float64 orbit / Float32 tangent",
+                    "mixed-ind64": "Float64 orbit and indicator frames / Float32 Lyapunov frames"}
 
 
 @dataclass
@@ -270,7 +272,7 @@ def propagate_frames(sys: System, x0, N: int, frames: list[FrameSpec], *, tau: i
     results = []
     for f, fr in enumerate(frames):
         prov = dict(backend="gpu", device=prov_dev.device.decode(), backend_fallback_reason="",
-                    precision="Float64" if precision == "fp64" else "Float64 orbit / Float32 tangent",
+                    precision=PRECISION_LABELS[precision],
                     threads=os.cpu_count(), cpu=platform.processor() or platform.machine(), seed=seed, tau=tau,
                     k=fr.k, chunk_size=csize, headroom=CHUNK_HEADROOM, gpu_chunks=chunks, gpu_chunk_size=csize,
                     launch_steps=int(prov_dev.launch_steps), launches_per_chunk=int(prov_dev.launches),

@@ -95,7 +95,10 @@ enum cl_qr_alg {
 /* Arithmetic of the tangent frames. The orbit, the Gauss-Legendre solve and the log sums are Float64 in both. */
 enum cl_precision {
     CL_PREC_FP64 = 0, /* plain kernel: the reference's Float64 algorithm, operation for operation           */
-    CL_PREC_MIXED = 1 /* tangent frames and their QR / norms in Float32, log sums Float64 (Neumaier)         */
+    CL_PREC_MIXED = 1, /* tangent frames and their QR / norms in Float32, log sums Float64 (Neumaier)        */
+    CL_PREC_MIXED_IND64 = 2 /* Float32 Lyapunov frames (QRSpectrum), Float64 indicator frames (GALI, SALI), the
+                             * orbit Float64; compiled for the coupled-maps pair QRSpectrum(Householder) k = 4 |
+                             * GALI + SALI k = 4 (cl_split_frames.cu)                                            */
 };
 
 enum cl_status {
