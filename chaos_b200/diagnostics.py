@@ -95,3 +95,48 @@ def orth_loss(Q) -> float:
     """eps_orth: max |Q'Q - I| (spec D4, residuals.jl:10)."""
     Q = np.asarray(Q, dtype=np.float64)
     return float(np.max(np.abs(Q.T @ Q - np.eye(Q.shape[1]))))
+
+
+SALI_ALIGNED = 1e-8   # SALI below this: the two deviation vectors aligned (chaotic orbit)
+FLOOR_FACTOR = 100.0  # GALI_k below FLOOR_FACTOR times its floor 2 k eps: at the measurement floor
+
+
+def precision_errors(ref, got, N: int) -> list[dict]:
+    """Per frame, how a run in reduced precision (`got`) differs from the Float64 run (`ref`) on the same orbits and
+    frames: the status agreement and completed fractions, then per reducer -- QRSpectrum: max and 99th percentile
+    |d lambda_i| over the orbits both completed; SALI and GALI_k: agreement of the class (SALI below 1e-8: aligned;
+    GALI_k below 100 times its floor 2 k eps(Float64)) and the largest |d log10| above those bounds. `ref` and `got`
+    are lists of PropagationResult (or records with .states, .code, .hstep, .reducers)."""
+    from .reducers import GALI, QRSpectrum, SALI
+
+    out = []
+    for a, b in zip(ref, got):
+        ok = (a.code == 0) & (b.code == 0)
+        rec = dict(code_agree=float(np.mean(a.code == b.code)), hstep_agree=float(np.mean(a.hstep == b.hstep)),
+                   completed_ref=float(np.mean((a.code == 0) & (a.hstep == N))),
+                   completed_got=float(np.mean((b.code == 0) & (b.hstep == N))),
+                   code_disagreements=[int(i) for i in np.flatnonzero(a.code != b.code)[:20]])
+        for i, r in enumerate(a.reducers):
+            sa, sb = a.states[f"r{i}"], b.states[f"r{i}"]
+            if isinstance(r, QRSpectrum):
+                d = np.abs(_lambdas(sa) - _lambdas(sb))[ok]
+                rec["dlambda_max"] = [float(v) for v in (d.max(axis=0) if len(d) else np.zeros(d.shape[1]))]
+                rec["dlambda_p99"] = [float(v) for v in (np.percentile(d, 99, axis=0) if len(d) else np.zeros(d.shape[1]))]
+            elif isinstance(r, SALI):
+                va, vb = sa["sali"][ok], sb["sali"][ok]
+                ca, cb = va < SALI_ALIGNED, vb < SALI_ALIGNED
+                big = ~ca & ~cb
+                rec["sali"] = dict(class_agree=float(np.mean(ca == cb)) if len(va) else 1.0, aligned_ref=float(np.mean(ca)) if len(va) else 0.0,
+                                   dlog10_max=float(np.max(np.abs(np.log10(va[big]) - np.log10(vb[big])), initial=0.0)))
+            elif isinstance(r, GALI):
+                g = []
+                for k in range(sa["gali"].shape[1]):
+                    va, vb = sa["gali"][ok, k], sb["gali"][ok, k]
+                    fl = FLOOR_FACTOR * 2 * (k + 2) * EPS
+                    ca, cb = va < fl, vb < fl
+                    big = ~ca & ~cb
+                    g.append(dict(k=k + 2, class_agree=float(np.mean(ca == cb)) if len(va) else 1.0,
+                                  dlog10_max=float(np.max(np.abs(np.log10(va[big]) - np.log10(vb[big])), initial=0.0))))
+                rec["gali"] = g
+        out.append(rec)
+    return out
