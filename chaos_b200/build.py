@@ -10,6 +10,7 @@ from __future__ import annotations
 import concurrent.futures as cf
 import glob
 import os
+import re
 import shutil
 import subprocess
 import sys
@@ -25,14 +26,31 @@ FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-fmad=false", "-Xcompiler", "-fPIC",
          "--expt-relaxed-constexpr", "-I" + os.path.join(ROOT, "include"), "-I" + CSRC]
 
 
-def _headers():
-    return glob.glob(os.path.join(CSRC, "*.cuh")) + glob.glob(os.path.join(CSRC, "*.h")) + \
-        glob.glob(os.path.join(ROOT, "include", "*.h"))
+_INCLUDE = re.compile(r'^\s*#\s*include\s+"([^"]+)"', re.M)
+
+
+def _deps(path: str, seen: set | None = None) -> set:
+    """The project headers `path` includes, transitively (quoted includes resolved beside the file, in csrc/ and in
+    include/)."""
+    seen = set() if seen is None else seen
+    try:
+        text = open(path).read()
+    except OSError:
+        return seen
+    for name in _INCLUDE.findall(text):
+        for base in (os.path.dirname(path), CSRC, os.path.join(ROOT, "include")):
+            cand = os.path.normpath(os.path.join(base, name))
+            if os.path.exists(cand):
+                if cand not in seen:
+                    seen.add(cand)
+                    _deps(cand, seen)
+                break
+    return seen
 
 
 def _compile(src: str, verbose_ptxas: bool) -> tuple[str, str]:
     obj = os.path.join(BUILD, os.path.basename(src).replace(".cu", ".o"))
-    newest = max([os.path.getmtime(src)] + [os.path.getmtime(h) for h in _headers()])
+    newest = max([os.path.getmtime(src)] + [os.path.getmtime(h) for h in _deps(src)])
     if os.path.exists(obj) and os.path.getmtime(obj) >= newest and not verbose_ptxas:
         return obj, ""
     cmd = [NVCC, *ARCH, *FLAGS, "-c", src, "-o", obj]

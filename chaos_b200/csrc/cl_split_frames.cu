@@ -16,8 +16,11 @@ using split::QRSlot;
 constexpr int D = 4, K = 4;
 constexpr int QWORDS = static_cast<int>(sizeof(QRState<4>) / 8);            // 17
 constexpr int GWORDS = static_cast<int>(sizeof(GALIFrameState<4, true>) / 8);   // 25
-// per-thread slot: an odd number of 8-byte words, so the 16 threads of a half-warp hit distinct bank pairs
-constexpr int SLOT_BYTES = ((static_cast<int>(sizeof(QRSlot) + sizeof(GSSlot)) / 8) | 1) * 8;
+// per-thread slot: the reducer fields, then room to park the point and the Float32 frame while the Float64 frame's
+// handoff runs (its Gram-Schmidt needs the registers); an odd number of 8-byte words, so the 16 threads of a
+// half-warp hit distinct bank pairs
+constexpr int PARK_BYTES = 4 * 8 + 16 * 4;
+constexpr int SLOT_BYTES = ((static_cast<int>(sizeof(QRSlot) + sizeof(GSSlot)) + PARK_BYTES) / 8 | 1) * 8;
 static_assert(sizeof(QRSlot) % 8 == 0 && sizeof(GSSlot) % 8 == 0, "slot layout");
 
 template <typename T>
@@ -55,8 +58,9 @@ __device__ __forceinline__ bool finite_x(const double* x) {
     return isfin(x[0]) && isfin(x[1]) && isfin(x[2]) && isfin(x[3]);
 }
 
-// Blocks of 64 threads, so that 65536 orbits (1024 blocks) fit one wave of 148 SMs at up to 7 blocks per SM; REGS is
-// the register budget of the variant (168: 6 blocks per SM, 144: 7, 128: 8).
+// Blocks of 64 threads: 65536 orbits are 1024 blocks, one wave of 148 SMs at 7 blocks per SM. Registers are
+// allocated per scheduler (16384 each), so 128 registers a thread hold 4 warps per scheduler, the 3.5 warps of that
+// ensemble; REGS is the budget of the variant.
 constexpr int SPLIT_BLOCK = 64;
 
 template <int REGS>
@@ -64,6 +68,8 @@ __global__ void __maxnreg__(REGS) split_frames_kernel(const KArgs a, const SysFr
     extern __shared__ __align__(16) unsigned char slots[];
     QRSlot& q = *reinterpret_cast<QRSlot*>(slots + threadIdx.x * SLOT_BYTES);
     GSSlot& g = *reinterpret_cast<GSSlot*>(slots + threadIdx.x * SLOT_BYTES + sizeof(QRSlot));
+    double* park_x = reinterpret_cast<double*>(slots + threadIdx.x * SLOT_BYTES + sizeof(QRSlot) + sizeof(GSSlot));
+    float* park_w = reinterpret_cast<float*>(park_x + 4);
     const i64 i = static_cast<i64>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (i >= a.n) return;
     const bool fresh = a.n0 == 0;
@@ -108,27 +114,56 @@ __global__ void __maxnreg__(REGS) split_frames_kernel(const KArgs a, const SysFr
     i64 n = a.n0;
     const i64 handoffs = a.steps / a.tau;
     for (i64 h = 0; h < handoffs; ++h) {
-        for (int t = 0; t < a.tau; ++t) {
-            split::Jac J;
-            split::jac(sys.nu, sys.kappa, sys.mu, x, J);
-            if (alive0) split::apply32<K>(J, W0);
-            if (alive1) split::apply64<K>(J, W1);
-            split::forward(sys.nu, sys.kappa, sys.mu, x, J);
+        if (alive0 && alive1) {   // the common case: one uniform test per window, not per step
+            for (int t = 0; t < a.tau; ++t) {
+                split::Jac J;
+                split::jac(sys.nu, sys.kappa, sys.mu, x, J);
+                split::apply32<K>(J, W0);
+                split::apply64<K>(J, W1);
+                split::forward(sys.nu, sys.kappa, sys.mu, x, J);
+            }
+        } else {
+            for (int t = 0; t < a.tau; ++t) {
+                split::Jac J;
+                split::jac(sys.nu, sys.kappa, sys.mu, x, J);
+                if (alive0) split::apply32<K>(J, W0);
+                if (alive1) split::apply64<K>(J, W1);
+                split::forward(sys.nu, sys.kappa, sys.mu, x, J);
+            }
         }
         n += a.tau;
         const bool xok = finite_x(x);
         if (alive0) {   // _status (orbit.jl:3), then the chain, then _any_failed (orbit.jl:54-57)
             int8_t c = xok ? (finite32(W0) ? STATUS_OK : STATUS_W) : STATUS_STATE;
             if (c == STATUS_OK) {
+                // the factorisation runs in the frame's registers: a failing handoff leaves the frame as it was
+#pragma unroll
+                for (int l = 0; l < 16; ++l) park_w[l] = W0[l];
                 split::qr_handoff(q, n, W0, orth_tol);
-                if (q.code != 0) c = STATUS_REDUCER;
+                if (q.code != 0) {
+                    c = STATUS_REDUCER;
+#pragma unroll
+                    for (int l = 0; l < 16; ++l) W0[l] = park_w[l];
+                }
             }
             if (c != STATUS_OK) { code0 = c; hstep0 = n; alive0 = false; }
         }
         if (alive1) {
             int8_t c = xok ? (finite64(W1) ? STATUS_OK : STATUS_W) : STATUS_STATE;
             if (c == STATUS_OK) {
+                // park the point and the Float32 frame in shared memory for the handoff (the clobber makes the
+                // compiler reload them afterwards instead of keeping them in registers)
+#pragma unroll
+                for (int l = 0; l < 4; ++l) park_x[l] = x[l];
+#pragma unroll
+                for (int l = 0; l < 16; ++l) park_w[l] = W0[l];
+                asm volatile("" ::: "memory");
                 split::gali_handoff(g, n, W1);
+                asm volatile("" ::: "memory");
+#pragma unroll
+                for (int l = 0; l < 4; ++l) x[l] = park_x[l];
+#pragma unroll
+                for (int l = 0; l < 16; ++l) W0[l] = park_w[l];
                 if (g.gcode != 0 || g.scode != 0) c = STATUS_REDUCER;
             }
             if (c != STATUS_OK) { code1 = c; hstep1 = n; alive1 = false; }
@@ -203,16 +238,13 @@ cudaError_t launch_split(const cl_run& run, const KArgs& a, const double*, cudaS
 
 cudaError_t launch_split_any(const cl_run& run, const KArgs& a, const double* A, cudaStream_t st, LaunchInfo* info,
                              int minb) {
-    switch (minb) {   // the variant index of the tuner: 2, 3, 4
-        case 2: return launch_split<168>(run, a, A, st, info);
-        case 4: return launch_split<128>(run, a, A, st, info);
-        default: return launch_split<144>(run, a, A, st, info);
-    }
+    (void)minb;   // one variant: 128 registers
+    return launch_split<128>(run, a, A, st, info);
 }
 
 // key of run_key for FroeschleMap (kind 3), d = 4, precision CL_PREC_MIXED_IND64, frames QRSpectrum(HouseholderQR) k = 4
 // and GALI + SALI k = 4
-const Registrar reg_split("s3d4p2|k4:QR4|k4:GALI,SALI|", launch_split_any, (1u << 1) | (1u << 2) | (1u << 3));
+const Registrar reg_split("s3d4p2|k4:QR4|k4:GALI,SALI|", launch_split_any, 1u << 3);
 
 }  // namespace
 }  // namespace cl

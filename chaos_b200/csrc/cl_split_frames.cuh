@@ -68,9 +68,11 @@ __device__ __forceinline__ void sincos_of(const Reduced& w, double* sn, double* 
     const double c = fma(z, pc, 1.0);
     const bool odd = (w.q & 1) != 0;
     const double a = odd ? c : s, b = odd ? s : c;
-    const double sv = (w.q & 2) ? -a : a;
+    // the quadrant's signs as sign-bit flips: sin negative in quadrants 2, 3; cos in 1, 2
+    const long long fs = static_cast<long long>(w.q & 2) << 62, fc = static_cast<long long>((w.q + 1) & 2) << 62;
+    const double sv = __longlong_as_double(__double_as_longlong(a) ^ fs);
     *sn = w.x == 0.0 ? w.x : sv;
-    *cs = ((w.q + 1) & 2) ? -b : b;
+    *cs = __longlong_as_double(__double_as_longlong(b) ^ fc);
 }
 
 // A positive running product m 2^e, m in [1, 2): multiply, then move the exponent into e (integer arithmetic). The
@@ -174,11 +176,11 @@ struct QRSlot {
     int code, pad;
 };
 
-// One handoff (qr_spectrum.jl:50-73 with householder.jl:19-80): W (4 x 4, column-major) is replaced by Q.
+// One handoff (qr_spectrum.jl:50-73 with householder.jl:19-80): W (4 x 4, column-major) is replaced by Q. The
+// factorisation runs in W's own registers (A aliases W; its lower part is dead once the reflectors are taken, its
+// upper part is R), so the handoff needs only the reflectors and R's inverse besides the frame.
 __device__ __forceinline__ void qr_handoff(QRSlot& st, i64 n, float* W, double orth_tol) {
-    float A[16];
-#pragma unroll
-    for (int l = 0; l < 16; ++l) A[l] = W[l];
+    float* A = W;
     float V[10], beta[3];   // reflector j: rows j..3 at V[off_j..], off = 0, 4, 7
     int count = 0;
 #pragma unroll
@@ -215,8 +217,53 @@ __device__ __forceinline__ void qr_handoff(QRSlot& st, i64 n, float* W, double o
         }
         A[j + 4 * j] = rho;
     }
-    // Q = H_0 H_1 H_2 I: each H_j touches rows j..3 of the columns j..3 (columns left of j are still e_l there)
-    float Q[16];
+    // _finish (householder.jl:66-75): R_ij = sg_i A_ij with sg_i the sign of A_ii, so that R_ii > 0
+    float sg[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) sg[i] = A[i + 4 * i] < 0.0f ? -1.0f : 1.0f;
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+#pragma unroll
+        for (int i = 0; i <= j; ++i) A[i + 4 * j] *= sg[i];
+    int bad = 0;   // _factor_failure (qr_spectrum.jl:43-48): the first pivot that is not finite and positive
+#pragma unroll
+    for (int j = 3; j >= 0; --j)
+        if (!(isfin(A[j + 4 * j]) && A[j + 4 * j] > 0.0f)) bad = j + 1;
+    if (bad) {
+        float pv = A[0];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) if (j + 1 == bad) pv = A[j + 4 * j];
+        st.code = 1; st.column = bad; st.value = pv; st.threshold = isfin(pv) ? 0.0 : __longlong_as_double(0x7ff0000000000000LL);
+        st.step = n;
+        return;
+    }
+    // window_Gw (orthonormalize.jl:112-127): |R|_F |R^-1|_F, R^-1 by back substitution with the pivots' reciprocals
+    float rd[4], rin[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) { rd[i] = A[i + 4 * i]; rin[i] = 1.0f / rd[i]; }
+    float ra = 0.0f, rb = 0.0f;
+    {
+        float Ri[16];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            Ri[j + 4 * j] = rin[j];
+#pragma unroll
+            for (int i = j - 1; i >= 0; --i) {
+                float s = A[i + 4 * (i + 1)] * Ri[(i + 1) + 4 * j];
+#pragma unroll
+                for (int l = i + 2; l <= j; ++l) s = __fmaf_rn(A[i + 4 * l], Ri[l + 4 * j], s);
+                Ri[i + 4 * j] = -s * rin[i];
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+#pragma unroll
+            for (int i = 0; i <= j; ++i) { ra = __fmaf_rn(A[i + 4 * j], A[i + 4 * j], ra); rb = __fmaf_rn(Ri[i + 4 * j], Ri[i + 4 * j], rb); }
+    }
+    const float Gw = sqrtf(ra) * sqrtf(rb);
+    // Q = H_0 H_1 H_2 I, formed in W's registers (R is no longer needed but its diagonal, kept in rd): each H_j
+    // touches rows j..3 of the columns j..3 (the columns left of j are still e_l there); then the column signs
+    float* Q = W;
 #pragma unroll
     for (int l = 0; l < 16; ++l) Q[l] = (l % 4) == (l / 4) ? 1.0f : 0.0f;
 #pragma unroll
@@ -233,57 +280,10 @@ __device__ __forceinline__ void qr_handoff(QRSlot& st, i64 n, float* W, double o
             for (int i = j; i < 4; ++i) Q[i + 4 * l] = __fmaf_rn(-f, V[off + i - j], Q[i + 4 * l]);
         }
     }
-    // _finish (householder.jl:66-75): signs so that R_ii > 0
-    float R[16];
-#pragma unroll
-    for (int j = 0; j < 4; ++j) {
-        const float sg = A[j + 4 * j] < 0.0f ? -1.0f : 1.0f;
-#pragma unroll
-        for (int i = 0; i < 4; ++i) {
-            Q[i + 4 * j] *= sg;
-            if (i <= j) R[i + 4 * j] = A[i + 4 * j];   // row sign applied below
-        }
-    }
-#pragma unroll
-    for (int i = 0; i < 4; ++i) {
-        const float sg = A[i + 4 * i] < 0.0f ? -1.0f : 1.0f;
-#pragma unroll
-        for (int j = i; j < 4; ++j) R[i + 4 * j] *= sg;
-    }
-    int bad = 0;   // _factor_failure (qr_spectrum.jl:43-48): the first pivot that is not finite and positive
-#pragma unroll
-    for (int j = 3; j >= 0; --j)
-        if (!(isfin(R[j + 4 * j]) && R[j + 4 * j] > 0.0f)) bad = j + 1;
-    if (bad) {
-        float pv = R[0];
-#pragma unroll
-        for (int j = 0; j < 4; ++j) if (j + 1 == bad) pv = R[j + 4 * j];
-        st.code = 1; st.column = bad; st.value = pv; st.threshold = isfin(pv) ? 0.0 : __longlong_as_double(0x7ff0000000000000LL);
-        st.step = n;
-        return;
-    }
-    // window_Gw (orthonormalize.jl:112-127): |R|_F |R^-1|_F, R^-1 by back substitution with the pivots' reciprocals
-    float rin[4];
-#pragma unroll
-    for (int i = 0; i < 4; ++i) rin[i] = 1.0f / R[i + 4 * i];
-    float Ri[16];
-#pragma unroll
-    for (int j = 0; j < 4; ++j) {
-        Ri[j + 4 * j] = rin[j];
-#pragma unroll
-        for (int i = j - 1; i >= 0; --i) {
-            float s = R[i + 4 * (i + 1)] * Ri[(i + 1) + 4 * j];
-#pragma unroll
-            for (int l = i + 2; l <= j; ++l) s = __fmaf_rn(R[i + 4 * l], Ri[l + 4 * j], s);
-            Ri[i + 4 * j] = -s * rin[i];
-        }
-    }
-    float ra = 0.0f, rb = 0.0f;
 #pragma unroll
     for (int j = 0; j < 4; ++j)
 #pragma unroll
-        for (int i = 0; i <= j; ++i) { ra = __fmaf_rn(R[i + 4 * j], R[i + 4 * j], ra); rb = __fmaf_rn(Ri[i + 4 * j], Ri[i + 4 * j], rb); }
-    const float Gw = sqrtf(ra) * sqrtf(rb);
+        for (int i = 0; i < 4; ++i) Q[i + 4 * j] *= sg[j];
     // orth_loss (qr_spectrum.jl:4): max |Q'Q - I| over the upper triangle (Q'Q is symmetric)
     float orth = 0.0f;
 #pragma unroll
@@ -302,14 +302,12 @@ __device__ __forceinline__ void qr_handoff(QRSlot& st, i64 n, float* W, double o
         return;
     }
 #pragma unroll
-    for (int i = 0; i < 4; ++i) lp_mul(st.lp[i], static_cast<double>(R[i + 4 * i]));
+    for (int i = 0; i < 4; ++i) lp_mul(st.lp[i], static_cast<double>(rd[i]));
     st.n = n;
     st.G_max = jl_max(st.G_max, static_cast<double>(Gw));   // _G_from_Gw is G_w for k > 2
     st.orth_max = jl_max(st.orth_max, static_cast<double>(orth));
     st.count_max = st.count_max > count ? st.count_max : count;
     st.column = 0;
-#pragma unroll
-    for (int l = 0; l < 16; ++l) W[l] = Q[l];
 }
 
 // ---- the indicator frame: GALI_4 with SALI of its columns 1-2, Float64 ------------------------------------------
@@ -371,21 +369,27 @@ __device__ __forceinline__ void gali_handoff(GSSlot& st, i64 n, double* W) {
         st.sali = m > 0.0 ? m * rsq64(m) : m;
         st.sn = n;
     }
-    // _gram_core! (gali.jl:81-100): each column orthogonalised twice against the earlier ones, then normalised;
-    // G_k = prod_{i <= k} r_i
+    // _gram_core! (gali.jl:81-100): each column orthogonalised twice against the earlier (orthonormal) ones, then
+    // normalised; G_k = prod_{i <= k} r_i. Each pass takes the projections on every earlier column at once (the
+    // classical form, twice: the same orthogonality as the modified form for these few columns, with the dots
+    // independent of one another)
     double g = 1.0;
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
 #pragma unroll
-        for (int pass = 0; pass < 2; ++pass)
+        for (int pass = 0; pass < 2; ++pass) {
+            double cc[4];
 #pragma unroll
             for (int p = 0; p < j; ++p) {
-                double cc = Q[4 * p] * Q[4 * j];
+                cc[p] = Q[4 * p] * Q[4 * j];
 #pragma unroll
-                for (int i = 1; i < 4; ++i) cc = fma(Q[i + 4 * p], Q[i + 4 * j], cc);
-#pragma unroll
-                for (int i = 0; i < 4; ++i) Q[i + 4 * j] = fma(-cc, Q[i + 4 * p], Q[i + 4 * j]);
+                for (int i = 1; i < 4; ++i) cc[p] = fma(Q[i + 4 * p], Q[i + 4 * j], cc[p]);
             }
+#pragma unroll
+            for (int p = 0; p < j; ++p)
+#pragma unroll
+                for (int i = 0; i < 4; ++i) Q[i + 4 * j] = fma(-cc[p], Q[i + 4 * p], Q[i + 4 * j]);
+        }
         const double r2 = sumsq64<4>(Q + 4 * j);
         const double ir = r2 > 0.0 ? rsq64(r2) : 1.0;
         const double r = r2 > 0.0 ? r2 * ir : 0.0;

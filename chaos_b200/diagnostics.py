@@ -97,16 +97,22 @@ def orth_loss(Q) -> float:
     return float(np.max(np.abs(Q.T @ Q - np.eye(Q.shape[1]))))
 
 
-SALI_ALIGNED = 1e-8   # SALI below this: the two deviation vectors aligned (chaotic orbit)
-FLOOR_FACTOR = 100.0  # GALI_k below FLOOR_FACTOR times its floor 2 k eps: at the measurement floor
+# The bounds below which SALI and GALI_k sit in their rounding noise at 1e5 steps of the coupled maps (two Float64
+# frames with different roundings agree within 0.02 decades above them and scatter below; measured on 65536 orbits):
+# SALI and GALI_2 1e-8, GALI_3 1e-14, GALI_4 and higher 1e-16.
+SALI_BOUND = 1e-8
+GALI_BOUNDS = {2: 1e-8, 3: 1e-14}
+GALI_BOUND_HIGH = 1e-16
 
 
 def precision_errors(ref, got, N: int) -> list[dict]:
     """Per frame, how a run in reduced precision (`got`) differs from the Float64 run (`ref`) on the same orbits and
     frames: the status agreement and completed fractions, then per reducer -- QRSpectrum: max and 99th percentile
-    |d lambda_i| over the orbits both completed; SALI and GALI_k: agreement of the class (SALI below 1e-8: aligned;
-    GALI_k below 100 times its floor 2 k eps(Float64)) and the largest |d log10| above those bounds. `ref` and `got`
-    are lists of PropagationResult (or records with .states, .code, .hstep, .reducers)."""
+    |d lambda_i| over the orbits both completed, and G_max's ratio on the windows the Float64 run finds well
+    conditioned (G_max < 1e6) with the fraction beyond 1e7 (where a Float32 frame cannot resolve the window:
+    G eps(Float32) > 1); SALI and GALI_k: agreement of the class at the noise bounds above (SALI_BOUND, GALI_BOUNDS)
+    and the largest |d log10| above them. `ref` and `got` are lists of PropagationResult (or records with .states,
+    .code, .hstep, .reducers)."""
     from .reducers import GALI, QRSpectrum, SALI
 
     out = []
@@ -122,9 +128,15 @@ def precision_errors(ref, got, N: int) -> list[dict]:
                 d = np.abs(_lambdas(sa) - _lambdas(sb))[ok]
                 rec["dlambda_max"] = [float(v) for v in (d.max(axis=0) if len(d) else np.zeros(d.shape[1]))]
                 rec["dlambda_p99"] = [float(v) for v in (np.percentile(d, 99, axis=0) if len(d) else np.zeros(d.shape[1]))]
+                ga, gb = sa["G_max"][ok], sb["G_max"][ok]
+                well = ga < 1e6
+                ratio = gb[well] / ga[well] if well.any() else np.ones(1)
+                rec["G_max"] = dict(ratio_well_conditioned=[float(ratio.min()), float(ratio.max())],
+                                    well_conditioned=float(np.mean(well)) if len(ga) else 0.0,
+                                    beyond_1e7=float(np.mean(ga >= 1e7)) if len(ga) else 0.0)
             elif isinstance(r, SALI):
                 va, vb = sa["sali"][ok], sb["sali"][ok]
-                ca, cb = va < SALI_ALIGNED, vb < SALI_ALIGNED
+                ca, cb = va < SALI_BOUND, vb < SALI_BOUND
                 big = ~ca & ~cb
                 rec["sali"] = dict(class_agree=float(np.mean(ca == cb)) if len(va) else 1.0, aligned_ref=float(np.mean(ca)) if len(va) else 0.0,
                                    dlog10_max=float(np.max(np.abs(np.log10(va[big]) - np.log10(vb[big])), initial=0.0)))
@@ -132,7 +144,7 @@ def precision_errors(ref, got, N: int) -> list[dict]:
                 g = []
                 for k in range(sa["gali"].shape[1]):
                     va, vb = sa["gali"][ok, k], sb["gali"][ok, k]
-                    fl = FLOOR_FACTOR * 2 * (k + 2) * EPS
+                    fl = GALI_BOUNDS.get(k + 2, GALI_BOUND_HIGH)
                     ca, cb = va < fl, vb < fl
                     big = ~ca & ~cb
                     g.append(dict(k=k + 2, class_agree=float(np.mean(ca == cb)) if len(va) else 1.0,

@@ -11,8 +11,10 @@ floor. A run of N steps is then ceil(N / L) launches per chunk that carry the st
 benchmark file per device and precision (ext/ChaoslabCUDAExt.jl:42-62) and falls back to DEFAULT_GPU_NS without it;
 here the record lives in chaos_b200/data/gpu-benchmark.toml (git-ignored; the reference's table layout
 `[<device name>."<precision label>"]`, so the Julia extension reads the same file) and is measured on first use on a
-device that has none (`record_step_ns`: 1024 orbits of the standard map K = 2 pi, k = 2, tau = 1, QRSpectrum(MGS), the
-reference's record workload, timed on the device).
+device that has none (`record_step_ns`: the standard map K = 2 pi, k = 2, tau = 1, QRSpectrum(MGS), the reference's
+record workload, timed on the device). The wave is the device's: LAUNCH_WAVE = 1024 is the orbits the reference's
+card runs concurrently (its D29 measurement); a B200 runs 148 SMs x 512 threads = 75776 orbit threads at once, so
+its record keeps `launch_wave` = SMs x 512 beside the value measured on that many orbits, and the plan uses both.
 
 `BEFORE_LAUNCH` is the `_before_launch(device, chunk_index, launch, carried)` hook: when set, `propagate` runs its
 launches one by one from the host and calls it before each with the live carried buffers.
@@ -42,13 +44,12 @@ def budget_orbits(ns: float, L: int) -> int:
     return int(math.floor(min(LAUNCH_BUDGET_S / (ns * 1e-9 * L), INT_MAX // 4)))
 
 
-def budget_steps(ns: float, tau: int) -> int:
-    """The largest multiple of tau with ns 1e-9 L LAUNCH_WAVE <= budget; 0 when L = tau exceeds it
-    (propagate.jl:154-167)."""
+def budget_steps(ns: float, tau: int, wave: int = LAUNCH_WAVE) -> int:
+    """The largest multiple of tau with ns 1e-9 L wave <= budget; 0 when L = tau exceeds it (propagate.jl:154-167)."""
     def fits(m):
-        return ns * 1e-9 * (m * tau) * LAUNCH_WAVE <= LAUNCH_BUDGET_S
+        return ns * 1e-9 * (m * tau) * wave <= LAUNCH_BUDGET_S
     cap = INT_MAX // (4 * tau)
-    m = int(math.floor(min(LAUNCH_BUDGET_S / (ns * 1e-9 * LAUNCH_WAVE * tau), cap)))
+    m = int(math.floor(min(LAUNCH_BUDGET_S / (ns * 1e-9 * wave * tau), cap)))
     while m > 0 and not fits(m):
         m -= 1
     while m < cap and fits(m + 1):
@@ -64,10 +65,10 @@ def forced_launch(tau: int) -> int | None:
     return L
 
 
-def device_plan(forced: int | None, N: int, tau: int, ns: float) -> tuple[int, int]:
+def device_plan(forced: int | None, N: int, tau: int, ns: float, wave: int = LAUNCH_WAVE) -> tuple[int, int]:
     """(steps per launch, orbit cap) (propagate.jl:183-190): (0, 0) when even L = tau exceeds the budget."""
-    L = min(budget_steps(ns, tau), N) if forced is None else min(forced, N)
-    return (0, 0) if L == 0 else (L, max(LAUNCH_WAVE, budget_orbits(ns, L)))
+    L = min(budget_steps(ns, tau, wave), N) if forced is None else min(forced, N)
+    return (0, 0) if L == 0 else (L, max(wave, budget_orbits(ns, L)))
 
 
 def launches(N: int, L: int) -> int:
@@ -106,7 +107,8 @@ def _write(rec: dict) -> None:
 
 
 def record_step_ns(precision: str = "fp64", device: str | None = None) -> float:
-    """Measure the one-wave ns per orbit-step on the current device and store it in the record."""
+    """Measure the one-wave ns per orbit-step on the current device (the standard map's kernel of the precision's
+    class: Float64, or Float32 tangent frames) and store it in the record with the device's wave."""
     import ctypes as C
 
     import numpy as np
@@ -117,13 +119,15 @@ def record_step_ns(precision: str = "fp64", device: str | None = None) -> float:
     from .reducers import MGS, QRSpectrum, chain_dtype
     from .systems import StandardMap
 
-    device = device or probe()["device"]
-    n, N = LAUNCH_WAVE, 2000
+    pr = probe()
+    device = device or pr["device"]
+    wave = int(pr["sm_count"]) * 512 if pr.get("sm_count") else LAUNCH_WAVE
+    n, N = wave, 2000
     sysm = StandardMap(2 * math.pi)
     x0 = np.random.default_rng(1).uniform(0, 2 * math.pi, (n, 2))
     W0 = np.ascontiguousarray(np.broadcast_to(np.eye(2), (n, 2, 2)))
     reds = (QRSpectrum(MGS()),)
-    run = build_run(sysm, N, 1, [FrameSpec(2, reds)], precision, 1)
+    run = build_run(sysm, N, 1, [FrameSpec(2, reds)], "fp64" if precision == "fp64" else "mixed", 1)
     x, W = np.empty((n, 2)), np.empty((n, 2, 2))
     st = np.zeros(n, dtype=chain_dtype(reds, 2, 2))
     code, hs = np.zeros(n, dtype=np.int8), np.zeros(n, dtype=np.int64)
@@ -141,23 +145,43 @@ def record_step_ns(precision: str = "fp64", device: str | None = None) -> float:
     ns = best * 1e6 / (n * N)
     with _lock:
         rec = _read()
-        rec.setdefault(device, {})[_label(precision)] = {"gpu_ns_per_step_wave": ns}
+        rec.setdefault(device, {})[_label(precision)] = {"gpu_ns_per_step_wave": ns, "launch_wave": wave}
         _write(rec)
-        _cache[(device, precision)] = ns
+        _cache[(device, _label(precision))] = (ns, wave)
     return ns
 
 
-def gpu_step_ns(precision: str = "fp64", device: str | None = None, measure: bool = True) -> float | None:
-    """The record's one-wave ns per orbit-step of (device, precision), measured and stored on first use when
-    `measure`; None when absent and not measured (the plan then uses DEFAULT_GPU_NS)."""
+def device_record(precision: str = "fp64", device: str | None = None, measure: bool = True) -> tuple[float, int] | None:
+    """(ns per orbit-step for one wave, the wave) of (device, precision) from the record, measured and stored on
+    first use when `measure`; None when absent and not measured."""
     if device is None:
-        from .propagate import probe
-        device = probe()["device"]
-    key = (device, precision)
+        device = _device_name()
+    key = (device, _label(precision))
     if key in _cache:
         return _cache[key]
-    v = _read().get(device, {}).get(_label(precision), {}).get("gpu_ns_per_step_wave")
-    if isinstance(v, (int, float)) and math.isfinite(v) and v > 0:
-        _cache[key] = float(v)
-        return float(v)
-    return record_step_ns(precision, device) if measure else None
+    e = _read().get(device, {}).get(_label(precision), {})
+    v, w = e.get("gpu_ns_per_step_wave"), e.get("launch_wave", LAUNCH_WAVE)
+    if isinstance(v, (int, float)) and math.isfinite(v) and v > 0 and isinstance(w, (int, float)) and w >= 1:
+        _cache[key] = (float(v), int(w))
+        return _cache[key]
+    if not measure:
+        return None
+    record_step_ns(precision, device)
+    return _cache[key]
+
+
+def gpu_step_ns(precision: str = "fp64", device: str | None = None, measure: bool = True) -> float | None:
+    """`gpu_step_ns(device, T)`: the record's one-wave ns per orbit-step (None without a record when not measuring;
+    the plan then uses DEFAULT_GPU_NS)."""
+    r = device_record(precision, device, measure)
+    return None if r is None else r[0]
+
+
+_names: dict = {}
+
+
+def _device_name() -> str:
+    from .propagate import probe
+    if "current" not in _names:
+        _names["current"] = probe()["device"]
+    return _names["current"]

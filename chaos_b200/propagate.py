@@ -197,8 +197,8 @@ def propagate_frames(sys: System, x0, N: int, frames: list[FrameSpec], *, tau: i
         raise DeviceError(rc, msg)
     # the launch plan (propagate.jl:183-190): steps per launch within the budget for one wave, and the orbit cap
     forced = launch_steps if launch_steps is not None else launch_plan.forced_launch(tau)
-    ns = launch_plan.gpu_step_ns(precision)
-    Lsteps, cap = launch_plan.device_plan(forced, N, tau, ns)
+    ns, wave = launch_plan.device_record(precision)
+    Lsteps, cap = launch_plan.device_plan(forced, N, tau, ns, wave)
     if Lsteps == 0:
         raise DeviceError(-8, f"a launch of tau = {tau} steps exceeds the launch budget for one wave")
     run.steps = Lsteps

@@ -12,7 +12,6 @@ from helpers import identity_frames, same_bits, uniform_starts
 pytestmark = pytest.mark.gpu
 
 SYS = FroeschleMap(1.5, 1.5, 0.05)
-EPS = 2.0 ** -52
 
 
 def _frames(n):
@@ -32,9 +31,10 @@ def _lam(r):
 def test_froeschle_fused_mixed():
     """8192 orbits uniform in [0, 2 pi)^4, N = 1e5, tau = 10, W0 = I (the benched workload's map, frames and
     horizon): the orbit bit for bit; |d lambda_i| <= 1e-3 for i = 1..4; the QR frame's status and step equal on
-    every orbit; the indicator frame (Float64) gives the same SALI class (below 1e-8: aligned, chaotic) and GALI_k
-    class (below 100 times its floor 2k eps) on every orbit, and above those bounds the same values within
-    |d log10| <= 1e-3; the indicator frame's log sums within 1e-9 relative; every orbit completes N steps in both."""
+    every orbit and its orthogonality loss within the Float32 threshold; G_max within 1e-3 relative where the Float64
+    window is well conditioned (G_max < 1e6); the indicator frame (Float64) gives the same class at the rounding-noise
+    bounds (SALI and GALI_2 1e-8, GALI_3 1e-14, GALI_4 1e-16) on every orbit and, above them, the same values within
+    |d log10| <= 0.05; its log sums within 1e-8 relative; every orbit completes N steps in both."""
     n, N = 8192, 100_000
     x0 = uniform_starts(n, 4, seed=1)
     a = _run(x0, N, "fp64")
@@ -50,20 +50,21 @@ def test_froeschle_fused_mixed():
     qa, qb = a[0].states["r0"], b[0].states["r0"]
     assert np.array_equal(qa["n"], qb["n"]) and np.array_equal(qa["count_max"], qb["count_max"])
     assert np.all(qb["orth_max"] <= 8 * 2.0 ** -23 * 4)
+    well = qa["G_max"] < 1e6
+    assert np.max(np.abs(qb["G_max"][well] / qa["G_max"][well] - 1.0), initial=0.0) <= 1e-3
     ga, gb = a[1].states, b[1].states
     sa, sb = ga["r1"]["sali"], gb["r1"]["sali"]
     assert np.array_equal(sa < 1e-8, sb < 1e-8)
     big = sa >= 1e-8
-    assert np.max(np.abs(np.log10(sa[big]) - np.log10(sb[big])), initial=0.0) <= 1e-3
-    for k in range(3):
+    assert np.max(np.abs(np.log10(sa[big]) - np.log10(sb[big])), initial=0.0) <= 0.05
+    for k, bound in enumerate((1e-8, 1e-14, 1e-16)):
         va, vb = ga["r0"]["gali"][:, k], gb["r0"]["gali"][:, k]
-        fl = 100 * 2 * (k + 2) * EPS
-        assert np.array_equal(va < fl, vb < fl), k
-        big = va >= fl
-        assert np.max(np.abs(np.log10(va[big]) - np.log10(vb[big])), initial=0.0) <= 1e-3, k
+        assert np.array_equal(va < bound, vb < bound), k
+        big = va >= bound
+        assert np.max(np.abs(np.log10(va[big]) - np.log10(vb[big])), initial=0.0) <= 0.05, k
     ta = ga["r0"]["s"] + ga["r0"]["c"]
     tb = gb["r0"]["s"] + gb["r0"]["c"]
-    assert np.max(np.abs(ta - tb) / np.maximum(np.abs(ta), 1.0)) <= 1e-9
+    assert np.max(np.abs(ta - tb) / np.maximum(np.abs(ta), 1.0)) <= 1e-8
     assert np.array_equal(ga["r1"]["n"], gb["r1"]["n"]) and np.array_equal(ga["r0"]["n"], gb["r0"]["n"])
 
 
@@ -105,3 +106,5 @@ def test_split_failures():
     sa, sb = a[1].states["r1"], b[1].states["r1"]
     assert int(sb["code"][10]) == int(sa["code"][10]) and int(sb["column"][10]) == int(sa["column"][10])
     assert same_bits(a[0].x, b[0].x)
+    # a failing handoff leaves the frame as it was (the factorisation runs in the frame's registers)
+    assert np.allclose(b[0].W[10], a[0].W[10], rtol=1e-4, atol=1e-6) and np.all(b[0].W[10][:, 0] == 0)
