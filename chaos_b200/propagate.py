@@ -237,20 +237,8 @@ def propagate_frames(sys: System, x0, N: int, frames: list[FrameSpec], *, tau: i
             if rc != 0:
                 raise DeviceError(rc, last_error())
             gpu_ms += prov_dev.gpu_ms
-        else:   # launch by launch, the hook before each with the live carried buffers (propagate.jl:101-104)
-            launch, n0, w = 0, 0, 0.0
-            while n0 < N:
-                launch += 1
-                hook(prov_dev.device.decode() or "B200", chunks + 1, launch,
-                     dict(x=x[lo:hi], W=[Wo[lo:hi] for Wo in Wout],
-                          states=[None if st is None else st[lo:hi] for st in states], workspace=None))
-                run.n0, run.steps = n0, min(Lsteps, N - n0)
-                rc = L.cl_b200_propagate(C.byref(run), hi - lo, C.byref(bufs), C.byref(prov_dev))
-                if rc != 0:
-                    raise DeviceError(rc, last_error())
-                w += prov_dev.gpu_ms
-                n0 += run.steps
-            run.n0, run.steps = 0, Lsteps
+        else:   # launch by launch, the hook before each with the live carried device buffers (propagate.jl:101-104)
+            w, launch = _hooked_chunk(L, run, hi - lo, bufs, frames, d, s, N, Lsteps, hook, prov_dev, chunks + 1)
             prov_dev.launch_steps, prov_dev.launches = Lsteps, launch
             gpu_ms += w
         chunks += 1
@@ -289,6 +277,72 @@ def propagate_frames(sys: System, x0, N: int, frames: list[FrameSpec], *, tau: i
                                          hstep=hsteps[f], reducers=tuple(fr.reducers)))
     return results
 
+
+
+def _hooked_chunk(L, run, n, hbufs, frames, d, s, N, Lsteps, hook, prov_dev, chunk_index):
+    """One chunk launch by launch on device buffers: the host inputs are staged once, `hook(device, chunk, launch,
+    carried)` runs before every launch with the live device buffers (torch tensors: x, W, states as bytes), each
+    launch is one window [n0, n0 + L) of `cl_b200_propagate_device`, and the outputs are copied back into the host
+    buffers at the end. Returns (device milliseconds, launches)."""
+    import torch
+
+    dev = torch.device("cuda", torch.cuda.current_device())
+    stream = torch.cuda.current_stream(dev)
+
+    def up(ptr, nbytes):
+        buf = torch.empty(nbytes, dtype=torch.uint8)
+        C.memmove(buf.data_ptr(), ptr, nbytes)
+        return buf.to(dev)
+
+    tx0 = up(hbufs.x0, 8 * n * s)
+    tx = torch.empty_like(tx0)
+    dbufs = _abi.cl_buffers()
+    dbufs.x0, dbufs.x = tx0.data_ptr(), tx.data_ptr()
+    keep, tW, tst = [tx0, tx], [], []
+    for f, fr in enumerate(frames):
+        wb = 8 * n * fr.k * d
+        W0 = up(hbufs.W0[f], wb) if hbufs.W0[f] else None
+        W = torch.empty(wb, dtype=torch.uint8, device=dev)
+        sb = _abi.frame_state_bytes(run.frames[f]) * n if hbufs.states[f] else 0
+        st = torch.zeros(max(sb, 1), dtype=torch.uint8, device=dev)
+        code = torch.zeros(n, dtype=torch.int8, device=dev)
+        hs = torch.zeros(n, dtype=torch.int64, device=dev)
+        dbufs.W0[f] = None if W0 is None else W0.data_ptr()
+        dbufs.W[f], dbufs.code[f], dbufs.hstep[f] = W.data_ptr(), code.data_ptr(), hs.data_ptr()
+        dbufs.states[f] = st.data_ptr() if sb else None
+        keep += [W0, W, st, code, hs]
+        tW.append(W.view(torch.float64).view(n, fr.k, d))
+        tst.append(st if sb else None)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    launch, n0, ms = 0, 0, 0.0
+    while n0 < N:
+        launch += 1
+        hook(prov_dev.device.decode() or "B200", chunk_index, launch,
+             dict(x=tx.view(torch.float64).view(n, s), W=tW, states=tst, workspace=None))
+        run.n0, run.steps = n0, min(Lsteps, N - n0)
+        e0.record(stream)
+        rc = L.cl_b200_propagate_device(C.byref(run), n, C.byref(dbufs), 0, C.c_void_p(stream.cuda_stream))
+        e1.record(stream)
+        if rc != 0:
+            raise DeviceError(rc, last_error())
+        e1.synchronize()
+        ms += e0.elapsed_time(e1)
+        n0 += run.steps
+    run.n0, run.steps = 0, Lsteps
+    torch.cuda.synchronize(dev)
+
+    def down(t, ptr, nbytes):
+        hb = t.reshape(-1).view(torch.uint8)[:nbytes].cpu()
+        C.memmove(ptr, hb.data_ptr(), nbytes)
+
+    down(tx, hbufs.x, 8 * n * s)
+    for f, fr in enumerate(frames):
+        down(tW[f], hbufs.W[f], 8 * n * fr.k * d)
+        if tst[f] is not None:
+            down(tst[f], hbufs.states[f], tst[f].numel())
+        down(keep[2 + 5 * f + 3], hbufs.code[f], n)
+        down(keep[2 + 5 * f + 4], hbufs.hstep[f], 8 * n)
+    return ms, launch
 
 def propagate(sys: System, x0, N: int, *, k: int, tau: int = 1, seed: int = 0, reducers=(), backend: str = "gpu",
               chunk: int | None = None, W0=None, precision: str = "fp64", launch_steps: int | None = None,
