@@ -713,13 +713,16 @@ def workload_screen(args):
           cpu_baseline=cpu, clocks=sampler.summary(), gpu_launches=int(launches))
 
 def workload_mlp(args):
-    """The learned screen's network on the tensor cores: inference (4 GEMMs with fused bias / GELU epilogues) and one
-    training step (forward, loss, backward GEMMs, Adam) at a batch of 262144 rows."""
+    """The learned screen's network on the tensor cores at a batch of 262144 rows: inference as one fused persistent
+    kernel (the headline), inference layer by layer (4 GEMMs with bias / GELU epilogues), and one training step
+    (forward, loss, backward GEMMs, Adam)."""
     torch, dev, L = _setup()
     from chaos_b200.mlp import DIMS, MLP, OUT_PAD
     B = args.orbits or 262144
     net = MLP(torch, dev, seed=0)
     rng = np.random.default_rng(SEED)
+    for lay in net.layers:   # nonzero biases, as after training
+        lay["b"].copy_(torch.tensor(rng.standard_normal(lay["b"].numel()).astype(np.float32) * 0.1, device=dev))
     X = torch.tensor(rng.standard_normal((B, 64)).astype(np.float32), device=dev).to(torch.bfloat16)
     label = torch.tensor((rng.random(B) < 0.5).astype(np.float32), device=dev)
     target = torch.tensor(rng.standard_normal(B).astype(np.float32), device=dev)
@@ -732,12 +735,27 @@ def workload_mlp(args):
     fout = [DIMS[1], DIMS[2], DIMS[3], OUT_PAD]
     fwd = sum(2 * B * a * b for a, b in zip(fin, fout))
     bwd = sum(2 * B * a * b for a, b in zip(fin, fout)) + sum(2 * B * a * b for a, b in zip(fin[1:], fout[1:]))
+    out = torch.empty((B, OUT_PAD), dtype=torch.float32, device=dev)
+    net.packed()
     sampler = ClockSampler(0)
     l0 = L.cl_b200_launch_count()
-    ms_fwd = _event_times(torch, dev, stream, lambda: net.forward(X), args.steps, args.warmup, flush, sampler)
-    n_fwd = L.cl_b200_launch_count() - l0
+    ms_fused = _event_times(torch, dev, stream, lambda: net.forward_fused(X, out=out), args.steps, args.warmup, flush,
+                            sampler)
+    n_fwd = (L.cl_b200_launch_count() - l0) // (args.steps + args.warmup) * args.steps   # timed launches only
+    ms_layer = _event_times(torch, dev, stream, lambda: net.forward(X), args.steps, args.warmup, flush)
+    same = bool(torch.equal(net.forward_fused(X), net.forward(X)))
     ms_train = _event_times(torch, dev, stream, lambda: net.train_step(X, label, target), args.steps, args.warmup,
                             flush)
+    # end to end: the rows' features from pinned host memory, the outputs back to it
+    Xh = X.cpu().pin_memory()
+    oh = torch.empty((B, OUT_PAD), dtype=torch.float32).pin_memory()
+    Xd = torch.empty_like(X)
+
+    def e2e():
+        Xd.copy_(Xh, non_blocking=True)
+        net.forward_fused(Xd, out=out)
+        oh.copy_(out, non_blocking=True)
+    ms_e2e = _event_times(torch, dev, stream, e2e, args.steps, args.warmup, flush)
     peaks = {}
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -745,16 +763,19 @@ def workload_mlp(args):
     except OSError:
         pass
     peak = peaks.get("bf16_tflops", 1590.0)
-    achieved = fwd / (np.mean(ms_fwd) / 1e3) / 1e12
-    _line("screen-MLP inference rows/s (BF16 tcgen05 GEMMs, FP32 accumulate, fused bias+GELU)",
-          B / (np.mean(ms_fwd) / 1e3), "rows/s", args, ms_fwd,
+    achieved = fwd / (np.mean(ms_fused) / 1e3) / 1e12
+    layered = fwd / (np.mean(ms_layer) / 1e3) / 1e12
+    _line("screen-MLP inference rows/s (one fused persistent tcgen05 kernel, BF16 operands, FP32 accumulate)",
+          B / (np.mean(ms_fused) / 1e3), "rows/s", args, ms_fused,
           dict(workload=f"mlp-64x256x256x256x2-batch{B}", batch=B, layers=list(DIMS),
                l2="flushed between timed steps (256 MB write)"),
           dtype="bf16 (f32 accumulate)",
+          e2e=dict(value=B / (np.mean(ms_e2e) / 1e3), unit="rows/s", h2d_bytes_per_step=int(B * 64 * 2),
+                   d2h_bytes_per_step=int(B * OUT_PAD * 4)),
           roofline=dict(bound="tensor", achieved=achieved, peak=peak, unit="TFLOP/s", frac=achieved / peak,
                         traffic=None, peak_source="MEASURED_PEAKS.json bf16_tflops (burst)" if peaks else "fallback",
-                        dram_read_per_layer_b=33.8e6 * B / 65536,
-                        dram_source="ncu: 256x256 layer at 65536 rows reads 33.8 MB (its input once), scaled by rows"),
+                        flops_per_row=fwd // B),
+          layered=dict(ms=float(np.mean(ms_layer)), tflops=layered, frac=layered / peak, bitwise_equal_fused=same),
           training_step=dict(ms=float(np.mean(ms_train)), tflops=(fwd + bwd) / (np.mean(ms_train) / 1e3) / 1e12),
           clocks=sampler.summary(), gpu_launches=int(n_fwd))
 

@@ -276,7 +276,7 @@ EXPORTS = ("cl_b200_propagate", "cl_b200_propagate_device", "cl_b200_check", "cl
            "cl_b200_menu_size", "cl_b200_menu_key", "cl_b200_ensemble_device", "cl_b200_ensemble",
            "cl_b200_ensemble_tune", "cl_b200_ensemble_graph_create", "cl_b200_ensemble_graph_launch",
            "cl_b200_ensemble_graph_destroy", "cl_b200_ensemble_device_noalloc", "cl_b200_tune",
-           "cl_b200_gemm_bf16", "cl_b200_mlp_status", "cl_b200_transpose_bf16", "cl_b200_gelu_backward",
+           "cl_b200_gemm_bf16", "cl_b200_mlp_pack_kmajor", "cl_b200_mlp_forward_fused", "cl_b200_mlp_status", "cl_b200_transpose_bf16", "cl_b200_gelu_backward",
            "cl_b200_col_sum", "cl_b200_head_loss", "cl_b200_adam", "cl_b200_to_bf16", "cl_b200_screen_features",
            "cl_b200_shadow_bytes", "cl_b200_shadow_device", "cl_b200_shadow", "cl_b200_record_columns",
            "cl_b200_record_state_bytes", "cl_b200_record_device", "cl_b200_record",

@@ -13,6 +13,7 @@
 // epilogue. Long-K products with few output tiles (weight gradients) split K over CTAs and add their partial tiles
 // atomically. Every wait on an mbarrier is bounded: past the limit the kernel records an error flag and returns
 // instead of spinning on.
+#include <cuda.h>
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
@@ -78,6 +79,85 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t phase) {
     }
     atomicExch(&g_mlp_error, 1u);
     return false;
+}
+
+// The network's activation: GELU in its tanh form (Hendrycks & Gimpel 2016), x (1 + tanh u) / 2 with
+// u = sqrt(2 / pi) (x + 0.044715 x^3). Since (1 + tanh u) / 2 = 1 / (1 + e^(-2u)), it is evaluated without the
+// cancellation of 1 + tanh u for negative x as x s, s = 1 / (1 + 2^z), z = -2 log2(e) u = x (G0 + G1 x^2) clamped
+// to 64 (beyond it s < 6e-20): one ex2 on the special-function unit, and the reciprocal by three Newton steps
+// r <- r + r (1 - d r) on the FMA pipe from the seed bits(r0) = 0x7EF311C2 - bits(d), whose relative error is at
+// most 0.0505 for every normal d (the constant minimises it over all mantissas; found by exhaustive search). The
+// steps square the error (0.0505 -> 2.6e-3 -> 6.5e-6 -> 4e-11) so s is within about one unit in the last place. The
+// pair form runs the same operations lane by lane on packed FP32 pairs (fma/mul/add .f32x2), so the scalar form
+// (the per-layer epilogue) and the pair form (the fused pass) agree bit for bit.
+constexpr float kG0 = -2.3022082f;     // -2 log2(e) sqrt(2 / pi)
+constexpr float kG1 = -0.10294324f;    // kG0 * 0.044715
+constexpr float kLn2 = 0.6931472f;
+constexpr float kZMax = 64.0f;
+constexpr uint32_t kRcpSeed = 0x7EF311C2u;
+__device__ __forceinline__ float ex2_approx(float z) {
+    float e;
+    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(e) : "f"(z));
+    return e;
+}
+// s = 1 / (1 + 2^z(x)) for one value.
+__device__ __forceinline__ float sig_t(float x) {
+    const float z = fminf(__fmul_rn(x, __fmaf_rn(kG1, __fmul_rn(x, x), kG0)), kZMax);
+    const float d = __fadd_rn(1.0f, ex2_approx(z));
+    const float nd = __fmul_rn(d, -1.0f);
+    float r = __uint_as_float(kRcpSeed - __float_as_uint(d));
+#pragma unroll
+    for (int i = 0; i < 3; ++i) r = __fmaf_rn(r, __fmaf_rn(nd, r, 1.0f), r);
+    return r;
+}
+__device__ __forceinline__ float gelu_t(float x) { return __fmul_rn(x, sig_t(x)); }
+
+// Packed FP32 pairs (the .f32x2 forms; lane by lane the same IEEE operations as the scalar ones).
+__device__ __forceinline__ uint64_t f2(float a, float b) {
+    uint64_t r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a), "f"(b));
+    return r;
+}
+__device__ __forceinline__ void f2split(uint64_t v, float& a, float& b) {
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(v));
+}
+__device__ __forceinline__ uint64_t fma2(uint64_t a, uint64_t b, uint64_t c) {
+    uint64_t d;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+    return d;
+}
+__device__ __forceinline__ uint64_t mul2(uint64_t a, uint64_t b) {
+    uint64_t d;
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ uint64_t add2(uint64_t a, uint64_t b) {
+    uint64_t d;
+    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+// gelu_t of both lanes of v, rounded to a BF16 pair (low half: lane 0).
+__device__ __forceinline__ uint32_t gelu_t2_bf16(uint64_t v) {
+    const uint64_t g1 = f2(kG1, kG1), g0 = f2(kG0, kG0), one = f2(1.0f, 1.0f), neg = f2(-1.0f, -1.0f);
+    float z0, z1;
+    f2split(mul2(v, fma2(g1, mul2(v, v), g0)), z0, z1);
+    const uint64_t d = add2(one, f2(ex2_approx(fminf(z0, kZMax)), ex2_approx(fminf(z1, kZMax))));
+    const uint64_t nd = mul2(d, neg);
+    float d0, d1;
+    f2split(d, d0, d1);
+    uint64_t r = f2(__uint_as_float(kRcpSeed - __float_as_uint(d0)), __uint_as_float(kRcpSeed - __float_as_uint(d1)));
+#pragma unroll
+    for (int i = 0; i < 3; ++i) r = fma2(r, fma2(nd, r, one), r);
+    float y0, y1;
+    f2split(mul2(v, r), y0, y1);
+    const __nv_bfloat162 h = __floats2bfloat162_rn(y0, y1);
+    return *reinterpret_cast<const uint32_t*>(&h);
+}
+// d/dx of gelu_t: s - x s (1 - s) ln2 (G0 + 3 G1 x^2).
+__device__ __forceinline__ float gelu_t_grad(float x) {
+    const float sg = sig_t(x);
+    const float dz = __fmaf_rn(3.0f * kG1, __fmul_rn(x, x), kG0);
+    return __fsub_rn(sg, __fmul_rn(__fmul_rn(__fmul_rn(x, sg), __fsub_rn(1.0f, sg)), __fmul_rn(kLn2, dz)));
 }
 
 // Async 16-byte global -> shared copy; src_bytes < 16 zero-fills the rest (0: nothing is read).
@@ -256,7 +336,7 @@ __global__ void __launch_bounds__(128, 1) gemm_bf16_tc(const __nv_bfloat16* __re
                     }
                     if (epilogue == 1) {
 #pragma unroll
-                        for (int j = 0; j < 16; ++j) v[j] = 0.5f * v[j] * (1.0f + erff(v[j] * 0.70710678118654752f));
+                        for (int j = 0; j < 16; ++j) v[j] = gelu_t(v[j]);
                     }
                     if (C32) {
 #pragma unroll
@@ -283,7 +363,7 @@ __global__ void __launch_bounds__(128, 1) gemm_bf16_tc(const __nv_bfloat16* __re
                         if (accumulate && C32) v += C32[at];
                         if (bias) v += bias[col];
                         if (pre) pre[at] = v;
-                        if (epilogue == 1) v = 0.5f * v * (1.0f + erff(v * 0.70710678118654752f));   // GELU (erf form)
+                        if (epilogue == 1) v = gelu_t(v);
                         if (C32) C32[at] = v;
                         if (Cb) Cb[at] = __float2bfloat16(v);
                     }
@@ -297,6 +377,373 @@ __global__ void __launch_bounds__(128, 1) gemm_bf16_tc(const __nv_bfloat16* __re
         asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" :: "r"(tmem), "r"(TCOLS) : "memory");
     }
+}
+
+// ---- the fused forward pass --------------------------------------------------------------------------------------
+// The screen network's whole inference pass (64 -> 256 -> 256 -> 256 -> 16) in one persistent kernel, one CTA of
+// eighteen warps per SM looping over 128-row tiles, the activations never leaving the SM:
+//   warp 0      producer: stages the next row tiles' inputs (plain loads -> the canonical K-major layout) and
+//               streams the weights through a 3-stage ring by bulk copies (cp.async.bulk, the untiled TMA) from their
+//               pre-packed layout (cl_b200_mlp_pack_kmajor), each stage's mbarrier counting the bytes in;
+//   warp 1      one thread issues the tcgen05.mma (M = 128, N = 256 / 16, K = 16 each) and commits them to the
+//               barriers that free a weight stage, an input slot or hand an accumulator to the epilogue;
+//   warps 2..17 epilogue: read the accumulator (tcgen05.ld, the next 16 columns loading while the current ones are
+//               processed), add the bias, apply GELU (packed FP32 pairs), round to BF16 into the activation tile,
+//               64 columns at a time; the next layer's MMAs on K block j start as soon as the sixteen epilogue warps
+//               have written block j, so the epilogue overlaps the tensor cores.
+// Tensor memory holds two 128 x 256 FP32 accumulators (512 columns): layers 1 and 3 use the first, layers 2 and 4 the
+// second, so a layer's MMAs run while the previous layer's accumulator is being drained. The MMAs see the operands in
+// the same order as the per-layer GEMM (K ascending in steps of 16, accumulate from zero) and the epilogue is the same
+// arithmetic, so the outputs are bit for bit the per-layer path's. Every wait is bounded: a wait that gives up sets
+// the error flag and a shared abort flag that every role polls, all roles leave their loops, the MMA thread waits
+// for its last commit and the producer for its copies in flight, then the accumulator is released.
+constexpr int F_STAGES = 3;
+constexpr int F_TILE = BM * BK * 2;                 // 16 KB: one 128 x 64 BF16 block (an input tile or activation block)
+constexpr int F_WCHUNK = 256 * BK * 2;              // 32 KB: one 256 x 64 weight block
+constexpr int F_OFF_X = 0;                          // 2 input slots
+constexpr int F_OFF_ACT = 2 * F_TILE;               // the activation tile: 4 K blocks of 64
+constexpr int F_OFF_W = F_OFF_ACT + 4 * F_TILE;     // the weight ring
+constexpr int F_OFF_BIAS = F_OFF_W + F_STAGES * F_WCHUNK;
+constexpr int F_NBIAS = 3 * 256 + 16;
+constexpr int F_SMEM = F_OFF_BIAS + F_NBIAS * 4;    // 199,744 bytes
+constexpr int F_CHUNKS = 10;                        // per tile: W1 (1 block), W2 (4), W3 (4), W4 (its 4 blocks, 8 KB)
+constexpr int F_THREADS = 576;                     // 18 warps: producer, MMA, 16 epilogue
+constexpr int F_EPI_WARPS = 16;
+
+struct FusedArgs {
+    const __nv_bfloat16* X;                         // B x 64 row-major, rows 16-byte aligned
+    const uint8_t* Wp[4];                           // packed weights: 32 KB, 128 KB, 128 KB, 8 KB
+    const float* bias[4];                           // 256, 256, 256, 16
+    float* out;                                     // B x 16
+    int B;
+    int tiles;
+};
+
+__device__ __forceinline__ uint32_t fchunk_bytes(int c) { return c == F_CHUNKS - 1 ? 4u * 16 * BK * 2 : static_cast<uint32_t>(F_WCHUNK); }
+__device__ __forceinline__ const uint8_t* fchunk_src(const FusedArgs& a, int c) {
+    if (c == 0) return a.Wp[0];
+    if (c <= 4) return a.Wp[1] + static_cast<size_t>(c - 1) * F_WCHUNK;
+    if (c <= 8) return a.Wp[2] + static_cast<size_t>(c - 5) * F_WCHUNK;
+    return a.Wp[3];
+}
+
+// Bounded wait that also gives up when another role has (the shared abort flag): the clock and the flag are
+// checked every 64 polls. (A suspend-time hint on the try_wait made the kernel slower: 58.8 us against 51.1 us at
+// 65536 rows.)
+__device__ __forceinline__ bool fwait(uint32_t bar, uint32_t parity, volatile int* abort_flag) {
+    const uint64_t t0 = global_ns();
+    for (unsigned it = 0;; ++it) {
+        uint32_t done;
+        asm volatile(
+            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+            : "=r"(done) : "r"(bar), "r"(parity) : "memory");
+        if (done) return true;
+        if ((it & 63u) == 63u) {
+            if (*abort_flag) return false;
+            if (it >= kWaitLimit || global_ns() - t0 > kWaitNs) {
+                *abort_flag = 1;
+                atomicExch(&g_mlp_error, 1u);
+                return false;
+            }
+        }
+    }
+}
+
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" :: "r"(bar) : "memory");
+}
+
+__device__ __forceinline__ void mma_commit(uint32_t bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" :: "r"(bar) : "memory");
+}
+
+__device__ __forceinline__ void mma_bf16(uint32_t tmem, uint64_t da, uint64_t db, uint32_t idesc, uint32_t acc) {
+    asm volatile("{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+                 " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n"
+                 :: "r"(tmem), "l"(da), "l"(db), "r"(idesc), "r"(acc) : "memory");
+}
+
+// 32 lanes x 16 columns of FP32 from tensor memory (no wait).
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&r)[16]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];\n"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+}
+
+// Waits for this thread's tensor-memory loads; the registers pass through the wait so no use of them is scheduled
+// before it.
+__device__ __forceinline__ void tmem_wait16(uint32_t (&r)[16]) {
+    asm volatile("tcgen05.wait::ld.sync.aligned;\n"
+                 : "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3]), "+r"(r[4]), "+r"(r[5]), "+r"(r[6]), "+r"(r[7]),
+                   "+r"(r[8]), "+r"(r[9]), "+r"(r[10]), "+r"(r[11]), "+r"(r[12]), "+r"(r[13]), "+r"(r[14]), "+r"(r[15])
+                 :: "memory");
+}
+
+__global__ void __launch_bounds__(F_THREADS, 1) mlp_forward_fused(const FusedArgs a, const __grid_constant__ CUtensorMap xmap) {
+    extern __shared__ __align__(1024) uint8_t fsm[];
+    __shared__ __align__(8) uint64_t w_full[F_STAGES], w_empty[F_STAGES], x_full[2], x_empty[2], acc_full[2],
+        acc_empty[2], act_full[4];
+    __shared__ uint32_t tmem_base;
+    __shared__ volatile int abort_flag;
+    __shared__ int consumed_chunks, consumed_x;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const uint32_t sbase = smem_u32(fsm);
+    const uint32_t sX = sbase + F_OFF_X, sAct = sbase + F_OFF_ACT, sW = sbase + F_OFF_W;
+    float* sBias = reinterpret_cast<float*>(fsm + F_OFF_BIAS);
+
+    for (int i = tid; i < F_NBIAS; i += F_THREADS) {
+        float v;
+        if (i < 256) v = a.bias[0][i];
+        else if (i < 512) v = a.bias[1][i - 256];
+        else if (i < 768) v = a.bias[2][i - 512];
+        else v = a.bias[3][i - 768];
+        sBias[i] = v;
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n"
+                     :: "r"(smem_u32(&tmem_base)), "r"(512) : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
+    }
+    if (tid == 0) {
+        auto init = [](uint64_t* b, int count) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" :: "r"(smem_u32(b)), "r"(count) : "memory");
+        };
+        for (int s = 0; s < F_STAGES; ++s) { init(&w_full[s], 1); init(&w_empty[s], 1); }
+        for (int s = 0; s < 2; ++s) {
+            init(&x_full[s], 1); init(&x_empty[s], 1); init(&acc_full[s], 1); init(&acc_empty[s], F_EPI_WARPS);
+        }
+        for (int j = 0; j < 4; ++j) init(&act_full[j], F_EPI_WARPS);
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+        abort_flag = 0;
+        consumed_chunks = 0;
+        consumed_x = 0;
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+    const uint32_t tmem = tmem_base;
+    const int ntiles = a.tiles > static_cast<int>(blockIdx.x) ? (a.tiles - 1 - static_cast<int>(blockIdx.x)) / static_cast<int>(gridDim.x) + 1 : 0;
+    int issued_chunks = 0;        // producer: weight chunks whose copies were issued
+    int issued_x = 0;             // producer: input tiles whose copies were issued
+    int last_commit = -1;         // MMA thread: the last weight chunk whose MMAs were committed
+
+    if (warp == 0) {
+        // ---------------------------------------------------------------- producer
+        bool ok = true;
+        int g = 0;
+        for (int i = 0; i < ntiles && ok; ++i) {
+            const int tile = static_cast<int>(blockIdx.x) + i * static_cast<int>(gridDim.x);
+            const int slot = i & 1;
+            // the 128 x 64 input tile: eight tensor copies of 128 rows x 8 columns, K group g landing at g * 2048
+            // bytes (8-row x 16-byte core matrices, K-adjacent 2048 B apart, 8-row groups 128 B apart); rows past B
+            // are zero filled
+            int xgood = 1;
+            if (lane == 0) {
+                xgood = fwait(smem_u32(&x_empty[slot]), static_cast<uint32_t>(((i >> 1) & 1) ^ 1), &abort_flag);
+                if (xgood) {
+                    const uint32_t bar = smem_u32(&x_full[slot]), dst = sX + slot * F_TILE;
+                    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" :: "r"(bar), "r"(F_TILE) : "memory");
+#pragma unroll
+                    for (int gk = 0; gk < 8; ++gk)
+                        asm volatile(
+                            "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];\n"
+                            :: "r"(dst + gk * 2048), "l"(reinterpret_cast<uint64_t>(&xmap)), "r"(gk * 8), "r"(tile * BM), "r"(bar)
+                            : "memory");
+                    ++issued_x;
+                }
+            }
+            ok = __shfl_sync(0xffffffffu, xgood, 0) != 0;
+            if (!ok) break;
+            for (int c = 0; c < F_CHUNKS; ++c, ++g) {
+                const int s = g % F_STAGES;
+                int good = 1;
+                if (lane == 0) {
+                    good = fwait(smem_u32(&w_empty[s]), static_cast<uint32_t>(((g / F_STAGES) & 1) ^ 1), &abort_flag);
+                    if (good) {
+                        const uint32_t bytes = fchunk_bytes(c), bar = smem_u32(&w_full[s]);
+                        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" :: "r"(bar), "r"(bytes) : "memory");
+                        asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n"
+                                     :: "r"(sW + s * F_WCHUNK), "l"(fchunk_src(a, c)), "r"(bytes), "r"(bar) : "memory");
+                        ++issued_chunks;
+                    }
+                }
+                ok = __shfl_sync(0xffffffffu, good, 0) != 0;
+                if (!ok) break;
+            }
+        }
+    } else if (warp == 1) {
+        // ---------------------------------------------------------------- MMA issuer
+        if (lane == 0) {
+            constexpr uint32_t id256 = idesc_bf16(BM, 256), id16 = idesc_bf16(BM, 16);
+            bool ok = true;
+            int g = 0;
+            for (int i = 0; i < ntiles && ok; ++i) {
+                const int slot = i & 1;
+                for (int l = 0; l < 4 && ok; ++l) {
+                    const int b = l & 1;
+                    const int u = 2 * i + (l >> 1);           // the use of accumulator b
+                    const uint32_t accum = tmem + static_cast<uint32_t>(b * 256);
+                    ok = fwait(smem_u32(&acc_empty[b]), static_cast<uint32_t>((u & 1) ^ 1), &abort_flag);
+                    if (l == 0 && ok) {
+                        ok = fwait(smem_u32(&x_full[slot]), static_cast<uint32_t>((i >> 1) & 1), &abort_flag);
+                        if (ok) consumed_x = i + 1;
+                    }
+                    if (!ok) break;
+                    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+                    const int nkb = l == 0 ? 1 : 4;
+                    const uint32_t act_parity = static_cast<uint32_t>((3 * i + l - 1) & 1);
+                    for (int kb = 0; kb < nkb && ok; ++kb) {
+                        // layers 1-3: one weight chunk per K block; layer 4: one chunk holds all four blocks
+                        const int s = g % F_STAGES;
+                        if (l != 3 || kb == 0)
+                            ok = fwait(smem_u32(&w_full[s]), static_cast<uint32_t>((g / F_STAGES) & 1), &abort_flag);
+                        if (ok && l > 0) ok = fwait(smem_u32(&act_full[kb]), act_parity, &abort_flag);
+                        if (!ok) break;
+                        asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+                        const uint32_t bbase = sW + s * F_WCHUNK + (l == 3 ? kb * (16 * BK * 2) : 0);
+                        // A: the input tile in the tensor copies' layout (LBO 2048, SBO 128) or an activation block
+                        // in the epilogue's (LBO 128, SBO 1024)
+                        const uint32_t abase = l == 0 ? sX + slot * F_TILE : sAct + kb * F_TILE;
+                        const uint32_t astep = l == 0 ? 4096u : 256u, albo = l == 0 ? 2048u : 128u, asbo = l == 0 ? 128u : 1024u;
+#pragma unroll
+                        for (int k = 0; k < BK / 16; ++k)
+                            mma_bf16(accum, smem_desc(abase + k * astep, albo, asbo),
+                                     smem_desc(bbase + k * 256, 128, (BK / 8) * 128), l == 3 ? id16 : id256,
+                                     (kb > 0 || k > 0) ? 1u : 0u);
+                        if (l != 3) {
+                            mma_commit(smem_u32(&w_empty[s]));
+                            last_commit = g;
+                            ++g;
+                        }
+                    }
+                    if (!ok) break;
+                    if (l == 3) {
+                        mma_commit(smem_u32(&w_empty[g % F_STAGES]));
+                        last_commit = g;
+                        ++g;
+                    }
+                    if (l == 0) mma_commit(smem_u32(&x_empty[slot]));
+                    mma_commit(smem_u32(&acc_full[b]));
+                }
+            }
+            consumed_chunks = g;
+        }
+    } else {
+        // ---------------------------------------------------------------- epilogue (warps 2..17)
+        // warp w reads TMEM lanes 32 (w % 4) .. +31 (its rows); the four warps of a lane quarter split each 64-column
+        // block into 16-column quarters h = (w - 2) / 4
+        const int e = warp - 2, q = warp & 3, h = e >> 2;
+        const int row = q * 32 + lane;
+        bool ok = true;
+        for (int i = 0; i < ntiles && ok; ++i) {
+            const int tile = static_cast<int>(blockIdx.x) + i * static_cast<int>(gridDim.x);
+            for (int l = 0; l < 4 && ok; ++l) {
+                const int b = l & 1;
+                const int u = 2 * i + (l >> 1);
+                ok = __all_sync(0xffffffffu, fwait(smem_u32(&acc_full[b]), static_cast<uint32_t>(u & 1), &abort_flag));
+                if (!ok) break;
+                asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+                const uint32_t tl = tmem + (static_cast<uint32_t>(q * 32) << 16) + static_cast<uint32_t>(b * 256);
+                if (l < 3) {
+                    const float4* bias4 = reinterpret_cast<const float4*>(sBias + l * 256);
+                    uint32_t r[2][16];
+                    tmem_ld16(tl + static_cast<uint32_t>(h * 16), r[0]);
+                    tmem_wait16(r[0]);
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) {
+                        // the next block's load is in flight while this one is processed
+                        if (j < 3) tmem_ld16(tl + static_cast<uint32_t>((j + 1) * 64 + h * 16), r[(j + 1) & 1]);
+                        const uint32_t* v = r[j & 1];
+                        const int c0 = j * 64 + h * 16;
+                        uint32_t w8[8];
+#pragma unroll
+                        for (int p = 0; p < 4; ++p) {
+                            const float4 bb = bias4[(c0 >> 2) + p];
+                            const uint64_t v01 = add2(f2(__uint_as_float(v[4 * p]), __uint_as_float(v[4 * p + 1])), f2(bb.x, bb.y));
+                            const uint64_t v23 = add2(f2(__uint_as_float(v[4 * p + 2]), __uint_as_float(v[4 * p + 3])), f2(bb.z, bb.w));
+                            w8[2 * p] = gelu_t2_bf16(v01);
+                            w8[2 * p + 1] = gelu_t2_bf16(v23);
+                        }
+                        const uint32_t blk = sAct + j * F_TILE;
+                        asm volatile("st.shared.v4.b32 [%0], {%1, %2, %3, %4};\n"
+                                     :: "r"(blk + kmajor_off(row, h * 16)), "r"(w8[0]), "r"(w8[1]), "r"(w8[2]), "r"(w8[3]) : "memory");
+                        asm volatile("st.shared.v4.b32 [%0], {%1, %2, %3, %4};\n"
+                                     :: "r"(blk + kmajor_off(row, h * 16 + 8)), "r"(w8[4]), "r"(w8[5]), "r"(w8[6]), "r"(w8[7]) : "memory");
+                        // block j of the activation tile is written: visible to the tensor cores, then announced
+                        asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+                        __syncwarp();
+                        if (lane == 0) mbar_arrive(smem_u32(&act_full[j]));
+                        if (j < 3) tmem_wait16(r[(j + 1) & 1]);
+                    }
+                } else {
+                    uint32_t r[4];
+                    asm volatile("tcgen05.ld.sync.aligned.32x32b.x4.b32 {%0,%1,%2,%3}, [%4];\n"
+                                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]) : "r"(tl + static_cast<uint32_t>(h * 4)));
+                    asm volatile("tcgen05.wait::ld.sync.aligned;\n" : "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3]) :: "memory");
+                    const int grow = tile * BM + row;
+                    if (grow < a.B) {
+                        const float4 bb = reinterpret_cast<const float4*>(sBias + 768)[h];
+                        reinterpret_cast<float4*>(a.out + static_cast<size_t>(grow) * 16)[h] =
+                            make_float4(__fadd_rn(__uint_as_float(r[0]), bb.x), __fadd_rn(__uint_as_float(r[1]), bb.y),
+                                        __fadd_rn(__uint_as_float(r[2]), bb.z), __fadd_rn(__uint_as_float(r[3]), bb.w));
+                    }
+                }
+                // the accumulator is drained: the MMAs of its next use may overwrite it
+                asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+                __syncwarp();
+                if (lane == 0) mbar_arrive(smem_u32(&acc_empty[b]));
+            }
+        }
+    }
+    __syncwarp();
+    __syncthreads();
+    // drain after an abort (nothing is outstanding on the normal path): the producer's copies in flight land, the
+    // MMA thread's last commit completes, before the shared memory and the accumulator are released
+    if (warp == 0 && lane == 0) {
+        for (int g = consumed_chunks; g < issued_chunks; ++g) {
+            int dummy = 0;
+            fwait(smem_u32(&w_full[g % F_STAGES]), static_cast<uint32_t>((g / F_STAGES) & 1), reinterpret_cast<volatile int*>(&dummy));
+        }
+        for (int t = consumed_x; t < issued_x; ++t) {
+            int dummy = 0;
+            fwait(smem_u32(&x_full[t & 1]), static_cast<uint32_t>((t >> 1) & 1), reinterpret_cast<volatile int*>(&dummy));
+        }
+    }
+    if (warp == 1 && lane == 0 && last_commit >= 0) {
+        int dummy = 0;
+        fwait(smem_u32(&w_empty[last_commit % F_STAGES]), static_cast<uint32_t>((last_commit / F_STAGES) & 1),
+              reinterpret_cast<volatile int*>(&dummy));
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+    __syncwarp();
+    __syncthreads();
+    if (warp == 0) {
+        asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" :: "r"(tmem), "r"(512) : "memory");
+    }
+}
+
+// Packs a row-major BF16 matrix (rows x cols, leading dimension ld) into tiles of `R` rows x 64 columns in the
+// canonical K-major no-swizzle layout the MMAs read (zero padded to whole tiles): tile (rt, kb) is contiguous at
+// (rt * nkb + kb) * R * 128 bytes. One thread per 16-byte chunk of the output.
+__global__ void pack_kmajor(const __nv_bfloat16* __restrict__ src, int rows, int cols, int ld, int R, int nrt, int nkb,
+                            __nv_bfloat16* __restrict__ dst) {
+    const int64_t idx = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    const int64_t per_tile = static_cast<int64_t>(R) * 8;
+    if (idx >= per_tile * nrt * nkb) return;
+    const int64_t t = idx / per_tile;
+    const int cc = static_cast<int>(idx % per_tile);
+    const int rt = static_cast<int>(t / nkb), kb = static_cast<int>(t % nkb);
+    const int r = rt * R + (cc >> 6) * 8 + (cc & 7), k0 = kb * 64 + ((cc >> 3) & 7) * 8;
+    __nv_bfloat16 v[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j)
+        v[j] = (r < rows && k0 + j < cols) ? src[static_cast<size_t>(r) * ld + k0 + j] : __float2bfloat16(0.f);
+    uint4 w;
+    memcpy(&w, v, 16);
+    reinterpret_cast<uint4*>(dst)[idx] = w;
 }
 
 // ---- elementwise kernels ---------------------------------------------------------------------------------------------
@@ -315,15 +762,12 @@ __global__ void transpose_bf16(const __nv_bfloat16* __restrict__ src, int rows, 
     }
 }
 
-// dH = dY * GELU'(pre) (erf form), written in BF16 for the next GEMMs and FP32 for the bias gradient.
+// dH = dY * GELU'(pre), written in BF16 for the next GEMMs and FP32 for the bias gradient.
 __global__ void gelu_backward(const float* __restrict__ dY, const float* __restrict__ pre, int64_t n,
                               __nv_bfloat16* __restrict__ dHb, float* __restrict__ dH32) {
     const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    const float x = pre[i];
-    const float cdf = 0.5f * (1.0f + erff(x * 0.70710678118654752f));
-    const float pdf = 0.39894228040143268f * __expf(-0.5f * x * x);
-    const float g = dY[i] * (cdf + x * pdf);
+    const float g = __fmul_rn(dY[i], gelu_t_grad(pre[i]));
     if (dHb) dHb[i] = __float2bfloat16(g);
     if (dH32) dH32[i] = g;
 }
@@ -482,6 +926,80 @@ int cl_b200_gemm_bf16(const void* A, int32_t lda, const void* B, int32_t ldb, in
     else e = launch_gemm<256>(A, lda, B, ldb, M, N, K, bias, epilogue, C32, Cbf16, ldc, pre, accumulate, splits, st);
     capi_count_launch();
     return e == cudaSuccess ? 0 : capi_map_cuda(e, "gemm launch");
+}
+
+// The input's tensor map: X (B x 64 BF16, rows of 128 bytes) as a 2D tensor, boxes of 8 columns x 128 rows, no
+// swizzle, zero fill past row B. cuTensorMapEncodeTiled is the driver's; it is reached through the runtime's entry
+// point query so the library links against the runtime alone.
+static int encode_x_map(CUtensorMap* m, const void* X, int32_t B) {
+    using Encode = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+    static Encode enc = nullptr;
+    if (!enc) {
+        void* fn = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        const cudaError_t e = cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q);
+        if (e != cudaSuccess || q != cudaDriverEntryPointSuccess || !fn)
+            return cl::capi_fail(CL_EUNSUPPORTED, "fused forward: cuTensorMapEncodeTiled unavailable");
+        enc = reinterpret_cast<Encode>(fn);
+    }
+    const cuuint64_t dims[2] = {64, static_cast<cuuint64_t>(B)};
+    const cuuint64_t strides[1] = {128};
+    const cuuint32_t box[2] = {8, 128};
+    const cuuint32_t estr[2] = {1, 1};
+    const CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(X), dims, strides, box, estr,
+                           CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_NONE,
+                           CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return cl::capi_fail(CL_EINVAL, "fused forward: input tensor map rejected");
+    return 0;
+}
+
+int cl_b200_mlp_pack_kmajor(const void* src, int32_t rows, int32_t cols, int32_t ld, int32_t tile_rows, void* dst,
+                            void* stream) {
+    if (!src || !dst || rows <= 0 || cols <= 0 || ld < cols || tile_rows <= 0 || (tile_rows % 8) != 0)
+        return capi_fail(CL_EINVAL, "pack: bad arguments (tile_rows a positive multiple of 8)");
+    if (reinterpret_cast<uintptr_t>(dst) % 16) return capi_fail(CL_EINVAL, "pack: dst needs 16-byte alignment");
+    const int nrt = (rows + tile_rows - 1) / tile_rows, nkb = (cols + 63) / 64;
+    const int64_t n = static_cast<int64_t>(tile_rows) * 8 * nrt * nkb;
+    pack_kmajor<<<static_cast<unsigned>((n + 255) / 256), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+        static_cast<const __nv_bfloat16*>(src), rows, cols, ld, tile_rows, nrt, nkb, static_cast<__nv_bfloat16*>(dst));
+    capi_count_launch();
+    const cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? 0 : capi_map_cuda(e, "pack launch");
+}
+
+int cl_b200_mlp_forward_fused(const void* X, int32_t B, const void* Wp1, const void* Wp2, const void* Wp3,
+                              const void* Wp4, const float* b1, const float* b2, const float* b3, const float* b4,
+                              float* out, int32_t max_ctas, void* stream) {
+    if (!X || !Wp1 || !Wp2 || !Wp3 || !Wp4 || !b1 || !b2 || !b3 || !b4 || !out || B <= 0 || max_ctas < 0)
+        return capi_fail(CL_EINVAL, "fused forward: bad arguments");
+    const void* ps[6] = {X, Wp1, Wp2, Wp3, Wp4, out};
+    for (const void* p : ps)
+        if (reinterpret_cast<uintptr_t>(p) % 16) return capi_fail(CL_EINVAL, "fused forward: X, the packed weights and out need 16-byte alignment");
+    int dev = 0, sms = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(mlp_forward_fused, cudaFuncAttributeMaxDynamicSharedMemorySize, F_SMEM);
+    if (e != cudaSuccess) return capi_map_cuda(e, "fused forward setup");
+    FusedArgs a;
+    a.X = static_cast<const __nv_bfloat16*>(X);
+    a.Wp[0] = static_cast<const uint8_t*>(Wp1);
+    a.Wp[1] = static_cast<const uint8_t*>(Wp2);
+    a.Wp[2] = static_cast<const uint8_t*>(Wp3);
+    a.Wp[3] = static_cast<const uint8_t*>(Wp4);
+    a.bias[0] = b1; a.bias[1] = b2; a.bias[2] = b3; a.bias[3] = b4;
+    a.out = out;
+    a.B = B;
+    a.tiles = (B + BM - 1) / BM;
+    int grid = a.tiles < sms ? a.tiles : sms;
+    if (max_ctas > 0 && grid > max_ctas) grid = max_ctas;
+    CUtensorMap xmap;
+    if (int rc = encode_x_map(&xmap, X, B)) return rc;
+    mlp_forward_fused<<<static_cast<unsigned>(grid), F_THREADS, F_SMEM, static_cast<cudaStream_t>(stream)>>>(a, xmap);
+    capi_count_launch();
+    e = cudaGetLastError();
+    return e == cudaSuccess ? 0 : capi_map_cuda(e, "fused forward launch");
 }
 
 int cl_b200_mlp_status(void) {

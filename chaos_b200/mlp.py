@@ -1,8 +1,9 @@
 """The learned screen's network: a BF16 MLP (FP32 accumulation) trained and run by this library's own tensor-core
 kernels (`cl_b200_gemm_bf16`: tcgen05.mma with a tensor-memory accumulator) and elementwise kernels (cl_mlp.cu).
 
-64 inputs -> 256 -> 256 -> 256 (GELU) -> 2 outputs: the logit of P(chaotic) and a prediction of the final
-lambda_1. No reference counterpart: the reference has no learned component. PyTorch only holds the device buffers
+64 inputs -> 256 -> 256 -> 256 (GELU, tanh form) -> 2 outputs: the logit of P(chaotic) and a prediction of the
+final lambda_1. Inference runs the whole network in one persistent tensor-core kernel (`cl_b200_mlp_forward_fused`)
+on weights packed once into the MMA layout; training runs it layer by layer, keeping the pre-activations. No reference counterpart: the reference has no learned component. PyTorch only holds the device buffers
 and the stream; every arithmetic step runs in the library's kernels.
 
 Training is mean binary cross-entropy on the label plus `w_reg` times the mean squared error on lambda_1, with Adam
@@ -41,7 +42,9 @@ def _declare(L):
     L.cl_b200_to_bf16.argtypes = [f32p, C.c_int64, vp, vp]
     L.cl_b200_screen_features.argtypes = [vp, C.c_int64, C.c_int64, C.c_int32, C.c_int32, f32p, vp, vp]
     L.cl_b200_mlp_status.argtypes = []
-    for nm in ("cl_b200_gemm_bf16", "cl_b200_transpose_bf16", "cl_b200_gelu_backward", "cl_b200_col_sum",
+    L.cl_b200_mlp_pack_kmajor.argtypes = [vp, C.c_int32, C.c_int32, C.c_int32, C.c_int32, vp, vp]
+    L.cl_b200_mlp_forward_fused.argtypes = [vp, C.c_int32, vp, vp, vp, vp, f32p, f32p, f32p, f32p, f32p, C.c_int32, vp]
+    for nm in ("cl_b200_mlp_pack_kmajor", "cl_b200_mlp_forward_fused", "cl_b200_gemm_bf16", "cl_b200_transpose_bf16", "cl_b200_gelu_backward", "cl_b200_col_sum",
                "cl_b200_head_loss", "cl_b200_adam", "cl_b200_to_bf16", "cl_b200_screen_features",
                "cl_b200_mlp_status"):
         getattr(L, nm).restype = C.c_int
@@ -95,6 +98,36 @@ class MLP:
 
     def stream(self):
         return self.t.cuda.current_stream(self.dev).cuda_stream
+
+    def packed(self):
+        """The BF16 weights packed into the tensor cores' K-major tiles (rows = each layer's output rows), made once
+        per weight update."""
+        if getattr(self, "_packed", None) is not None and self._packed[0] == self.step:
+            return self._packed[1]
+        L, t = _declare(lib()), self.t
+        out = []
+        for lay in self.layers:
+            r, c = lay["Wb"].shape
+            buf = t.empty(r * ((c + 63) // 64) * 64, dtype=t.bfloat16, device=self.dev)
+            _ck(L.cl_b200_mlp_pack_kmajor(lay["Wb"].data_ptr(), r, c, c, r, buf.data_ptr(), self.stream()), "pack")
+            out.append(buf)
+        self._packed = (self.step, out)
+        return out
+
+    def forward_fused(self, Xb, out=None, max_ctas: int = 0):
+        """Inference: Xb (B, 64) BF16 contiguous -> FP32 outputs (B, 16) in one kernel, bit for bit `forward`."""
+        if self.dims != DIMS:
+            raise ValueError("the fused pass is built for the screen network's shape 64-256-256-256-16")
+        t, L = self.t, _declare(lib())
+        Xb = Xb.contiguous()
+        B = Xb.shape[0]
+        if out is None:
+            out = t.empty((B, OUT_PAD), dtype=t.float32, device=self.dev)
+        P = self.packed()
+        b = [lay["b"] for lay in self.layers]
+        _ck(L.cl_b200_mlp_forward_fused(Xb.data_ptr(), B, *[p.data_ptr() for p in P], *[x.data_ptr() for x in b],
+                                        out.data_ptr(), int(max_ctas), self.stream()), "fused forward")
+        return out
 
     def weights_numpy(self):
         return [(l["W"].cpu().numpy().copy(), l["b"].cpu().numpy().copy()) for l in self.layers]
@@ -180,13 +213,7 @@ class MLP:
         self.adam(lr=lr)
         return rl
 
-    def predict(self, Xb, batch=65536):
-        """Outputs (n, 16) FP32 for every row of Xb in batches: column 0 the chaos logit (P = sigmoid), column 1
-        the lambda_1 prediction."""
-        t = self.t
-        n = Xb.shape[0]
-        out = t.empty((n, OUT_PAD), dtype=t.float32, device=self.dev)
-        for lo in range(0, n, batch):
-            hi = min(n, lo + batch)
-            out[lo:hi] = self.forward(Xb[lo:hi])
-        return out
+    def predict(self, Xb):
+        """Outputs (n, 16) FP32 for every row of Xb: column 0 the chaos logit (P = sigmoid), column 1 the lambda_1
+        prediction. One fused launch over all rows."""
+        return self.forward_fused(Xb)

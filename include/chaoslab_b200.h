@@ -436,12 +436,27 @@ CL_API int cl_b200_indicator_pair(const cl_run* run, int64_t n, int32_t ns, doub
  * All enqueue on `stream` and take device pointers. BF16 matrices are row-major with 16-byte aligned rows. */
 
 /* C[M x N] = A[M x K] . B[N x K]^T on the tcgen05 tensor cores (BF16 operands, FP32 accumulator in tensor memory),
- * + bias[N] (NULL: none), epilogue 0 none / 1 GELU (erf form); C32 (FP32) and/or Cbf16 written with row stride ldc;
+ * + bias[N] (NULL: none), epilogue 0 none / 1 GELU (tanh form, x / (1 + 2^z) with z = -2 log2(e) sqrt(2/pi)
+ * (x + 0.044715 x^3)); C32 (FP32) and/or Cbf16 written with row stride ldc;
  * pre (FP32, NULL: none) receives the value before the epilogue; accumulate adds the old C32. */
 CL_API int cl_b200_gemm_bf16(const void* A, int32_t lda, const void* B, int32_t ldb, int32_t M, int32_t N, int32_t K,
                              const float* bias, int32_t epilogue, float* C32, void* Cbf16, int32_t ldc, float* pre,
                              int32_t accumulate, void* stream);
-/* 0, or CL_EDEVICE_LOST after a GEMM's bounded wait on its MMA barrier gave up. */
+/* Packs a row-major BF16 matrix (rows x cols, row stride ld elements) into tiles of tile_rows (a multiple of 8) x 64
+ * columns in the canonical K-major layout the tensor cores read, zero padded to whole tiles: tile (rt, kb) is
+ * contiguous at byte (rt * ceil(cols / 64) + kb) * tile_rows * 128. dst holds ceil(rows / tile_rows) * tile_rows *
+ * ceil(cols / 64) * 64 elements, 16-byte aligned. The fused forward pass reads its weights in this layout (tile_rows =
+ * the layer's output rows: 256, 256, 256, 16). */
+CL_API int cl_b200_mlp_pack_kmajor(const void* src, int32_t rows, int32_t cols, int32_t ld, int32_t tile_rows,
+                                   void* dst, void* stream);
+/* The screen network's inference pass, 64 -> 256 -> 256 -> 256 (GELU) -> 16 (linear), in one persistent kernel:
+ * X (B x 64 BF16, contiguous), Wp1..Wp4 the packed weights (256 x 64, 256 x 256, 256 x 256, 16 x 256), b1..b4 the
+ * biases (FP32), out (B x 16 FP32). Bit for bit the per-layer cl_b200_gemm_bf16 chain. max_ctas > 0 caps the grid
+ * (default: one CTA per SM). Pointers 16-byte aligned. */
+CL_API int cl_b200_mlp_forward_fused(const void* X, int32_t B, const void* Wp1, const void* Wp2, const void* Wp3,
+                                     const void* Wp4, const float* b1, const float* b2, const float* b3,
+                                     const float* b4, float* out, int32_t max_ctas, void* stream);
+/* 0, or CL_EDEVICE_LOST after a bounded wait on an MMA or copy barrier (GEMM or fused pass) gave up. */
 CL_API int cl_b200_mlp_status(void);
 CL_API int cl_b200_transpose_bf16(const void* src, int32_t rows, int32_t cols, int32_t lds, void* dst, int32_t ldd,
                                   void* stream);

@@ -9,7 +9,6 @@ from __future__ import annotations
 import math
 
 import numpy as np
-from scipy.special import erf
 
 
 def bf16_round(x):
@@ -20,12 +19,23 @@ def bf16_round(x):
     return r.astype(np.uint32).view(np.float32).astype(np.float64)
 
 
+_K = math.sqrt(2.0 / math.pi)
+
+
 def gelu(x):
-    return 0.5 * x * (1.0 + erf(x / math.sqrt(2.0)))
+    """GELU, tanh form (Hendrycks & Gimpel 2016): x (1 + tanh u) / 2 = x / (1 + exp(-2u)),
+    u = sqrt(2/pi) (x + 0.044715 x^3)."""
+    x = np.asarray(x, dtype=np.float64)
+    with np.errstate(over="ignore"):
+        return x / (1.0 + np.exp(-2.0 * _K * (x + 0.044715 * x ** 3)))
 
 
 def gelu_grad(x):
-    return 0.5 * (1.0 + erf(x / math.sqrt(2.0))) + x * np.exp(-0.5 * x * x) / math.sqrt(2 * math.pi)
+    """d gelu / dx = s + x s (1 - s) 2 sqrt(2/pi) (1 + 3 0.044715 x^2), s = 1 / (1 + exp(-2u))."""
+    x = np.asarray(x, dtype=np.float64)
+    with np.errstate(over="ignore"):
+        sg = 1.0 / (1.0 + np.exp(-2.0 * _K * (x + 0.044715 * x ** 3)))
+    return sg + x * sg * (1.0 - sg) * 2.0 * _K * (1.0 + 3.0 * 0.044715 * x * x)
 
 
 def forward(weights, X):
