@@ -133,7 +133,10 @@ class Screen:
         ok = code == 0
         return fb[self.t.tensor(np.flatnonzero(ok), device=self.dev)], label[ok], lam[ok].astype(np.float32)
 
-    def train(self, X, label, lam, epochs=8, batch=4096, lr=2e-3, w_reg=1.0, seed=0, val_frac=0.1):
+    def train(self, X, label, lam, epochs=8, batch=4096, lr=2e-3, w_reg=1.0, seed=0, val_frac=0.1,
+              balance: bool = True):
+        """Train the network on (features, label, lambda_1). With balance, every epoch draws its rows with
+        replacement so that both classes are equally likely (the coupled-maps ensemble is ~98 % chaotic)."""
         t = self.t
         n = X.shape[0]
         rng = np.random.default_rng(seed)
@@ -144,8 +147,13 @@ class Screen:
         lt = t.tensor(label, device=self.dev)
         tt = t.tensor(lam, device=self.dev)
         hist = []
+        if balance and len(ti):
+            pos = label[ti] > 0.5
+            fp = max(pos.mean(), 1e-12)
+            w = np.where(pos, 0.5 / fp, 0.5 / max(1.0 - fp, 1e-12))
+            w = w / w.sum()
         for ep in range(epochs):
-            order = rng.permutation(ti)
+            order = rng.choice(ti, size=len(ti), replace=True, p=w) if balance and len(ti) else rng.permutation(ti)
             for lo in range(0, len(order) - batch + 1, batch):
                 idx = t.tensor(order[lo:lo + batch], device=self.dev)
                 rl = net.train_step(X.index_select(0, idx), lt.index_select(0, idx), tt.index_select(0, idx),
@@ -155,7 +163,7 @@ class Screen:
         acc = float(((out[:, 0] > 0) == (label[vi] > 0.5)).mean()) if nv else float("nan")
         return net, dict(loss=hist, val_accuracy=acc, n_train=len(ti), n_val=nv)
 
-    def screen_grid(self, net, G: int, N: int = N_FULL, lo=0.05, hi=0.95, audit=0.05, seed=3):
+    def screen_grid(self, net, G: int, N: int = N_FULL, lo=0.01, hi=0.99, audit=0.05, seed=3):
         """Classify a G x G grid of (x1, p1) starts in [0, 2 pi)^2 with x2 = p2 = 0.1: features for all, full
         integration for the uncertain ones (lo < P < hi) and a random audit fraction of the rest."""
         t = self.t
