@@ -400,6 +400,8 @@ int cl_b200_propagate_device(const cl_run* run, int64_t n_orbits, const cl_buffe
     return 0;
 }
 
+constexpr int kMaxVariant = 8;   // variants 1..8 (bit v - 1 of an instance's mask)
+
 // The register budget of a run whose key the tuner has not seen: the compiled variants timed once on a sample of
 // the run's own start data (the first min(n, 65536) orbits, 20 handoffs), written into scratch outputs so the inputs
 // stay untouched, and the fastest kept for the key. Short runs (where the sample would cost more than ~2 % of the
@@ -408,7 +410,7 @@ static int auto_minb(const cl_run& run, const Instance* in, int64_t n, double* d
     const int have = tuned_minb(run);
     if (have) return have;
     int variants = 0;
-    for (int m = 1; m <= 4; ++m) variants += (in->minb_mask >> (m - 1)) & 1u;
+    for (int m = 1; m <= kMaxVariant; ++m) variants += (in->minb_mask >> (m - 1)) & 1u;
     const int64_t ns = std::min<int64_t>(n, 65536);
     const int64_t sample = 20 * static_cast<int64_t>(run.tau);
     const double run_work = static_cast<double>(n) * static_cast<double>(run.N - run.n0);
@@ -605,7 +607,7 @@ int cl_b200_tune(const cl_run* run, int64_t n_orbits, const cl_buffers* dev, int
     int best = 1;
     float best_ms = 1e30f;
     int rc = 0;
-    for (int m = 1; m <= 4 && rc == 0; ++m) {
+    for (int m = 1; m <= kMaxVariant && rc == 0; ++m) {
         if (!(in->minb_mask & (1u << (m - 1)))) continue;
         float ms = 0.f;
         for (int rep = 0; rep < 2; ++rep) {   // the first run warms up
@@ -638,7 +640,7 @@ int cl_b200_set_variant(const cl_run* run, int32_t variant) {
     if (v) return v;
     const Instance* in = lookup(*run);
     if (!in) return CL_EUNSUPPORTED;
-    if (variant != 0 && !(variant >= 1 && variant <= 4 && (in->minb_mask >> (variant - 1)) & 1u))
+    if (variant != 0 && !(variant >= 1 && variant <= kMaxVariant && (in->minb_mask >> (variant - 1)) & 1u))
         return fail(CL_EINVAL, "variant not compiled for this instance");
     set_tuned_minb(*run, variant);
     return 0;
