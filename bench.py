@@ -184,7 +184,7 @@ def main() -> None:
     ap.add_argument("--orbits", type=int, default=None, help="orbits per GPU (default: the workload's own)")
     ap.add_argument("--N", type=int, default=N_STEPS)
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
-    ap.add_argument("--only", choices=["fp64", "mixed"], default=None,
+    ap.add_argument("--only", choices=["fp64", "mixed", "mixed-ind64"], default=None,
                     help="time one kernel of the default workload and print a short line (a small case for ncu)")
     ap.add_argument("--workload", default="coupled", choices=["coupled", "standard", "gauss", "lattice", "screen", "mlp", "split", "shadow",
                                                              "record", "indicators", "advance", "torus", "record_mixed"])
