@@ -63,7 +63,7 @@ MU = 0.05
 SEED = 1
 # DRAM bytes per orbit of one launch of the mixed kernel (ncu capture of 32768 orbits: 5.376 MB read, 4.6 KB
 # written; the records written stay in the 126 MB L2 at that size)
-TRAFFIC_PER_ORBIT = (5.376256e6 + 4.608e3) / 32768
+TRAFFIC_PER_ORBIT = 16474112 / 65536   # ncu DRAM read + write of split_frames_kernel, 65536 orbits x 2000 steps
 METRIC = "orbit-steps/s (4D coupled standard maps, QRSpectrum(Householder) + GALI_4 + SALI, mixed-precision kernel)"
 # the headline kernel: Float64 orbit and GALI / SALI frame, Float32 QRSpectrum frame (the precision every output holds)
 HEADLINE = "mixed-ind64"
@@ -409,9 +409,9 @@ def main() -> None:
                      calls=len(te), statistic="median call", mean_call_value=e2e_mean_value),
             roofline=dict(bound="fp64", achieved=achieved, peak=fp64_peak, unit="TFLOP/s", frac=achieved / fp64_peak,
                           traffic=TRAFFIC_PER_ORBIT * n,
-                          traffic_source="ncu dram__bytes_read + dram__bytes_write of the mixed kernel on 32768 orbits "
-                                         "x 2000 steps (5.38e6 B), scaled by orbits: DRAM bytes grow with the orbits "
-                                         "loaded and stored, not with the steps",
+                          traffic_source="ncu dram__bytes_read + dram__bytes_write of split_frames_kernel on 65536 "
+                                         "orbits x 2000 steps (1.647e7 B), scaled by orbits: DRAM bytes grow with the "
+                                         "orbits loaded and stored, not with the steps",
                           peak_source="cuBLAS DGEMM 8192^3 measured here (burst)",
                           flops_per_orbit_step=fl),
             cpu_baseline=cpu, clocks=clocks, gpu_launches=int(launches),
