@@ -700,7 +700,7 @@ def workload_screen(args):
     _line("screened orbits/s (learned BF16 MLP screen, 4D coupled-map grid, label final MEGNO > 2.2)", value,
           "orbits/s", args, [res["seconds"] * 1e3],
           dict(workload=f"screen-froeschle-grid{G}x{G}-N1e5", grid=G, N=N_FULL, feature_steps=FEATURE_STEPS,
-               training_orbits=n_train, audit=0.05, band=[0.01, 0.99], balanced_training=True),
+               training_orbits=n_train, audit=0.05, band=[0.05, 0.95], regular_fraction_in_training_draws=0.1),
           dtype="bf16 mlp (f32 accumulate) + f64/f32 orbits", e2e=dict(value=value, unit="orbits/s",
                                                                        h2d_bytes_per_step=int(res["n"] * 32),
                                                                        d2h_bytes_per_step=int(res["n"] * 64)),
