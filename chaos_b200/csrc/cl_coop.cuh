@@ -85,8 +85,9 @@ struct CoopQR {
     int8_t code;
 };
 
-// One lane's lattice site: its coordinates and its two rows of the frame, and the step of the chain on them.
-template <int NS, typename Real, int K>
+// One lane's lattice site: its coordinates and its two rows of the frame, and the step of the chain on them. The
+// group has G >= NS lanes (shuffle width G); lanes past the lattice (j >= NS) step a dummy site with no bonds.
+template <int NS, typename Real, int K, int G = NS>
 struct CoopSite {
     double q, p;
     Real Wq[K], Wp[K];
@@ -96,7 +97,6 @@ struct CoopSite {
     // neighbours' rows by shuffles. forward (standard_map_chain.jl:38-44): p' = p + (K sin q + eps s), s = (0 +
     // sin(q_j - q_left)) + sin(q_j - q_right); q' = q + p'.
     __device__ __forceinline__ void step(unsigned gm, int jl, int jr, bool hasL, bool hasR, double Kc, double eps) {
-        constexpr int G = NS;
         const double qr_ = __shfl_sync(gm, q, jr, G);
         double sb = 0.0, sq;
         Real g, gl, gr;

@@ -178,13 +178,24 @@ namespace {{
 """
 
 
+def coop(kind, d, frames):
+    """Lattices with d >= 8 and one frame run `propagate` cooperatively (cl_coop_orbit.cuh) by default."""
+    return kind == SYS_CHAIN and d >= 8 and len(frames) == 1
+
+
 def render(group, entries):
     extra = ('#include "cl_gauss.cuh"\n' if any(e[0] == SYS_HH for e in entries) else "") + \
-            ('#include "cl_split.cuh"\n' if any(e[0] == SYS_SPLIT for e in entries) else "")
+            ('#include "cl_split.cuh"\n' if any(e[0] == SYS_SPLIT for e in entries) else "") + \
+            ('#include "cl_coop_orbit.cuh"\n' if any(coop(e[0], e[1], e[3]) for e in entries) else "")
     out = [HEADER.format(group=group, extra=extra)]
     for idx, (kind, d, prec, frames, minbs) in enumerate(entries):
         real = "double" if prec == 0 else "float"
         ftypes = [f"Frame<{k}{''.join(', ' + t for t in red_type(ch))}>" for k, ch in frames]
+        if coop(kind, d, frames):   # variant V_COOP (the default) and the one-thread kernel as variant 1
+            out.append(f"cudaError_t L{idx}(const cl_run& r, const KArgs& a, const double* A, cudaStream_t s, LaunchInfo* i, int m) {{\n"
+                       f"    return launch_chain_instance<{d // 2}, {real}, {ftypes[0]}>(r, a, A, s, i, m);\n}}\n"
+                       f"const Registrar R{idx}(\"{key(kind, d, prec, frames)}\", L{idx}, minb_mask<1>() | (1u << (V_COOP - 1)));\n")
+            continue
         while len(ftypes) < 3:
             ftypes.append("NoFrame")
         mb = ", ".join(str(m) for m in minbs)
