@@ -413,7 +413,11 @@ def main() -> None:
                                          "orbits x 2000 steps (1.647e7 B), scaled by orbits: DRAM bytes grow with the "
                                          "orbits loaded and stored, not with the steps",
                           peak_source="cuBLAS DGEMM 8192^3 measured here (burst)",
-                          flops_per_orbit_step=fl),
+                          flops_per_orbit_step=fl,
+                          pipes_ncu=dict(fp64=0.468, fma_fp32=0.130, alu=0.210, xu_sfu=0.162, issue_active=0.607,
+                                         warps_active=0.170,
+                                         source="ncu --set full of split_frames_kernel, 65536 orbits x 2000 steps "
+                                                "(profiles/split_frames_kernel_froeschle_65536x2000_ncu.md)")),
             cpu_baseline=cpu, clocks=clocks, gpu_launches=int(launches),
         )
         print(json.dumps(line), flush=True)
