@@ -84,33 +84,37 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t phase) {
 // The network's activation: GELU in its tanh form (Hendrycks & Gimpel 2016), x (1 + tanh u) / 2 with
 // u = sqrt(2 / pi) (x + 0.044715 x^3). Since (1 + tanh u) / 2 = 1 / (1 + e^(-2u)), it is evaluated without the
 // cancellation of 1 + tanh u for negative x as x s, s = 1 / (1 + 2^z), z = -2 log2(e) u = x (G0 + G1 x^2) clamped
-// to 64 (beyond it s < 6e-20): one ex2 on the special-function unit, and the reciprocal by three Newton steps
-// r <- r + r (1 - d r) on the FMA pipe from the seed bits(r0) = 0x7EF311C2 - bits(d), whose relative error is at
-// most 0.0505 for every normal d (the constant minimises it over all mantissas; found by exhaustive search). The
-// steps square the error (0.0505 -> 2.6e-3 -> 6.5e-6 -> 4e-11) so s is within about one unit in the last place. The
-// pair form runs the same operations lane by lane on packed FP32 pairs (fma/mul/add .f32x2), so the scalar form
-// (the per-layer epilogue) and the pair form (the fused pass) agree bit for bit.
+// to 64 (beyond it s < 6e-20): one ex2 on the special-function unit, and the reciprocal on the FMA pipe from the
+// seed bits(r0) = 0x7EF311C2 - bits(d), whose relative error is at most 0.0505 for every normal d (the constant
+// minimises it over all mantissas; found by exhaustive search), refined by one Newton step r <- r + r t (error
+// squared: 2.6e-3) and one third-order step r <- r + r (t + t^2) (error cubed: 1.7e-8), t = 1 - d r (run on -r,
+// below, which costs one multiply fewer a pair); s is within
+// 1.3 units in the last place (checked over 2e6 arguments). The pair form runs the same operations lane by lane on
+// packed FP32 pairs (fma/mul/add .f32x2), so the scalar form (the per-layer epilogue) and the pair form (the fused
+// pass) agree bit for bit.
 constexpr float kG0 = -2.3022082f;     // -2 log2(e) sqrt(2 / pi)
 constexpr float kG1 = -0.10294324f;    // kG0 * 0.044715
 constexpr float kLn2 = 0.6931472f;
 constexpr float kZMax = 64.0f;
-constexpr uint32_t kRcpSeed = 0x7EF311C2u;
+constexpr uint32_t kRcpSeedNeg = 0xFEF311C2u;   // 0x7EF311C2 with the sign bit: the seed of -1 / d
 __device__ __forceinline__ float ex2_approx(float z) {
     float e;
     asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(e) : "f"(z));
     return e;
 }
-// s = 1 / (1 + 2^z(x)) for one value.
-__device__ __forceinline__ float sig_t(float x) {
+// w = -1 / (1 + 2^z(x)) = -s for one value. The iteration runs on w ~ -1 / d so that its error term t = 1 + d w is
+// one fused multiply-add of d itself (no negated copy of d): w <- w + w t (Newton), then w <- w + w (t + t^2); each
+// operation is the exact negation of the same iteration on r ~ 1 / d, so -w is that iteration's s bit for bit.
+__device__ __forceinline__ float negsig_t(float x) {
     const float z = fminf(__fmul_rn(x, __fmaf_rn(kG1, __fmul_rn(x, x), kG0)), kZMax);
     const float d = __fadd_rn(1.0f, ex2_approx(z));
-    const float nd = __fmul_rn(d, -1.0f);
-    float r = __uint_as_float(kRcpSeed - __float_as_uint(d));
-#pragma unroll
-    for (int i = 0; i < 3; ++i) r = __fmaf_rn(r, __fmaf_rn(nd, r, 1.0f), r);
-    return r;
+    float w = __uint_as_float(kRcpSeedNeg - __float_as_uint(d));
+    w = __fmaf_rn(w, __fmaf_rn(d, w, 1.0f), w);
+    const float t = __fmaf_rn(d, w, 1.0f);
+    return __fmaf_rn(w, __fmaf_rn(t, t, t), w);
 }
-__device__ __forceinline__ float gelu_t(float x) { return __fmul_rn(x, sig_t(x)); }
+__device__ __forceinline__ float sig_t(float x) { return -negsig_t(x); }
+__device__ __forceinline__ float gelu_t(float x) { return -__fmul_rn(x, negsig_t(x)); }   // = x s exactly
 
 // Packed FP32 pairs (the .f32x2 forms; lane by lane the same IEEE operations as the scalar ones).
 __device__ __forceinline__ uint64_t f2(float a, float b) {
@@ -136,22 +140,23 @@ __device__ __forceinline__ uint64_t add2(uint64_t a, uint64_t b) {
     asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
     return d;
 }
-// gelu_t of both lanes of v, rounded to a BF16 pair (low half: lane 0).
+// gelu_t of both lanes of v, rounded to a BF16 pair (low half: lane 0): the pair form of negsig_t, then v w = -(v s)
+// rounded to BF16 and both signs flipped (rounding to nearest is symmetric, so the bits are those of v s).
 __device__ __forceinline__ uint32_t gelu_t2_bf16(uint64_t v) {
-    const uint64_t g1 = f2(kG1, kG1), g0 = f2(kG0, kG0), one = f2(1.0f, 1.0f), neg = f2(-1.0f, -1.0f);
+    const uint64_t g1 = f2(kG1, kG1), g0 = f2(kG0, kG0), one = f2(1.0f, 1.0f);
     float z0, z1;
     f2split(mul2(v, fma2(g1, mul2(v, v), g0)), z0, z1);
     const uint64_t d = add2(one, f2(ex2_approx(fminf(z0, kZMax)), ex2_approx(fminf(z1, kZMax))));
-    const uint64_t nd = mul2(d, neg);
     float d0, d1;
     f2split(d, d0, d1);
-    uint64_t r = f2(__uint_as_float(kRcpSeed - __float_as_uint(d0)), __uint_as_float(kRcpSeed - __float_as_uint(d1)));
-#pragma unroll
-    for (int i = 0; i < 3; ++i) r = fma2(r, fma2(nd, r, one), r);
+    uint64_t w = f2(__uint_as_float(kRcpSeedNeg - __float_as_uint(d0)), __uint_as_float(kRcpSeedNeg - __float_as_uint(d1)));
+    w = fma2(w, fma2(d, w, one), w);
+    const uint64_t t = fma2(d, w, one);
+    w = fma2(w, fma2(t, t, t), w);
     float y0, y1;
-    f2split(mul2(v, r), y0, y1);
+    f2split(mul2(v, w), y0, y1);
     const __nv_bfloat162 h = __floats2bfloat162_rn(y0, y1);
-    return *reinterpret_cast<const uint32_t*>(&h);
+    return *reinterpret_cast<const uint32_t*>(&h) ^ 0x80008000u;
 }
 // d/dx of gelu_t: s - x s (1 - s) ln2 (G0 + 3 G1 x^2).
 __device__ __forceinline__ float gelu_t_grad(float x) {
@@ -381,31 +386,31 @@ __global__ void __launch_bounds__(128, 1) gemm_bf16_tc(const __nv_bfloat16* __re
 
 // ---- the fused forward pass --------------------------------------------------------------------------------------
 // The screen network's whole inference pass (64 -> 256 -> 256 -> 256 -> 16) in one persistent kernel, one CTA of
-// eighteen warps per SM looping over 128-row tiles, the activations never leaving the SM:
-//   warp 0      producer: stages the next row tiles' inputs (plain loads -> the canonical K-major layout) and
-//               streams the weights through a 3-stage ring by bulk copies (cp.async.bulk, the untiled TMA) from their
-//               pre-packed layout (cl_b200_mlp_pack_kmajor), each stage's mbarrier counting the bytes in;
-//   warp 1      one thread issues the tcgen05.mma (M = 128, N = 256 / 16, K = 16 each) and commits them to the
-//               barriers that free a weight stage, an input slot or hand an accumulator to the epilogue;
+// eighteen warps per SM looping over 128-row tiles in pairs, the activations never leaving the SM. The two tiles of a
+// pair sit in two slots, each with its activation tile in shared memory (64 KB; the input tile is copied into its
+// last K block) and its 256-column FP32 accumulator in tensor memory (512 columns for both), and run ping-pong: the
+// tensor cores compute one slot's layer while the epilogue drains the other slot's accumulator.
+//   warp 0      producer: copies each tile's input by tensor-map TMA (eight 128-row x 8-column boxes landing as
+//               K-major core matrices) and streams the weights through a 3-stage ring by bulk copies (cp.async.bulk)
+//               from their pre-packed layout (cl_b200_mlp_pack_kmajor), each stage's mbarrier counting the bytes in;
+//   warp 1      one thread issues the tcgen05.mma (M = 128, N = 256 / 16, K = 16 each) in the order slot 0, slot 1
+//               per layer and commits them to the barriers that free a weight stage, a slot's input or hand an
+//               accumulator to the epilogue;
 //   warps 2..17 epilogue: read the accumulator (tcgen05.ld, the next 16 columns loading while the current ones are
-//               processed), add the bias, apply GELU (packed FP32 pairs), round to BF16 into the activation tile,
-//               64 columns at a time; the next layer's MMAs on K block j start as soon as the sixteen epilogue warps
-//               have written block j, so the epilogue overlaps the tensor cores.
-// Tensor memory holds two 128 x 256 FP32 accumulators (512 columns): layers 1 and 3 use the first, layers 2 and 4 the
-// second, so a layer's MMAs run while the previous layer's accumulator is being drained. The MMAs see the operands in
-// the same order as the per-layer GEMM (K ascending in steps of 16, accumulate from zero) and the epilogue is the same
-// arithmetic, so the outputs are bit for bit the per-layer path's. Every wait is bounded: a wait that gives up sets
-// the error flag and a shared abort flag that every role polls, all roles leave their loops, the MMA thread waits
-// for its last commit and the producer for its copies in flight, then the accumulator is released.
+//               processed), add the bias, apply GELU (packed FP32 pairs), round to BF16 into the slot's activation
+//               tile, then release the slot to its next layer's MMAs.
+// The MMAs see the operands in the same order as the per-layer GEMM (K ascending in steps of 16, accumulate from
+// zero) and the epilogue is the same arithmetic, so the outputs are bit for bit the per-layer path's. Every wait is
+// bounded: a wait that gives up sets the error flag and a shared abort flag that every role polls, all roles leave
+// their loops, the MMA thread waits for its last commit and the producer for its copies in flight, then the
+// accumulator is released.
 constexpr int F_STAGES = 3;
 constexpr int F_TILE = BM * BK * 2;                 // 16 KB: one 128 x 64 BF16 block (an input tile or activation block)
+constexpr int F_SLOT = 4 * F_TILE;                  // 64 KB: one slot's activation tile, 4 K blocks of 64
 constexpr int F_WCHUNK = 256 * BK * 2;              // 32 KB: one 256 x 64 weight block
-constexpr int F_OFF_X = 0;                          // 2 input slots
-constexpr int F_OFF_ACT = 2 * F_TILE;               // the activation tile: 4 K blocks of 64
-constexpr int F_OFF_W = F_OFF_ACT + 4 * F_TILE;     // the weight ring
-constexpr int F_OFF_BIAS = F_OFF_W + F_STAGES * F_WCHUNK;
-constexpr int F_NBIAS = 3 * 256 + 16;
-constexpr int F_SMEM = F_OFF_BIAS + F_NBIAS * 4;    // 199,744 bytes
+constexpr int F_OFF_ACT = 0;                        // two slots
+constexpr int F_OFF_W = F_OFF_ACT + 2 * F_SLOT;     // the weight ring
+constexpr int F_SMEM = F_OFF_W + F_STAGES * F_WCHUNK;   // 229,376 bytes
 constexpr int F_CHUNKS = 10;                        // per tile: W1 (1 block), W2 (4), W3 (4), W4 (its 4 blocks, 8 KB)
 constexpr int F_THREADS = 576;                     // 18 warps: producer, MMA, 16 epilogue
 constexpr int F_EPI_WARPS = 16;
@@ -484,23 +489,14 @@ __device__ __forceinline__ void tmem_wait16(uint32_t (&r)[16]) {
 __global__ void __launch_bounds__(F_THREADS, 1) mlp_forward_fused(const FusedArgs a, const __grid_constant__ CUtensorMap xmap) {
     extern __shared__ __align__(1024) uint8_t fsm[];
     __shared__ __align__(8) uint64_t w_full[F_STAGES], w_empty[F_STAGES], x_full[2], x_empty[2], acc_full[2],
-        acc_empty[2], act_full[4];
+        epi_done[2];
     __shared__ uint32_t tmem_base;
     __shared__ volatile int abort_flag;
     __shared__ int consumed_chunks, consumed_x;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const uint32_t sbase = smem_u32(fsm);
-    const uint32_t sX = sbase + F_OFF_X, sAct = sbase + F_OFF_ACT, sW = sbase + F_OFF_W;
-    float* sBias = reinterpret_cast<float*>(fsm + F_OFF_BIAS);
+    const uint32_t sAct = sbase + F_OFF_ACT, sW = sbase + F_OFF_W;
 
-    for (int i = tid; i < F_NBIAS; i += F_THREADS) {
-        float v;
-        if (i < 256) v = a.bias[0][i];
-        else if (i < 512) v = a.bias[1][i - 256];
-        else if (i < 768) v = a.bias[2][i - 512];
-        else v = a.bias[3][i - 768];
-        sBias[i] = v;
-    }
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n"
                      :: "r"(smem_u32(&tmem_base)), "r"(512) : "memory");
@@ -512,9 +508,8 @@ __global__ void __launch_bounds__(F_THREADS, 1) mlp_forward_fused(const FusedArg
         };
         for (int s = 0; s < F_STAGES; ++s) { init(&w_full[s], 1); init(&w_empty[s], 1); }
         for (int s = 0; s < 2; ++s) {
-            init(&x_full[s], 1); init(&x_empty[s], 1); init(&acc_full[s], 1); init(&acc_empty[s], F_EPI_WARPS);
+            init(&x_full[s], 1); init(&x_empty[s], 1); init(&acc_full[s], 1); init(&epi_done[s], F_EPI_WARPS);
         }
-        for (int j = 0; j < 4; ++j) init(&act_full[j], F_EPI_WARPS);
         asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
         abort_flag = 0;
         consumed_chunks = 0;
@@ -524,110 +519,111 @@ __global__ void __launch_bounds__(F_THREADS, 1) mlp_forward_fused(const FusedArg
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
     const uint32_t tmem = tmem_base;
+    // this CTA's tiles k = 0, 1, ... (tile blockIdx.x + k gridDim.x) run in pairs: tile k in slot k & 1
     const int ntiles = a.tiles > static_cast<int>(blockIdx.x) ? (a.tiles - 1 - static_cast<int>(blockIdx.x)) / static_cast<int>(gridDim.x) + 1 : 0;
+    const int npairs = (ntiles + 1) / 2;
     int issued_chunks = 0;        // producer: weight chunks whose copies were issued
     int issued_x = 0;             // producer: input tiles whose copies were issued
     int last_commit = -1;         // MMA thread: the last weight chunk whose MMAs were committed
 
     if (warp == 0) {
-        // ---------------------------------------------------------------- producer
+        // ---------------------------------------------------------------- producer (lane 0 issues)
         bool ok = true;
         int g = 0;
-        for (int i = 0; i < ntiles && ok; ++i) {
-            const int tile = static_cast<int>(blockIdx.x) + i * static_cast<int>(gridDim.x);
-            const int slot = i & 1;
-            // the 128 x 64 input tile: eight tensor copies of 128 rows x 8 columns, K group g landing at g * 2048
-            // bytes (8-row x 16-byte core matrices, K-adjacent 2048 B apart, 8-row groups 128 B apart); rows past B
-            // are zero filled
-            int xgood = 1;
-            if (lane == 0) {
-                xgood = fwait(smem_u32(&x_empty[slot]), static_cast<uint32_t>(((i >> 1) & 1) ^ 1), &abort_flag);
-                if (xgood) {
-                    const uint32_t bar = smem_u32(&x_full[slot]), dst = sX + slot * F_TILE;
-                    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" :: "r"(bar), "r"(F_TILE) : "memory");
+        for (int p = 0; p < npairs && ok; ++p)
+            for (int l = 0; l < 4 && ok; ++l)
+                for (int s = 0; s < 2 && ok; ++s) {
+                    const int k = 2 * p + s;
+                    if (k >= ntiles) continue;
+                    int good = 1;
+                    if (lane == 0) {
+                        if (l == 0) {
+                            // the 128 x 64 input tile into K block 3 of the slot's activation tile: eight tensor copies
+                            // of 128 rows x 8 columns, K group g at g * 2048 bytes; rows past B are zero filled
+                            good = fwait(smem_u32(&x_empty[s]), static_cast<uint32_t>((p & 1) ^ 1), &abort_flag);
+                            if (good) {
+                                const int tile = static_cast<int>(blockIdx.x) + k * static_cast<int>(gridDim.x);
+                                const uint32_t bar = smem_u32(&x_full[s]), dst = sAct + s * F_SLOT + 3 * F_TILE;
+                                asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" :: "r"(bar), "r"(F_TILE) : "memory");
 #pragma unroll
-                    for (int gk = 0; gk < 8; ++gk)
-                        asm volatile(
-                            "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];\n"
-                            :: "r"(dst + gk * 2048), "l"(reinterpret_cast<uint64_t>(&xmap)), "r"(gk * 8), "r"(tile * BM), "r"(bar)
-                            : "memory");
-                    ++issued_x;
-                }
-            }
-            ok = __shfl_sync(0xffffffffu, xgood, 0) != 0;
-            if (!ok) break;
-            for (int c = 0; c < F_CHUNKS; ++c, ++g) {
-                const int s = g % F_STAGES;
-                int good = 1;
-                if (lane == 0) {
-                    good = fwait(smem_u32(&w_empty[s]), static_cast<uint32_t>(((g / F_STAGES) & 1) ^ 1), &abort_flag);
-                    if (good) {
-                        const uint32_t bytes = fchunk_bytes(c), bar = smem_u32(&w_full[s]);
-                        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" :: "r"(bar), "r"(bytes) : "memory");
-                        asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n"
-                                     :: "r"(sW + s * F_WCHUNK), "l"(fchunk_src(a, c)), "r"(bytes), "r"(bar) : "memory");
-                        ++issued_chunks;
+                                for (int gk = 0; gk < 8; ++gk)
+                                    asm volatile(
+                                        "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];\n"
+                                        :: "r"(dst + gk * 2048), "l"(reinterpret_cast<uint64_t>(&xmap)), "r"(gk * 8), "r"(tile * BM), "r"(bar)
+                                        : "memory");
+                                ++issued_x;
+                            }
+                        }
+                        const int c_lo = l == 0 ? 0 : l == 1 ? 1 : l == 2 ? 5 : 9, c_hi = l == 0 ? 1 : l == 1 ? 5 : l == 2 ? 9 : 10;
+                        for (int c = c_lo; c < c_hi && good; ++c, ++g) {
+                            const int sw = g % F_STAGES;
+                            good = fwait(smem_u32(&w_empty[sw]), static_cast<uint32_t>(((g / F_STAGES) & 1) ^ 1), &abort_flag);
+                            if (!good) break;
+                            const uint32_t bytes = fchunk_bytes(c), bar = smem_u32(&w_full[sw]);
+                            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" :: "r"(bar), "r"(bytes) : "memory");
+                            asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n"
+                                         :: "r"(sW + sw * F_WCHUNK), "l"(fchunk_src(a, c)), "r"(bytes), "r"(bar) : "memory");
+                            ++issued_chunks;
+                        }
                     }
+                    ok = __shfl_sync(0xffffffffu, good, 0) != 0;
                 }
-                ok = __shfl_sync(0xffffffffu, good, 0) != 0;
-                if (!ok) break;
-            }
-        }
     } else if (warp == 1) {
-        // ---------------------------------------------------------------- MMA issuer
+        // ---------------------------------------------------------------- MMA issuer (lane 0)
+        // Order: per pair, per layer, slot 0 then slot 1, so one slot's MMAs run while the epilogue drains the
+        // other slot's accumulator. A slot's layer l waits for its epilogue of layer l - 1 (the accumulator drained and
+        // the activation tile written: epi_done, completion 4u + l - 1 for its u-th tile).
         if (lane == 0) {
             constexpr uint32_t id256 = idesc_bf16(BM, 256), id16 = idesc_bf16(BM, 16);
             bool ok = true;
-            int g = 0;
-            for (int i = 0; i < ntiles && ok; ++i) {
-                const int slot = i & 1;
-                for (int l = 0; l < 4 && ok; ++l) {
-                    const int b = l & 1;
-                    const int u = 2 * i + (l >> 1);           // the use of accumulator b
-                    const uint32_t accum = tmem + static_cast<uint32_t>(b * 256);
-                    ok = fwait(smem_u32(&acc_empty[b]), static_cast<uint32_t>((u & 1) ^ 1), &abort_flag);
-                    if (l == 0 && ok) {
-                        ok = fwait(smem_u32(&x_full[slot]), static_cast<uint32_t>((i >> 1) & 1), &abort_flag);
-                        if (ok) consumed_x = i + 1;
-                    }
-                    if (!ok) break;
-                    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-                    const int nkb = l == 0 ? 1 : 4;
-                    const uint32_t act_parity = static_cast<uint32_t>((3 * i + l - 1) & 1);
-                    for (int kb = 0; kb < nkb && ok; ++kb) {
-                        // layers 1-3: one weight chunk per K block; layer 4: one chunk holds all four blocks
-                        const int s = g % F_STAGES;
-                        if (l != 3 || kb == 0)
-                            ok = fwait(smem_u32(&w_full[s]), static_cast<uint32_t>((g / F_STAGES) & 1), &abort_flag);
-                        if (ok && l > 0) ok = fwait(smem_u32(&act_full[kb]), act_parity, &abort_flag);
+            int g = 0, xw = 0;
+            for (int p = 0; p < npairs && ok; ++p)
+                for (int l = 0; l < 4 && ok; ++l)
+                    for (int s = 0; s < 2 && ok; ++s) {
+                        const int k = 2 * p + s;
+                        if (k >= ntiles) continue;
+                        ok = fwait(smem_u32(&epi_done[s]), static_cast<uint32_t>((4 * p + l - 1) & 1), &abort_flag);
+                        if (ok && l == 0) {
+                            ok = fwait(smem_u32(&x_full[s]), static_cast<uint32_t>(p & 1), &abort_flag);
+                            if (ok) consumed_x = ++xw;
+                        }
                         if (!ok) break;
                         asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-                        const uint32_t bbase = sW + s * F_WCHUNK + (l == 3 ? kb * (16 * BK * 2) : 0);
-                        // A: the input tile in the tensor copies' layout (LBO 2048, SBO 128) or an activation block
-                        // in the epilogue's (LBO 128, SBO 1024)
-                        const uint32_t abase = l == 0 ? sX + slot * F_TILE : sAct + kb * F_TILE;
-                        const uint32_t astep = l == 0 ? 4096u : 256u, albo = l == 0 ? 2048u : 128u, asbo = l == 0 ? 128u : 1024u;
+                        const uint32_t accum = tmem + static_cast<uint32_t>(s * 256);
+                        const uint32_t act = sAct + s * F_SLOT;
+                        const int nkb = l == 0 ? 1 : 4;
+                        for (int kb = 0; kb < nkb && ok; ++kb) {
+                            // layers 1-3: one weight chunk per K block; layer 4: one chunk holds all four blocks
+                            const int sw = g % F_STAGES;
+                            if (l != 3 || kb == 0)
+                                ok = fwait(smem_u32(&w_full[sw]), static_cast<uint32_t>((g / F_STAGES) & 1), &abort_flag);
+                            if (!ok) break;
+                            asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+                            const uint32_t bbase = sW + sw * F_WCHUNK + (l == 3 ? kb * (16 * BK * 2) : 0);
+                            // A: the input tile in the tensor copies' layout (LBO 2048, SBO 128) or an activation
+                            // block in the epilogue's (LBO 128, SBO 1024)
+                            const uint32_t abase = l == 0 ? act + 3 * F_TILE : act + kb * F_TILE;
+                            const uint32_t astep = l == 0 ? 4096u : 256u, albo = l == 0 ? 2048u : 128u, asbo = l == 0 ? 128u : 1024u;
 #pragma unroll
-                        for (int k = 0; k < BK / 16; ++k)
-                            mma_bf16(accum, smem_desc(abase + k * astep, albo, asbo),
-                                     smem_desc(bbase + k * 256, 128, (BK / 8) * 128), l == 3 ? id16 : id256,
-                                     (kb > 0 || k > 0) ? 1u : 0u);
-                        if (l != 3) {
-                            mma_commit(smem_u32(&w_empty[s]));
+                            for (int kk = 0; kk < BK / 16; ++kk)
+                                mma_bf16(accum, smem_desc(abase + kk * astep, albo, asbo),
+                                         smem_desc(bbase + kk * 256, 128, (BK / 8) * 128), l == 3 ? id16 : id256,
+                                         (kb > 0 || kk > 0) ? 1u : 0u);
+                            if (l != 3) {
+                                mma_commit(smem_u32(&w_empty[sw]));
+                                last_commit = g;
+                                ++g;
+                            }
+                        }
+                        if (!ok) break;
+                        if (l == 3) {
+                            mma_commit(smem_u32(&w_empty[g % F_STAGES]));
                             last_commit = g;
                             ++g;
+                            mma_commit(smem_u32(&x_empty[s]));   // the activation tile is free for the next input
                         }
+                        mma_commit(smem_u32(&acc_full[s]));
                     }
-                    if (!ok) break;
-                    if (l == 3) {
-                        mma_commit(smem_u32(&w_empty[g % F_STAGES]));
-                        last_commit = g;
-                        ++g;
-                    }
-                    if (l == 0) mma_commit(smem_u32(&x_empty[slot]));
-                    mma_commit(smem_u32(&acc_full[b]));
-                }
-            }
             consumed_chunks = g;
         }
     } else {
@@ -637,65 +633,64 @@ __global__ void __launch_bounds__(F_THREADS, 1) mlp_forward_fused(const FusedArg
         const int e = warp - 2, q = warp & 3, h = e >> 2;
         const int row = q * 32 + lane;
         bool ok = true;
-        for (int i = 0; i < ntiles && ok; ++i) {
-            const int tile = static_cast<int>(blockIdx.x) + i * static_cast<int>(gridDim.x);
-            for (int l = 0; l < 4 && ok; ++l) {
-                const int b = l & 1;
-                const int u = 2 * i + (l >> 1);
-                ok = __all_sync(0xffffffffu, fwait(smem_u32(&acc_full[b]), static_cast<uint32_t>(u & 1), &abort_flag));
-                if (!ok) break;
-                asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-                const uint32_t tl = tmem + (static_cast<uint32_t>(q * 32) << 16) + static_cast<uint32_t>(b * 256);
-                if (l < 3) {
-                    const float4* bias4 = reinterpret_cast<const float4*>(sBias + l * 256);
-                    uint32_t r[2][16];
-                    tmem_ld16(tl + static_cast<uint32_t>(h * 16), r[0]);
-                    tmem_wait16(r[0]);
+        for (int p = 0; p < npairs && ok; ++p)
+            for (int l = 0; l < 4 && ok; ++l)
+                for (int s = 0; s < 2 && ok; ++s) {
+                    const int k = 2 * p + s;
+                    if (k >= ntiles) continue;
+                    const int tile = static_cast<int>(blockIdx.x) + k * static_cast<int>(gridDim.x);
+                    ok = __all_sync(0xffffffffu, fwait(smem_u32(&acc_full[s]), static_cast<uint32_t>(l & 1), &abort_flag));
+                    if (!ok) break;
+                    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+                    const uint32_t tl = tmem + (static_cast<uint32_t>(q * 32) << 16) + static_cast<uint32_t>(s * 256);
+                    if (l < 3) {
+                        const float4* bias4 = reinterpret_cast<const float4*>(l == 0 ? a.bias[0] : l == 1 ? a.bias[1] : a.bias[2]);
+                        const uint32_t act = sAct + s * F_SLOT;
+                        uint32_t r[2][16];
+                        tmem_ld16(tl + static_cast<uint32_t>(h * 16), r[0]);
+                        tmem_wait16(r[0]);
 #pragma unroll
-                    for (int j = 0; j < 4; ++j) {
-                        // the next block's load is in flight while this one is processed
-                        if (j < 3) tmem_ld16(tl + static_cast<uint32_t>((j + 1) * 64 + h * 16), r[(j + 1) & 1]);
-                        const uint32_t* v = r[j & 1];
-                        const int c0 = j * 64 + h * 16;
-                        uint32_t w8[8];
+                        for (int j = 0; j < 4; ++j) {
+                            // the next block's load is in flight while this one is processed
+                            if (j < 3) tmem_ld16(tl + static_cast<uint32_t>((j + 1) * 64 + h * 16), r[(j + 1) & 1]);
+                            const uint32_t* v = r[j & 1];
+                            const int c0 = j * 64 + h * 16;
+                            uint32_t w8[8];
 #pragma unroll
-                        for (int p = 0; p < 4; ++p) {
-                            const float4 bb = bias4[(c0 >> 2) + p];
-                            const uint64_t v01 = add2(f2(__uint_as_float(v[4 * p]), __uint_as_float(v[4 * p + 1])), f2(bb.x, bb.y));
-                            const uint64_t v23 = add2(f2(__uint_as_float(v[4 * p + 2]), __uint_as_float(v[4 * p + 3])), f2(bb.z, bb.w));
-                            w8[2 * p] = gelu_t2_bf16(v01);
-                            w8[2 * p + 1] = gelu_t2_bf16(v23);
+                            for (int pp = 0; pp < 4; ++pp) {
+                                const float4 bb = __ldg(bias4 + (c0 >> 2) + pp);
+                                const uint64_t v01 = add2(f2(__uint_as_float(v[4 * pp]), __uint_as_float(v[4 * pp + 1])), f2(bb.x, bb.y));
+                                const uint64_t v23 = add2(f2(__uint_as_float(v[4 * pp + 2]), __uint_as_float(v[4 * pp + 3])), f2(bb.z, bb.w));
+                                w8[2 * pp] = gelu_t2_bf16(v01);
+                                w8[2 * pp + 1] = gelu_t2_bf16(v23);
+                            }
+                            const uint32_t blk = act + j * F_TILE;
+                            asm volatile("st.shared.v4.b32 [%0], {%1, %2, %3, %4};\n"
+                                         :: "r"(blk + kmajor_off(row, h * 16)), "r"(w8[0]), "r"(w8[1]), "r"(w8[2]), "r"(w8[3]) : "memory");
+                            asm volatile("st.shared.v4.b32 [%0], {%1, %2, %3, %4};\n"
+                                         :: "r"(blk + kmajor_off(row, h * 16 + 8)), "r"(w8[4]), "r"(w8[5]), "r"(w8[6]), "r"(w8[7]) : "memory");
+                            if (j < 3) tmem_wait16(r[(j + 1) & 1]);
                         }
-                        const uint32_t blk = sAct + j * F_TILE;
-                        asm volatile("st.shared.v4.b32 [%0], {%1, %2, %3, %4};\n"
-                                     :: "r"(blk + kmajor_off(row, h * 16)), "r"(w8[0]), "r"(w8[1]), "r"(w8[2]), "r"(w8[3]) : "memory");
-                        asm volatile("st.shared.v4.b32 [%0], {%1, %2, %3, %4};\n"
-                                     :: "r"(blk + kmajor_off(row, h * 16 + 8)), "r"(w8[4]), "r"(w8[5]), "r"(w8[6]), "r"(w8[7]) : "memory");
-                        // block j of the activation tile is written: visible to the tensor cores, then announced
+                        // the activation tile is written: visible to the tensor cores
                         asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
-                        __syncwarp();
-                        if (lane == 0) mbar_arrive(smem_u32(&act_full[j]));
-                        if (j < 3) tmem_wait16(r[(j + 1) & 1]);
+                    } else {
+                        uint32_t r[4];
+                        asm volatile("tcgen05.ld.sync.aligned.32x32b.x4.b32 {%0,%1,%2,%3}, [%4];\n"
+                                     : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]) : "r"(tl + static_cast<uint32_t>(h * 4)));
+                        asm volatile("tcgen05.wait::ld.sync.aligned;\n" : "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3]) :: "memory");
+                        const int grow = tile * BM + row;
+                        if (grow < a.B) {
+                            const float4 bb = __ldg(reinterpret_cast<const float4*>(a.bias[3]) + h);
+                            reinterpret_cast<float4*>(a.out + static_cast<size_t>(grow) * 16)[h] =
+                                make_float4(__fadd_rn(__uint_as_float(r[0]), bb.x), __fadd_rn(__uint_as_float(r[1]), bb.y),
+                                            __fadd_rn(__uint_as_float(r[2]), bb.z), __fadd_rn(__uint_as_float(r[3]), bb.w));
+                        }
                     }
-                } else {
-                    uint32_t r[4];
-                    asm volatile("tcgen05.ld.sync.aligned.32x32b.x4.b32 {%0,%1,%2,%3}, [%4];\n"
-                                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]) : "r"(tl + static_cast<uint32_t>(h * 4)));
-                    asm volatile("tcgen05.wait::ld.sync.aligned;\n" : "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3]) :: "memory");
-                    const int grow = tile * BM + row;
-                    if (grow < a.B) {
-                        const float4 bb = reinterpret_cast<const float4*>(sBias + 768)[h];
-                        reinterpret_cast<float4*>(a.out + static_cast<size_t>(grow) * 16)[h] =
-                            make_float4(__fadd_rn(__uint_as_float(r[0]), bb.x), __fadd_rn(__uint_as_float(r[1]), bb.y),
-                                        __fadd_rn(__uint_as_float(r[2]), bb.z), __fadd_rn(__uint_as_float(r[3]), bb.w));
-                    }
+                    // the accumulator is drained (and the activation tile written): the slot's next MMAs may start
+                    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+                    __syncwarp();
+                    if (lane == 0) mbar_arrive(smem_u32(&epi_done[s]));
                 }
-                // the accumulator is drained: the MMAs of its next use may overwrite it
-                asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
-                __syncwarp();
-                if (lane == 0) mbar_arrive(smem_u32(&acc_empty[b]));
-            }
-        }
     }
     __syncwarp();
     __syncthreads();
@@ -707,6 +702,8 @@ __global__ void __launch_bounds__(F_THREADS, 1) mlp_forward_fused(const FusedArg
             fwait(smem_u32(&w_full[g % F_STAGES]), static_cast<uint32_t>((g / F_STAGES) & 1), reinterpret_cast<volatile int*>(&dummy));
         }
         for (int t = consumed_x; t < issued_x; ++t) {
+            // input copy t went to slot (its tile index) & 1 as the slot's (t >> 1)-th use: the k-th tile of this CTA
+            // has slot k & 1 and use k >> 1, and the copies were issued for k = 0, 1, 2, ...
             int dummy = 0;
             fwait(smem_u32(&x_full[t & 1]), static_cast<uint32_t>((t >> 1) & 1), reinterpret_cast<volatile int*>(&dummy));
         }
@@ -974,9 +971,9 @@ int cl_b200_mlp_forward_fused(const void* X, int32_t B, const void* Wp1, const v
                               float* out, int32_t max_ctas, void* stream) {
     if (!X || !Wp1 || !Wp2 || !Wp3 || !Wp4 || !b1 || !b2 || !b3 || !b4 || !out || B <= 0 || max_ctas < 0)
         return capi_fail(CL_EINVAL, "fused forward: bad arguments");
-    const void* ps[6] = {X, Wp1, Wp2, Wp3, Wp4, out};
+    const void* ps[10] = {X, Wp1, Wp2, Wp3, Wp4, out, b1, b2, b3, b4};
     for (const void* p : ps)
-        if (reinterpret_cast<uintptr_t>(p) % 16) return capi_fail(CL_EINVAL, "fused forward: X, the packed weights and out need 16-byte alignment");
+        if (reinterpret_cast<uintptr_t>(p) % 16) return capi_fail(CL_EINVAL, "fused forward: X, the packed weights, the biases and out need 16-byte alignment");
     int dev = 0, sms = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
