@@ -414,6 +414,7 @@ constexpr int F_SMEM = F_OFF_W + F_STAGES * F_WCHUNK;   // 229,376 bytes
 constexpr int F_CHUNKS = 10;                        // per tile: W1 (1 block), W2 (4), W3 (4), W4 (its 4 blocks, 8 KB)
 constexpr int F_THREADS = 576;                     // 18 warps: producer, MMA, 16 epilogue
 constexpr int F_EPI_WARPS = 16;
+constexpr int F_SLEEP_NS = 32;                     // the producer's and MMA issuer's poll interval
 
 struct FusedArgs {
     const __nv_bfloat16* X;                         // B x 64 row-major, rows 16-byte aligned
@@ -435,6 +436,9 @@ __device__ __forceinline__ const uint8_t* fchunk_src(const FusedArgs& a, int c) 
 // Bounded wait that also gives up when another role has (the shared abort flag): the clock and the flag are
 // checked every 64 polls. (A suspend-time hint on the try_wait made the kernel slower: 58.8 us against 51.1 us at
 // 65536 rows.)
+// SLEEP_NS > 0 (the single-thread roles: producer, MMA issuer) sleeps between polls, leaving the issue slots of its
+// scheduler to the epilogue warps that share it.
+template <int SLEEP_NS = 0>
 __device__ __forceinline__ bool fwait(uint32_t bar, uint32_t parity, volatile int* abort_flag) {
     const uint64_t t0 = global_ns();
     for (unsigned it = 0;; ++it) {
@@ -443,6 +447,7 @@ __device__ __forceinline__ bool fwait(uint32_t bar, uint32_t parity, volatile in
             "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
             : "=r"(done) : "r"(bar), "r"(parity) : "memory");
         if (done) return true;
+        if (SLEEP_NS > 0) __nanosleep(SLEEP_NS);
         if ((it & 63u) == 63u) {
             if (*abort_flag) return false;
             if (it >= kWaitLimit || global_ns() - t0 > kWaitNs) {
@@ -540,7 +545,7 @@ __global__ void __launch_bounds__(F_THREADS, 1) mlp_forward_fused(const FusedArg
                         if (l == 0) {
                             // the 128 x 64 input tile into K block 3 of the slot's activation tile: eight tensor copies
                             // of 128 rows x 8 columns, K group g at g * 2048 bytes; rows past B are zero filled
-                            good = fwait(smem_u32(&x_empty[s]), static_cast<uint32_t>((p & 1) ^ 1), &abort_flag);
+                            good = fwait<F_SLEEP_NS>(smem_u32(&x_empty[s]), static_cast<uint32_t>((p & 1) ^ 1), &abort_flag);
                             if (good) {
                                 const int tile = static_cast<int>(blockIdx.x) + k * static_cast<int>(gridDim.x);
                                 const uint32_t bar = smem_u32(&x_full[s]), dst = sAct + s * F_SLOT + 3 * F_TILE;
@@ -557,7 +562,7 @@ __global__ void __launch_bounds__(F_THREADS, 1) mlp_forward_fused(const FusedArg
                         const int c_lo = l == 0 ? 0 : l == 1 ? 1 : l == 2 ? 5 : 9, c_hi = l == 0 ? 1 : l == 1 ? 5 : l == 2 ? 9 : 10;
                         for (int c = c_lo; c < c_hi && good; ++c, ++g) {
                             const int sw = g % F_STAGES;
-                            good = fwait(smem_u32(&w_empty[sw]), static_cast<uint32_t>(((g / F_STAGES) & 1) ^ 1), &abort_flag);
+                            good = fwait<F_SLEEP_NS>(smem_u32(&w_empty[sw]), static_cast<uint32_t>(((g / F_STAGES) & 1) ^ 1), &abort_flag);
                             if (!good) break;
                             const uint32_t bytes = fchunk_bytes(c), bar = smem_u32(&w_full[sw]);
                             asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" :: "r"(bar), "r"(bytes) : "memory");
@@ -582,9 +587,9 @@ __global__ void __launch_bounds__(F_THREADS, 1) mlp_forward_fused(const FusedArg
                     for (int s = 0; s < 2 && ok; ++s) {
                         const int k = 2 * p + s;
                         if (k >= ntiles) continue;
-                        ok = fwait(smem_u32(&epi_done[s]), static_cast<uint32_t>((4 * p + l - 1) & 1), &abort_flag);
+                        ok = fwait<F_SLEEP_NS>(smem_u32(&epi_done[s]), static_cast<uint32_t>((4 * p + l - 1) & 1), &abort_flag);
                         if (ok && l == 0) {
-                            ok = fwait(smem_u32(&x_full[s]), static_cast<uint32_t>(p & 1), &abort_flag);
+                            ok = fwait<F_SLEEP_NS>(smem_u32(&x_full[s]), static_cast<uint32_t>(p & 1), &abort_flag);
                             if (ok) consumed_x = ++xw;
                         }
                         if (!ok) break;
@@ -596,7 +601,7 @@ __global__ void __launch_bounds__(F_THREADS, 1) mlp_forward_fused(const FusedArg
                             // layers 1-3: one weight chunk per K block; layer 4: one chunk holds all four blocks
                             const int sw = g % F_STAGES;
                             if (l != 3 || kb == 0)
-                                ok = fwait(smem_u32(&w_full[sw]), static_cast<uint32_t>((g / F_STAGES) & 1), &abort_flag);
+                                ok = fwait<F_SLEEP_NS>(smem_u32(&w_full[sw]), static_cast<uint32_t>((g / F_STAGES) & 1), &abort_flag);
                             if (!ok) break;
                             asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
                             const uint32_t bbase = sW + sw * F_WCHUNK + (l == 3 ? kb * (16 * BK * 2) : 0);
