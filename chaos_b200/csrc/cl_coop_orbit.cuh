@@ -11,8 +11,9 @@
 // (`_status`, orbit.jl:3) with a vote, stages the frame column-major in shared memory, and the frame's reducer chain
 // runs on it there: QRSpectrum(HouseholderQR) column-parallel over the group (the reflectors built by the column
 // owners in shared memory and applied by every lane to its own columns, as the ensemble's cooperative kernel does),
-// every other chain (MGS / CGS / RGS / Givens QR, GALI, SALI, MEGNO, FLI, Benettin) by the group's first lane with the
-// same reducer code as the one-thread kernel. Every entry is computed by the same operations in the same order and
+// QRSpectrum(MGS) in Float64 column-parallel by rounds (coop_qr_step), every other chain (MGS in Float32, CGS / RGS /
+// Givens QR, GALI, SALI, MEGNO, FLI, Benettin) by the group's first lane with the same reducer code as the one-thread
+// kernel. Every entry is computed by the same operations in the same order and
 // type, so the results are bit-identical to the one-thread kernel (and, in Float64, to the oracle).
 #pragma once
 
@@ -23,14 +24,21 @@ namespace cl {
 
 template <int NS> struct CoopWidth { static constexpr int G = NS <= 2 ? 2 : NS <= 4 ? 4 : 8; };
 
-// QRSpectrum(HouseholderQR) on the staged frame, column-parallel (householder.jl:19-80, qr_spectrum.jl:36-74): the
+// QRSpectrum on the staged frame, column-parallel (qr_spectrum.jl:36-74): lane j owns columns j, j + G, ... The
 // QRState sums of this lane's columns and the shared scalars (kept equal in every lane) are read from and written
 // back to the Julia-layout state `st` in shared memory by lane 0 / the column owners. Returns true on failure.
-template <int D, int K, int G, typename Real>
-__device__ __forceinline__ bool coop_householder_step(QRState<K>& st, i64 n, Real* sT, Real* sQ, Real* sU, Real* sR,
-                                                      unsigned gm, int j, double orth_tol) {
+//   HouseholderQR (householder.jl:19-80): the owner of column jj builds reflector jj in shared memory, every lane
+//   applies it to its own columns and forms its own columns of Q.
+//   MGS (orthonormalize.jl:49-58, 88-105): in round r the owner of column r, projected already on q_0 .. q_{r-1},
+//   takes its norm and normalises it into q_r (the first column whose norm fails stops the factorisation, as the
+//   serial loop does); then every lane projects its later columns on q_r (c = q_r . u, u - c q_r): each column sees
+//   the same projections in the same order as in the serial loop.
+template <int ALG, int D, int K, int G, typename Real>
+__device__ __forceinline__ bool coop_qr_step(QRState<K>& st, i64 n, Real* sT, Real* sQ, Real* sU, Real* sR,
+                                             unsigned gm, int j, double orth_tol) {
     constexpr int NREF = K < D ? K : K - 1;
     constexpr int KPL = (K + G - 1) / G;   // columns per lane (the last lanes may own fewer)
+    constexpr bool HH = ALG == CL_QR_HOUSEHOLDER;
     Real A[KPL][D];
 #pragma unroll
     for (int m = 0; m < KPL; ++m) {
@@ -38,7 +46,48 @@ __device__ __forceinline__ bool coop_householder_step(QRState<K>& st, i64 n, Rea
 #pragma unroll
         for (int r = 0; r < D; ++r) A[m][r] = cc < K ? sT[cc * D + r] : Real(0);
     }
-    int count = 0;
+    int count = HH ? 0 : 1;
+    int status = QR_OK, fcol = 0;
+    if constexpr (!HH) {
+        Real Rc[KPL][K];
+#pragma unroll
+        for (int m = 0; m < KPL; ++m)
+#pragma unroll
+            for (int i = 0; i < K; ++i) Rc[m][i] = Real(0);
+#pragma unroll
+        for (int rr = 0; rr < K; ++rr) {
+            const int owner = rr % G, mo = rr / G;
+            int bad = 0;
+            if (j == owner) {
+#pragma unroll
+                for (int m = 0; m < KPL; ++m) {
+                    if (m != mo) continue;
+                    const Real gamma = nrm<D>(A[m]);
+#pragma unroll
+                    for (int i = 0; i < K; ++i) sR[i + rr * K] = i < rr ? Rc[m][i] : (i == rr ? gamma : Real(0));
+                    if (!(isfin(gamma) && gamma > Real(0))) {
+                        bad = 1;
+                    } else {
+#pragma unroll
+                        for (int l = 0; l < D; ++l) { A[m][l] = dv(A[m][l], gamma); sQ[rr * D + l] = A[m][l]; }
+                    }
+                }
+            }
+            __syncwarp(gm);
+            if (__shfl_sync(gm, bad, owner, G)) { status = QR_PIVOT; fcol = rr + 1; break; }
+            const Real* qr_ = sQ + rr * D;
+#pragma unroll
+            for (int m = 0; m < KPL; ++m) {
+                const int cc = j + m * G;
+                if (cc <= rr || cc >= K) continue;
+                const Real c = dotv<D>(qr_, A[m]);
+                Rc[m][rr] = c;
+#pragma unroll
+                for (int l = 0; l < D; ++l) A[m][l] = A[m][l] - c * qr_[l];
+            }
+            __syncwarp(gm);
+        }
+    } else {
 #pragma unroll
     for (int jj = 0; jj < NREF; ++jj) {
         const int owner = jj % G, mj = jj / G;
@@ -133,12 +182,12 @@ __device__ __forceinline__ bool coop_householder_step(QRState<K>& st, i64 n, Rea
         for (int r = 0; r < D; ++r) { A[m][r] = A[m][r] * sgc; sQ[cc * D + r] = A[m][r]; }
     }
     __syncwarp(gm);
-    int status = QR_OK, fcol = 0;
 #pragma unroll
     for (int jj = K - 1; jj >= 0; --jj) {
         const Real pv = sR[jj + jj * K];
         if (!(isfin(pv) && pv > Real(0))) { status = QR_PIVOT; fcol = jj + 1; }
     }
+    }   // HouseholderQR
     bool replace = false, fail = false;
     if (status != QR_OK) {
         Real pv = sR[0];
@@ -155,6 +204,14 @@ __device__ __forceinline__ bool coop_householder_step(QRState<K>& st, i64 n, Rea
         Real Gw = Real(0);
         if (j == 0) Gw = window_Gw_sm<K>(sR, sU);   // the reflectors are spent: sU is scratch
         Gw = __shfl_sync(gm, Gw, 0, G);
+        // conditioning (the Gram-Schmidt family only, qr_spectrum.jl:54-58)
+        if (!HH && !(static_cast<double>(Gw * epsT) < 0.5)) {
+            if (j == 0) {
+                st.code = 3; st.column = 0; st.value = static_cast<double>(Gw * epsT); st.threshold = 0.5; st.step = n;
+            }
+            __syncwarp(gm);
+            return true;
+        }
         Real om = Real(0);
         bool first = true;
 #pragma unroll
@@ -179,7 +236,7 @@ __device__ __forceinline__ bool coop_householder_step(QRState<K>& st, i64 n, Rea
 #pragma unroll
         for (int off = G / 2; off >= 1; off >>= 1) om = mx(om, __shfl_xor_sync(gm, om, off, G));
         const Real orth = K >= 2 ? om : Real(0);
-        const Real thr = static_cast<Real>(orth_tol) * epsT * static_cast<Real>(K);
+        const Real thr = static_cast<Real>(orth_tol) * epsT * static_cast<Real>(K) * (HH ? Real(1) : Gw);
         if (K >= 2 && !(orth <= thr)) {
             if (j == 0) {
                 st.code = 4; st.column = 0; st.value = static_cast<double>(orth);
@@ -217,16 +274,21 @@ __device__ __forceinline__ bool coop_householder_step(QRState<K>& st, i64 n, Rea
     return fail;
 }
 
-// The column-parallel QR runs when every lane owns at least one column (K >= G); other chains on the first lane.
-template <class F, int G> struct IsHouseholderQR { static constexpr bool value = false; };
-template <int KK, int G> struct IsHouseholderQR<Frame<KK, RQR<CL_QR_HOUSEHOLDER>>, G> { static constexpr bool value = KK >= G; };
+// The column-parallel QR runs when every lane owns at least one column (K >= G): HouseholderQR in both precisions,
+// MGS in Float64 (in Float32 its rounds ran slower than the first lane's serial MGS: d = 16, 2048 orbits, 36.8
+// against 22.5 ms; in Float64 116 against 119 ms, 8192 orbits 246 against 280 ms); other chains on the first lane.
+template <class F, typename Real, int G> struct CoopQRForm { static constexpr bool value = false; static constexpr int alg = 0; };
+template <int KK, int ALG, typename Real, int G> struct CoopQRForm<Frame<KK, RQR<ALG>>, Real, G> {
+    static constexpr bool value = KK >= G && (ALG == CL_QR_HOUSEHOLDER || (ALG == CL_QR_MGS && sizeof(Real) == 8));
+    static constexpr int alg = ALG;
+};
 
 template <int NS, typename Real, class F0>
 __global__ void __launch_bounds__(128) coop_orbit_kernel(const KArgs a, const SysChain<NS> sys) {
     constexpr int G = CoopWidth<NS>::G, D = 2 * NS, S = 2 * NS, K = F0::K;
     using Ch = typename F0::template Chain_<D>;
     constexpr int words = Ch::bytes / 8;
-    constexpr bool HH = IsHouseholderQR<F0, G>::value;
+    constexpr bool HH = CoopQRForm<F0, Real, G>::value;
     constexpr int NREF = K < D ? K : K - 1;
     // per group: the staged frame, then (Householder) Q, the reflectors and R, then the chain's state
     constexpr int FW = D * K, QW = HH ? D * K : 0, UW = HH ? (D * NREF > K ? D * NREF : K) : 0, RW = HH ? K * K : 0;
@@ -306,7 +368,7 @@ __global__ void __launch_bounds__(128) coop_orbit_kernel(const KArgs a, const Sy
             int failed = 0;
             if constexpr (HH) {
                 QRState<K>& st = *reinterpret_cast<QRState<K>*>(sSt);
-                failed = coop_householder_step<D, K, G>(st, n, sT, sQ, sU, sR, gm, j, a.prm[0][0].orthogonality_tol) ? 1 : 0;
+                failed = coop_qr_step<CoopQRForm<F0, Real, G>::alg, D, K, G>(st, n, sT, sQ, sU, sR, gm, j, a.prm[0][0].orthogonality_tol) ? 1 : 0;
             } else {
                 if (j == 0) {
                     Ch ch;
@@ -356,7 +418,7 @@ __global__ void __launch_bounds__(128) coop_orbit_kernel(const KArgs a, const Sy
 template <int NS, typename Real, class F0>
 cudaError_t launch_coop_orbit(const cl_run& run, const KArgs& a, cudaStream_t st, LaunchInfo* info) {
     constexpr int G = CoopWidth<NS>::G, D = 2 * NS, K = F0::K;
-    constexpr bool HH = IsHouseholderQR<F0, G>::value;
+    constexpr bool HH = CoopQRForm<F0, Real, G>::value;
     constexpr int NREF = K < D ? K : K - 1;
     constexpr int FW = D * K, QW = HH ? D * K : 0, UW = HH ? (D * NREF > K ? D * NREF : K) : 0, RW = HH ? K * K : 0;
     constexpr int words = F0::template Chain_<D>::bytes / 8;
