@@ -11,9 +11,9 @@
 // (`_status`, orbit.jl:3) with a vote, stages the frame column-major in shared memory, and the frame's reducer chain
 // runs on it there: QRSpectrum(HouseholderQR) column-parallel over the group (the reflectors built by the column
 // owners in shared memory and applied by every lane to its own columns, as the ensemble's cooperative kernel does),
-// QRSpectrum(MGS) in Float64 column-parallel by rounds (coop_qr_step), every other chain (MGS in Float32, CGS / RGS /
-// Givens QR, GALI, SALI, MEGNO, FLI, Benettin) by the group's first lane with the same reducer code as the one-thread
-// kernel. Every entry is computed by the same operations in the same order and
+// QRSpectrum(MGS) and GALI in Float64 column-parallel by rounds (coop_qr_step, coop_gali_step), every other chain
+// (in Float32 MGS and GALI, CGS / RGS / Givens QR, SALI, MEGNO, FLI, Benettin) by the group's first lane with the same
+// reducer code as the one-thread kernel. Every entry is computed by the same operations in the same order and
 // type, so the results are bit-identical to the one-thread kernel (and, in Float64, to the oracle).
 #pragma once
 
@@ -274,6 +274,95 @@ __device__ __forceinline__ bool coop_qr_step(QRState<K>& st, i64 n, Real* sT, Re
     return fail;
 }
 
+// GALI (gali.jl:17-201, the frame's unit columns and _gram_core! at :81-100) on the staged frame, column-parallel:
+// every lane takes its own columns' norms, log sums and unit columns; the first failing column over the group (the
+// lowest index) stops the step as the serial loop does. The twice-orthogonalised Gram core runs by rounds: in round r
+// the owner of column r, projected already once on the final q_0 .. q_{r-1}, projects it a second time on all of them,
+// takes its norm and normalises it, and G_r = G_{r-1} r_r is formed in every lane from the broadcast norm; then every
+// lane makes the first projection of its later columns on q_r. Each column sees the serial loop's projections in its
+// order. The frame becomes the unit columns (not Q). Returns true on failure.
+template <int D, int K, int G, typename Real>
+__device__ __forceinline__ bool coop_gali_step(GALIState<K>& st, i64 n, Real* sT, Real* sQ, unsigned gm, int j) {
+    constexpr int KPL = (K + G - 1) / G;
+    Real A[KPL][D], a[KPL];
+    int mybad = K + 1;
+#pragma unroll
+    for (int m = KPL - 1; m >= 0; --m) {
+        const int cc = j + m * G;
+        if (cc >= K) continue;
+#pragma unroll
+        for (int r = 0; r < D; ++r) A[m][r] = sT[cc * D + r];
+        a[m] = nrm<D>(A[m]);
+        if (!(isfin(a[m]) && a[m] >= Eps<Real>::floatmin())) mybad = cc + 1;
+    }
+    const int bad = __reduce_min_sync(gm, static_cast<unsigned>(mybad));
+    if (bad <= K) {
+        const int owner = (bad - 1) % G, mo = (bad - 1) / G;
+        Real v = Real(0);
+#pragma unroll
+        for (int m = 0; m < KPL; ++m) if (m == mo) v = a[m];
+        v = __shfl_sync(gm, v, owner, G);
+        if (j == 0) { st.value = static_cast<double>(v); st.step = n; st.code = 1; st.column = bad; }
+        __syncwarp(gm);
+        return true;
+    }
+#pragma unroll
+    for (int m = 0; m < KPL; ++m) {
+        const int cc = j + m * G;
+        if (cc >= K) continue;
+        CS acc{st.s[cc], st.c[cc]};
+        cs_add(acc, lnr(a[m]));
+        st.s[cc] = acc.s; st.c[cc] = acc.c;
+#pragma unroll
+        for (int r = 0; r < D; ++r) { A[m][r] = dv(A[m][r], a[m]); sT[cc * D + r] = A[m][r]; }
+    }
+    Real g = Real(1);
+#pragma unroll
+    for (int rr = 0; rr < K; ++rr) {
+        const int owner = rr % G, mo = rr / G;
+        Real rn = Real(0);
+        if (j == owner) {
+#pragma unroll
+            for (int m = 0; m < KPL; ++m) {
+                if (m != mo) continue;
+#pragma unroll
+                for (int p = 0; p < rr; ++p) {   // the second pass
+                    const Real* qp = sQ + p * D;
+                    Real cc = Real(0);
+#pragma unroll
+                    for (int i = 0; i < D; ++i) cc = cc + qp[i] * A[m][i];
+#pragma unroll
+                    for (int i = 0; i < D; ++i) A[m][i] = A[m][i] - cc * qp[i];
+                }
+                rn = nrm<D>(A[m]);
+                const Real sc = rn == Real(0) ? Real(1) : rn;
+#pragma unroll
+                for (int i = 0; i < D; ++i) { A[m][i] = dv(A[m][i], sc); sQ[rr * D + i] = A[m][i]; }
+            }
+        }
+        rn = __shfl_sync(gm, rn, owner, G);
+        if (rr > 0) {
+            g = g * rn;
+            if (j == owner) st.gali[rr - 1] = static_cast<double>(g);
+        }
+        __syncwarp(gm);
+        const Real* qr_ = sQ + rr * D;
+#pragma unroll
+        for (int m = 0; m < KPL; ++m) {   // the first pass of the later columns on q_rr
+            const int cc = j + m * G;
+            if (cc <= rr || cc >= K) continue;
+            Real c = Real(0);
+#pragma unroll
+            for (int i = 0; i < D; ++i) c = c + qr_[i] * A[m][i];
+#pragma unroll
+            for (int i = 0; i < D; ++i) A[m][i] = A[m][i] - c * qr_[i];
+        }
+    }
+    if (j == 0) st.n = n;
+    __syncwarp(gm);
+    return false;
+}
+
 // The column-parallel QR runs when every lane owns at least one column (K >= G): HouseholderQR in both precisions,
 // MGS in Float64 (in Float32 its rounds ran slower than the first lane's serial MGS: d = 16, 2048 orbits, 36.8
 // against 22.5 ms; in Float64 116 against 119 ms, 8192 orbits 246 against 280 ms); other chains on the first lane.
@@ -283,12 +372,18 @@ template <int KK, int ALG, typename Real, int G> struct CoopQRForm<Frame<KK, RQR
     static constexpr int alg = ALG;
 };
 
+// GALI (without SALI) runs column-parallel in Float64 when every lane owns at least one column.
+template <class F, typename Real, int G> struct CoopGaliForm { static constexpr bool value = false; };
+template <int KK, typename Real, int G> struct CoopGaliForm<Frame<KK, RGALI<false>>, Real, G> {
+    static constexpr bool value = KK >= G && KK >= 2 && sizeof(Real) == 8;
+};
+
 template <int NS, typename Real, class F0>
 __global__ void __launch_bounds__(128) coop_orbit_kernel(const KArgs a, const SysChain<NS> sys) {
     constexpr int G = CoopWidth<NS>::G, D = 2 * NS, S = 2 * NS, K = F0::K;
     using Ch = typename F0::template Chain_<D>;
     constexpr int words = Ch::bytes / 8;
-    constexpr bool HH = CoopQRForm<F0, Real, G>::value;
+    constexpr bool HH = CoopQRForm<F0, Real, G>::value || CoopGaliForm<F0, Real, G>::value;   // shared-memory workspace
     constexpr int NREF = K < D ? K : K - 1;
     // per group: the staged frame, then (Householder) Q, the reflectors and R, then the chain's state
     constexpr int FW = D * K, QW = HH ? D * K : 0, UW = HH ? (D * NREF > K ? D * NREF : K) : 0, RW = HH ? K * K : 0;
@@ -366,9 +461,12 @@ __global__ void __launch_bounds__(128) coop_orbit_kernel(const KArgs a, const Sy
             }
             __syncwarp(gm);
             int failed = 0;
-            if constexpr (HH) {
+            if constexpr (CoopQRForm<F0, Real, G>::value) {
                 QRState<K>& st = *reinterpret_cast<QRState<K>*>(sSt);
                 failed = coop_qr_step<CoopQRForm<F0, Real, G>::alg, D, K, G>(st, n, sT, sQ, sU, sR, gm, j, a.prm[0][0].orthogonality_tol) ? 1 : 0;
+            } else if constexpr (CoopGaliForm<F0, Real, G>::value) {
+                GALIState<K>& st = *reinterpret_cast<GALIState<K>*>(sSt);
+                failed = coop_gali_step<D, K, G>(st, n, sT, sQ, gm, j) ? 1 : 0;
             } else {
                 if (j == 0) {
                     Ch ch;
@@ -418,7 +516,7 @@ __global__ void __launch_bounds__(128) coop_orbit_kernel(const KArgs a, const Sy
 template <int NS, typename Real, class F0>
 cudaError_t launch_coop_orbit(const cl_run& run, const KArgs& a, cudaStream_t st, LaunchInfo* info) {
     constexpr int G = CoopWidth<NS>::G, D = 2 * NS, K = F0::K;
-    constexpr bool HH = CoopQRForm<F0, Real, G>::value;
+    constexpr bool HH = CoopQRForm<F0, Real, G>::value || CoopGaliForm<F0, Real, G>::value;   // shared-memory workspace
     constexpr int NREF = K < D ? K : K - 1;
     constexpr int FW = D * K, QW = HH ? D * K : 0, UW = HH ? (D * NREF > K ? D * NREF : K) : 0, RW = HH ? K * K : 0;
     constexpr int words = F0::template Chain_<D>::bytes / 8;
@@ -447,14 +545,11 @@ cudaError_t launch_coop_orbit(const cl_run& run, const KArgs& a, cudaStream_t st
 constexpr int V_COOP = 8;
 
 // Orbits up to which an untuned run takes the cooperative form. Measured at N = 2e4, tau = 10, k = 8 (ms, one-thread
-// / cooperative): d = 16 at 512 and 2048 orbits 2-3x faster cooperatively (Float64 MGS 232 / 119, mixed Householder
-// 120 / 41), even at 8192 (Float64 Householder 329 / 304, mixed MGS 68 / 44), slower at 65536 orbits (Float64
-// Householder 127 / 213 at N = 2000), where one thread per orbit already fills the GPU; d = 8 Float64 1.2-1.5x faster
-// at 2048 and 8192. The exception is GALI in Float64, whose handoff (twice-orthogonalised columns and norms with
-// divisions) runs on one lane of the group: 295 / 407 at 2048 orbits, so it stays one thread per orbit.
+// / cooperative): d = 16 at 512 and 2048 orbits 1.6-3x faster cooperatively (Float64 MGS 232 / 116, Float64 GALI
+// 295 / 186, mixed Householder 120 / 41), at 8192 about even (Float64 Householder 329 / 304, Float64 GALI 303 / 401),
+// slower at 65536 orbits (Float64 Householder 127 / 213 at N = 2000), where one thread per orbit already fills the
+// GPU; d = 8 Float64 1.2-1.9x faster at 2048 and 8192 (GALI 135 / 71).
 constexpr i64 kCoopMaxOrbits = 4096;
-template <class F, typename Real> struct CoopByDefault { static constexpr bool value = true; };
-template <int KK, bool WS> struct CoopByDefault<Frame<KK, RGALI<WS>>, double> { static constexpr bool value = false; };
 
 // A lattice instance of `propagate` with d >= 8: variant 1 is the one-thread kernel, variant V_COOP the cooperative
 // form; an untuned run (any other variant number) takes the cooperative form for ensembles of at most
@@ -462,7 +557,7 @@ template <int KK, bool WS> struct CoopByDefault<Frame<KK, RGALI<WS>>, double> { 
 template <int NS, typename Real, class F0>
 cudaError_t launch_chain_instance(const cl_run& run, const KArgs& a, const double* devA, cudaStream_t st,
                                   LaunchInfo* info, int minb) {
-    const bool coop = minb == V_COOP || (minb != 1 && CoopByDefault<F0, Real>::value && a.n <= kCoopMaxOrbits);
+    const bool coop = minb == V_COOP || (minb != 1 && a.n <= kCoopMaxOrbits);
     if (!coop) return launch_variant<SysChain<NS>, Real, F0, Frame<1>, Frame<1>, 1, 1>(run, a, devA, st, info);
     return launch_coop_orbit<NS, Real, F0>(run, a, st, info);
 }
