@@ -119,13 +119,13 @@ class QRSpectrum(Reducer):
                     orth_max=float(st["orth_max"]), count_max=int(st["count_max"]))
 
     def finals(self, st, d=None):
-        n = st["n"].astype(np.int64)
-        s = st["sums"][:, :, 0].astype(np.float64)
-        c = st["sums"][:, :, 1].astype(np.float64)
+        n = st["n"].astype(np.int64, copy=False)
+        s = st["sums"][:, :, 0].astype(np.float64, copy=False)
+        c = st["sums"][:, :, 1].astype(np.float64, copy=False)
         with np.errstate(invalid="ignore", divide="ignore"):
-            lam = np.where(n[:, None] == 0, 0.0, (s + c) / n[:, None].astype(np.float64))
-        return dict(n=n, sum=s, comp=c, **{"lambda": lam}, G_max=st["G_max"].astype(np.float64),
-                    orth_max=st["orth_max"].astype(np.float64), count_max=st["count_max"].astype(np.int64))
+            lam = np.where(n[:, None] == 0, 0.0, (s + c) / n[:, None].astype(np.float64, copy=False))
+        return dict(n=n, sum=s, comp=c, **{"lambda": lam}, G_max=st["G_max"].astype(np.float64, copy=False),
+                    orth_max=st["orth_max"].astype(np.float64, copy=False), count_max=st["count_max"].astype(np.int64, copy=False))
 
     def error(self, st, orbit, backend):   # qr_spectrum.jl:80-83
         kind = "orthogonality" if int(st["code"]) == 4 else "orthonormalisation breakdown"
@@ -154,10 +154,10 @@ class Benettin(Reducer):
         return dict(n=n, sum=np.array([st["sum_s"]]), comp=np.array([st["sum_c"]]), **{"lambda": np.array([lam])})
 
     def finals(self, st, d=None):
-        n = st["n"].astype(np.int64)
-        s, c = st["sum_s"].astype(np.float64), st["sum_c"].astype(np.float64)
+        n = st["n"].astype(np.int64, copy=False)
+        s, c = st["sum_s"].astype(np.float64, copy=False), st["sum_c"].astype(np.float64, copy=False)
         with np.errstate(invalid="ignore", divide="ignore"):
-            lam = np.where(n == 0, 0.0, (s + c) / n.astype(np.float64))
+            lam = np.where(n == 0, 0.0, (s + c) / n.astype(np.float64, copy=False))
         return dict(n=n, sum=s[:, None], comp=c[:, None], **{"lambda": lam[:, None]})
 
     def error(self, st, orbit, backend):
@@ -189,11 +189,11 @@ class SALI(Reducer):
         return dict(n=n, sali=float(st["sali"]), L=float(L), sum=s, comp=c, floor=4 * EPS)
 
     def finals(self, st, d=None):
-        n = st["n"].astype(np.int64)
-        s = np.stack([st["s1_s"], st["s2_s"]], axis=1).astype(np.float64)
-        c = np.stack([st["s1_c"], st["s2_c"]], axis=1).astype(np.float64)
+        n = st["n"].astype(np.int64, copy=False)
+        s = np.stack([st["s1_s"], st["s2_s"]], axis=1).astype(np.float64, copy=False)
+        c = np.stack([st["s1_c"], st["s2_c"]], axis=1).astype(np.float64, copy=False)
         L = np.where(n == 0, 0.0, -((s[:, 0] + s[:, 1]) + (c[:, 0] + c[:, 1])))
-        return dict(n=n, sali=st["sali"].astype(np.float64), L=L, sum=s, comp=c, floor=np.full(len(n), 4 * EPS))
+        return dict(n=n, sali=st["sali"].astype(np.float64, copy=False), L=L, sum=s, comp=c, floor=np.full(len(n), 4 * EPS))
 
     def error(self, st, orbit, backend):
         v = float(st["value"])
@@ -235,9 +235,9 @@ class GALI(Reducer):
 
     def finals(self, st, d=None):
         k = st["s"].shape[1]
-        n = st["n"].astype(np.int64)
-        S = st["s"].astype(np.float64)
-        Cc = st["c"].astype(np.float64)
+        n = st["n"].astype(np.int64, copy=False)
+        S = st["s"].astype(np.float64, copy=False)
+        Cc = st["c"].astype(np.float64, copy=False)
         L = None
         if d is not None and k == d:
             s, c = S[:, 0].copy(), Cc[:, 0].copy()
@@ -246,7 +246,7 @@ class GALI(Reducer):
                 c = c + Cc[:, i]
             L = np.where(n == 0, 0.0, -(s + c))
         floors = np.broadcast_to(np.array([2 * (i + 1) * EPS for i in range(1, k)]), (len(n), k - 1))
-        return dict(n=n, gali=st["gali"].astype(np.float64), L=L, sum=S, comp=Cc, floor=floors)
+        return dict(n=n, gali=st["gali"].astype(np.float64, copy=False), L=L, sum=S, comp=Cc, floor=floors)
 
     def error(self, st, orbit, backend):
         v = float(st["value"])
@@ -307,22 +307,22 @@ class MEGNO(Reducer):
                     sum=pair("s", "s"), comp=pair("s", "c"), R1=tot("R1"), R2=tot("R2"), Q=tot("Q"), Q2=tot("Q2"))
 
     def finals(self, st, d=None):
-        n, K = st["n"].astype(np.int64), st["K"].astype(np.int64)
+        n, K = st["n"].astype(np.int64, copy=False), st["K"].astype(np.int64, copy=False)
         f = np.float64
-        tn = n.astype(f)
+        tn = n.astype(f, copy=False)
         cols = {nm: np.zeros((len(n), 2)) for nm in ("Y", "Ybar", "Ybar20")}
         with np.errstate(invalid="ignore", divide="ignore"):
-            nk = np.where(K == 0, 0, n // np.where(K == 0, 1, K)).astype(f)
+            nk = np.where(K == 0, 0, n // np.where(K == 0, 1, K)).astype(f, copy=False)
             for j, col in enumerate(("c1", "c2")):
-                R1 = st[f"{col}_R1_s"].astype(f) + st[f"{col}_R1_c"].astype(f)
-                Q = st[f"{col}_Q_s"].astype(f) + st[f"{col}_Q_c"].astype(f)
-                Q2 = st[f"{col}_Q2_s"].astype(f) + st[f"{col}_Q2_c"].astype(f)
+                R1 = st[f"{col}_R1_s"].astype(f, copy=False) + st[f"{col}_R1_c"].astype(f, copy=False)
+                Q = st[f"{col}_Q_s"].astype(f, copy=False) + st[f"{col}_Q_c"].astype(f, copy=False)
+                Q2 = st[f"{col}_Q2_s"].astype(f, copy=False) + st[f"{col}_Q2_c"].astype(f, copy=False)
                 cols["Y"][:, j] = np.where(K == 0, 0.0, 2 * R1 / tn)
-                cols["Ybar"][:, j] = np.where(K == 0, 0.0, Q / K.astype(f))
+                cols["Ybar"][:, j] = np.where(K == 0, 0.0, Q / K.astype(f, copy=False))
                 cols["Ybar20"][:, j] = np.where(K == 0, 0.0, nk * Q2 / (tn * tn * tn))
-        pair = lambda nm, comp: np.stack([st[f"c1_{nm}_{comp}"], st[f"c2_{nm}_{comp}"]], axis=1).astype(f)  # noqa
-        tot = lambda nm: np.stack([st[f"c1_{nm}_s"].astype(f) + st[f"c1_{nm}_c"].astype(f),  # noqa
-                                   st[f"c2_{nm}_s"].astype(f) + st[f"c2_{nm}_c"].astype(f)], axis=1)
+        pair = lambda nm, comp: np.stack([st[f"c1_{nm}_{comp}"], st[f"c2_{nm}_{comp}"]], axis=1).astype(f, copy=False)  # noqa
+        tot = lambda nm: np.stack([st[f"c1_{nm}_s"].astype(f, copy=False) + st[f"c1_{nm}_c"].astype(f, copy=False),  # noqa
+                                   st[f"c2_{nm}_s"].astype(f, copy=False) + st[f"c2_{nm}_c"].astype(f, copy=False)], axis=1)
         return dict(n=n, handoffs=K, Y=cols["Y"], Ybar=cols["Ybar"], Ybar20=cols["Ybar20"], sum=pair("s", "s"),
                     comp=pair("s", "c"), R1=tot("R1"), R2=tot("R2"), Q=tot("Q"), Q2=tot("Q2"))
 
@@ -365,11 +365,11 @@ class FLI(Reducer):
                     stepB=int(st["stepB"]), colB=int(st["colB"]), step1=int(st["step1"]))
 
     def finals(self, st, d=None):
-        return dict(n=st["n"].astype(np.int64), fli=st["fB"].astype(np.float64), fli1=st["f1"].astype(np.float64),
-                    sum=np.stack([st["s1_s"], st["s2_s"]], axis=1).astype(np.float64),
-                    comp=np.stack([st["s1_c"], st["s2_c"]], axis=1).astype(np.float64),
-                    stepB=st["stepB"].astype(np.int64), colB=st["colB"].astype(np.int64),
-                    step1=st["step1"].astype(np.int64))
+        return dict(n=st["n"].astype(np.int64, copy=False), fli=st["fB"].astype(np.float64, copy=False), fli1=st["f1"].astype(np.float64, copy=False),
+                    sum=np.stack([st["s1_s"], st["s2_s"]], axis=1).astype(np.float64, copy=False),
+                    comp=np.stack([st["s1_c"], st["s2_c"]], axis=1).astype(np.float64, copy=False),
+                    stepB=st["stepB"].astype(np.int64, copy=False), colB=st["colB"].astype(np.int64, copy=False),
+                    step1=st["step1"].astype(np.int64, copy=False))
 
     def error(self, st, orbit, backend):
         v = float(st["value"])
