@@ -937,15 +937,14 @@ static int encode_x_map(CUtensorMap* m, const void* X, int32_t B) {
     using Encode = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
                                 const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
                                 CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
-    static Encode enc = nullptr;
-    if (!enc) {
+    // looked up once per process (a function-local static: thread-safe initialisation); null if unavailable
+    static const Encode enc = []() -> Encode {
         void* fn = nullptr;
         cudaDriverEntryPointQueryResult q;
         const cudaError_t e = cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q);
-        if (e != cudaSuccess || q != cudaDriverEntryPointSuccess || !fn)
-            return cl::capi_fail(CL_EUNSUPPORTED, "fused forward: cuTensorMapEncodeTiled unavailable");
-        enc = reinterpret_cast<Encode>(fn);
-    }
+        return (e == cudaSuccess && q == cudaDriverEntryPointSuccess) ? reinterpret_cast<Encode>(fn) : nullptr;
+    }();
+    if (!enc) return cl::capi_fail(CL_EUNSUPPORTED, "fused forward: cuTensorMapEncodeTiled unavailable");
     const cuuint64_t dims[2] = {64, static_cast<cuuint64_t>(B)};
     const cuuint64_t strides[1] = {128};
     const cuuint32_t box[2] = {8, 128};
