@@ -187,7 +187,8 @@ def main() -> None:
     ap.add_argument("--only", choices=["fp64", "mixed", "mixed-ind64"], default=None,
                     help="time one kernel of the default workload and print a short line (a small case for ncu)")
     ap.add_argument("--workload", default="coupled", choices=["coupled", "standard", "gauss", "lattice", "screen", "mlp", "split", "shadow",
-                                                             "record", "indicators", "advance", "torus", "record_mixed"])
+                                                             "record", "indicators", "advance", "torus", "record_mixed",
+                                                             "coop"])
     args = ap.parse_args()
     if args.workload != "coupled":
         run_workload(args)
@@ -1035,11 +1036,57 @@ def workload_torus(args):
                              tau=TAU, W0="I"))
 
 
+def workload_coop(args):
+    """`propagate` on a lattice of 8 sites (StandardMapChain, d = 16, k = 8, tau = 10, Float64) through the public
+    call: one thread per orbit (variant 1) against one orbit per group of 8 lanes (the cooperative form, variant 8),
+    for QRSpectrum(HouseholderQR), QRSpectrum(MGS) and GALI, with the records compared bit for bit. The headline value
+    is the cooperative Householder run's orbit-steps/s."""
+    torch, dev, L = _setup()
+    from chaos_b200 import GALI, MGS, HouseholderQR, QRSpectrum, StandardMapChain
+    from chaos_b200.propagate import FrameSpec, build_run, propagate_frames
+    n = args.orbits or 2048
+    N, tau, d, k = 20000, 10, 16, 8
+    sysm = StandardMapChain(8, 1.2, 0.05)
+    x0 = np.random.default_rng(SEED).uniform(0, 2 * np.pi, (n, d))
+    W0 = np.ascontiguousarray(np.broadcast_to(np.eye(d)[:, :k], (n, d, k)))
+    rows, first = {}, None
+    for name, chain in (("householder", (QRSpectrum(HouseholderQR()),)), ("mgs", (QRSpectrum(MGS()),)),
+                        ("gali", (GALI(),))):
+        fr = FrameSpec(k, chain, W0)
+        r = build_run(sysm, N, tau, [fr], "fp64", SEED)
+        res = {}
+        for v in (1, 8):
+            L.cl_b200_set_variant(C.byref(r), v)
+            out = propagate_frames(sysm, x0, N, [fr], tau=tau, seed=SEED, finals=False, throw=False)[0]
+            ms = []
+            for _ in range(max(1, args.steps)):
+                t0 = time.perf_counter()
+                out = propagate_frames(sysm, x0, N, [fr], tau=tau, seed=SEED, finals=False, throw=False)[0]
+                ms.append((time.perf_counter() - t0) * 1e3)
+            res[v] = (float(np.median(ms)), out, ms)
+        L.cl_b200_set_variant(C.byref(r), 0)
+        same = bool(np.array_equal(res[1][1].x.view(np.int64), res[8][1].x.view(np.int64)) and
+                    np.array_equal(res[1][1].W.view(np.int64), res[8][1].W.view(np.int64)) and
+                    res[1][1].states.tobytes() == res[8][1].states.tobytes())
+        rows[name] = dict(one_thread=n * N / (res[1][0] / 1e3), cooperative=n * N / (res[8][0] / 1e3),
+                          speedup=res[1][0] / res[8][0], bitwise_equal=same)
+        if first is None:
+            first = res[8][2]
+    _line("orbit-steps/s (propagate, StandardMapChain 8 sites d=16 k=8, cooperative lane groups, Float64, host buffers)",
+          rows["householder"]["cooperative"], "orbit-steps/s", args, first,
+          dict(workload=f"lattice-propagate-d16k8-{n}x{N}-tau{tau}", orbits=n, N=N, tau=tau),
+          dtype="f64", per_chain=rows,
+          e2e=dict(value=rows["householder"]["cooperative"], unit="orbit-steps/s",
+                   h2d_bytes_per_step=int(x0.nbytes + W0.nbytes), d2h_bytes_per_step=int(x0.nbytes + W0.nbytes)),
+          gpu_launches=1)
+
+
 def run_workload(args):
     {"standard": workload_standard, "gauss": workload_gauss, "lattice": workload_lattice,
      "screen": workload_screen, "mlp": workload_mlp, "split": workload_split, "shadow": workload_shadow,
      "record": workload_record, "indicators": workload_indicators, "advance": workload_advance,
-     "torus": workload_torus, "record_mixed": lambda a: workload_record(a, "mixed")}[args.workload](args)
+     "torus": workload_torus, "record_mixed": lambda a: workload_record(a, "mixed"),
+     "coop": workload_coop}[args.workload](args)
 
 
 
