@@ -153,3 +153,19 @@ def test_variant_pinning_on_the_host():
     mask = lb.cl_b200_variants(C.byref(s))
     assert mask != 0 and lb.cl_b200_set_variant(C.byref(s), 1 + int(np.log2(mask & -mask))) == 0
     lb.cl_b200_set_variant(C.byref(s), 0)
+
+
+def test_lattice_instances_offer_the_cooperative_variant():
+    """Lattices with d >= 8 and one frame have the one-thread kernel (variant 1) and the cooperative form (variant
+    8); d = 4 lattices and two-frame runs have no cooperative form."""
+    from chaos_b200 import GALI, MGS, FrameSpec as FS, HouseholderQR, QRSpectrum, StandardMapChain
+    from chaos_b200.propagate import build_run
+    lb = lib()
+    for sites in (4, 5, 8):
+        for chain in ((QRSpectrum(HouseholderQR()),), (QRSpectrum(MGS()),), (GALI(),)):
+            for prec in ("fp64", "mixed"):
+                r = build_run(StandardMapChain(sites, 1.0, 0.05), 10, 1, [FS(8, chain)], prec, 0)
+                assert lb.cl_b200_variants(C.byref(r)) == (1 | 1 << 7)
+    r = build_run(StandardMapChain(2, 1.0, 0.05), 10, 1, [FS(4, (QRSpectrum(MGS()),))], "fp64", 0)
+    assert lb.cl_b200_variants(C.byref(r)) == 1
+    assert lb.cl_b200_set_variant(C.byref(r), 8) == _abi.EINVAL
