@@ -71,7 +71,7 @@ __device__ __forceinline__ void sincos_of(const Reduced& w, double* sn, double* 
     // the quadrant's signs as sign-bit flips: sin negative in quadrants 2, 3; cos in 1, 2
     const long long fs = static_cast<long long>(w.q & 2) << 62, fc = static_cast<long long>((w.q + 1) & 2) << 62;
     const double sv = __longlong_as_double(__double_as_longlong(a) ^ fs);
-    *sn = w.x == 0.0 ? w.x : sv;
+    *sn = (__double_as_longlong(w.x) << 1) == 0 ? w.x : sv;   // x = +-0, tested on the bits (the ALU, not the FP64 pipe)
     *cs = __longlong_as_double(__double_as_longlong(b) ^ fc);
 }
 
