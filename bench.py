@@ -225,7 +225,9 @@ def main() -> None:
 
     if world > 1:
         torch.cuda.set_device(local)
-        dist.init_process_group("nccl", device_id=torch.device("cuda", local))
+        import datetime
+        # a short timeout: a rank that waits for a lost peer ends with an error instead of hanging
+        dist.init_process_group("nccl", device_id=torch.device("cuda", local), timeout=datetime.timedelta(seconds=180))
     dev = torch.device("cuda", local if world > 1 else 0)
     torch.cuda.set_device(dev)
 
