@@ -129,6 +129,39 @@ class MLP:
                                         out.data_ptr(), int(max_ctas), self.stream()), "fused forward")
         return out
 
+    def forward_fused_host(self, Xh, out_h, chunk_rows: int = 65536):
+        """Inference from and to host memory: Xh (B, 64) BF16 and out_h (B, 16) FP32, pinned CPU tensors. The rows go
+        in chunks over two streams, so the copies of one chunk (host to device, then the outputs back) overlap the
+        fused pass over the other; the outputs are those of `forward_fused`, bit for bit. Returns out_h once the
+        current stream has them (synchronise it before reading)."""
+        if self.dims != DIMS:
+            raise ValueError("the fused pass is built for the screen network's shape 64-256-256-256-16")
+        t, L = self.t, _declare(lib())
+        B = Xh.shape[0]
+        P = self.packed()
+        pp = [p.data_ptr() for p in P] + [lay["b"].data_ptr() for lay in self.layers]
+        cur = t.cuda.current_stream(self.dev)
+        streams = [t.cuda.Stream(self.dev) for _ in range(2)]
+        rows = min(chunk_rows, max(B, 1))
+        bufs = [(t.empty((rows, 64), dtype=t.bfloat16, device=self.dev),
+                 t.empty((rows, OUT_PAD), dtype=t.float32, device=self.dev)) for _ in streams]
+        for s_, (xd, od) in zip(streams, bufs):
+            s_.wait_stream(cur)             # the weights and inputs the caller enqueued before
+            xd.record_stream(s_)
+            od.record_stream(s_)
+        for i, lo in enumerate(range(0, B, rows)):
+            s_ = streams[i % 2]
+            xd, od = bufs[i % 2]
+            n = min(B, lo + rows) - lo
+            with t.cuda.stream(s_):
+                xd[:n].copy_(Xh[lo:lo + n], non_blocking=True)
+                _ck(L.cl_b200_mlp_forward_fused(xd.data_ptr(), n, *pp, od.data_ptr(), 0, s_.cuda_stream),
+                    "fused forward")
+                out_h[lo:lo + n].copy_(od[:n], non_blocking=True)
+        for s_ in streams:
+            cur.wait_stream(s_)
+        return out_h
+
     def weights_numpy(self):
         return [(l["W"].cpu().numpy().copy(), l["b"].cpu().numpy().copy()) for l in self.layers]
 

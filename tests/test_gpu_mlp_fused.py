@@ -121,3 +121,19 @@ def test_fused_rejects_bad_arguments(torch_dev):
                                        None) != 0
     assert L.cl_b200_mlp_forward_fused(X.data_ptr(), 0, *[p.data_ptr() for p in P], *b, out.data_ptr(), 0, None) != 0
     assert L.cl_b200_launch_count() == before
+
+
+def test_fused_from_host_memory(torch_dev):
+    """The host-data call (chunks over two streams, copies overlapping the passes) gives the device pass's outputs bit
+    for bit, with a ragged last chunk."""
+    torch, dev = torch_dev
+    net = _net(torch, dev, 9)
+    rng = np.random.default_rng(6)
+    B = 3 * 4096 + 777
+    X = torch.tensor(rng.standard_normal((B, 64)).astype(np.float32), device=dev).to(torch.bfloat16)
+    want = net.forward_fused(X)
+    Xh = X.cpu().pin_memory()
+    oh = torch.full((B, 16), 7.0, dtype=torch.float32).pin_memory()
+    net.forward_fused_host(Xh, oh, chunk_rows=4096)
+    torch.cuda.synchronize(dev)
+    assert torch.equal(oh, want.cpu())
