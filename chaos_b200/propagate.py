@@ -258,6 +258,19 @@ def propagate_frames(sys: System, x0, N: int, frames: list[FrameSpec], *, tau: i
             if e is not None:
                 raise e
     results = []
+    # the frames' vectorised finals, on host threads when there are several frames of many orbits (numpy releases
+    # the interpreter lock in the column arithmetic)
+    fins: list = [None] * len(frames)
+    todo = [f for f, fr in enumerate(frames) if finals and states[f] is not None]
+    if len(todo) > 1 and n >= 8192:
+        from concurrent.futures import ThreadPoolExecutor
+        with ThreadPoolExecutor(max_workers=len(todo)) as ex:
+            futs = {f: ex.submit(Finals, tuple(frames[f].reducers), states[f], d) for f in todo}
+            for f, fu in futs.items():
+                fins[f] = fu.result()
+    else:
+        for f in todo:
+            fins[f] = Finals(tuple(frames[f].reducers), states[f], d)
     for f, fr in enumerate(frames):
         prov = dict(backend="gpu", device=prov_dev.device.decode(), backend_fallback_reason="",
                     precision=PRECISION_LABELS[precision],
@@ -268,10 +281,8 @@ def propagate_frames(sys: System, x0, N: int, frames: list[FrameSpec], *, tau: i
         for r in fr.reducers:
             prov.update(r.provenance())
         W = Wout[f].transpose(0, 2, 1)
-        fin = None
-        if finals and states[f] is not None:
-            fin = Finals(tuple(fr.reducers), states[f], d)
-        elif finals:
+        fin = fins[f]
+        if finals and states[f] is None:
             fin = [() for _ in range(n)]
         results.append(PropagationResult(x=x, W=W, finals=fin, provenance=prov, states=states[f], code=codes[f],
                                          hstep=hsteps[f], reducers=tuple(fr.reducers)))
