@@ -107,3 +107,32 @@ def test_record_mixed(name):
     ok = (a.code == 0) & (b.code == 0)
     assert ok.mean() > 0.99
     assert np.max(np.abs(a.R[ok][:, :, :2] - b.R[ok][:, :, :2])) <= 1e-3
+
+
+@pytest.mark.parametrize("name", ["standard", "wrapped"])
+def test_record_to_run_store(oracle, tmp_path, name):
+    """The device record of a chunk (some orbits failing) through the run store: the orbit records built from it
+    equal, bit for bit, those built from the oracle's record, and the chunk file reads back bit for bit."""
+    from types import SimpleNamespace
+
+    from chaos_b200 import run_store as RS
+    sys, x0 = _system(name)
+    x = x0[:24].copy()
+    x[3, 0] = np.nan
+    grid = [5, 20, 100, 200]
+    est = QRSpectrum(MGS())
+    dev = record(sys, x, 200, 5, est, grid)
+    ref = oracle.oracle_record(sys, x, 200, 5, est, grid)
+    tol = {"det_residual_tol": 16.0, "pairing_residual_tol": 16.0, "orthogonality_tol": 16.0}
+    items = [{"orbit": i + 1, "system": name, "param": "6.0", "x0": "x", "p0": "p", "design_class": "chaotic",
+              "orbit_seed": str(i), "hash": "h%d" % i, "method": "L4", "horizon": 200, "tau": 5, "vectors": 2,
+              "coordinate_mode": "wrapped" if name == "wrapped" else "lifted"} for i in range(len(x))]
+    a = RS.orbit_records(dev, items, tol)
+    b = RS.orbit_records(SimpleNamespace(R=ref["R"], grid=np.asarray(grid), fail=ref["fail"], k=2,
+                                         states=ref["states"], code=ref["code"], hstep=ref["hstep"]), items, tol)
+    assert all(RS.same_orbit(u, v) for u, v in zip(a, b))
+    assert np.all(np.isnan(a[3].state)) and a[3].t.sum() == 0
+    p = str(tmp_path / "chunk-00001.h5")
+    RS.write_chunk(p, {"schema_version": 2, "backend": "gpu", "method": "L4"}, a)
+    back = RS.read_chunk(p)
+    assert back.attrs["complete"] is True and all(RS.same_orbit(u, v) for u, v in zip(a, back.orbits))
