@@ -9,15 +9,13 @@
 // library until the process exits.
 //
 // In host code `g_queue_heads` names a host-side stand-in, not the device array, so a kernel is never handed the
-// symbol itself: once per device, with that device current, the first call asks the runtime for the array's device
-// address (cudaGetSymbolAddress) and keeps it; every call passes that address to the kernels. That first call on
-// a device should come before any stream capture. Every call shares the array and clears the heads it uses
-// (cudaMemsetAsync, on the caller's stream) before its launches; calls that overlap on the GPU race on it. A call
-// whose classes are rejected enqueues nothing. The address is kept for the life of the process, so the device must
-// not be reset (cudaDeviceReset, or a reset of its primary context) between calls.
+// symbol itself: every call asks the runtime for the array's device address in the current context
+// (cudaGetSymbolAddress, a lookup that allocates nothing and is allowed during stream capture) and passes it to the
+// kernels, so a reset of the device or its primary context between calls leaves no stale address. Every call shares
+// the array and clears the heads it uses (cudaMemsetAsync, on the caller's stream) before its launches; calls that
+// overlap on the GPU race on it. A call whose classes are rejected enqueues nothing.
 #include <cuda_runtime.h>
 
-#include <mutex>
 #include <string>
 
 #include "../../include/chaoslab_b200.h"
@@ -34,24 +32,13 @@ namespace {
 
 static __device__ __align__(256) unsigned long long g_queue_heads[CL_NOALLOC_MAX_CLASSES];
 
-constexpr int kMaxDevices = 64;
-std::mutex g_mu;
-unsigned long long* g_heads[kMaxDevices] = {};
-
-// The device address of g_queue_heads on the current device, looked up once per device.
+// The device address of g_queue_heads in the current context, looked up on every call (a lookup, no allocation):
+// a cached address would go stale when the context is reset and the module reloaded.
 int heads_on_current_device(unsigned long long** out) {
-    int dev = 0;
-    cudaError_t e = cudaGetDevice(&dev);
-    if (e != cudaSuccess) return capi_map_cuda(e, "current device");
-    if (dev < 0 || dev >= kMaxDevices) return capi_fail(CL_EINVAL, "device index beyond the set-up table");
-    std::lock_guard<std::mutex> g(g_mu);
-    if (!g_heads[dev]) {
-        void* p = nullptr;
-        e = cudaGetSymbolAddress(&p, g_queue_heads);
-        if (e != cudaSuccess) return capi_map_cuda(e, "address of the fixed queue heads");
-        g_heads[dev] = static_cast<unsigned long long*>(p);
-    }
-    *out = g_heads[dev];
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_queue_heads);
+    if (e != cudaSuccess) return capi_map_cuda(e, "address of the fixed queue heads");
+    *out = static_cast<unsigned long long*>(p);
     return 0;
 }
 

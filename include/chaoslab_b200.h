@@ -26,7 +26,9 @@
  * (src/Foundation/Foundation.jl:71-75): -2 no functional device (reason 2), -3 kernel not built for this system /
  * chain / precision (reason 3), -4 device out of memory (reason 4), -9 device lost or a bounded device wait
  * timed out (reason 9); -1 is an invalid argument (the reference throws ArgumentError before any work).
- * Per-orbit numerical failures are not call errors: they come back in code / hstep / states.
+ * Per-orbit numerical failures are not call errors: they come back in code / hstep / states. After a non-zero
+ * return the contents of the output arrays (x, W, states, code, hstep and the in/out arrays among them) are
+ * unspecified: a failure that surfaces at the final synchronisation can come after their copies began.
  */
 #ifndef CHAOSLAB_B200_H
 #define CHAOSLAB_B200_H
@@ -281,10 +283,10 @@ CL_API int cl_b200_ensemble_device(const cl_ensemble_class* classes, int32_t n_c
  * whose own allocator owns the device heap, a plugin host that forbids allocation calls, a latency-bound loop).
  * No counterpart in the reference. The classes run one after another on `stream`; their queue heads live in a
  * fixed array inside the library, CL_NOALLOC_MAX_CLASSES heads (512 bytes) held on every GPU that loads the
- * library until exit, and more classes than that are rejected with CL_EINVAL. The first call on a device looks
- * the array's device address up (make it before any stream capture) and keeps it for the life of the process, so
- * the device must not be reset between calls; each call clears the heads it uses on `stream`, and a call whose
- * classes are rejected enqueues nothing; calls that overlap on the GPU race on the shared array. */
+ * library until exit, and more classes than that are rejected with CL_EINVAL. Every call looks the array's device
+ * address up in the current context (no allocation; allowed during stream capture, so a call can be captured into
+ * a CUDA graph of memset and kernel nodes), clears the heads it uses on `stream`, and a call whose classes are
+ * rejected enqueues nothing; calls that overlap on the GPU race on the shared array. */
 #define CL_NOALLOC_MAX_CLASSES 64
 CL_API int cl_b200_ensemble_device_noalloc(const cl_ensemble_class* classes, int32_t n_classes, void* stream);
 

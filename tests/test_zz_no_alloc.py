@@ -98,3 +98,51 @@ def test_noalloc_rejects_too_many_classes():
     arr = (_abi.cl_ensemble_class * (_abi.NOALLOC_MAX_CLASSES + 1))()
     rc = L.cl_b200_ensemble_device_noalloc(arr, _abi.NOALLOC_MAX_CLASSES + 1, None)
     assert rc == _abi.EINVAL and "at most 64 classes" in last_error()
+
+
+def test_noalloc_captures_into_a_graph_of_memsets_and_kernels():
+    """The call captured on a stream in global capture mode (where an allocation call from any thread would end the
+    capture with an error) gives a graph whose nodes are memsets and kernels only -- no allocation node -- and the
+    graph, replayed, gives the allocating entry point's bits."""
+    torch = pytest.importorskip("torch")
+    rt = pytest.importorskip("cuda.bindings.runtime")
+    dev = torch.device("cuda", 0)
+    L = lib()
+    classes = _classes()
+    arr, outs, keep = _on_device(classes, torch, dev)
+    assert L.cl_b200_ensemble_device(arr, len(classes), C.c_void_p(torch.cuda.current_stream(dev).cuda_stream)) == 0
+    torch.cuda.synchronize(dev)
+    want = _records(outs)
+
+    arr2, outs2, keep2 = _on_device(classes, torch, dev)
+    torch.cuda.synchronize(dev)
+    err, s = rt.cudaStreamCreate()
+    assert err == rt.cudaError_t.cudaSuccess
+    graph = gexec = None
+    try:
+        err, = rt.cudaStreamBeginCapture(s, rt.cudaStreamCaptureMode.cudaStreamCaptureModeGlobal)
+        assert err == rt.cudaError_t.cudaSuccess
+        rc = L.cl_b200_ensemble_device_noalloc(arr2, len(classes), C.c_void_p(int(s)))
+        err, graph = rt.cudaStreamEndCapture(s)
+        assert rc == 0, last_error()
+        assert err == rt.cudaError_t.cudaSuccess
+        err, _, count = rt.cudaGraphGetNodes(graph, 0)
+        err, nodes, count = rt.cudaGraphGetNodes(graph, count)
+        assert err == rt.cudaError_t.cudaSuccess and count >= 2
+        kinds = {rt.cudaGraphNodeGetType(nd)[1] for nd in nodes[:count]}
+        assert kinds <= {rt.cudaGraphNodeType.cudaGraphNodeTypeKernel, rt.cudaGraphNodeType.cudaGraphNodeTypeMemset}, kinds
+        assert rt.cudaGraphNodeType.cudaGraphNodeTypeKernel in kinds
+        err, gexec = rt.cudaGraphInstantiate(graph, 0)
+        assert err == rt.cudaError_t.cudaSuccess
+        assert rt.cudaGraphLaunch(gexec, s)[0] == rt.cudaError_t.cudaSuccess
+        assert rt.cudaStreamSynchronize(s)[0] == rt.cudaError_t.cudaSuccess
+    finally:
+        if gexec is not None:
+            rt.cudaGraphExecDestroy(gexec)
+        if graph is not None:
+            rt.cudaGraphDestroy(graph)
+        rt.cudaStreamDestroy(s)
+    got = _records(outs2)
+    for w, g in zip(want, got):
+        for k in w:
+            assert np.array_equal(w[k].view(np.uint8), g[k].view(np.uint8)), k
