@@ -82,16 +82,14 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t phase) {
 }
 
 // The network's activation: GELU in its tanh form (Hendrycks & Gimpel 2016), x (1 + tanh u) / 2 with
-// u = sqrt(2 / pi) (x + 0.044715 x^3). Since (1 + tanh u) / 2 = 1 / (1 + e^(-2u)), it is evaluated without the
-// cancellation of 1 + tanh u for negative x as x s, s = 1 / (1 + 2^z), z = -2 log2(e) u = x (G0 + G1 x^2) clamped
-// to 64 (beyond it s < 6e-20): one ex2 on the special-function unit, and the reciprocal on the FMA pipe from the
-// seed bits(r0) = 0x7EF311C2 - bits(d), whose relative error is at most 0.0505 for every normal d (the constant
+// u = sqrt(2 / pi) (x + 0.044715 x^3). The forward pass (gelu_t, below) uses the special-function unit's tanh. The
+// backward pass needs s = (1 + tanh u) / 2 = 1 / (1 + e^(-2u)) with its derivative, evaluated without the
+// cancellation of 1 + tanh u for negative x as s = 1 / (1 + 2^z), z = -2 log2(e) u = x (G0 + G1 x^2) clamped to 64
+// (beyond it s < 6e-20): one ex2 on the special-function unit, and the reciprocal on the FMA pipe from the seed
+// bits(r0) = 0x7EF311C2 - bits(d), whose relative error is at most 0.0505 for every normal d (the constant
 // minimises it over all mantissas; found by exhaustive search), refined by one Newton step r <- r + r t (error
 // squared: 2.6e-3) and one third-order step r <- r + r (t + t^2) (error cubed: 1.7e-8), t = 1 - d r (run on -r,
-// below, which costs one multiply fewer a pair); s is within
-// 1.3 units in the last place (checked over 2e6 arguments). The pair form runs the same operations lane by lane on
-// packed FP32 pairs (fma/mul/add .f32x2), so the scalar form (the per-layer epilogue) and the pair form (the fused
-// pass) agree bit for bit.
+// below); s is within 1.3 units in the last place (checked over 2e6 arguments).
 constexpr float kG0 = -2.3022082f;     // -2 log2(e) sqrt(2 / pi)
 constexpr float kG1 = -0.10294324f;    // kG0 * 0.044715
 constexpr float kLn2 = 0.6931472f;
@@ -114,7 +112,23 @@ __device__ __forceinline__ float negsig_t(float x) {
     return __fmaf_rn(w, __fmaf_rn(t, t, t), w);
 }
 __device__ __forceinline__ float sig_t(float x) { return -negsig_t(x); }
-__device__ __forceinline__ float gelu_t(float x) { return -__fmul_rn(x, negsig_t(x)); }   // = x s exactly
+// The forward activation: (x / 2)(1 + tanh u), u = x (T0 + T1 x^2), with the special-function unit's tanh
+// (tanh.approx.f32, relative error at most 2^-10.99): one special-function operation and four FP32 operations a
+// value. Where tanh u is near -1 (x below about -2) the sum 1 + tanh u loses relative accuracy, but its absolute
+// error stays below |x| 2^-12 (under 1e-3 for x > -4, and the value is ~0 beyond), smaller than the BF16 rounding
+// of the activations the next layer adds it to.
+constexpr float kT0 = 0.7978845608f;    // sqrt(2 / pi)
+constexpr float kT1 = 0.0356774081f;    // sqrt(2 / pi) * 0.044715
+__device__ __forceinline__ float tanh_approx(float u) {
+    float t;
+    asm("tanh.approx.f32 %0, %1;" : "=f"(t) : "f"(u));
+    return t;
+}
+__device__ __forceinline__ float gelu_t(float x) {
+    const float u = __fmul_rn(x, __fmaf_rn(kT1, __fmul_rn(x, x), kT0));
+    const float h = __fmul_rn(x, 0.5f);
+    return __fmaf_rn(h, tanh_approx(u), h);
+}
 
 // Packed FP32 pairs (the .f32x2 forms; lane by lane the same IEEE operations as the scalar ones).
 __device__ __forceinline__ uint64_t f2(float a, float b) {
@@ -140,25 +154,20 @@ __device__ __forceinline__ uint64_t add2(uint64_t a, uint64_t b) {
     asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
     return d;
 }
-// gelu_t of both lanes of v, rounded to a BF16 pair (low half: lane 0): the pair form of negsig_t, then v w = -(v s)
-// rounded to BF16 and both signs flipped (rounding to nearest is symmetric, so the bits are those of v s).
+// gelu_t of both lanes of v, rounded to a BF16 pair (low half: lane 0): the same operations lane by lane on packed
+// FP32 pairs (fma/mul .f32x2), so the scalar form (the per-layer epilogue) and this one agree bit for bit.
 __device__ __forceinline__ uint32_t gelu_t2_bf16(uint64_t v) {
-    const uint64_t g1 = f2(kG1, kG1), g0 = f2(kG0, kG0), one = f2(1.0f, 1.0f);
-    float z0, z1;
-    f2split(mul2(v, fma2(g1, mul2(v, v), g0)), z0, z1);
-    const uint64_t d = add2(one, f2(ex2_approx(fminf(z0, kZMax)), ex2_approx(fminf(z1, kZMax))));
-    float d0, d1;
-    f2split(d, d0, d1);
-    uint64_t w = f2(__uint_as_float(kRcpSeedNeg - __float_as_uint(d0)), __uint_as_float(kRcpSeedNeg - __float_as_uint(d1)));
-    w = fma2(w, fma2(d, w, one), w);
-    const uint64_t t = fma2(d, w, one);
-    w = fma2(w, fma2(t, t, t), w);
+    const uint64_t t1 = f2(kT1, kT1), t0 = f2(kT0, kT0), half = f2(0.5f, 0.5f);
+    float u0, u1;
+    f2split(mul2(v, fma2(t1, mul2(v, v), t0)), u0, u1);
+    const uint64_t h = mul2(v, half);
     float y0, y1;
-    f2split(mul2(v, w), y0, y1);
-    const __nv_bfloat162 h = __floats2bfloat162_rn(y0, y1);
-    return *reinterpret_cast<const uint32_t*>(&h) ^ 0x80008000u;
+    f2split(fma2(h, f2(tanh_approx(u0), tanh_approx(u1)), h), y0, y1);
+    const __nv_bfloat162 b = __floats2bfloat162_rn(y0, y1);
+    return *reinterpret_cast<const uint32_t*>(&b);
 }
-// d/dx of gelu_t: s - x s (1 - s) ln2 (G0 + 3 G1 x^2).
+// d/dx of the tanh-form GELU, s - x s (1 - s) ln2 (G0 + 3 G1 x^2) with s = 1 / (1 + 2^z) (the training's
+// backward pass; the forward's tanh.approx differs from s by its rounding only).
 __device__ __forceinline__ float gelu_t_grad(float x) {
     const float sg = sig_t(x);
     const float dz = __fmaf_rn(3.0f * kG1, __fmul_rn(x, x), kG0);

@@ -438,8 +438,8 @@ CL_API int cl_b200_indicator_pair(const cl_run* run, int64_t n, int32_t ns, doub
  * All enqueue on `stream` and take device pointers. BF16 matrices are row-major with 16-byte aligned rows. */
 
 /* C[M x N] = A[M x K] . B[N x K]^T on the tcgen05 tensor cores (BF16 operands, FP32 accumulator in tensor memory),
- * + bias[N] (NULL: none), epilogue 0 none / 1 GELU (tanh form, x / (1 + 2^z) with z = -2 log2(e) sqrt(2/pi)
- * (x + 0.044715 x^3)); C32 (FP32) and/or Cbf16 written with row stride ldc;
+ * + bias[N] (NULL: none), epilogue 0 none / 1 GELU (tanh form, (x / 2)(1 + tanh u), u = sqrt(2/pi)
+ * (x + 0.044715 x^3), tanh by the special-function unit); C32 (FP32) and/or Cbf16 written with row stride ldc;
  * pre (FP32, NULL: none) receives the value before the epilogue; accumulate adds the old C32. */
 CL_API int cl_b200_gemm_bf16(const void* A, int32_t lda, const void* B, int32_t ldb, int32_t M, int32_t N, int32_t K,
                              const float* bias, int32_t epilogue, float* C32, void* Cbf16, int32_t ldc, float* pre,
