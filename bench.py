@@ -78,24 +78,29 @@ HEADLINE = "mixed-ind64"
 #   map: x' = x + p (2), x1' + x2' (1), _abc (5), forward (8) and the force sums (4): 20 flops + 3 sin + 3 cos
 #   tangent products: 2 d^2 k = 128 per frame
 #   per handoff: Householder QR 4 d k^2 = 256; window_Gw 2 k^3 / 3 + 2 k^2 = 74; orth_loss (the k (k + 1) / 2
-#   distinct dots of Q'Q) 2 d k (k + 1) / 2 = 80; GALI: column norms 2 d k, unit columns d k, the twice-orthogonalised
-#   Gram-Schmidt 2 sum_j j 4 d = 192, the nested norms 2 d k and scaling d k, the k - 1 products: 307; SALI 3 d 2 = 24;
-#   k + k logs with a Neumaier add (4 flops) each: 32 (Float64 in both kernels)
-def flops_per_orbit_step(tau: int = TAU, precision: str = "fp64") -> dict:
+#   distinct dots of Q'Q) 2 d k (k + 1) / 2 = 80; GALI: column norms 2 d k and unit columns d k = 48 (these decide
+#   the stop and carry the frame); k + k logs with a Neumaier add (4 flops) each: 32 (Float64 in both kernels)
+#   once per run: GALI's values, the twice-orthogonalised Gram-Schmidt 2 sum_j j 4 d = 192, the nested norms 2 d k
+#   and scaling d k, the k - 1 products, and SALI 3 d 2 = 24: 267. A handoff's values are overwritten by the next
+#   one and read only after the last (gali.jl:156, sali.jl:108), so the algorithm needs them once; the mixed kernel
+#   forms them once a launch, the Float64 kernel (the reference's loop, bit for bit) at every handoff
+def flops_per_orbit_step(tau: int = TAU, precision: str = "fp64", n_steps: int = N_STEPS) -> dict:
     d, k = 4, 4
     map_flops, trig = 20, 6
     product = 2 * d * d * k
     qr = 4 * d * k * k + (2 * k ** 3 // 3 + 2 * k * k) + d * k * (k + 1)        # Householder, window_Gw, orth_loss
-    gali = 2 * d * k + d * k + 2 * sum(j * 4 * d for j in range(k)) + 2 * d * k + d * k + (k - 1) + 6 * d   # + SALI
+    gali = 2 * d * k + d * k                                                      # norms and unit columns
+    values = 2 * sum(j * 4 * d for j in range(k)) + 2 * d * k + d * k + (k - 1) + 6 * d   # GALI's values + SALI
     logsum = k * 4                                                                # per frame: k Neumaier adds
-    out = dict(trig_fp64=trig, trig_fp32=0.0, log=2 * k / tau, handoff_flops=qr + gali + 2 * logsum)
+    out = dict(trig_fp64=trig, trig_fp32=0.0, log=2 * k / tau, handoff_flops=qr + gali + 2 * logsum,
+               values_flops_per_run=values)
     if precision == "mixed":   # both frames Float32; the orbit, its trigonometry and the log sums Float64
-        out.update(fp64=map_flops + 2 * logsum / tau, fp32=2 * product + (qr + gali) / tau, trig_fp64=trig / 2,
-                   trig_fp32=trig / 2)
+        out.update(fp64=map_flops + 2 * logsum / tau, fp32=2 * product + (qr + gali) / tau + values / n_steps,
+                   trig_fp64=trig / 2, trig_fp32=trig / 2)
     elif precision == "mixed-ind64":   # the QR frame Float32; the orbit and the GALI / SALI frame Float64
-        out.update(fp64=map_flops + product + (gali + 2 * logsum) / tau, fp32=product + qr / tau)
+        out.update(fp64=map_flops + product + (gali + 2 * logsum) / tau + values / n_steps, fp32=product + qr / tau)
     else:
-        out.update(fp64=map_flops + 2 * product + (qr + gali + 2 * logsum) / tau, fp32=0.0)
+        out.update(fp64=map_flops + 2 * product + (qr + gali + 2 * logsum) / tau + values / n_steps, fp32=0.0)
     return out
 
 

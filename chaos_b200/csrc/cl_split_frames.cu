@@ -39,6 +39,12 @@ __device__ __forceinline__ void store_frame(const KArgs& a, int f, i64 i, const 
 #pragma unroll
     for (int l = 0; l < D * K; ++l) a.W_out[f][i * so + l * sc] = static_cast<double>(W[l]);
 }
+// the Float64 frame as store_frame left it in the output (the unit columns of its last successful handoff)
+__device__ __forceinline__ void load_stored64(const KArgs& a, int f, i64 i, double* W) {
+    const i64 so = a.soa ? 1 : D * K, sc = a.soa ? a.n : 1;
+#pragma unroll
+    for (int l = 0; l < D * K; ++l) W[l] = a.W_out[f][i * so + l * sc];
+}
 
 // the Float32 frame holds no non-finite entry (a NaN or infinity turns the fma chain's zero into NaN)
 __device__ __forceinline__ bool finite32(const float* W) {
@@ -107,6 +113,7 @@ __global__ void __maxnreg__(REGS) split_frames_kernel(const KArgs a, const SysFr
     }
 #pragma unroll
     for (int c = 0; c < 4; ++c) { q.lp[c] = split::LogProd{1.0, 0, 0}; g.lp[c] = split::LogProd{1.0, 0, 0}; }
+    g.pending = 0;
     bool alive0 = code0 == STATUS_OK, alive1 = code1 == STATUS_OK;
     if (!alive0 && !alive1) return;   // frozen since an earlier launch: nothing is rewritten
     const double orth_tol = a.prm[0][0].orthogonality_tol;
@@ -158,7 +165,9 @@ __global__ void __maxnreg__(REGS) split_frames_kernel(const KArgs a, const SysFr
 #pragma unroll
                 for (int l = 0; l < 16; ++l) park_w[l] = W0[l];
                 asm volatile("" ::: "memory");
-                split::gali_handoff(g, n, W1);
+                // the unit columns of a successful handoff go to the frame's output, where the values are formed
+                // from them once, after the loop (the last successful handoff's are the ones the state keeps)
+                if (split::gali_step(g, n, W1)) store_frame(a, 1, i, W1);
                 asm volatile("" ::: "memory");
 #pragma unroll
                 for (int l = 0; l < 4; ++l) x[l] = park_x[l];
@@ -178,6 +187,11 @@ __global__ void __maxnreg__(REGS) split_frames_kernel(const KArgs a, const SysFr
 #pragma unroll
     for (int c = 0; c < 4; ++c) a.x_out[i * xso + c * xsc] = x[c];
     const bool was0 = fresh || a.code[0][i] == STATUS_OK, was1 = fresh || a.code[1][i] == STATUS_OK;
+    if (g.pending) {   // GALI's and SALI's values of the last successful handoff of this launch
+        double U[16];
+        load_stored64(a, 1, i, U);
+        split::gali_values(g, U);
+    }
     if (was0) store_frame(a, 0, i, W0);
     if (was1) store_frame(a, 1, i, W1);
     // the records, one logarithm at a time (the frames are stored, so this tail needs few registers)

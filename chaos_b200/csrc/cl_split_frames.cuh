@@ -311,14 +311,22 @@ __device__ __forceinline__ void qr_handoff(QRSlot& st, i64 n, float* W, double o
 }
 
 // ---- the indicator frame: GALI_4 with SALI of its columns 1-2, Float64 ------------------------------------------
+// `pending` marks a successful handoff whose values are not yet formed (bit 0: GALI's, bit 1: SALI's; below).
 struct GSSlot {
     LogProd lp[4];
     double gali[3], gvalue, svalue, sali;
     i64 gn, gstep, gcolumn, sn, sstep;
-    int gcode, scode, scolumn, pad;
+    int gcode, scode, scolumn, pending;
 };
 
-__device__ __forceinline__ void gali_handoff(GSSlot& st, i64 n, double* W) {
+// One handoff of the indicator frame without its values: the column norms, both reducers' failure checks, the log
+// sums and the unit columns (which continue as the frame), as gali.jl:145-160 and sali.jl:100-110 run them. Of
+// what a handoff writes only the stop decision and the frame depend on the norms alone; GALI's values (the nested
+// Gram-Schmidt of the unit columns, gali.jl:156) and SALI's (min(d-, d+) of unit columns 1-2, sali.jl:108) are
+// overwritten by every later successful handoff and read only after the last one. So they are formed once, by
+// gali_values on the unit columns of the last successful handoff, bit for bit what forming them at every handoff
+// leaves in the state. Returns whether the handoff succeeded (W then holds the unit columns).
+__device__ __forceinline__ bool gali_step(GSSlot& st, i64 n, double* W) {
     double s[4], a[4], inv[4];
 #pragma unroll
     for (int j = 0; j < 4; ++j) s[j] = sumsq64<4>(W + 4 * j);
@@ -348,27 +356,37 @@ __device__ __forceinline__ void gali_handoff(GSSlot& st, i64 n, double* W) {
 #pragma unroll
         for (int j = 0; j < 4; ++j) if (j + 1 == bad) v = a[j];
         st.gvalue = v; st.gstep = n; st.gcode = 1; st.gcolumn = bad;
-        return;
+        return false;
     }
 #pragma unroll
     for (int j = 0; j < 4; ++j) lp_mul(st.lp[j], a[j]);
-    double Q[16];
 #pragma unroll
     for (int j = 0; j < 4; ++j)
 #pragma unroll
-        for (int i = 0; i < 4; ++i) { const double u = W[i + 4 * j] * inv[j]; W[i + 4 * j] = u; Q[i + 4 * j] = u; }
-    if (sali_ok) {   // sali.jl:107-110 on the unit columns 1-2
-        double dm = W[0] - W[4], dp = W[0] + W[4];
+        for (int i = 0; i < 4; ++i) W[i + 4 * j] *= inv[j];
+    if (sali_ok) st.sn = n;
+    st.gn = n;
+    st.pending = sali_ok ? 3 : 1;
+    return true;
+}
+
+// The values of the last successful handoff from its unit columns U (column-major): SALI of columns 1-2 (sali.jl:
+// 107-110) when that handoff ran SALI, and G_2..G_4 (gali.jl:81-100).
+__device__ __forceinline__ void gali_values(GSSlot& st, const double* U) {
+    if (st.pending & 2) {
+        double dm = U[0] - U[4], dp = U[0] + U[4];
         double sm = dm * dm, sp = dp * dp;
 #pragma unroll
         for (int i = 1; i < 4; ++i) {
-            dm = W[i] - W[4 + i]; dp = W[i] + W[4 + i];
+            dm = U[i] - U[4 + i]; dp = U[i] + U[4 + i];
             sm = fma(dm, dm, sm); sp = fma(dp, dp, sp);
         }
         const double m = fmin(sm, sp);
         st.sali = m > 0.0 ? m * rsq64(m) : m;
-        st.sn = n;
     }
+    double Q[16];
+#pragma unroll
+    for (int l = 0; l < 16; ++l) Q[l] = U[l];
     // _gram_core! (gali.jl:81-100): each column orthogonalised twice against the earlier (orthonormal) ones, then
     // normalised; G_k = prod_{i <= k} r_i. Each pass takes the projections on every earlier column at once (the
     // classical form, twice: the same orthogonality as the modified form for these few columns, with the dots
@@ -397,7 +415,7 @@ __device__ __forceinline__ void gali_handoff(GSSlot& st, i64 n, double* W) {
         for (int i = 0; i < 4; ++i) Q[i + 4 * j] *= ir;
         if (j > 0) { g *= r; st.gali[j - 1] = g; }
     }
-    st.gn = n;
+    st.pending = 0;
 }
 
 }  // namespace split

@@ -108,3 +108,30 @@ def test_split_failures():
     assert same_bits(a[0].x, b[0].x)
     # a failing handoff leaves the frame as it was (the factorisation runs in the frame's registers)
     assert np.allclose(b[0].W[10], a[0].W[10], rtol=1e-4, atol=1e-6) and np.all(b[0].W[10][:, 0] == 0)
+
+
+def test_split_values_of_last_successful_handoff():
+    """GALI's and SALI's values are formed once, from the unit columns of a launch's last successful handoff: orbits
+    whose state overflows at the 2nd and 5th handoff (x1 near the Float64 maximum, p1 carrying it over) stop with the
+    state status there, and keep the values of the handoff before -- the Float64 kernel's (which forms them at every
+    handoff) within the tolerances above; in one launch and in launches of one window each."""
+    n, N = 64, 400
+    x0 = uniform_starts(n, 4, seed=11)
+    x0[5] = [1e308, 0.3, 5e306, 0.1]       # x1 passes the maximum at step 16: stops at the handoff of step 20
+    x0[9] = [1e308, 0.2, 1.6e306, 0.0]     # at step 50
+    a = _run(x0, N, "fp64")
+    for kw in ({}, {"launch_steps": 10}):
+        b = _run(x0, N, "mixed-ind64", **kw)
+        for f in range(2):
+            assert np.array_equal(a[f].code, b[f].code) and np.array_equal(a[f].hstep, b[f].hstep)
+        assert int(b[1].code[5]) == 1 and int(b[1].hstep[5]) == 20
+        assert int(b[1].code[9]) == 1 and int(b[1].hstep[9]) == 50
+        ga, gb = a[1].states, b[1].states
+        assert np.array_equal(ga["r0"]["n"], gb["r0"]["n"]) and np.array_equal(ga["r1"]["n"], gb["r1"]["n"])
+        assert int(gb["r0"]["n"][5]) == 10 and int(gb["r0"]["n"][9]) == 40
+        for i in (5, 9, 0, 1):
+            va, vb = ga["r0"]["gali"][i], gb["r0"]["gali"][i]
+            assert np.all(vb > 0) and np.all(np.isfinite(vb)), (i, vb)
+            assert np.max(np.abs(np.log10(va) - np.log10(vb))) <= 0.05, (i, va, vb)
+            sa, sb = ga["r1"]["sali"][i], gb["r1"]["sali"][i]
+            assert sb > 0 and abs(np.log10(sa) - np.log10(sb)) <= 0.05, (i, sa, sb)
