@@ -61,9 +61,9 @@ TAU = 10
 NU = KAPPA = 1.5
 MU = 0.05
 SEED = 1
-# DRAM bytes per orbit of one launch of the mixed kernel (ncu capture of 32768 orbits: 5.376 MB read, 4.6 KB
-# written; the records written stay in the 126 MB L2 at that size)
-TRAFFIC_PER_ORBIT = 16474112 / 65536   # ncu DRAM read + write of split_frames_kernel, 65536 orbits x 2000 steps
+# DRAM bytes per orbit of one launch of the mixed kernel: ncu DRAM read + write of split_frames_kernel on 65536
+# orbits x 2000 steps (15.53 MB read, 1.48 MB written: the orbit, both frames and the records once in, once out)
+TRAFFIC_PER_ORBIT = 17013504 / 65536
 METRIC = "orbit-steps/s (4D coupled standard maps, QRSpectrum(Householder) + GALI_4 + SALI, mixed-precision kernel)"
 # the headline kernel: Float64 orbit and GALI / SALI frame, Float32 QRSpectrum frame (the precision every output holds)
 HEADLINE = "mixed-ind64"
@@ -418,12 +418,12 @@ def main() -> None:
             roofline=dict(bound="fp64", achieved=achieved, peak=fp64_peak, unit="TFLOP/s", frac=achieved / fp64_peak,
                           traffic=TRAFFIC_PER_ORBIT * n,
                           traffic_source="ncu dram__bytes_read + dram__bytes_write of split_frames_kernel on 65536 "
-                                         "orbits x 2000 steps (1.647e7 B), scaled by orbits: DRAM bytes grow with the "
+                                         "orbits x 2000 steps (1.701e7 B), scaled by orbits: DRAM bytes grow with the "
                                          "orbits loaded and stored, not with the steps",
                           peak_source="cuBLAS DGEMM 8192^3 measured here (burst)",
                           flops_per_orbit_step=fl,
-                          pipes_ncu=dict(fp64=0.468, fma_fp32=0.130, alu=0.210, xu_sfu=0.162, issue_active=0.607,
-                                         warps_active=0.170,
+                          pipes_ncu=dict(fp64=0.448, fma_fp32=0.140, alu=0.234, xu_sfu=0.171, issue_active=0.632,
+                                         warps_active=0.171,
                                          source="ncu --set full of split_frames_kernel, 65536 orbits x 2000 steps "
                                                 "(profiles/split_frames_kernel_froeschle_65536x2000_ncu.md)")),
             cpu_baseline=cpu, clocks=clocks, gpu_launches=int(launches),
