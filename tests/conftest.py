@@ -15,6 +15,9 @@ sys.path.insert(0, os.path.join(ROOT, "oracle"))
 
 def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a B200 (runs the CUDA kernels)")
+    # the files tests write (the run store's chunk files) stay inside the checkout, in a folder pytest clears
+    if not config.option.basetemp:
+        config.option.basetemp = os.path.join(ROOT, ".pytest_tmp")
 
 
 @pytest.fixture(scope="session")
