@@ -384,8 +384,8 @@ def main() -> None:
 
     fp64_peak = _dgemm_peak(torch, dev)
 
-    fl = flops_per_orbit_step(TAU, HEADLINE)
-    fl64 = flops_per_orbit_step(TAU, "fp64")
+    fl = flops_per_orbit_step(TAU, HEADLINE, N)
+    fl64 = flops_per_orbit_step(TAU, "fp64", N)
     per_launch_ms = float(np.mean(msmx))
     # FP64-pipe equivalent: a Float32 op takes half an FP64 issue slot on B200 (FP32 rate = 2 x FP64 rate)
     achieved = n * N * (fl["fp64"] + fl["fp32"] / 2) / (per_launch_ms / 1e3) / 1e12
