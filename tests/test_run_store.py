@@ -318,3 +318,42 @@ def test_oracle_record_chunk(oracle, tmp_path, name):
     RS.write_chunk(p, _attrs(coordinate_mode="wrapped" if name == "wrapped" else "lifted"), orbs)
     back = RS.read_chunk(p)
     assert all(RS.same_orbit(u, v) for u, v in zip(orbs, back.orbits))
+
+
+def test_h5_dataset_header_by_hand():
+    """A dataset's version 1 object header walked by hand (not through the package's reader): Dataspace, Datatype
+    (constant), Fill Value and Data Layout messages in that order, then an Attribute message; the layout's address and
+    size point at the array's little-endian bytes; the bool and string attribute types carry the format's class bits."""
+    data = np.array([[1.5, -2.0, 3.25], [0.0, 7.0, -0.5]])
+    root = h5.Group()
+    root.put("d", h5.Dataset(data, attrs={"ok": True, "name": "ab"}))
+    b = h5.image(root)
+    # the root group's only member: its symbol table node entry gives the dataset's header
+    bt = struct.unpack_from("<Q", b, 80)[0]
+    snod = struct.unpack_from("<Q", b, bt + 32)[0]
+    assert b[snod:snod + 4] == b"SNOD" and struct.unpack_from("<H", b, snod + 6)[0] == 1
+    hdr = struct.unpack_from("<Q", b, snod + 8 + 8)[0]
+    ver, _, nmsg, refc, size = struct.unpack_from("<BBHII", b, hdr)
+    assert (ver, nmsg, refc) == (1, 6, 1)
+    p, end, kinds = hdr + 16, hdr + 16 + size, []
+    while p < end:
+        mtype, msize, flags = struct.unpack_from("<HHB", b, p)
+        kinds.append((mtype, flags))
+        body = p + 8
+        if mtype == 0x1:
+            assert b[body] == 1 and b[body + 1] == 2 and struct.unpack_from("<QQ", b, body + 8) == (2, 3)
+        if mtype == 0x8:
+            assert b[body] == 3 and b[body + 1] == 1
+            addr, nbytes = struct.unpack_from("<QQ", b, body + 2)
+            assert nbytes == 48 and b[addr:addr + nbytes] == data.astype("<f8").tobytes()
+        if mtype == 0xC:
+            nlen, dlen = struct.unpack_from("<HH", b, body + 2)
+            name = b[body + 8:body + 8 + nlen - 1].decode()
+            dt = body + 8 + ((nlen + 7) & ~7)
+            if name == "ok":
+                assert b[dt] == 0x18 and b[dt + 1] == 2 and b[dt + 8] == 0x10   # enum of 2 members, int8 base
+            else:
+                assert b[dt] == 0x13 and b[dt + 1] == 0x10 and struct.unpack_from("<I", b, dt + 4)[0] == 2
+        p = body + msize
+    assert [k for k, _ in kinds] == [0x1, 0x3, 0x5, 0x8, 0xC, 0xC]
+    assert dict(kinds)[0x3] == 1
